@@ -1,0 +1,227 @@
+/*
+ * mixgpu.h -- C-ABI of the B200 SIMPLE/PISO pressure-velocity hot path.
+ *
+ * Plain C types only (no torch, no C++), so a Fortran ISO_C_BINDING interface,
+ * ctypes or any other FFI can bind it. Every entry point returns an int status:
+ *   0                  success
+ *   MGPU_E_ARG   (-1)  invalid argument (null pointer, bad size, bad option)
+ *   MGPU_E_CUDA  (-2)  a CUDA runtime call failed (message: mgpu_last_error)
+ *   MGPU_E_MESH  (-3)  mesh rejected (bad node/cell reference, zero volume, ...)
+ *   MGPU_E_BC    (-4)  boundary specification rejected (same codes as build_bc)
+ *   MGPU_E_TIMEOUT(-5) a bounded device wait ran out (kernel returned early)
+ *   MGPU_E_NOMEM (-6)  device memory budget exceeded
+ * Solver outcomes are reported separately through the reference's own codes
+ * (argument `ier` / `ierr`), see each function.
+ *
+ * Index convention: the mesh and CSR arrays crossing this boundary are 1-based,
+ * exactly as the reference's Fortran derived types hold them, so the Fortran
+ * side passes its arrays without renumbering. Field arrays are cell-major
+ * AoS u(3,ncells) (Fortran column-major), as in fields_t.
+ */
+#ifndef MIXGPU_H
+#define MIXGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MGPU_OK 0
+#define MGPU_E_ARG (-1)
+#define MGPU_E_CUDA (-2)
+#define MGPU_E_MESH (-3)
+#define MGPU_E_BC (-4)
+#define MGPU_E_TIMEOUT (-5)
+#define MGPU_E_NOMEM (-6)
+
+/* Boundary type codes: identical values to mod_uns_control.f90:32-56. */
+#define MGPU_BC_NONE 0
+#define MGPU_BC_WALL 1
+#define MGPU_BC_SYMMETRY 2
+#define MGPU_BC_VINLET 3
+#define MGPU_BC_POUTLET 4
+#define MGPU_BC_FARFIELD 5
+#define MGPU_BC_SLIPWALL 6
+#define MGPU_BC_MASSINLET 7
+#define MGPU_BC_OUTFLOW 8
+#define MGPU_BC_INTERFACE 9
+#define MGPU_BC_VINLET_PARAB 10
+
+#define MGPU_MAXBC 32 /* MAXBC, mod_uns_control.f90:58 */
+
+/* Linear-solver selections. The first value of each is the reference's. */
+#define MGPU_PPE_JACOBI 0 /* cg_jacobi  (ppe_precond /= 'ic0')           */
+#define MGPU_PPE_IC0 1    /* cg_ic0     (ppe_precond = 'ic0', default)    */
+#define MGPU_PPE_ILU0 2   /* PCG with ILU(0) (extension; reference lacks) */
+#define MGPU_MOM_ILU0 0   /* bicgstab_ilu0 (the reference's only choice)  */
+#define MGPU_MOM_JACOBI 1 /* BiCGStab+Jacobi (extension)                   */
+
+/* Arithmetic form of the Krylov solves. */
+#define MGPU_PREC_FP64 0  /* plain FP64, parity form                       */
+#define MGPU_PREC_MIXED 1 /* FP32 SpMV/preconditioner inside FP64 refinement */
+
+/* One control "bc" line: mirrors bc_spec_t, mod_uns_control.f90:114-145
+ * (thermal plane filters are not part of this path). */
+typedef struct {
+  int32_t zone;
+  int32_t btype;
+  double uvel[3];
+  double pval;
+  double mdot;
+  double umean, uspan, uorigin; /* parabolic inlet profile */
+  int32_t uaxis;                /* 1=x 2=y 3=z */
+  int32_t has_lid;
+  int32_t lid_dir;
+  int32_t pad0;
+  double lid_coord;
+  double lid_vel[3];
+  int32_t ttype; /* thermal type: must be 0 (adiabatic) on this path */
+  int32_t pad1;
+  double tval, qval;
+} MgpuBcSpec;
+
+/* Control scalars: mirrors ctrl_t, mod_uns_control.f90:148-280. */
+typedef struct {
+  double rho, mu, alpha_u, alpha_p;
+  int32_t outer_max;
+  int32_t lin_max;
+  double outer_tol, lin_tol;
+  double conv_blend, nonorth_corr;
+  int32_t ppe_precond; /* MGPU_PPE_* */
+  int32_t mom_solver;  /* MGPU_MOM_* */
+  int32_t transient, time_scheme;
+  double dt;
+  int32_t n_time_max, n_correct;
+  double body_force[3];
+  int32_t inlet_ramp;
+  int32_t precision; /* MGPU_PREC_* */
+  double mixed_tol;  /* inner FP32 relative tolerance per refinement sweep */
+  int32_t nbc;
+  int32_t pad0;
+  MgpuBcSpec bc[MGPU_MAXBC];
+} MgpuCtrl;
+
+/* Face-list mesh: mirrors mesh_t/face_t, mod_uns_mesh.f90:17-54. */
+typedef struct {
+  int32_t nnodes, nfaces, ncells;
+  int32_t pad0;
+  const double* x;          /* 3*nnodes, x(1:3,node) */
+  const int32_t* fnode_ptr; /* nfaces+1, 0-based offsets into fnodes */
+  const int32_t* fnodes;    /* node ids, 1-based */
+  const int32_t* c0;        /* owner cell, 1-based */
+  const int32_t* c1;        /* neighbour cell, 1-based, 0 = boundary */
+  const int32_t* zone;      /* face zone id */
+} MgpuMesh;
+
+/* Per outer iteration (SIMPLE) or time step (PISO) record. Solve slots:
+ * 0..2 momentum components, 3.. pressure-correction sweeps. */
+#define MGPU_MAXSOLVE 8
+typedef struct {
+  int32_t it;
+  int32_t itl_max;
+  int32_t nsolve;
+  int32_t pad0;
+  int32_t lin_it[MGPU_MAXSOLVE];
+  int32_t lin_ierr[MGPU_MAXSOLVE];
+  double lin_res[MGPU_MAXSOLVE];
+  double imbal, du_max, dT_max, ressum;
+  double umax, cfl_max, t_now;
+} MgpuIterRec;
+
+typedef struct MgpuCase MgpuCase;
+
+/* Library version and last error message (thread-local, static storage). */
+int mgpu_version(void);
+const char* mgpu_last_error(void);
+/* Selects the CUDA device used by subsequent mgpu_case_create calls. */
+int mgpu_set_device(int device);
+
+/* Case lifetime. Replaces uns_solver_init's work after the .cas/.control have
+ * been read (mod_uns_driver.f90:60-239: connectivity :91, geometry :94,
+ * build_bc :144, init_fields :147): the mesh is uploaded once and every
+ * derived array (connectivity, geometry, CSR pattern, face slot maps,
+ * triangular level sets) is built and kept resident in HBM.
+ * Returns MGPU_E_BC with *ier set to the build_bc code (10..14) on a bad BC. */
+int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out, int* ier);
+int mgpu_case_destroy(MgpuCase* c);
+/* Device bytes held by the case (mesh, matrices, fields, work vectors). */
+int mgpu_case_device_bytes(const MgpuCase* c, int64_t* bytes);
+
+/* Fields in/out: fields_t (mod_uns_fields.f90:29-79). u is u(3,ncells) AoS,
+ * p(ncells), flux(nfaces). Any pointer may be NULL to skip that field. */
+int mgpu_fields_upload(MgpuCase* c, const double* u, const double* p, const double* flux,
+                       const double* u_old, const double* u_old_old);
+int mgpu_fields_download(MgpuCase* c, double* u, double* p, double* flux, double* gp,
+                         double* gu, double* apc);
+
+/* Steady SIMPLE: simple_run (mod_uns_simple.f90:88-288). Runs at most
+ * min(outer_max, nsteps) outer iterations (nsteps <= 0: no cap), stopping early
+ * on convergence. log: optional, capacity logcap records; *nrec = records
+ * written. *ier: 0, 20 momentum breakdown, 21 PPE breakdown, 60 non-finite. */
+int mgpu_simple_run(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nrec, int* ier);
+
+/* Transient PISO: piso_run_mpi at one rank (mod_uns_simple_mpi.f90:298-571).
+ * *ier: 0, 30 transient=false, 31 dt<=0, 33 momentum breakdown, 34 PPE
+ * breakdown, 60 non-finite. */
+int mgpu_piso_run(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nrec, int* ier);
+
+/* First non-finite value: nan_scan (mod_uns_simple.f90:2375-2426). field:
+ * 1 u_x, 2 u_y, 3 u_z, 4 p, 5 T, 6 T_s; cell 1-based; kind 1 NaN, 2 Inf;
+ * *ifin = 0 when every value is finite. */
+int mgpu_nan_scan(MgpuCase* c, int* ifin, int* field, int* cell, double* val, int* kind);
+
+/* Stand-alone Krylov solves on a host CSR matrix (1-based row_ptr/col_idx,
+ * columns sorted per row, as csr_t in mod_uns_linsolver.f90:27-33). The matrix
+ * and vectors are copied to the device, solved there, x copied back.
+ * Contract of the reference: (tol, maxit) -> (it, res, ierr) with ierr 0
+ * converged, 1 maxit, 2 breakdown, +10 factorisation failure.
+ *   method: 0 bicgstab_ilu0 (:148-224), 1 cg_jacobi (:230-291),
+ *           2 cg_ic0 (:405-461), 3 BiCGStab+Jacobi, 4 PCG+ILU(0).
+ *   norm_mode: 0 = serial solvers (gfortran norm2), 1 = the one-rank
+ *           distributed solvers of mod_uns_linsolver_mpi.f90 (sqrt of gdot). */
+int mgpu_krylov_solve(int n, const int32_t* row_ptr, const int32_t* col_idx, const double* val,
+                      const double* b, double* x, double tol, int maxit, int method,
+                      int norm_mode, int* it, double* res, int* ierr);
+
+/* y = A x on a host CSR matrix (csr_matvec, mod_uns_linsolver.f90:40-52). */
+int mgpu_csr_matvec(int n, const int32_t* row_ptr, const int32_t* col_idx, const double* val,
+                    const double* x, double* y);
+
+/* Integer mesh pipeline, bit-exact with the reference:
+ * build_connectivity (mod_uns_connectivity.f90:28-108) and build_cell_csr
+ * (mod_uns_simple.f90:835-887). Outputs are 1-based like the Fortran arrays.
+ * Sizes: cf_ptr ncells+1, cf 2*nint+nbnd, c2c_ptr ncells+1, c2c 2*nint,
+ * row_ptr ncells+1, col_idx ncells+2*nint (upper bound; *nnz returned). */
+int mgpu_build_connectivity(const MgpuMesh* mesh, int32_t* cf_ptr, int32_t* cf, int32_t* c2c_ptr,
+                            int32_t* c2c, int32_t* row_ptr, int32_t* col_idx, int32_t* nnz);
+
+/* Geometry: compute_geometry (mod_uns_geometry.f90:40-92) plus the face
+ * weights lf of init_fields (mod_uns_fields.f90:147-157), computed on the
+ * device. Sizes: xf,sf 3*nfaces; area,lf nfaces; vol ncells; xc 3*ncells. */
+int mgpu_geometry(const MgpuMesh* mesh, double* xf, double* sf, double* area, double* vol,
+                  double* xc, double* lf);
+
+/* Reverse Cuthill-McKee cell ordering of the cell graph (no counterpart in the
+ * reference, which takes the cell order of the .cas file): new_of_old[c-1] is
+ * the new 1-based number of cell c. */
+int mgpu_rcm_order(const MgpuMesh* mesh, int32_t* new_of_old);
+
+/* Timing of the last run on the case's stream (CUDA events): total device ms
+ * and, for the dominant kernel family, launches and summed device ms. */
+typedef struct {
+  double total_ms;
+  int64_t spmv_launches;
+  double spmv_ms;
+  int64_t krylov_launches;
+  double krylov_ms;
+  int64_t gpu_launches; /* kernels this library launched during the run */
+} MgpuTiming;
+int mgpu_case_timing(const MgpuCase* c, MgpuTiming* t);
+/* 1 = record CUDA events around every Krylov-kernel launch of later runs. */
+int mgpu_case_set_profiling(MgpuCase* c, int on);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,134 @@
+"""Regenerate the committed golden fixtures under tests/golden/.
+
+Run from the repository root in a checkout where the reference project is
+available (default path below, or MIXSOLVER_REF):
+
+    python tests/golden/make_golden.py
+
+Produces
+  * ghia_pin.json -- the oracle's steady SIMPLE on the reference's own cavity
+    meshes (cluster_cases/cavity_Re1000/unMesh.cas, 80x80; cases/natconv/cavity.cas,
+    40x40) with the control of cluster_cases/cavity_Re1000/unMesh.control, scored
+    with the centre-line probe of mod_uns_output.f90:246-350. The Ghia table is
+    read from the reference source at generation time; only the resulting L2
+    is stored. The reference publishes 2.897e-2 (80x80, unMesh.control:63,
+    cluster_cases/README.md:189) and 9.12e-2 (40x40, cluster_cases/README.md:190).
+  * oracle_cases.npz -- oracle histories and final fields on small synthetic
+    workloads (the same generators the CUDA tests use), used by the CPU suite
+    to detect any change in the oracle's results.
+The oracle source hash is stored in each fixture so a stale fixture is caught.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import re
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+
+from casread import read_cas  # noqa: E402
+from mixsolver_b200 import cases  # noqa: E402
+from mixsolver_b200.abi import (BC_SYMMETRY, BC_WALL, MOM_ILU0, PPE_IC0, BcSpec,  # noqa: E402
+                                Ctrl)
+from oracle import oracle as O  # noqa: E402
+
+REF = os.environ.get("MIXSOLVER_REF", "/root/reference")
+
+
+def oracle_hash() -> str:
+    return hashlib.sha256(open(os.path.join(ROOT, "oracle", "oracle.cpp"), "rb").read()).hexdigest()[:16]
+
+
+def ghia_table():
+    src = open(os.path.join(REF, "src/unstructured/mod_uns_output.f90")).read()
+
+    def arr(name):
+        mm = re.search(name + r"\s*=\s*\[(.*?)\]", src, re.S)
+        return np.array([float(v.replace("_dp", "")) for v in mm.group(1).replace("&", " ").split(",")])
+    return arr("yg"), arr("u1000")
+
+
+def probe_l2(xc, u, yg, uref):
+    """probe_velocity (8 nearest centroids, w = 1/(d^2+1e-12)) at (0.5, y, 0.5)
+    and the relative L2 over the 15 interior stations, as ghia_compare does."""
+    num = den = 0.0
+    for i, (y, ur) in enumerate(zip(yg, uref)):
+        d2 = ((xc - np.array([0.5, y, 0.5])) ** 2).sum(1)
+        idx = np.argsort(d2, kind="stable")[:8]
+        w = 1.0 / (d2[idx] + 1e-12)
+        uq = (w[:, None] * u[idx]).sum(0) / w.sum()
+        if 0 < i < len(yg) - 1:
+            num += (uq[0] - ur) ** 2
+            den += ur * ur
+    return float(np.sqrt(num / den))
+
+
+def cavity_control(outer_max):
+    # cluster_cases/cavity_Re1000/unMesh.control
+    return Ctrl(rho=1.0, mu=0.001, alpha_u=0.7, alpha_p=0.3, outer_max=outer_max, outer_tol=0.0,
+                lin_tol=1e-8, lin_max=300, conv_blend=1.0, nonorth_corr=0.0, ppe_precond=PPE_IC0,
+                mom_solver=MOM_ILU0,
+                bcs=[BcSpec(zone=5, btype=BC_WALL, lid=(2, 1.0, (1.0, 0.0, 0.0))),
+                     BcSpec(zone=4, btype=BC_SYMMETRY)])
+
+
+def make_ghia():
+    yg, u1000 = ghia_table()
+    out = {"oracle_sha": oracle_hash(), "runs": []}
+    for rel, iters, published in (("cluster_cases/cavity_Re1000/unMesh.cas", 1000, 2.897e-2),
+                                  ("cases/natconv/cavity.cas", 3000, 9.12e-2)):
+        mesh = read_cas(os.path.join(REF, rel))
+        oc = O.OracleCase(mesh, cavity_control(iters))
+        ier, log = oc.simple_run(logcap=iters)
+        xc = oc.geometry()["xc"]
+        u = oc.fields()["u"]
+        out["runs"].append(dict(mesh=rel, ncells=mesh.ncells, outer_iterations=len(log), ier=ier,
+                                ghia_l2=probe_l2(xc, u, yg, u1000), published_l2=published,
+                                final_imbal=log[-1]["imbal"], final_du_max=log[-1]["du_max"],
+                                it1=log[0]))
+        print(rel, out["runs"][-1]["ghia_l2"])
+    with open(os.path.join(ROOT, "tests/golden/ghia_pin.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
+def hist_arrays(log):
+    return dict(lin_it=np.array([r["lin_it"] for r in log], np.int32),
+                lin_res=np.array([r["lin_res"] for r in log]),
+                imbal=np.array([r["imbal"] for r in log]),
+                du_max=np.array([r["du_max"] for r in log]))
+
+
+def make_cases():
+    data = {"oracle_sha": np.array(oracle_hash())}
+    # 2-D cavity, 16x16, 30 SIMPLE iterations (reference solvers)
+    m, c = cases.cavity2d(16, outer_max=30)
+    oc = O.OracleCase(m, c)
+    ier, log = oc.simple_run()
+    f = oc.fields()
+    for k, v in hist_arrays(log).items():
+        data[f"cav16_{k}"] = v
+    data["cav16_u"], data["cav16_p"], data["cav16_flux"] = f["u"], f["p"], f["flux"]
+    # small jittered channel, 10 iterations, BiCGStab+Jacobi / PCG+ILU(0)
+    m, c = cases.channel3d(12, 6, 6, seed=3, outer_max=10)
+    oc = O.OracleCase(m, c)
+    ier, log = oc.simple_run()
+    f = oc.fields()
+    for k, v in hist_arrays(log).items():
+        data[f"chan_{k}"] = v
+    data["chan_u"], data["chan_p"] = f["u"], f["p"]
+    np.savez_compressed(os.path.join(ROOT, "tests/golden/oracle_cases.npz"), **data)
+    print("oracle_cases.npz written")
+
+
+if __name__ == "__main__":
+    make_cases()
+    if os.path.isdir(REF):
+        make_ghia()
+    else:
+        print("reference checkout not found; ghia_pin.json left unchanged")

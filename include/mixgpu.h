@@ -207,6 +207,15 @@ int mgpu_geometry(const MgpuMesh* mesh, double* xf, double* sf, double* area, do
  * the new 1-based number of cell c. */
 int mgpu_rcm_order(const MgpuMesh* mesh, int32_t* new_of_old);
 
+/* One stage of the outer iteration on the case's current fields, for
+ * element-wise checks of each kernel: what = 0 compute_gradients, 1..3
+ * momentum_assembly of component what (A values, rhs, ap out), 4 flux_rhiechow,
+ * 5 ppe_assembly (A values, rhs out), 6 correct_fields with p' = pp.
+ * ts_order sets fields_t%ts_order; apc (optional) replaces the stored apc.
+ * aval has room for the CSR pattern (nnz values, mgpu_build_connectivity order). */
+int mgpu_case_stage(MgpuCase* c, int what, int ts_order, const double* apc, double* aval, double* rhs,
+                    double* ap, const double* pp);
+
 /* Timing of the last run on the case's stream (CUDA events): total device ms
  * and, for the dominant kernel family, launches and summed device ms. */
 typedef struct {

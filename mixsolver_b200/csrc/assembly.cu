@@ -1,0 +1,768 @@
+// assembly.cu -- face-loop kernels of the SIMPLE/PISO path (FP64 parity form).
+//
+// The reference accumulates cell sums inside face loops (grad(c0) += ...,
+// grad(c1) -= ...). Here every cell gathers its own faces in ascending face
+// order through the cell->face lists of build_connectivity, so each cell sum
+// sees exactly the same addends in exactly the same order: no atomics, and the
+// results are bit-identical to the Fortran loops (compiled without FMA
+// contraction). Per-face quantities (Rhie-Chow flux, flux correction) run one
+// thread per face.
+//
+// Reference: src/unstructured/mod_uns_geometry.f90:40-174 (geometry),
+// mod_uns_fields.f90:147-157 (lf) and :164-374 (Green-Gauss gradients),
+// mod_uns_simple.f90:928-1338 (momentum_assembly), :1346-1408
+// (velocity_limiter), :1413-1450 (flux_rhiechow), :1463-1547 (outflow
+// scaling), :1552-1644 (ppe_assembly), :1649-1739 (correct_fields),
+// :236-247 and :2375-2426 (diagnostics, nan_scan).
+
+#include "assembly.cuh"
+
+namespace mgpu {
+
+namespace {
+
+__device__ __forceinline__ Ramp ramp_of(const AsmParams& P, const DevStatus* st) {
+  Ramp r{1.0, 1.0};
+  if (P.inlet_ramp > 1) {
+    double f = (double)(st->cur_it + 1) / (double)P.inlet_ramp;
+    f = fmax(0.0, fmin(1.0, f));
+    r.inlet = f;
+    r.pval = f;
+  }
+  return r;
+}
+
+// ---------------- geometry (setup) ----------------------------------------
+
+// face_props: Newell area vector, area, fan-triangulated centroid
+__global__ void k_face_props(int F, const double* __restrict__ x, const int* __restrict__ fptr,
+                             const int* __restrict__ fnodes, double* xf, double* sf, double* area) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= F) return;
+  const int b = fptr[i], n = fptr[i + 1] - b;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int j = 0; j < n; ++j) {
+    const int jn = (j + 1) % n;
+    const double* p1 = x + 3 * (long)fnodes[b + j];
+    const double* p2 = x + 3 * (long)fnodes[b + jn];
+    const double c0 = p1[1] * p2[2] - p1[2] * p2[1];
+    const double c1 = p1[2] * p2[0] - p1[0] * p2[2];
+    const double c2 = p1[0] * p2[1] - p1[1] * p2[0];
+    s0 = s0 + 0.5 * c0;
+    s1 = s1 + 0.5 * c1;
+    s2 = s2 + 0.5 * c2;
+  }
+  const double a = norm3(s0, s1, s2);
+  double e0 = 0.0, e1 = 0.0, e2 = 0.0, at = 0.0;
+  const double* p1 = x + 3 * (long)fnodes[b];
+  for (int j = 1; j < n - 1; ++j) {
+    const double* p2 = x + 3 * (long)fnodes[b + j];
+    const double* p3 = x + 3 * (long)fnodes[b + j + 1];
+    const double u0 = p2[0] - p1[0], u1 = p2[1] - p1[1], u2 = p2[2] - p1[2];
+    const double v0 = p3[0] - p1[0], v1 = p3[1] - p1[1], v2 = p3[2] - p1[2];
+    const double t0 = (u1 * v2 - u2 * v1) * 0.5;
+    const double t1 = (u2 * v0 - u0 * v2) * 0.5;
+    const double t2 = (u0 * v1 - u1 * v0) * 0.5;
+    const double ns = norm3(t0, t1, t2);
+    e0 = e0 + ns * ((p1[0] + p2[0]) + p3[0]) / 3.0;
+    e1 = e1 + ns * ((p1[1] + p2[1]) + p3[1]) / 3.0;
+    e2 = e2 + ns * ((p1[2] + p2[2]) + p3[2]) / 3.0;
+    at = at + ns;
+  }
+  if (at > 0.0) {
+    e0 = e0 / at;
+    e1 = e1 / at;
+    e2 = e2 / at;
+  }
+  xf[i] = e0;
+  xf[F + i] = e1;
+  xf[2 * F + i] = e2;
+  sf[i] = s0;
+  sf[F + i] = s1;
+  sf[2 * F + i] = s2;
+  area[i] = a;
+}
+
+// prov_centers: node average of each cell (nodes counted once per face visit)
+__global__ void k_prov_centers(int N, const double* __restrict__ x, const int* __restrict__ fptr,
+                               const int* __restrict__ fnodes, const int* __restrict__ cf_ptr,
+                               const int* __restrict__ cf, double* pcen) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  int cnt = 0;
+  for (int k = cf_ptr[c]; k < cf_ptr[c + 1]; ++k) {
+    const int f = cf[k];
+    for (int j = fptr[f]; j < fptr[f + 1]; ++j) {
+      const double* xn = x + 3 * (long)fnodes[j];
+      a0 = a0 + xn[0];
+      a1 = a1 + xn[1];
+      a2 = a2 + xn[2];
+      ++cnt;
+    }
+  }
+  if (cnt > 0) {
+    a0 = a0 / (double)cnt;
+    a1 = a1 / (double)cnt;
+    a2 = a2 / (double)cnt;
+  }
+  pcen[c] = a0;
+  pcen[N + c] = a1;
+  pcen[2 * N + c] = a2;
+}
+
+__global__ void k_orient(int F, int N, const int* __restrict__ c0, const double* __restrict__ xf,
+                         const double* __restrict__ pcen, double* sf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= F) return;
+  const int a = c0[i];
+  const double d0 = xf[i] - pcen[a], d1 = xf[F + i] - pcen[N + a], d2 = xf[2 * F + i] - pcen[2 * N + a];
+  const double dotv = dot3(sf[i], sf[F + i], sf[2 * F + i], d0, d1, d2);
+  if (dotv < 0.0) {
+    sf[i] = -sf[i];
+    sf[F + i] = -sf[F + i];
+    sf[2 * F + i] = -sf[2 * F + i];
+  }
+}
+
+// pyramid decomposition (accumulate_cell) gathered per cell in face order
+__global__ void k_cell_volumes(int N, int F, const int* __restrict__ c0, const int* __restrict__ cf_ptr,
+                               const int* __restrict__ cf, const double* __restrict__ xf,
+                               const double* __restrict__ sf, const double* __restrict__ pcen, double* vol,
+                               double* xc) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  const double THIRD = 1.0 / 3.0, QRTR = 1.0 / 4.0;
+  const double p0 = pcen[c], p1 = pcen[N + c], p2 = pcen[2 * N + c];
+  double v = 0.0, x0 = 0.0, x1 = 0.0, x2 = 0.0;
+  for (int k = cf_ptr[c]; k < cf_ptr[c + 1]; ++k) {
+    const int f = cf[k];
+    const double sgn = (c0[f] == c) ? 1.0 : -1.0;
+    const double f0 = xf[f], f1 = xf[F + f], f2 = xf[2 * F + f];
+    const double dv = THIRD * dot3(sf[f], sf[F + f], sf[2 * F + f], f0 - p0, f1 - p1, f2 - p2) * sgn;
+    v = v + dv;
+    x0 = x0 + dv * ((1.0 - QRTR) * f0 + QRTR * p0);
+    x1 = x1 + dv * ((1.0 - QRTR) * f1 + QRTR * p1);
+    x2 = x2 + dv * ((1.0 - QRTR) * f2 + QRTR * p2);
+  }
+  if (v > 0.0) {
+    x0 = x0 / v;
+    x1 = x1 / v;
+    x2 = x2 / v;
+  }
+  vol[c] = v;
+  xc[c] = x0;
+  xc[N + c] = x1;
+  xc[2 * N + c] = x2;
+}
+
+// Per-face constants: lf (init_fields), |d|, d.S, the momentum diffusion
+// coefficient and the non-orthogonal correction vector, each formed with the
+// reference's expression so it equals the value recomputed in its face loops.
+__global__ void k_face_consts(DeviceCase d, AsmParams P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int F = d.F, N = d.N;
+  if (i >= F) return;
+  const int a = d.c0[i], b = d.c1[i];
+  const double s0 = d.sf[i], s1 = d.sf[F + i], s2 = d.sf[2 * F + i];
+  const double f0 = d.xf[i], f1 = d.xf[F + i], f2 = d.xf[2 * F + i];
+  const double area = d.area[i];
+  const double POROSITY_FLOOR = 1.0e-8;
+  const double mu_eff = P.mu / fmax(1.0, POROSITY_FLOOR);  // pure fluid: porosity 1
+  if (b < 0) {
+    d.lf[i] = 1.0;
+    const double dw = norm3(f0 - d.xc[a], f1 - d.xc[N + a], f2 - d.xc[2 * N + a]);
+    d.dn[i] = dw;
+    d.Dm[i] = mu_eff * area / dw;
+    d.dsf[i] = 0.0;
+    d.mnc[i] = 0.0;
+    d.tv[i] = d.tv[F + i] = d.tv[2 * F + i] = 0.0;
+    return;
+  }
+  const double d0 = norm3(f0 - d.xc[a], f1 - d.xc[N + a], f2 - d.xc[2 * N + a]);
+  const double d1 = norm3(d.xc[b] - f0, d.xc[N + b] - f1, d.xc[2 * N + b] - f2);
+  const double lf = d1 / (d0 + d1);
+  d.lf[i] = lf;
+  const double v0 = d.xc[b] - d.xc[a], v1 = d.xc[N + b] - d.xc[N + a], v2 = d.xc[2 * N + b] - d.xc[2 * N + a];
+  const double dn = norm3(v0, v1, v2);
+  d.dn[i] = dn;
+  d.dsf[i] = dot3(v0, v1, v2, s0, s1, s2);
+  const double mu_f = lf * mu_eff + (1.0 - lf) * mu_eff;
+  if (P.nonorth_corr > 0.0) {
+    const double sd = dot3(s0, s1, s2, v0, v1, v2);
+    d.Dm[i] = mu_f * (area * area) / sd;
+    const double q = (area * area) / sd;
+    d.tv[i] = s0 - v0 * q;
+    d.tv[F + i] = s1 - v1 * q;
+    d.tv[2 * F + i] = s2 - v2 * q;
+  } else {
+    d.Dm[i] = mu_f * area / dn;
+    d.tv[i] = d.tv[F + i] = d.tv[2 * F + i] = 0.0;
+  }
+  d.mnc[i] = P.nonorth_corr * mu_f;
+}
+
+// ---------------- per-iteration kernels ------------------------------------
+
+// compute_gradients: Green-Gauss gp and gu (gu plane = comp*3 + dir)
+__global__ void __launch_bounds__(256) k_gradients(DeviceCase d, AsmParams P) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d.st->abort || c >= d.N) return;
+  const int N = d.N, F = d.F;
+  const Ramp rp = ramp_of(P, d.st);
+  const double *u0 = d.u, *u1 = d.u + N, *u2 = d.u + 2 * N;
+  double g[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) g[k] = 0.0;
+  for (int k = d.cf_ptr[c]; k < d.cf_ptr[c + 1]; ++k) {
+    const int f = d.cf[k];
+    const int a = d.c0[f], b = d.c1[f];
+    double pf, w0, w1, w2;
+    if (b >= 0) {
+      const double lf = d.lf[f], l1 = 1.0 - lf;
+      pf = lf * d.p[a] + l1 * d.p[b];
+      w0 = lf * u0[a] + l1 * u0[b];
+      w1 = lf * u1[a] + l1 * u1[b];
+      w2 = lf * u2[a] + l1 * u2[b];
+    } else {
+      const DevGroup& gr = d.groups[d.fgrp[f]];
+      pf = bc_face_p(gr, rp, d.p[a]);
+      bc_face_vel(gr, rp, d.xf[f], d.xf[F + f], d.xf[2 * F + f], d.sf[f], d.sf[F + f], d.sf[2 * F + f], u0[a],
+                  u1[a], u2[a], w0, w1, w2);
+    }
+    const double s0 = d.sf[f], s1 = d.sf[F + f], s2 = d.sf[2 * F + f];
+    const double phi[4] = {pf, w0, w1, w2};
+    if (a == c) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        g[3 * q + 0] = g[3 * q + 0] + phi[q] * s0;
+        g[3 * q + 1] = g[3 * q + 1] + phi[q] * s1;
+        g[3 * q + 2] = g[3 * q + 2] + phi[q] * s2;
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        g[3 * q + 0] = g[3 * q + 0] - phi[q] * s0;
+        g[3 * q + 1] = g[3 * q + 1] - phi[q] * s1;
+        g[3 * q + 2] = g[3 * q + 2] - phi[q] * s2;
+      }
+    }
+  }
+  const double v = d.vol[c];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) d.gp[k * N + c] = g[k] / v;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) d.gu[k * N + c] = g[3 + k] / v;
+}
+
+// velocity_limiter for one component (Barth-Jespersen psi)
+__global__ void __launch_bounds__(256) k_limiter(DeviceCase d, AsmParams P, int comp) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d.st->abort || c >= d.N) return;
+  const int N = d.N, F = d.F;
+  const Ramp rp = ramp_of(P, d.st);
+  const double* uc_ = d.u + (long)comp * N;
+  const double uc = uc_[c];
+  double pmin = uc, pmax = uc;
+  for (int k = d.cf_ptr[c]; k < d.cf_ptr[c + 1]; ++k) {
+    const int f = d.cf[k];
+    const int a = d.c0[f], b = d.c1[f];
+    if (b >= 0) {
+      const double v = uc_[a == c ? b : a];
+      pmin = fmin(pmin, v);
+      pmax = fmax(pmax, v);
+    } else if (d.fgrp[f] >= 0) {
+      double w[3];
+      bc_face_vel(d.groups[d.fgrp[f]], rp, d.xf[f], d.xf[F + f], d.xf[2 * F + f], d.sf[f], d.sf[F + f],
+                  d.sf[2 * F + f], d.u[a], d.u[N + a], d.u[2 * N + a], w[0], w[1], w[2]);
+      pmin = fmin(pmin, w[comp]);
+      pmax = fmax(pmax, w[comp]);
+    }
+  }
+  const double g0 = d.gu[(comp * 3 + 0) * N + c], g1 = d.gu[(comp * 3 + 1) * N + c],
+               g2 = d.gu[(comp * 3 + 2) * N + c];
+  const double x0 = d.xc[c], x1 = d.xc[N + c], x2 = d.xc[2 * N + c];
+  double psi = 1.0;
+  for (int k = d.cf_ptr[c]; k < d.cf_ptr[c + 1]; ++k) {
+    const int f = d.cf[k];
+    const double fr = uc + dot3(g0, g1, g2, d.xf[f] - x0, d.xf[F + f] - x1, d.xf[2 * F + f] - x2);
+    const double df = fr - uc;
+    if (df > 0.0)
+      psi = fmin(psi, (pmax - uc) / df);
+    else if (df < 0.0)
+      psi = fmin(psi, (pmin - uc) / df);
+  }
+  d.psi[c] = fmax(0.0, fmin(1.0, psi));
+}
+
+// momentum_assembly for component comp: row c of A, rhs(c), ap(c)
+__global__ void __launch_bounds__(256) k_momentum(DeviceCase d, AsmParams P, int comp) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d.st->abort || c >= d.N) return;
+  const int N = d.N, F = d.F;
+  const Ramp rp = ramp_of(P, d.st);
+  const double *u0 = d.u, *u1 = d.u + N, *u2 = d.u + 2 * N;
+  const double* ucomp = d.u + (long)comp * N;
+  const double* sfc = d.sf + (long)comp * F;
+  double* A = d.aval;
+  const int rb = d.row_ptr[c], re = d.row_ptr[c + 1];
+  for (int k = rb; k < re; ++k) A[k] = 0.0;
+  double ap = 0.0, rhs = 0.0;
+  const int kb = d.cf_ptr[c], ke = d.cf_ptr[c + 1];
+  // interior faces
+  for (int k = kb; k < ke; ++k) {
+    const int f = d.cf[k];
+    const int b = d.c1[f];
+    if (b < 0) continue;
+    const int a = d.c0[f];
+    const bool own = (a == c);
+    const double Fm = d.flux[f];
+    const double D = d.Dm[f];
+    const int slot = d.cf_slot[k];
+    if (own) {
+      ap = ap + fmax(Fm, 0.0) + D;
+      A[slot] = A[slot] - (D + fmax(-Fm, 0.0));
+    } else {
+      ap = ap + fmax(-Fm, 0.0) + D;
+      A[slot] = A[slot] - (D + fmax(Fm, 0.0));
+    }
+    const double lf = d.lf[f], l1 = 1.0 - lf;
+    if (P.conv_blend > 0.0) {
+      const int cu = (Fm > 0.0) ? a : b;
+      const double dcv = d.psi[cu] * dot3(d.gu[(comp * 3 + 0) * N + cu], d.gu[(comp * 3 + 1) * N + cu],
+                                          d.gu[(comp * 3 + 2) * N + cu], d.xf[f] - d.xc[cu],
+                                          d.xf[F + f] - d.xc[N + cu], d.xf[2 * F + f] - d.xc[2 * N + cu]);
+      const double dc = P.conv_blend * Fm * dcv;
+      rhs = own ? rhs - dc : rhs + dc;
+    }
+    if (P.nonorth_corr > 0.0) {
+      const double gf0 = lf * d.gu[(comp * 3 + 0) * N + a] + l1 * d.gu[(comp * 3 + 0) * N + b];
+      const double gf1 = lf * d.gu[(comp * 3 + 1) * N + a] + l1 * d.gu[(comp * 3 + 1) * N + b];
+      const double gf2 = lf * d.gu[(comp * 3 + 2) * N + a] + l1 * d.gu[(comp * 3 + 2) * N + b];
+      const double noc = d.mnc[f] * dot3(gf0, gf1, gf2, d.tv[f], d.tv[F + f], d.tv[2 * F + f]);
+      rhs = own ? rhs + noc : rhs - noc;
+    }
+    const double pf = lf * d.p[a] + l1 * d.p[b];
+    const double S = sfc[f];
+    rhs = own ? rhs - pf * S : rhs + pf * S;
+  }
+  // boundary faces
+  for (int k = kb; k < ke; ++k) {
+    const int f = d.cf[k];
+    if (d.c1[f] >= 0) continue;
+    const int gi = d.fgrp[f];
+    if (gi < 0) continue;
+    const DevGroup& gr = d.groups[gi];
+    const double s0 = d.sf[f], s1 = d.sf[F + f], s2 = d.sf[2 * F + f];
+    double w[3];
+    bc_face_vel(gr, rp, d.xf[f], d.xf[F + f], d.xf[2 * F + f], s0, s1, s2, u0[c], u1[c], u2[c], w[0], w[1],
+                w[2]);
+    const double pf = bc_face_p(gr, rp, d.p[c]);
+    const double D = d.Dm[f];
+    const double Fm = P.rho * dot3(w[0], w[1], w[2], s0, s1, s2);
+    switch (gr.btype) {
+      case MGPU_BC_WALL:
+      case MGPU_BC_SYMMETRY:
+      case MGPU_BC_VINLET:
+      case MGPU_BC_VINLET_PARAB:
+      case MGPU_BC_SLIPWALL:
+      case MGPU_BC_MASSINLET:
+        ap = ap + D + fmax(Fm, 0.0);
+        rhs = rhs + D * w[comp] - Fm * w[comp];
+        break;
+      case MGPU_BC_POUTLET:
+      case MGPU_BC_OUTFLOW:
+        ap = ap + fmax(Fm, 0.0);
+        rhs = rhs - fmin(Fm, 0.0) * ucomp[c];
+        break;
+      case MGPU_BC_FARFIELD:
+        if (Fm < 0.0) {
+          ap = ap + D + fmax(Fm, 0.0);
+          rhs = rhs + D * w[comp] - Fm * w[comp];
+        } else {
+          ap = ap + Fm;
+        }
+        break;
+      default:
+        break;
+    }
+    rhs = rhs - pf * sfc[f];
+  }
+  const double vol = d.vol[c];
+  if (P.has_body_force) rhs = rhs + P.body_force[comp] * vol;
+  const int ts = d.st->ts_order;
+  if (ts == 1) {
+    const double at = P.rho * vol / P.dt;
+    ap = ap + at;
+    rhs = rhs + at * d.u_old[(long)comp * N + c];
+  } else if (ts == 2) {
+    const double at = P.rho * vol / (2.0 * P.dt);
+    ap = ap + 3.0 * at;
+    rhs = rhs + at * (4.0 * d.u_old[(long)comp * N + c] - d.u_old_old[(long)comp * N + c]);
+  }
+  if (ts > 0) {
+    A[d.diag[c]] = ap;
+  } else {
+    A[d.diag[c]] = ap / P.alpha_u;
+    rhs = rhs + (1.0 - P.alpha_u) / P.alpha_u * ap * ucomp[c];
+  }
+  d.rhs[c] = rhs;
+  d.ap[c] = ap;
+}
+
+__global__ void k_apc(DeviceCase d, double div) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d.st->abort || c >= d.N) return;
+  d.apc[c] = (div == 1.0) ? d.ap[c] : d.ap[c] / div;
+}
+
+__global__ void k_fill(double* a, long n, double v) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+
+// flux_rhiechow: one thread per face
+__global__ void __launch_bounds__(256) k_rhiechow(DeviceCase d, AsmParams P) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d.st->abort || f >= d.F) return;
+  const int N = d.N, F = d.F;
+  const int a = d.c0[f], b = d.c1[f];
+  const double s0 = d.sf[f], s1 = d.sf[F + f], s2 = d.sf[2 * F + f];
+  if (b < 0) {
+    const Ramp rp = ramp_of(P, d.st);
+    double w0, w1, w2;
+    bc_face_vel(d.groups[d.fgrp[f]], rp, d.xf[f], d.xf[F + f], d.xf[2 * F + f], s0, s1, s2, d.u[a], d.u[N + a],
+                d.u[2 * N + a], w0, w1, w2);
+    d.flux[f] = P.rho * dot3(w0, w1, w2, s0, s1, s2);
+    return;
+  }
+  const double lf = d.lf[f], l1 = 1.0 - lf;
+  const double uf0 = lf * d.u[a] + l1 * d.u[b];
+  const double uf1 = lf * d.u[N + a] + l1 * d.u[N + b];
+  const double uf2 = lf * d.u[2 * N + a] + l1 * d.u[2 * N + b];
+  const double gp0 = lf * d.gp[a] + l1 * d.gp[b];
+  const double gp1 = lf * d.gp[N + a] + l1 * d.gp[N + b];
+  const double gp2 = lf * d.gp[2 * N + a] + l1 * d.gp[2 * N + b];
+  const double dn = d.dn[f];
+  const double pfgrad_n = (d.p[b] - d.p[a]) / dn;
+  const double dbf = lf * d.vol[a] / d.apc[a] + l1 * d.vol[b] / d.apc[b];
+  d.flux[f] = P.rho * (dot3(uf0, uf1, uf2, s0, s1, s2) +
+                       dbf * (dot3(gp0, gp1, gp2, s0, s1, s2) - pfgrad_n * d.dsf[f] / dn));
+}
+
+// outflow_mass_sums + outflow_mass_scale in face order (one thread: the sums
+// are sequential in the reference; only cases with an outflow zone use it)
+__global__ void k_outflow(DeviceCase d) {
+  if (d.st->abort || blockIdx.x != 0 || threadIdx.x != 0) return;
+  double m_req = 0.0, m_out = 0.0, area_out = 0.0;
+  for (int i = 0; i < d.F; ++i) {
+    if (d.c1[i] >= 0 || d.fgrp[i] < 0) continue;
+    const int bt = d.groups[d.fgrp[i]].btype;
+    if (bt == MGPU_BC_OUTFLOW) {
+      m_out = m_out + d.flux[i];
+      area_out = area_out + d.area[i];
+    } else if (bt != MGPU_BC_POUTLET && bt != MGPU_BC_FARFIELD) {
+      m_req = m_req - d.flux[i];
+    }
+  }
+  if (area_out <= 0.0 || m_req <= 0.0) return;
+  const bool scaled = m_out > 1.0e-2 * m_req;
+  const double beta = scaled ? m_req / m_out : 0.0;
+  for (int i = 0; i < d.F; ++i) {
+    if (d.c1[i] >= 0 || d.fgrp[i] < 0 || d.groups[d.fgrp[i]].btype != MGPU_BC_OUTFLOW) continue;
+    d.flux[i] = scaled ? beta * d.flux[i] : m_req * d.area[i] / area_out;
+  }
+}
+
+// ppe_assembly: row c of the pressure-correction matrix, rhs(c), pin, pp := 0
+__global__ void __launch_bounds__(256) k_ppe(DeviceCase d, AsmParams P) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d.st->abort || c >= d.N) return;
+  double* A = d.pval;
+  const int rb = d.row_ptr[c], re = d.row_ptr[c + 1], dg = d.diag[c];
+  for (int k = rb; k < re; ++k) A[k] = 0.0;
+  double rhs = 0.0;
+  for (int k = d.cf_ptr[c]; k < d.cf_ptr[c + 1]; ++k) {
+    const int f = d.cf[k];
+    const int a = d.c0[f], b = d.c1[f];
+    if (b < 0) {
+      const int gi = d.fgrp[f];
+      if (gi >= 0 && p_dirichlet(d.groups[gi].btype)) {
+        const double dbf = d.vol[c] / d.apc[c];
+        const double af = P.rho * dbf * d.area[f] / d.dn[f];
+        A[dg] = A[dg] + af;
+        d.af[f] = af;
+      }
+      rhs = rhs - d.flux[f];
+      continue;
+    }
+    const double lf = d.lf[f];
+    const double dbf = lf * d.vol[a] / d.apc[a] + (1.0 - lf) * d.vol[b] / d.apc[b];
+    const double af = P.rho * dbf * d.area[f] / d.dn[f];
+    A[dg] = A[dg] + af;
+    const int slot = d.cf_slot[k];
+    A[slot] = A[slot] - af;
+    if (a == c) {
+      rhs = rhs - d.flux[f];
+      d.af[f] = af;
+    } else {
+      rhs = rhs + d.flux[f];
+    }
+  }
+  if (!P.has_pdir) {
+    if (c == 0) {
+      for (int k = rb; k < re; ++k) A[k] = (d.col[k] == 0) ? 1.0 : 0.0;
+      rhs = 0.0;
+    } else if (d.col[rb] == 0) {
+      A[rb] = 0.0;
+    }
+  }
+  d.rhs[c] = rhs;
+  d.pp[c] = 0.0;
+}
+
+// correct_fields, cell part: Green-Gauss grad(p') and the u, p updates
+__global__ void __launch_bounds__(256) k_correct_cells(DeviceCase d, AsmParams P) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d.st->abort || c >= d.N) return;
+  const int N = d.N, F = d.F;
+  double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+  for (int k = d.cf_ptr[c]; k < d.cf_ptr[c + 1]; ++k) {
+    const int f = d.cf[k];
+    const int a = d.c0[f], b = d.c1[f];
+    double phif;
+    if (b >= 0) {
+      const double lf = d.lf[f];
+      phif = lf * d.pp[a] + (1.0 - lf) * d.pp[b];
+    } else {
+      const int gi = d.fgrp[f];
+      phif = (gi >= 0 && p_dirichlet(d.groups[gi].btype)) ? 0.0 : d.pp[a];
+    }
+    const double s0 = d.sf[f], s1 = d.sf[F + f], s2 = d.sf[2 * F + f];
+    if (a == c) {
+      g0 = g0 + phif * s0;
+      g1 = g1 + phif * s1;
+      g2 = g2 + phif * s2;
+    } else {
+      g0 = g0 - phif * s0;
+      g1 = g1 - phif * s1;
+      g2 = g2 - phif * s2;
+    }
+  }
+  const double vol = d.vol[c];
+  g0 = g0 / vol;
+  g1 = g1 / vol;
+  g2 = g2 / vol;
+  const double va = vol / d.apc[c];
+  d.u[c] = d.u[c] - va * g0;
+  d.u[N + c] = d.u[N + c] - va * g1;
+  d.u[2 * N + c] = d.u[2 * N + c] - va * g2;
+  d.p[c] = (d.st->ts_order > 0) ? d.p[c] + d.pp[c] : d.p[c] + P.alpha_p * d.pp[c];
+}
+
+// correct_fields, flux part
+__global__ void k_correct_flux(DeviceCase d) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d.st->abort || f >= d.F) return;
+  const int a = d.c0[f], b = d.c1[f];
+  if (b < 0) {
+    const int gi = d.fgrp[f];
+    if (gi >= 0 && p_dirichlet(d.groups[gi].btype)) d.flux[f] = d.flux[f] + d.af[f] * d.pp[a];
+    return;
+  }
+  d.flux[f] = d.flux[f] - d.af[f] * (d.pp[b] - d.pp[a]);
+}
+
+__device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {
+  atomicMax(a, (unsigned long long)__double_as_longlong(v));
+}
+
+// Diagnostics of one outer iteration / step: max|imbalance|, max|du|,
+// max|u| (transient), first non-finite value (min over cell*4+field).
+__global__ void __launch_bounds__(256) k_diag(DeviceCase d, int transient) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d.st->abort) return;
+  double im = 0.0, du = 0.0, um = 0.0;
+  unsigned long long key = ~0ull;
+  if (c < d.N) {
+    const int N = d.N;
+    for (int k = d.cf_ptr[c]; k < d.cf_ptr[c + 1]; ++k) {
+      const int f = d.cf[k];
+      im = (d.c0[f] == c) ? im + d.flux[f] : im - d.flux[f];
+    }
+    im = fabs(im);
+    const double* ref = transient ? d.u_old : d.uo;
+    const double v[4] = {d.u[c], d.u[N + c], d.u[2 * N + c], d.p[c]};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) du = fmax(du, fabs(v[q] - ref[(long)q * N + c]));
+    if (transient) um = norm3(v[0], v[1], v[2]);
+#pragma unroll
+    for (int q = 3; q >= 0; --q)
+      if (!isfinite(v[q])) key = (unsigned long long)c * 4ull + (unsigned long long)q;
+    if (isnan(im)) im = 0.0;  // a non-finite field is reported by the scan
+    if (isnan(du)) du = 0.0;
+    if (isnan(um)) um = 0.0;
+  }
+  // warp-level max (exact, order-independent) before the atomics
+  for (int o = 16; o > 0; o >>= 1) {
+    im = fmax(im, __shfl_xor_sync(0xffffffffu, im, o));
+    du = fmax(du, __shfl_xor_sync(0xffffffffu, du, o));
+    um = fmax(um, __shfl_xor_sync(0xffffffffu, um, o));
+    unsigned long long ko = __shfl_xor_sync(0xffffffffu, key, o);
+    key = ko < key ? ko : key;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_pos(&d.st->imbal_bits, im);
+    atomic_max_pos(&d.st->du_bits, du);
+    if (transient) atomic_max_pos(&d.st->umax_bits, um);
+    if (key != ~0ull) atomicMin(&d.st->nan_key, key);
+  }
+}
+
+// Close the iteration: record, NaN guard (ier 60), convergence, advance.
+__global__ void k_diag_finalize(DeviceCase d, AsmParams P, int transient) {
+  DevStatus* st = d.st;
+  if (st->abort) return;
+  MgpuIterRec* rec = d.recs + st->cur_it;
+  if (st->nan_key != ~0ull) {
+    const unsigned long long k = st->nan_key;
+    const int cell = (int)(k >> 2), q = (int)(k & 3ull);
+    const double v = q < 3 ? d.u[(long)q * d.N + cell] : d.p[cell];
+    st->nan_field = q + 1;
+    st->nan_cell = cell + 1;
+    st->nan_val = v;
+    st->nan_kind = isnan(v) ? 1 : 2;
+    st->ier = 60;
+    st->abort = 1;
+    return;
+  }
+  const double imbal = __longlong_as_double((long long)st->imbal_bits) / P.flux_ref;
+  double du = __longlong_as_double((long long)st->du_bits);
+  int itl_max = 0;
+  double ressum = 0.0;
+  for (int s = 0; s < rec->nsolve && s < MGPU_MAXSOLVE; ++s) itl_max = max(itl_max, rec->lin_it[s]);
+  for (int s = 0; s < 3; ++s) ressum = ressum + rec->lin_res[s];
+  rec->it = st->cur_it + 1;
+  rec->itl_max = itl_max;
+  rec->ressum = ressum;
+  rec->imbal = imbal;
+  rec->dT_max = 0.0;
+  if (transient) {
+    st->t_now = st->t_now + P.dt;
+    du = du / P.dt;
+    const double umax = __longlong_as_double((long long)st->umax_bits);
+    rec->umax = umax;
+    rec->cfl_max = umax * P.dt / P.min_cbrt_vol;
+    rec->t_now = st->t_now;
+  }
+  rec->du_max = du;
+  st->imbal_bits = st->du_bits = st->umax_bits = 0ull;
+  st->cur_it = st->cur_it + 1;
+  if (!transient && imbal < P.outer_tol && du < P.outer_tol && 0.0 < P.outer_tol) {
+    st->converged = 1;
+    st->abort = 1;
+  }
+}
+
+// SIMPLE: uo := u ; PISO: history shift and time-scheme order
+__global__ void k_begin_iter(DeviceCase d, int transient, int time_scheme) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (d.st->abort) return;
+  const long n3 = 3l * d.N;
+  if (i < n3) {
+    if (transient) {
+      d.u_old_old[i] = d.u_old[i];
+      d.u_old[i] = d.u[i];
+    } else {
+      d.uo[i] = d.u[i];
+    }
+  }
+  if (i == 0) {
+    MgpuIterRec* rec = d.recs + d.st->cur_it;
+    rec->nsolve = 0;
+    if (transient) d.st->ts_order = (d.st->cur_it == 0 || time_scheme == 1) ? 1 : 2;
+  }
+}
+
+}  // namespace
+
+// ---------------- launchers -------------------------------------------------
+
+#define GRID(n) ceil_div((n), 256), 256, 0, s
+
+int geometry_setup(DeviceCase& d, const double* x, const int* fptr, const int* fnodes, double* pcen,
+                   const AsmParams& P, cudaStream_t s) {
+  k_face_props<<<GRID(d.F)>>>(d.F, x, fptr, fnodes, d.xf, d.sf, d.area);
+  MGPU_LAUNCH_CHECK("k_face_props");
+  k_prov_centers<<<GRID(d.N)>>>(d.N, x, fptr, fnodes, d.cf_ptr, d.cf, pcen);
+  MGPU_LAUNCH_CHECK("k_prov_centers");
+  k_orient<<<GRID(d.F)>>>(d.F, d.N, d.c0, d.xf, pcen, d.sf);
+  MGPU_LAUNCH_CHECK("k_orient");
+  k_cell_volumes<<<GRID(d.N)>>>(d.N, d.F, d.c0, d.cf_ptr, d.cf, d.xf, d.sf, pcen, d.vol, d.xc);
+  MGPU_LAUNCH_CHECK("k_cell_volumes");
+  k_face_consts<<<GRID(d.F)>>>(d, P);
+  MGPU_LAUNCH_CHECK("k_face_consts");
+  return 0;
+}
+
+int launch_gradients(const DeviceCase& d, const AsmParams& P, cudaStream_t s) {
+  k_gradients<<<GRID(d.N)>>>(d, P);
+  MGPU_LAUNCH_CHECK("k_gradients");
+  return 0;
+}
+int launch_limiter(const DeviceCase& d, const AsmParams& P, int comp, cudaStream_t s) {
+  k_limiter<<<GRID(d.N)>>>(d, P, comp);
+  MGPU_LAUNCH_CHECK("k_limiter");
+  return 0;
+}
+int launch_momentum(const DeviceCase& d, const AsmParams& P, int comp, cudaStream_t s) {
+  k_momentum<<<GRID(d.N)>>>(d, P, comp);
+  MGPU_LAUNCH_CHECK("k_momentum");
+  return 0;
+}
+int launch_apc(const DeviceCase& d, double div, cudaStream_t s) {
+  k_apc<<<GRID(d.N)>>>(d, div);
+  MGPU_LAUNCH_CHECK("k_apc");
+  return 0;
+}
+int launch_fill(double* a, long n, double v, cudaStream_t s) {
+  k_fill<<<GRID(n)>>>(a, n, v);
+  MGPU_LAUNCH_CHECK("k_fill");
+  return 0;
+}
+int launch_rhiechow(const DeviceCase& d, const AsmParams& P, cudaStream_t s) {
+  k_rhiechow<<<GRID(d.F)>>>(d, P);
+  MGPU_LAUNCH_CHECK("k_rhiechow");
+  return 0;
+}
+int launch_outflow(const DeviceCase& d, cudaStream_t s) {
+  k_outflow<<<1, 32, 0, s>>>(d);
+  MGPU_LAUNCH_CHECK("k_outflow");
+  return 0;
+}
+int launch_ppe(const DeviceCase& d, const AsmParams& P, cudaStream_t s) {
+  k_ppe<<<GRID(d.N)>>>(d, P);
+  MGPU_LAUNCH_CHECK("k_ppe");
+  return 0;
+}
+int launch_correct(const DeviceCase& d, const AsmParams& P, cudaStream_t s) {
+  k_correct_cells<<<GRID(d.N)>>>(d, P);
+  MGPU_LAUNCH_CHECK("k_correct_cells");
+  k_correct_flux<<<GRID(d.F)>>>(d);
+  MGPU_LAUNCH_CHECK("k_correct_flux");
+  return 0;
+}
+int launch_diag(const DeviceCase& d, const AsmParams& P, int transient, cudaStream_t s) {
+  k_diag<<<GRID(d.N)>>>(d, transient);
+  MGPU_LAUNCH_CHECK("k_diag");
+  k_diag_finalize<<<1, 1, 0, s>>>(d, P, transient);
+  MGPU_LAUNCH_CHECK("k_diag_finalize");
+  return 0;
+}
+int launch_begin_iter(const DeviceCase& d, int transient, int time_scheme, cudaStream_t s) {
+  k_begin_iter<<<GRID(3l * d.N)>>>(d, transient, time_scheme);
+  MGPU_LAUNCH_CHECK("k_begin_iter");
+  return 0;
+}
+
+}  // namespace mgpu

@@ -1,0 +1,609 @@
+// case.cu -- the C-ABI of include/mixgpu.h: case lifetime, field transfer,
+// the SIMPLE and PISO drivers, and the stand-alone entry points.
+//
+// A case keeps mesh, geometry, matrices, fields and Krylov work resident in
+// HBM from mgpu_case_create to mgpu_case_destroy. A run enqueues every outer
+// iteration on the case's stream without host round trips: kernels return at
+// once after an abort (breakdown, non-finite value, convergence), so the
+// reference's early returns hold while the host only syncs at the end.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "assembly.cuh"
+#include "case.cuh"
+#include "mesh_host.h"
+
+namespace mgpu {
+
+static thread_local std::string g_err;
+static int g_device = 0;
+
+void set_error(const std::string& msg) { g_err = msg; }
+
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
+  g_err = std::string(what) + ": " + cudaGetErrorString(e) + " (" + file + ":" + std::to_string(line) + ")";
+  return MGPU_E_CUDA;
+}
+
+}  // namespace mgpu
+
+using namespace mgpu;
+
+struct MgpuCase {
+  DeviceCase d;
+  AsmParams P;
+  MgpuCtrl ctrl;
+  cudaStream_t stream = nullptr;
+  std::vector<void*> allocs;
+  int64_t bytes = 0;
+  int has_outflow = 0;
+  int profiling = 0;
+  MgpuTiming timing{};
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;
+  int64_t launches = 0;
+  int kblock = 256;
+
+  template <typename T>
+  int alloc(T*& p, size_t n) {
+    p = nullptr;
+    if (n == 0) n = 1;
+    void* q = nullptr;
+    MGPU_CUDA(cudaMalloc(&q, n * sizeof(T)));
+    allocs.push_back(q);
+    bytes += (int64_t)(n * sizeof(T));
+    p = (T*)q;
+    return 0;
+  }
+  template <typename T>
+  int upload(T*& p, const std::vector<T>& h) {
+    if (int e = alloc(p, h.size())) return e;
+    if (!h.empty()) MGPU_CUDA(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return 0;
+  }
+  ~MgpuCase() {
+    for (auto e : ev_pool) cudaEventDestroy(e);
+    if (ev_run0) cudaEventDestroy(ev_run0);
+    if (ev_run1) cudaEventDestroy(ev_run1);
+    for (void* p : allocs) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+#define TRY(x)                 \
+  do {                         \
+    int rc_ = (x);             \
+    if (rc_ != 0) return rc_;  \
+  } while (0)
+
+KrylovArgs base_args(MgpuCase* c) {
+  DeviceCase& d = c->d;
+  KrylovArgs a{};
+  a.n = d.N;
+  a.row_ptr = d.row_ptr;
+  a.col = d.col;
+  a.diag = d.diag;
+  a.fval = d.fval;
+  const long N = d.N;
+  a.r = d.kw;
+  a.r0 = d.kw + N;
+  a.p = d.kw + 2 * N;
+  a.v = d.kw + 3 * N;
+  a.s = d.kw + 4 * N;
+  a.t = d.kw + 5 * N;
+  a.ph = d.kw + 6 * N;
+  a.sh = d.kw + 7 * N;
+  a.z = d.kw + 8 * N;
+  a.w = d.kw + 9 * N;
+  a.nlev_lo = d.nlev_lo;
+  a.lo_ptr = d.lo_ptr;
+  a.lo_rows = d.lo_rows;
+  a.nlev_up = d.nlev_up;
+  a.up_ptr = d.up_ptr;
+  a.up_rows = d.up_rows;
+  a.lt_pos = d.lt_pos;
+  a.partials = d.partials;
+  a.bar = d.bar;
+  a.st = d.st;
+  a.recs = d.recs;
+  a.ferr = d.ferr;
+  a.tol = c->ctrl.lin_tol;
+  a.maxit = c->ctrl.lin_max;
+  return a;
+}
+
+cudaEvent_t next_event(MgpuCase* c) {
+  if (c->ev_used >= c->ev_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    c->ev_pool.push_back(e);
+  }
+  return c->ev_pool[c->ev_used++];
+}
+
+// factor (if needed) + solve; precond 0 ILU0, 1 Jacobi, 2 IC0
+int krylov(MgpuCase* c, KrylovArgs a, bool bicg) {
+  cudaStream_t s = c->stream;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (c->profiling) {
+    e0 = next_event(c);
+    e1 = next_event(c);
+    cudaEventRecord(e0, s);
+  }
+  if (a.precond != 1) {
+    TRY(launch_factor(a, a.precond, s));
+    c->launches++;
+  }
+  if (bicg)
+    TRY(launch_krylov_bicgstab(a, s));
+  else
+    TRY(launch_krylov_pcg(a, s));
+  c->launches++;
+  if (c->profiling) cudaEventRecord(e1, s);
+  return 0;
+}
+
+int momentum_solve(MgpuCase* c, int comp, bool transient) {
+  KrylovArgs a = base_args(c);
+  a.aval = c->d.aval;
+  a.b = c->d.rhs;
+  a.x = c->d.u + (long)comp * c->d.N;
+  a.precond = c->ctrl.mom_solver == MGPU_MOM_JACOBI ? 1 : 0;
+  a.zero_x = 0;
+  a.mpi_mode = transient ? 1 : 0;
+  a.slot = comp;
+  a.ier_breakdown = transient ? 33 : 20;
+  return krylov(c, a, true);
+}
+
+int ppe_solve(MgpuCase* c, int slot, bool transient) {
+  KrylovArgs a = base_args(c);
+  a.aval = c->d.pval;
+  a.b = c->d.rhs;
+  a.x = c->d.pp;
+  a.precond = c->ctrl.ppe_precond == MGPU_PPE_IC0 ? 2 : (c->ctrl.ppe_precond == MGPU_PPE_ILU0 ? 0 : 1);
+  a.zero_x = 1;
+  a.mpi_mode = transient ? 1 : 0;
+  a.slot = slot;
+  a.ier_breakdown = transient ? 34 : 21;
+  return krylov(c, a, false);
+}
+
+int reset_status(MgpuCase* c, int ts_order, int nrec) {
+  DevStatus h{};
+  h.ts_order = ts_order;
+  h.nan_key = ~0ull;
+  MGPU_CUDA(cudaMemcpyAsync(c->d.st, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+  MGPU_CUDA(cudaMemsetAsync(c->d.bar, 0, sizeof(unsigned long long), c->stream));
+  MGPU_CUDA(cudaMemsetAsync(c->d.recs, 0, sizeof(MgpuIterRec) * (size_t)nrec, c->stream));
+  return 0;
+}
+
+int ensure_recs(MgpuCase* c, int n) {
+  if (n <= c->d.rec_cap) return 0;
+  MgpuIterRec* r = nullptr;
+  TRY(c->alloc(r, (size_t)n));
+  c->d.recs = r;  // the old buffer stays owned by the case until destroy
+  c->d.rec_cap = n;
+  return 0;
+}
+
+int begin_run(MgpuCase* c) {
+  c->ev_used = 0;
+  c->launches = 0;
+  c->timing = MgpuTiming{};
+  if (!c->ev_run0) {
+    MGPU_CUDA(cudaEventCreate(&c->ev_run0));
+    MGPU_CUDA(cudaEventCreate(&c->ev_run1));
+  }
+  MGPU_CUDA(cudaEventRecord(c->ev_run0, c->stream));
+  return 0;
+}
+
+int end_run(MgpuCase* c, int nsteps_done, MgpuIterRec* log, int logcap, int* nrec, int* ier) {
+  MGPU_CUDA(cudaEventRecord(c->ev_run1, c->stream));
+  DevStatus h{};
+  MGPU_CUDA(cudaMemcpyAsync(&h, c->d.st, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  MGPU_CUDA(cudaStreamSynchronize(c->stream));
+  (void)nsteps_done;
+  const int done = h.cur_it;
+  if (nrec) *nrec = done;
+  if (log && logcap > 0 && done > 0)
+    MGPU_CUDA(cudaMemcpy(log, c->d.recs, sizeof(MgpuIterRec) * (size_t)std::min(done, logcap),
+                         cudaMemcpyDeviceToHost));
+  if (ier) *ier = h.ier;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev_run0, c->ev_run1);
+  c->timing.total_ms = ms;
+  c->timing.gpu_launches = c->launches;
+  if (c->profiling) {
+    double kms = 0.0;
+    for (size_t i = 0; i + 1 < c->ev_used; i += 2) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, c->ev_pool[i], c->ev_pool[i + 1]);
+      kms += t;
+    }
+    c->timing.krylov_launches = (int64_t)(c->ev_used / 2);
+    c->timing.krylov_ms = kms;
+  }
+  if (h.timeout) {
+    set_error("a bounded device wait ran out (grid barrier)");
+    return MGPU_E_TIMEOUT;
+  }
+  return 0;
+}
+
+int outer_iteration(MgpuCase* c, bool transient) {
+  DeviceCase& d = c->d;
+  const AsmParams& P = c->P;
+  cudaStream_t s = c->stream;
+  TRY(launch_begin_iter(d, transient ? 1 : 0, c->ctrl.time_scheme, s));
+  c->launches++;
+  for (int comp = 0; comp < 3; ++comp) {
+    if (P.conv_blend > 0.0) {
+      TRY(launch_limiter(d, P, comp, s));
+      c->launches++;
+    }
+    TRY(launch_momentum(d, P, comp, s));
+    c->launches++;
+    TRY(momentum_solve(c, comp, transient));
+  }
+  TRY(launch_apc(d, transient ? 1.0 : P.alpha_u, s));
+  TRY(launch_gradients(d, P, s));
+  TRY(launch_rhiechow(d, P, s));
+  c->launches += 3;
+  if (c->has_outflow) {
+    TRY(launch_outflow(d, s));
+    c->launches++;
+  }
+  const int ncorr = transient ? std::max(1, c->ctrl.n_correct) : 1;
+  for (int icorr = 0; icorr < ncorr; ++icorr) {
+    TRY(launch_ppe(d, P, s));
+    c->launches++;
+    TRY(ppe_solve(c, std::min(3 + icorr, MGPU_MAXSOLVE - 1), transient));
+    TRY(launch_correct(d, P, s));
+    c->launches += 2;
+  }
+  TRY(launch_diag(d, P, transient ? 1 : 0, s));
+  c->launches += 2;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mgpu_version(void) { return 100; }
+
+const char* mgpu_last_error(void) { return g_err.c_str(); }
+
+int mgpu_set_device(int device) {
+  MGPU_CUDA(cudaSetDevice(device));
+  g_device = device;
+  return 0;
+}
+
+int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out, int* ier) {
+  if (ier) *ier = 0;
+  if (!out || !ctrl) {
+    set_error("mgpu_case_create: null argument");
+    return MGPU_E_ARG;
+  }
+  *out = nullptr;
+  HostMesh hm;
+  std::string why;
+  if (int e = load_host_mesh(mesh, hm, why)) {
+    set_error(why);
+    return e;
+  }
+  std::vector<DevGroup> groups;
+  std::vector<int> fgrp;
+  int bier = 0;
+  if (int e = build_groups(hm, *ctrl, groups, fgrp, bier, why)) {
+    if (ier) *ier = bier;
+    set_error(why);
+    return e;
+  }
+  if (ctrl->conv_blend < 0.0 || ctrl->alpha_u <= 0.0 || ctrl->lin_max < 0) {
+    set_error("ctrl: invalid alpha_u / conv_blend / lin_max");
+    return MGPU_E_ARG;
+  }
+  HostTopo t;
+  build_topology(hm, t);
+  MGPU_CUDA(cudaSetDevice(g_device));
+  MgpuCase* c = new MgpuCase();
+  auto fail = [&](int e) {
+    delete c;
+    return e;
+  };
+  c->ctrl = *ctrl;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error("cudaStreamCreate failed");
+    return fail(MGPU_E_CUDA);
+  }
+  DeviceCase& d = c->d;
+  d.N = hm.N;
+  d.F = hm.F;
+  d.nnz = (int)t.col.size();
+  const long N = d.N, F = d.F;
+  int e = 0;
+  double *x = nullptr, *pcen = nullptr;
+  int *fptr = nullptr, *fnodes = nullptr;
+  if ((e = c->upload(d.c0, hm.c0)) || (e = c->upload(d.c1, hm.c1)) || (e = c->upload(d.fgrp, fgrp)) ||
+      (e = c->upload(d.cf_ptr, t.cf_ptr)) || (e = c->upload(d.cf, t.cf)) || (e = c->upload(d.cf_slot, t.cf_slot)) ||
+      (e = c->upload(d.row_ptr, t.row_ptr)) || (e = c->upload(d.col, t.col)) || (e = c->upload(d.diag, t.diag)) ||
+      (e = c->upload(d.lt_pos, t.mirror)) || (e = c->upload(d.lo_ptr, t.lo_ptr)) ||
+      (e = c->upload(d.lo_rows, t.lo_rows)) || (e = c->upload(d.up_ptr, t.up_ptr)) ||
+      (e = c->upload(d.up_rows, t.up_rows)) || (e = c->upload(d.groups, groups)))
+    return fail(e);
+  d.nlev_lo = t.nlev_lo;
+  d.nlev_up = t.nlev_up;
+  d.ngroups = (int)groups.size();
+  if ((e = c->alloc(d.xf, 3 * F)) || (e = c->alloc(d.sf, 3 * F)) || (e = c->alloc(d.area, F)) ||
+      (e = c->alloc(d.lf, F)) || (e = c->alloc(d.vol, N)) || (e = c->alloc(d.xc, 3 * N)) ||
+      (e = c->alloc(d.dn, F)) || (e = c->alloc(d.dsf, F)) || (e = c->alloc(d.Dm, F)) ||
+      (e = c->alloc(d.tv, 3 * F)) || (e = c->alloc(d.mnc, F)) || (e = c->alloc(d.u, 3 * N)) ||
+      (e = c->alloc(d.p, N)) || (e = c->alloc(d.gp, 3 * N)) || (e = c->alloc(d.gu, 9 * N)) ||
+      (e = c->alloc(d.flux, F)) || (e = c->alloc(d.apc, N)) || (e = c->alloc(d.ap, N)) ||
+      (e = c->alloc(d.rhs, N)) || (e = c->alloc(d.pp, N)) || (e = c->alloc(d.uo, 3 * N)) ||
+      (e = c->alloc(d.u_old, 3 * N)) || (e = c->alloc(d.u_old_old, 3 * N)) || (e = c->alloc(d.psi, N)) ||
+      (e = c->alloc(d.af, F)) || (e = c->alloc(d.aval, d.nnz)) || (e = c->alloc(d.pval, d.nnz)) ||
+      (e = c->alloc(d.fval, d.nnz)) || (e = c->alloc(d.kw, 10 * N)) || (e = c->alloc(d.partials, 4 * 4096)) ||
+      (e = c->alloc(d.bar, 1)) || (e = c->alloc(d.ferr, 1)) || (e = c->alloc(d.st, 1)))
+    return fail(e);
+  if ((e = ensure_recs(c, 64))) return fail(e);
+  // geometry (device), scratch for the node arrays and provisional centres
+  std::vector<int> fptr_h(hm.fptr.begin(), hm.fptr.end());
+  if ((e = c->upload(x, hm.x)) || (e = c->upload(fptr, fptr_h)) || (e = c->upload(fnodes, hm.fnodes)) ||
+      (e = c->alloc(pcen, 3 * N)))
+    return fail(e);
+  AsmParams& P = c->P;
+  P = AsmParams{};
+  P.rho = ctrl->rho;
+  P.mu = ctrl->mu;
+  P.alpha_u = ctrl->alpha_u;
+  P.alpha_p = ctrl->alpha_p;
+  P.conv_blend = ctrl->conv_blend;
+  P.nonorth_corr = ctrl->nonorth_corr;
+  P.dt = ctrl->dt;
+  P.outer_tol = ctrl->outer_tol;
+  P.inlet_ramp = ctrl->inlet_ramp;
+  for (int k = 0; k < 3; ++k) P.body_force[k] = ctrl->body_force[k];
+  P.has_body_force = (ctrl->body_force[0] != 0.0 || ctrl->body_force[1] != 0.0 || ctrl->body_force[2] != 0.0);
+  P.has_pdir = 0;
+  for (int k = 0; k < hm.F; ++k)
+    if (hm.c1[k] < 0 && (groups[fgrp[k]].btype == MGPU_BC_POUTLET || groups[fgrp[k]].btype == MGPU_BC_FARFIELD))
+      P.has_pdir = 1;
+  for (auto& g : groups)
+    if (g.btype == MGPU_BC_OUTFLOW) c->has_outflow = 1;
+  P.has_outflow = c->has_outflow;
+  DeviceCase dd = d;
+  DevStatus h0{};
+  h0.nan_key = ~0ull;
+  MGPU_CUDA(cudaMemcpy(d.st, &h0, sizeof(h0), cudaMemcpyHostToDevice));
+  if ((e = geometry_setup(dd, x, fptr, fnodes, pcen, P, c->stream))) return fail(e);
+  // init_fields: everything at rest, apc = 1
+  MGPU_CUDA(cudaMemsetAsync(d.u, 0, sizeof(double) * 3 * N, c->stream));
+  MGPU_CUDA(cudaMemsetAsync(d.p, 0, sizeof(double) * N, c->stream));
+  MGPU_CUDA(cudaMemsetAsync(d.flux, 0, sizeof(double) * F, c->stream));
+  MGPU_CUDA(cudaMemsetAsync(d.u_old, 0, sizeof(double) * 3 * N, c->stream));
+  MGPU_CUDA(cudaMemsetAsync(d.u_old_old, 0, sizeof(double) * 3 * N, c->stream));
+  MGPU_CUDA(cudaMemsetAsync(d.gp, 0, sizeof(double) * 3 * N, c->stream));
+  MGPU_CUDA(cudaMemsetAsync(d.gu, 0, sizeof(double) * 9 * N, c->stream));
+  MGPU_CUDA(cudaMemsetAsync(d.af, 0, sizeof(double) * F, c->stream));
+  MGPU_CUDA(cudaMemsetAsync(d.bar, 0, sizeof(unsigned long long), c->stream));
+  if ((e = launch_fill(d.apc, N, 1.0, c->stream))) return fail(e);
+  MGPU_CUDA(cudaStreamSynchronize(c->stream));
+  // scalars needing a sequential pass: flux_ref (group/face order) and the
+  // smallest vol**(1/3) (CFL estimate); computed once on the host
+  std::vector<double> area(F), vol(N);
+  MGPU_CUDA(cudaMemcpy(area.data(), d.area, sizeof(double) * F, cudaMemcpyDeviceToHost));
+  MGPU_CUDA(cudaMemcpy(vol.data(), d.vol, sizeof(double) * N, cudaMemcpyDeviceToHost));
+  for (long i = 0; i < N; ++i)
+    if (!(vol[i] > 0.0)) {
+      set_error("mesh: non-positive cell volume");
+      return fail(MGPU_E_MESH);
+    }
+  double uscale = 0.0, area_btot = 0.0;
+  for (int gi = 0; gi < (int)groups.size(); ++gi) {
+    const DevGroup& g = groups[gi];
+    uscale = std::max(std::max(std::max(uscale, norm3(g.lid_vel[0], g.lid_vel[1], g.lid_vel[2])),
+                               norm3(g.uvel[0], g.uvel[1], g.uvel[2])),
+                      g.uspeed);
+    for (int k = 0; k < hm.F; ++k)
+      if (fgrp[k] == gi) area_btot = area_btot + area[k];
+  }
+  if (uscale <= 0.0) uscale = 1.0;
+  if (area_btot <= 0.0) area_btot = 1.0;
+  P.flux_ref = ctrl->rho * uscale * area_btot;
+  double mc = HUGE_VAL;
+  for (long i = 0; i < N; ++i) mc = std::min(mc, std::pow(vol[i], 1.0 / 3.0));
+  P.min_cbrt_vol = mc;
+  *out = c;
+  return 0;
+}
+
+int mgpu_case_destroy(MgpuCase* c) {
+  delete c;
+  return 0;
+}
+
+int mgpu_case_device_bytes(const MgpuCase* c, int64_t* bytes) {
+  if (!c || !bytes) return MGPU_E_ARG;
+  *bytes = c->bytes;
+  return 0;
+}
+
+int mgpu_fields_upload(MgpuCase* c, const double* u, const double* p, const double* flux, const double* u_old,
+                       const double* u_old_old) {
+  if (!c) return MGPU_E_ARG;
+  const long N = c->d.N;
+  auto up3 = [&](double* dst, const double* src) -> int {
+    std::vector<double> soa(3 * N);
+    for (long i = 0; i < N; ++i)
+      for (int k = 0; k < 3; ++k) soa[k * N + i] = src[3 * i + k];
+    MGPU_CUDA(cudaMemcpy(dst, soa.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice));
+    return 0;
+  };
+  if (u) TRY(up3(c->d.u, u));
+  if (u_old) TRY(up3(c->d.u_old, u_old));
+  if (u_old_old) TRY(up3(c->d.u_old_old, u_old_old));
+  if (p) MGPU_CUDA(cudaMemcpy(c->d.p, p, sizeof(double) * N, cudaMemcpyHostToDevice));
+  if (flux) MGPU_CUDA(cudaMemcpy(c->d.flux, flux, sizeof(double) * c->d.F, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int mgpu_fields_download(MgpuCase* c, double* u, double* p, double* flux, double* gp, double* gu, double* apc) {
+  if (!c) return MGPU_E_ARG;
+  MGPU_CUDA(cudaStreamSynchronize(c->stream));
+  const long N = c->d.N;
+  auto down = [&](double* dst, const double* src, int planes) -> int {
+    std::vector<double> soa((size_t)planes * N);
+    MGPU_CUDA(cudaMemcpy(soa.data(), src, sizeof(double) * planes * N, cudaMemcpyDeviceToHost));
+    for (long i = 0; i < N; ++i)
+      for (int k = 0; k < planes; ++k) dst[(long)planes * i + k] = soa[k * N + i];
+    return 0;
+  };
+  if (u) TRY(down(u, c->d.u, 3));
+  if (gp) TRY(down(gp, c->d.gp, 3));
+  if (gu) {
+    // device planes comp*3+dir -> Fortran gu(comp,dir,cell): index comp + 3*dir + 9*cell
+    std::vector<double> soa(9 * N);
+    MGPU_CUDA(cudaMemcpy(soa.data(), c->d.gu, sizeof(double) * 9 * N, cudaMemcpyDeviceToHost));
+    for (long i = 0; i < N; ++i)
+      for (int comp = 0; comp < 3; ++comp)
+        for (int dir = 0; dir < 3; ++dir) gu[9 * i + comp + 3 * dir] = soa[(comp * 3 + dir) * N + i];
+  }
+  if (p) MGPU_CUDA(cudaMemcpy(p, c->d.p, sizeof(double) * N, cudaMemcpyDeviceToHost));
+  if (apc) MGPU_CUDA(cudaMemcpy(apc, c->d.apc, sizeof(double) * N, cudaMemcpyDeviceToHost));
+  if (flux) MGPU_CUDA(cudaMemcpy(flux, c->d.flux, sizeof(double) * c->d.F, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int mgpu_simple_run(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nrec, int* ier) {
+  if (!c || !ier) return MGPU_E_ARG;
+  *ier = 0;
+  if (nrec) *nrec = 0;
+  int it_max = c->ctrl.outer_max;
+  if (nsteps > 0) it_max = std::min(it_max, nsteps);
+  if (it_max <= 0) return 0;
+  TRY(ensure_recs(c, it_max + 1));
+  TRY(begin_run(c));
+  TRY(reset_status(c, 0, it_max + 1));
+  TRY(launch_fill(c->d.apc, c->d.N, 1.0, c->stream));
+  TRY(launch_gradients(c->d, c->P, c->stream));
+  c->launches += 2;
+  for (int it = 0; it < it_max; ++it) {
+    TRY(outer_iteration(c, false));
+    if ((it + 1) % 64 == 0 && it + 1 < it_max) {
+      // stop enqueuing once a run has aborted (convergence, breakdown, NaN)
+      int ab = 0;
+      MGPU_CUDA(cudaMemcpyAsync(&ab, &c->d.st->abort, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      MGPU_CUDA(cudaStreamSynchronize(c->stream));
+      if (ab) break;
+    }
+  }
+  return end_run(c, it_max, log, logcap, nrec, ier);
+}
+
+int mgpu_piso_run(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nrec, int* ier) {
+  if (!c || !ier) return MGPU_E_ARG;
+  *ier = 0;
+  if (nrec) *nrec = 0;
+  if (!c->ctrl.transient) {
+    *ier = 30;
+    return 0;
+  }
+  if (c->ctrl.dt <= 0.0) {
+    *ier = 31;
+    return 0;
+  }
+  int n_steps = std::max(1, c->ctrl.n_time_max);
+  if (nsteps > 0) n_steps = std::min(n_steps, nsteps);
+  TRY(ensure_recs(c, n_steps + 1));
+  TRY(begin_run(c));
+  TRY(reset_status(c, 1, n_steps + 1));
+  TRY(launch_fill(c->d.apc, c->d.N, 1.0, c->stream));
+  TRY(launch_gradients(c->d, c->P, c->stream));
+  TRY(launch_rhiechow(c->d, c->P, c->stream));
+  c->launches += 3;
+  for (int it = 0; it < n_steps; ++it) {
+    TRY(outer_iteration(c, true));
+    if ((it + 1) % 64 == 0 && it + 1 < n_steps) {
+      int ab = 0;
+      MGPU_CUDA(cudaMemcpyAsync(&ab, &c->d.st->abort, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      MGPU_CUDA(cudaStreamSynchronize(c->stream));
+      if (ab) break;
+    }
+  }
+  return end_run(c, n_steps, log, logcap, nrec, ier);
+}
+
+int mgpu_nan_scan(MgpuCase* c, int* ifin, int* field, int* cell, double* val, int* kind) {
+  if (!c || !ifin || !field || !cell || !val || !kind) return MGPU_E_ARG;
+  TRY(reset_status(c, 0, 1));
+  TRY(launch_diag(c->d, c->P, 0, c->stream));
+  DevStatus h{};
+  MGPU_CUDA(cudaMemcpyAsync(&h, c->d.st, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  MGPU_CUDA(cudaStreamSynchronize(c->stream));
+  *ifin = h.ier == 60 ? 1 : 0;
+  *field = h.nan_field;
+  *cell = h.nan_cell;
+  *val = h.nan_val;
+  *kind = h.nan_kind;
+  return 0;
+}
+
+int mgpu_case_stage(MgpuCase* c, int what, int ts_order, const double* apc, double* aval, double* rhs, double* ap,
+                    const double* pp) {
+  if (!c || what < 0 || what > 6) return MGPU_E_ARG;
+  DeviceCase& d = c->d;
+  cudaStream_t s = c->stream;
+  const long N = d.N;
+  TRY(reset_status(c, ts_order, 1));
+  if (apc) MGPU_CUDA(cudaMemcpyAsync(d.apc, apc, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  if (what == 0) {
+    TRY(launch_gradients(d, c->P, s));
+  } else if (what <= 3) {
+    if (c->P.conv_blend > 0.0) TRY(launch_limiter(d, c->P, what - 1, s));
+    TRY(launch_momentum(d, c->P, what - 1, s));
+  } else if (what == 4) {
+    TRY(launch_rhiechow(d, c->P, s));
+  } else if (what == 5) {
+    TRY(launch_ppe(d, c->P, s));
+  } else {
+    if (!pp) return MGPU_E_ARG;
+    MGPU_CUDA(cudaMemcpyAsync(d.pp, pp, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    // af of the last PPE assembly is reused by the flux correction
+    TRY(launch_correct(d, c->P, s));
+  }
+  MGPU_CUDA(cudaStreamSynchronize(s));
+  const double* A = (what == 5) ? d.pval : d.aval;
+  if (aval && (what >= 1 && what <= 5)) MGPU_CUDA(cudaMemcpy(aval, A, sizeof(double) * d.nnz, cudaMemcpyDeviceToHost));
+  if (rhs && (what >= 1 && what <= 5)) MGPU_CUDA(cudaMemcpy(rhs, d.rhs, sizeof(double) * N, cudaMemcpyDeviceToHost));
+  if (ap && (what >= 1 && what <= 3)) MGPU_CUDA(cudaMemcpy(ap, d.ap, sizeof(double) * N, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int mgpu_case_timing(const MgpuCase* c, MgpuTiming* t) {
+  if (!c || !t) return MGPU_E_ARG;
+  *t = c->timing;
+  return 0;
+}
+
+int mgpu_case_set_profiling(MgpuCase* c, int on) {
+  if (!c) return MGPU_E_ARG;
+  c->profiling = on ? 1 : 0;
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,106 @@
+// case.cuh -- device-resident state of one SIMPLE/PISO case.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace mgpu {
+
+// Run status shared by every kernel of a run. A kernel returns at once when
+// `abort` is set, which gives the reference's early returns (ier /= 0,
+// convergence) without a host round trip per outer iteration.
+struct DevStatus {
+  int abort;      // set on ier /= 0 or convergence
+  int ier;        // reference driver code (20, 21, 33, 34, 60, ...)
+  int cur_it;     // 0-based index of the outer iteration / step in progress
+  int converged;
+  int timeout;    // a bounded grid barrier ran out
+  int ts_order;   // 0 steady, 1 Euler, 2 BDF2 (fields_t%ts_order)
+  int nan_field, nan_cell;
+  int nan_kind;
+  int pad;
+  double nan_val;
+  double t_now;
+  unsigned long long imbal_bits, du_bits, umax_bits;  // max-reductions (bit patterns of x >= 0)
+  unsigned long long nan_key;                          // min (cell*4+field)
+};
+
+// Krylov solve arguments (matrix, preconditioner data, work, result slot).
+struct KrylovArgs {
+  int n;
+  const int* row_ptr;
+  const int* col;
+  const int* diag;
+  const double* aval;
+  double* fval;  // ILU(0)/IC(0) factor values (same pattern)
+  const double* b;
+  double* x;
+  double *r, *r0, *p, *v, *s, *t, *ph, *sh, *z, *w;
+  int nlev_lo;
+  const int* lo_ptr;
+  const int* lo_rows;
+  int nlev_up;
+  const int* up_ptr;
+  const int* up_rows;
+  const int* lt_ptr;  // transposed strictly-lower part, per column k: rows i > k (descending)
+  const int* lt_pos;  // position of L(i,k) in row i
+  double tol;
+  int maxit;
+  int precond;  // 0 ILU0, 1 Jacobi, 2 IC0
+  int zero_x;   // x := 0 before the solve (pressure correction)
+  int mpi_mode; // 1: the one-rank distributed solver variants (mod_uns_linsolver_mpi.f90)
+  double* partials;  // 4 * gridDim doubles
+  unsigned long long* bar;  // grid-barrier arrival counter (zeroed before each launch)
+  DevStatus* st;
+  MgpuIterRec* recs;
+  int slot;            // record slot of this solve
+  int ier_breakdown;   // driver code when ierr == 2 (0: none)
+  int* ferr;           // factorisation status written by the factor kernel
+};
+
+struct DeviceCase {
+  int N = 0, F = 0, nnz = 0;
+  // faces
+  int *c0 = nullptr, *c1 = nullptr, *fgrp = nullptr;
+  double *xf = nullptr, *sf = nullptr, *area = nullptr, *lf = nullptr;  // xf,sf: 3 SoA planes
+  // cells
+  double *vol = nullptr, *xc = nullptr;  // xc: 3 SoA planes
+  int *cf_ptr = nullptr, *cf = nullptr, *cf_slot = nullptr;
+  // per-face constants (bit-identical to recomputing them in the face loops)
+  double *dn = nullptr;   // interior |xc1-xc0|, boundary |xf-xc0|
+  double *dsf = nullptr;  // interior (xc1-xc0).sf
+  double *Dm = nullptr;   // momentum diffusion coefficient
+  double *tv = nullptr;   // 3 planes: sf - dvec*(area^2/sd)
+  double *mnc = nullptr;  // nonorth_corr*mu_f
+  // CSR pattern and level sets
+  int *row_ptr = nullptr, *col = nullptr, *diag = nullptr;
+  int nlev_lo = 0, nlev_up = 0;
+  int *lo_ptr = nullptr, *lo_rows = nullptr, *up_ptr = nullptr, *up_rows = nullptr;
+  int *lt_ptr = nullptr, *lt_pos = nullptr;
+  DevGroup* groups = nullptr;
+  int ngroups = 0;
+  // fields (SoA)
+  double *u = nullptr, *p = nullptr, *gp = nullptr, *gu = nullptr, *flux = nullptr, *apc = nullptr;
+  double *ap = nullptr, *rhs = nullptr, *pp = nullptr, *uo = nullptr, *u_old = nullptr, *u_old_old = nullptr;
+  double *psi = nullptr, *af = nullptr;
+  double *aval = nullptr, *pval = nullptr, *fval = nullptr;
+  // Krylov work
+  double *kw = nullptr;  // 10*N
+  double* partials = nullptr;
+  unsigned long long* bar = nullptr;
+  int* ferr = nullptr;
+  DevStatus* st = nullptr;
+  MgpuIterRec* recs = nullptr;
+  int rec_cap = 0;
+};
+
+// Launch helpers implemented in the .cu files.
+int launch_krylov_bicgstab(const KrylovArgs& a, cudaStream_t s);
+int launch_krylov_pcg(const KrylovArgs& a, cudaStream_t s);
+int launch_factor(const KrylovArgs& a, int kind, cudaStream_t s);
+int krylov_grid(int n, int& block, int which);
+int launch_spmv(int n, const int* rp, const int* col, const double* val, const double* x, double* y,
+                cudaStream_t s);
+
+}  // namespace mgpu

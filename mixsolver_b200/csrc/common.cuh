@@ -1,0 +1,178 @@
+// common.cuh -- shared device helpers of the B200 SIMPLE/PISO path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cfloat>
+#include <cmath>
+#include <string>
+
+#include "../../include/mixgpu.h"
+
+namespace mgpu {
+
+using std::fabs;
+using std::fmax;
+using std::fmin;
+using std::sqrt;
+
+// --- error plumbing -------------------------------------------------------
+void set_error(const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+
+#define MGPU_CUDA(call)                                                    \
+  do {                                                                     \
+    cudaError_t e_ = (call);                                               \
+    if (e_ != cudaSuccess) return ::mgpu::cuda_fail(e_, #call, __FILE__, __LINE__); \
+  } while (0)
+
+#define MGPU_LAUNCH_CHECK(what)                                            \
+  do {                                                                     \
+    cudaError_t e_ = cudaGetLastError();                                   \
+    if (e_ != cudaSuccess) return ::mgpu::cuda_fail(e_, what, __FILE__, __LINE__); \
+  } while (0)
+
+constexpr double DTINY = DBL_MIN;  // tiny(1.0_dp)
+
+// gfortran NORM2 of a 3-vector (scaled sum of squares, scale starting at 1).
+__host__ __device__ inline double norm3(double a, double b, double c) {
+  double result = 0.0, scale = 1.0;
+  double v[3] = {a, b, c};
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    if (v[i] != 0.0) {
+      double ax = fabs(v[i]);
+      if (ax > scale) {
+        double val = scale / ax;
+        result = 1.0 + result * val * val;
+        scale = ax;
+      } else {
+        double val = ax / scale;
+        result += val * val;
+      }
+    }
+  }
+  return scale * sqrt(result);
+}
+
+// dot_product of 3-vectors in gfortran's inline order ((0+a1b1)+a2b2)+a3b3.
+__host__ __device__ inline double dot3(double a0, double a1, double a2, double b0, double b1, double b2) {
+  double s = 0.0;
+  s = s + a0 * b0;
+  s = s + a1 * b1;
+  s = s + a2 * b2;
+  return s;
+}
+
+// Boundary group as the device sees it (bcgroup_t, mod_uns_bc.f90:80-110).
+struct DevGroup {
+  int btype;
+  int prfl_axis;  // 0-based
+  int has_lid;
+  int lid_dir;  // 0-based
+  double uvel[3];
+  double pval;
+  double uspeed;
+  double prfl_mean, prfl_span, prfl_origin;
+  double lid_coord, lid_tol;
+  double lid_vel[3];
+};
+
+struct Ramp {
+  double inlet, pval;  // g_inlet_ramp_factor, g_pval_ramp_factor
+};
+
+#ifdef __CUDACC__
+// bc_face_vel, mod_uns_bc.f90:400-509
+__device__ inline void bc_face_vel(const DevGroup& g, const Ramp& rp, double xf0, double xf1, double xf2,
+                                   double s0, double s1, double s2, double u0, double u1, double u2,
+                                   double& f0, double& f1, double& f2) {
+  double xf[3] = {xf0, xf1, xf2};
+  switch (g.btype) {
+    case MGPU_BC_WALL:
+      if (g.has_lid && fabs(xf[g.lid_dir] - g.lid_coord) <= g.lid_tol) {
+        f0 = g.lid_vel[0];
+        f1 = g.lid_vel[1];
+        f2 = g.lid_vel[2];
+      } else {
+        f0 = f1 = f2 = 0.0;
+      }
+      return;
+    case MGPU_BC_SYMMETRY: {
+      double ns = norm3(s0, s1, s2);
+      double n0 = s0 / ns, n1 = s1 / ns, n2 = s2 / ns;
+      double un = dot3(u0, u1, u2, n0, n1, n2);
+      f0 = u0 - 2.0 * un * n0;
+      f1 = u1 - 2.0 * un * n1;
+      f2 = u2 - 2.0 * un * n2;
+      return;
+    }
+    case MGPU_BC_VINLET:
+      f0 = g.uvel[0];
+      f1 = g.uvel[1];
+      f2 = g.uvel[2];
+      return;
+    case MGPU_BC_VINLET_PARAB: {
+      double ns = norm3(s0, s1, s2);
+      double n0 = s0 / ns, n1 = s1 / ns, n2 = s2 / ns;
+      double xi = (xf[g.prfl_axis] - g.prfl_origin) / g.prfl_span;
+      xi = fmax(0.0, fmin(1.0, xi));
+      double uspc = 6.0 * g.prfl_mean * xi * (1.0 - xi);
+      f0 = -uspc * n0;
+      f1 = -uspc * n1;
+      f2 = -uspc * n2;
+      return;
+    }
+    case MGPU_BC_MASSINLET: {
+      double ns = norm3(s0, s1, s2);
+      double n0 = s0 / ns, n1 = s1 / ns, n2 = s2 / ns;
+      f0 = -g.uspeed * rp.inlet * n0;
+      f1 = -g.uspeed * rp.inlet * n1;
+      f2 = -g.uspeed * rp.inlet * n2;
+      return;
+    }
+    case MGPU_BC_FARFIELD: {
+      double ns = norm3(s0, s1, s2);
+      double n0 = s0 / ns, n1 = s1 / ns, n2 = s2 / ns;
+      double un = dot3(g.uvel[0], g.uvel[1], g.uvel[2], n0, n1, n2);
+      if (un < 0.0) {
+        f0 = g.uvel[0];
+        f1 = g.uvel[1];
+        f2 = g.uvel[2];
+      } else {
+        f0 = u0;
+        f1 = u1;
+        f2 = u2;
+      }
+      return;
+    }
+    case MGPU_BC_SLIPWALL: {
+      double ns = norm3(s0, s1, s2);
+      double n0 = s0 / ns, n1 = s1 / ns, n2 = s2 / ns;
+      double un = dot3(u0, u1, u2, n0, n1, n2);
+      f0 = u0 - un * n0;
+      f1 = u1 - un * n1;
+      f2 = u2 - un * n2;
+      return;
+    }
+    default:
+      f0 = u0;
+      f1 = u1;
+      f2 = u2;
+  }
+}
+
+// bc_face_p, mod_uns_bc.f90:514-549
+__device__ inline double bc_face_p(const DevGroup& g, const Ramp& rp, double pP) {
+  if (g.btype == MGPU_BC_POUTLET || g.btype == MGPU_BC_FARFIELD) return g.pval * rp.pval;
+  return pP;
+}
+
+__device__ inline bool p_dirichlet(int btype) { return btype == MGPU_BC_POUTLET || btype == MGPU_BC_FARFIELD; }
+#endif
+
+
+inline unsigned ceil_div(long a, long b) { return (unsigned)((a + b - 1) / b); }
+
+}  // namespace mgpu

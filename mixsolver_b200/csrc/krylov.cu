@@ -1,0 +1,601 @@
+// krylov.cu -- persistent Krylov solves of the FP64 parity form.
+//
+// One cooperative kernel per linear solve (PCG or BiCGStab): every phase of
+// the reference's iteration runs as a grid-stride pass, dot products and norms
+// are two-level deterministic reductions (warp butterfly + fixed-order sum of
+// per-block partials), and the phases are separated by a bounded grid barrier,
+// so the Krylov scalars never leave the GPU and the solve costs one launch.
+// ILU(0)/IC(0) factorisation and triangular sweeps are level-scheduled: rows
+// of one level are independent, and each row is computed by one thread in the
+// reference's sequential order, so factor values and sweep results are
+// bit-identical to mod_uns_linsolver.f90.
+//
+// Reference: src/unstructured/mod_uns_linsolver.f90 (csr_matvec :40-52,
+// ilu0_factor :79-115, ilu0_apply :120-142, bicgstab_ilu0 :148-224, cg_jacobi
+// :230-291, ic0_factor :328-365, ic0_apply :371-399, cg_ic0 :405-461) and
+// mod_uns_linsolver_mpi.f90:155-363 at one rank.
+
+#include <type_traits>
+
+#include "case.cuh"
+
+namespace mgpu {
+
+namespace {
+
+constexpr int kSingleBlockRows = 32768;  // rows up to which one block runs a solve
+constexpr unsigned kSpinLimit = 1u << 25;  // ~2 s of polling: then flag a timeout
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ int ld_acquire_i32(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Bounded grid barrier over a monotone 64-bit arrival counter (zeroed before
+// every cooperative launch; all blocks are co-resident). Each block adds one
+// arrival and waits until the counter reaches the end of the current round.
+// Returns false when the wait ran out; the caller then leaves the kernel.
+__device__ bool grid_sync(unsigned long long* bar, DevStatus* st) {
+  __shared__ int s_ok;
+  if (gridDim.x == 1) {
+    __syncthreads();
+    return true;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned long long nb = gridDim.x;
+    __threadfence();
+    const unsigned long long old = atomicAdd(bar, 1ull);
+    const unsigned long long target = (old / nb + 1ull) * nb;
+    unsigned spins = 0;
+    while (ld_acquire_u64(bar) < target) {
+      if (++spins > 256u) __nanosleep(64);
+      if (spins > kSpinLimit) {
+        atomicExch(&st->timeout, 1);
+        ok = 0;
+        break;
+      }
+    }
+    __threadfence();
+    if (ok && ld_acquire_i32(&st->timeout) != 0) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Vector loads inside a persistent kernel: with one block every thread sits on
+// the same SM and __syncthreads orders its global accesses, so plain (L1)
+// loads are coherent; with several blocks, data written by another block is
+// read from L2.
+template <bool L1, typename T>
+__device__ __forceinline__ T ldv(const T* p) {
+  if constexpr (L1)
+    return *p;
+  else
+    return __ldcg(p);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = v + __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic grid-wide sum of NQ values: block tree -> per-block partials
+// -> barrier -> every block sums the partials in the same fixed order.
+template <int NQ, bool L1>
+__device__ bool grid_sum(double (&v)[NQ], double* partials, unsigned long long* bar, DevStatus* st) {
+  __shared__ double sh[NQ][32];
+  __shared__ double tot[NQ];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double s = warp_sum(v[q]);
+    if (lane == 0) sh[q][warp] = s;
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      double s = lane < nw ? sh[q][lane] : 0.0;
+      s = warp_sum(s);
+      if (lane == 0) partials[q * gridDim.x + blockIdx.x] = s;
+    }
+  }
+  if (!grid_sync(bar, st)) return false;
+  if (warp == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      double s = 0.0;
+      for (int j = lane; j < (int)gridDim.x; j += 32) s = s + ldv<L1>(&partials[q * gridDim.x + j]);
+      s = warp_sum(s);
+      if (lane == 0) tot[q] = s;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) v[q] = tot[q];
+  __syncthreads();
+  return true;
+}
+
+// y_i = A_i . x in csr_matvec order (x may have been written by other blocks).
+template <bool L1>
+__device__ __forceinline__ double row_spmv(const int* __restrict__ rp, const int* __restrict__ col,
+                                           const double* __restrict__ val, const double* x, int i) {
+  double y = 0.0;
+  const int e = rp[i + 1];
+  for (int k = rp[i]; k < e; ++k) y = y + val[k] * ldv<L1>(&x[col[k]]);
+  return y;
+}
+
+// z = M^{-1} src for ILU(0) (kind 0) or IC(0) (kind 2); src may alias nothing
+// but z. Level-scheduled forward and backward sweeps.
+template <bool L1>
+__device__ bool apply_lu(const KrylovArgs& a, int kind, const double* src, double* z) {
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstr = gridDim.x * blockDim.x;
+  const double* f = a.fval;
+  for (int lev = 0; lev < a.nlev_lo; ++lev) {
+    const int e = a.lo_ptr[lev + 1];
+    for (int idx = a.lo_ptr[lev] + gtid; idx < e; idx += gstr) {
+      const int i = a.lo_rows[idx];
+      double s = ldv<L1>(&src[i]);
+      const int d = a.diag[i];
+      for (int k = a.row_ptr[i]; k < d; ++k) s = s - f[k] * ldv<L1>(&z[a.col[k]]);
+      z[i] = (kind == 2) ? s / f[d] : s;
+    }
+    if (!grid_sync(a.bar, a.st)) return false;
+  }
+  for (int lev = 0; lev < a.nlev_up; ++lev) {
+    const int e = a.up_ptr[lev + 1];
+    for (int idx = a.up_ptr[lev] + gtid; idx < e; idx += gstr) {
+      const int i = a.up_rows[idx];
+      const int d = a.diag[i], re = a.row_ptr[i + 1];
+      double s = ldv<L1>(&z[i]);
+      if (kind == 2) {
+        // L^T z = y, column sweep of ic0_apply: w(i) collects -L(j,i) z(j)
+        // for j = n..i+1 (descending), then z(i) = w(i)/L(i,i).
+        for (int k = re - 1; k > d; --k) s = s - f[a.lt_pos[k]] * ldv<L1>(&z[a.col[k]]);
+        z[i] = s / f[d];
+      } else {
+        for (int k = d + 1; k < re; ++k) s = s - f[k] * ldv<L1>(&z[a.col[k]]);
+        z[i] = s / f[d];
+      }
+    }
+    if (!grid_sync(a.bar, a.st)) return false;
+  }
+  return true;
+}
+
+__device__ void write_result(const KrylovArgs& a, int it, double res, int ierr) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    MgpuIterRec* rec = a.recs + a.st->cur_it;
+    if (a.slot >= 0 && a.slot < MGPU_MAXSOLVE) {
+      rec->lin_it[a.slot] = it;
+      rec->lin_res[a.slot] = res;
+      rec->lin_ierr[a.slot] = ierr;
+      if (rec->nsolve < a.slot + 1) rec->nsolve = a.slot + 1;
+    }
+    if (ierr == 2 && a.ier_breakdown != 0) {
+      a.st->ier = a.ier_breakdown;
+      a.st->abort = 1;
+    }
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Factorisation kernel: ILU(0) (kind 0) or IC(0) (kind 2) of aval into fval.
+// ---------------------------------------------------------------------------
+template <bool L1>
+__global__ void __launch_bounds__(L1 ? 512 : 256) k_factor(KrylovArgs a, int kind) {
+  if (a.st->abort) return;
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstr = gridDim.x * blockDim.x;
+  if (gtid == 0) *a.ferr = 0;
+  const int nnz = a.row_ptr[a.n];
+  for (int k = gtid; k < nnz; k += gstr) a.fval[k] = a.aval[k];
+  if (!grid_sync(a.bar, a.st)) return;
+  double* f = a.fval;
+  for (int lev = 0; lev < a.nlev_lo; ++lev) {
+    const int e = a.lo_ptr[lev + 1];
+    for (int idx = a.lo_ptr[lev] + gtid; idx < e; idx += gstr) {
+      const int i = a.lo_rows[idx];
+      const int rb = a.row_ptr[i], re = a.row_ptr[i + 1], di = a.diag[i];
+      if (kind == 0) {
+        // ilu0_factor row i (IKJ): rows k < i are final
+        for (int kk = rb; kk < di; ++kk) {
+          const int k = a.col[kk];
+          const double piv = ldv<L1>(&f[a.diag[k]]);
+          if (fabs(piv) < DTINY) {
+            atomicExch(a.ferr, 2);
+            continue;
+          }
+          const double aik = f[kk] / piv;
+          f[kk] = aik;
+          int pos = kk + 1;  // merge pointer into row i (columns ascending)
+          const int ke = a.row_ptr[k + 1];
+          for (int jj = a.diag[k]; jj < ke; ++jj) {
+            const int j = a.col[jj];
+            if (j <= k) continue;
+            while (pos < re && a.col[pos] < j) ++pos;
+            if (pos < re && a.col[pos] == j) f[pos] = f[pos] - aik * ldv<L1>(&f[jj]);
+          }
+        }
+      } else {
+        // ic0_factor row i
+        for (int kp = rb; kp < di; ++kp) {
+          const int k = a.col[kp];
+          // ic0_dot(row i [rb, kp-1], row k [row_ptr(k), diag(k)-1])
+          int p = rb, q = a.row_ptr[k];
+          const int p2 = kp - 1, q2 = a.diag[k] - 1;
+          double dsum = 0.0;
+          while (p <= p2 && q <= q2) {
+            const int cp = a.col[p], cq = a.col[q];
+            if (cp < cq)
+              ++p;
+            else if (cp > cq)
+              ++q;
+            else {
+              dsum = dsum + f[p] * ldv<L1>(&f[q]);
+              ++p;
+              ++q;
+            }
+          }
+          const double s = f[kp] - dsum;
+          f[kp] = s / ldv<L1>(&f[a.diag[k]]);
+        }
+        double s = f[di];
+        for (int kp = rb; kp < di; ++kp) s = s - f[kp] * f[kp];
+        if (s <= 0.0) atomicExch(a.ferr, 2);
+        f[di] = sqrt(s);
+      }
+    }
+    if (!grid_sync(a.bar, a.st)) return;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// PCG: cg_jacobi / cg_ic0 (and PCG with ILU(0)); `it` ends at maxit+1 on
+// non-convergence, as the Fortran DO loop leaves it.
+// ---------------------------------------------------------------------------
+template <bool L1>
+__global__ void __launch_bounds__(L1 ? 512 : 256) k_pcg(KrylovArgs a) {
+  if (a.st->abort) return;
+  const int n = a.n;
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstr = gridDim.x * blockDim.x;
+  const bool jac = a.precond == 1;
+  double* x = a.x;
+  double *r = a.r, *z = a.z, *p = a.p, *q = a.v;
+  // b.b and (Jacobi, one-rank distributed form) the count of |diag| < tiny
+  double v2[2] = {0.0, 0.0};
+  for (int i = gtid; i < n; i += gstr) {
+    if (a.zero_x) x[i] = 0.0;
+    const double bi = a.b[i];
+    v2[0] = v2[0] + bi * bi;
+    if (jac && fabs(a.aval[a.diag[i]]) < DTINY) v2[1] = v2[1] + 1.0;
+  }
+  if (!grid_sum<2, L1>(v2, a.partials, a.bar, a.st)) return;
+  const double bnrm = sqrt(v2[0]);
+  if (bnrm == 0.0) {
+    for (int i = gtid; i < n; i += gstr) x[i] = 0.0;
+    write_result(a, 0, 0.0, 0);
+    return;
+  }
+  if (!jac && *a.ferr != 0) {
+    write_result(a, 0, 0.0, *a.ferr + 10);
+    return;
+  }
+  if (jac && v2[1] != 0.0 && a.mpi_mode) {  // cg_jacobi_mpi rejects |diag| < tiny
+    write_result(a, 0, 0.0, 2);
+    return;
+  }
+  // r = b - A x ; (Jacobi) z = r/diag
+  double w2[2] = {0.0, 0.0};
+  for (int i = gtid; i < n; i += gstr) {
+    const double ri = a.b[i] - row_spmv<L1>(a.row_ptr, a.col, a.aval, x, i);
+    r[i] = ri;
+    w2[0] = w2[0] + ri * ri;
+    if (jac) {
+      const double zi = ri / a.aval[a.diag[i]];
+      z[i] = zi;
+      w2[1] = w2[1] + ri * zi;
+    }
+  }
+  if (!grid_sum<2, L1>(w2, a.partials, a.bar, a.st)) return;
+  double res = sqrt(w2[0]) / bnrm;
+  if (res <= a.tol) {
+    write_result(a, 0, res, 0);
+    return;
+  }
+  double rz;
+  if (jac) {
+    rz = w2[1];
+  } else {
+    if (!apply_lu<L1>(a, a.precond, r, z)) return;
+    double v1[1] = {0.0};
+    for (int i = gtid; i < n; i += gstr) v1[0] = v1[0] + r[i] * ldv<L1>(&z[i]);
+    if (!grid_sum<1, L1>(v1, a.partials, a.bar, a.st)) return;
+    rz = v1[0];
+  }
+  for (int i = gtid; i < n; i += gstr) p[i] = ldv<L1>(&z[i]);
+  if (!grid_sync(a.bar, a.st)) return;
+  int ierr = 0, it;
+  for (it = 1; it <= a.maxit; ++it) {
+    double pq[1] = {0.0};
+    for (int i = gtid; i < n; i += gstr) {
+      const double qi = row_spmv<L1>(a.row_ptr, a.col, a.aval, p, i);
+      q[i] = qi;
+      pq[0] = pq[0] + p[i] * qi;
+    }
+    if (!grid_sum<1, L1>(pq, a.partials, a.bar, a.st)) return;
+    const double pap = pq[0];
+    if (fabs(pap) < DTINY) {
+      ierr = 2;
+      break;
+    }
+    const double alpha = rz / pap;
+    double u2[2] = {0.0, 0.0};
+    for (int i = gtid; i < n; i += gstr) {
+      x[i] = x[i] + alpha * p[i];
+      const double ri = r[i] - alpha * q[i];
+      r[i] = ri;
+      u2[0] = u2[0] + ri * ri;
+      if (jac) {
+        const double zi = ri / a.aval[a.diag[i]];
+        z[i] = zi;
+        u2[1] = u2[1] + ri * zi;
+      }
+    }
+    if (!grid_sum<2, L1>(u2, a.partials, a.bar, a.st)) return;
+    res = sqrt(u2[0]) / bnrm;
+    if (res <= a.tol) {
+      write_result(a, it, res, 0);
+      return;
+    }
+    double rz_new;
+    if (jac) {
+      rz_new = u2[1];
+    } else {
+      if (!apply_lu<L1>(a, a.precond, r, z)) return;
+      double v1[1] = {0.0};
+      for (int i = gtid; i < n; i += gstr) v1[0] = v1[0] + r[i] * ldv<L1>(&z[i]);
+      if (!grid_sum<1, L1>(v1, a.partials, a.bar, a.st)) return;
+      rz_new = v1[0];
+    }
+    if (fabs(rz) < DTINY) {
+      ierr = 2;
+      break;
+    }
+    const double beta = rz_new / rz;
+    for (int i = gtid; i < n; i += gstr) p[i] = ldv<L1>(&z[i]) + beta * p[i];
+    if (!grid_sync(a.bar, a.st)) return;
+    rz = rz_new;
+  }
+  if (ierr == 0) ierr = 1;
+  write_result(a, it, res, ierr);
+}
+
+// ---------------------------------------------------------------------------
+// BiCGStab, right-preconditioned with ILU(0) (bicgstab_ilu0) or Jacobi.
+// ---------------------------------------------------------------------------
+template <bool L1>
+__global__ void __launch_bounds__(L1 ? 512 : 256) k_bicgstab(KrylovArgs a) {
+  if (a.st->abort) return;
+  const int n = a.n;
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstr = gridDim.x * blockDim.x;
+  const bool jac = a.precond == 1;
+  double* x = a.x;
+  double *r = a.r, *r0 = a.r0, *p = a.p, *v = a.v, *s = a.s, *t = a.t, *ph = a.ph, *sh = a.sh;
+  double v2[2] = {0.0, 0.0};
+  for (int i = gtid; i < n; i += gstr) {
+    const double bi = a.b[i];
+    v2[0] = v2[0] + bi * bi;
+    if (jac && fabs(a.aval[a.diag[i]]) < DTINY) v2[1] = v2[1] + 1.0;
+  }
+  if (!grid_sum<2, L1>(v2, a.partials, a.bar, a.st)) return;
+  const double bnrm = sqrt(v2[0]);
+  if (bnrm == 0.0) {
+    for (int i = gtid; i < n; i += gstr) x[i] = 0.0;
+    write_result(a, 0, 0.0, 0);
+    return;
+  }
+  if (!jac && *a.ferr != 0) {
+    write_result(a, 0, 0.0, *a.ferr + 10);
+    return;
+  }
+  if (jac && v2[1] != 0.0) {
+    write_result(a, 0, 0.0, 12);
+    return;
+  }
+  double w1[1] = {0.0};
+  for (int i = gtid; i < n; i += gstr) {
+    const double ri = a.b[i] - row_spmv<L1>(a.row_ptr, a.col, a.aval, x, i);
+    r0[i] = ri;
+    r[i] = ri;
+    p[i] = 0.0;
+    v[i] = 0.0;
+    w1[0] = w1[0] + ri * ri;
+  }
+  if (!grid_sum<1, L1>(w1, a.partials, a.bar, a.st)) return;
+  double res = sqrt(w1[0]) / bnrm;
+  if (res <= a.tol) {
+    write_result(a, 0, res, 0);
+    return;
+  }
+  double rho_next = w1[0];  // dot(r, r0) with r == r0: the same sum as r0.r0
+  double rho_old = 1.0, alpha = 1.0, omega = 1.0;
+  int ierr = 0, it;
+  for (it = 1; it <= a.maxit; ++it) {
+    const double rho = rho_next;
+    if (fabs(rho) < DTINY) {
+      ierr = 2;
+      break;
+    }
+    const double beta = (rho / rho_old) * (alpha / omega);
+    for (int i = gtid; i < n; i += gstr) {
+      const double pi = r[i] + beta * (p[i] - omega * v[i]);
+      p[i] = pi;
+      if (jac) ph[i] = pi / a.aval[a.diag[i]];
+    }
+    if (!grid_sync(a.bar, a.st)) return;
+    if (!jac && !apply_lu<L1>(a, 0, p, ph)) return;
+    double d1[1] = {0.0};
+    for (int i = gtid; i < n; i += gstr) {
+      const double vi = row_spmv<L1>(a.row_ptr, a.col, a.aval, ph, i);
+      v[i] = vi;
+      d1[0] = d1[0] + r0[i] * vi;
+    }
+    if (!grid_sum<1, L1>(d1, a.partials, a.bar, a.st)) return;
+    alpha = rho / d1[0];
+    double d2[1] = {0.0};
+    for (int i = gtid; i < n; i += gstr) {
+      const double si = r[i] - alpha * v[i];
+      s[i] = si;
+      d2[0] = d2[0] + si * si;
+      if (jac) sh[i] = si / a.aval[a.diag[i]];
+    }
+    if (!grid_sum<1, L1>(d2, a.partials, a.bar, a.st)) return;
+    const double snrm = sqrt(d2[0]);
+    if (snrm / bnrm <= a.tol) {
+      for (int i = gtid; i < n; i += gstr) x[i] = x[i] + alpha * ldv<L1>(&ph[i]);
+      write_result(a, it, snrm / bnrm, 0);
+      return;
+    }
+    if (!jac && !apply_lu<L1>(a, 0, s, sh)) return;
+    double d3[2] = {0.0, 0.0};
+    for (int i = gtid; i < n; i += gstr) {
+      const double ti = row_spmv<L1>(a.row_ptr, a.col, a.aval, sh, i);
+      t[i] = ti;
+      d3[0] = d3[0] + ti * ti;
+      d3[1] = d3[1] + ti * s[i];
+    }
+    if (!grid_sum<2, L1>(d3, a.partials, a.bar, a.st)) return;
+    const double tt = d3[0];
+    if (tt < DTINY) {
+      ierr = 2;
+      break;
+    }
+    omega = d3[1] / tt;
+    if (fabs(omega) < DTINY) {
+      ierr = 2;
+      break;
+    }
+    double d4[2] = {0.0, 0.0};
+    for (int i = gtid; i < n; i += gstr) {
+      x[i] = x[i] + alpha * ldv<L1>(&ph[i]) + omega * ldv<L1>(&sh[i]);
+      const double ri = s[i] - omega * t[i];
+      r[i] = ri;
+      d4[0] = d4[0] + ri * ri;
+      d4[1] = d4[1] + ri * r0[i];
+    }
+    if (!grid_sum<2, L1>(d4, a.partials, a.bar, a.st)) return;
+    res = sqrt(d4[0]) / bnrm;
+    if (res <= a.tol) {
+      write_result(a, it, res, 0);
+      return;
+    }
+    rho_next = d4[1];
+    rho_old = rho;
+  }
+  if (ierr == 0) {
+    ierr = 1;
+    it = a.maxit;
+  }
+  write_result(a, it, res, ierr);
+}
+
+__global__ void k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ col,
+                       const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  const int e = rp[i + 1];
+  for (int k = rp[i]; k < e; ++k) s = s + val[k] * x[col[k]];
+  y[i] = s;
+}
+
+int launch_coop(const void* fn, void** args, unsigned long long* bar, int grid, int block, cudaStream_t s,
+                bool coop) {
+  cudaError_t e = cudaMemsetAsync(bar, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return cuda_fail(e, "barrier reset", __FILE__, __LINE__);
+  if (coop)
+    e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(block), args, 0, s);
+  else
+    e = cudaLaunchKernel(fn, dim3(grid), dim3(block), args, 0, s);
+  if (e != cudaSuccess) return cuda_fail(e, "cooperative launch", __FILE__, __LINE__);
+  return 0;
+}
+
+}  // namespace
+
+// Grid of a persistent Krylov kernel: one 512-thread block (single-SM mode,
+// no grid barrier) for small systems, else enough 256-thread blocks for ~4
+// rows per thread, capped by co-residency.
+int krylov_grid(int n, int& block, int which) {
+  static int max_blocks[3] = {0, 0, 0};
+  if (n <= kSingleBlockRows) {
+    block = 512;
+    return 1;
+  }
+  block = 256;
+  if (max_blocks[which] == 0) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const void* fn = which == 0 ? (const void*)k_pcg<false>
+                                : which == 1 ? (const void*)k_bicgstab<false> : (const void*)k_factor<false>;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, block, 0);
+    if (per < 1) per = 1;
+    max_blocks[which] = sms * per;
+  }
+  long want = ((long)n + (long)block * 4 - 1) / ((long)block * 4);
+  if (want < 1) want = 1;
+  if (want > max_blocks[which]) want = max_blocks[which];
+  return (int)want;
+}
+
+int launch_krylov_pcg(const KrylovArgs& a, cudaStream_t s) {
+  int block = 0;
+  const int grid = krylov_grid(a.n, block, 0);
+  KrylovArgs aa = a;
+  void* args[] = {&aa};
+  return launch_coop(grid == 1 ? (const void*)k_pcg<true> : (const void*)k_pcg<false>, args, a.bar, grid, block, s,
+                     true);
+}
+
+int launch_krylov_bicgstab(const KrylovArgs& a, cudaStream_t s) {
+  int block = 0;
+  const int grid = krylov_grid(a.n, block, 1);
+  KrylovArgs aa = a;
+  void* args[] = {&aa};
+  return launch_coop(grid == 1 ? (const void*)k_bicgstab<true> : (const void*)k_bicgstab<false>, args, a.bar, grid,
+                     block, s, true);
+}
+
+int launch_factor(const KrylovArgs& a, int kind, cudaStream_t s) {
+  int block = 0;
+  const int grid = krylov_grid(a.n, block, 2);
+  KrylovArgs aa = a;
+  int kk = kind;
+  void* args[] = {&aa, &kk};
+  return launch_coop(grid == 1 ? (const void*)k_factor<true> : (const void*)k_factor<false>, args, a.bar, grid, block,
+                     s, true);
+}
+
+int launch_spmv(int n, const int* rp, const int* col, const double* val, const double* x, double* y,
+                cudaStream_t s) {
+  k_spmv<<<ceil_div(n, 256), 256, 0, s>>>(n, rp, col, val, x, y);
+  MGPU_LAUNCH_CHECK("k_spmv");
+  return 0;
+}
+
+}  // namespace mgpu

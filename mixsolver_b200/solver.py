@@ -1,0 +1,211 @@
+"""Host-side mirror of the reference's unstructured-solver module interface.
+
+The names and argument meanings follow the Fortran modules this library
+replaces, so a caller of the reference finds the same operations:
+
+* :class:`UnsCase` -- ``uns_solver_init`` / ``uns_solver_step``
+  (``src/unstructured/mod_uns_driver.f90:60-255``): a case built from a mesh and a
+  control, kept resident on the GPU; :meth:`UnsCase.simple_run` is ``simple_run``
+  (``mod_uns_simple.f90:88-288``) and :meth:`UnsCase.piso_run` is ``piso_run_mpi`` at
+  one rank (``mod_uns_simple_mpi.f90:298-571``). Both return the reference's ``ier``.
+* :func:`bicgstab_ilu0`, :func:`cg_jacobi`, :func:`cg_ic0` and :func:`csr_matvec`
+  -- ``mod_uns_linsolver.f90``: ``(A, b, x, tol, maxit) -> (x, it, res, ierr)``.
+* :func:`build_connectivity`, :func:`compute_geometry` -- the mesh pipeline.
+
+Every call runs on the GPU through ``libmixgpu.so``; there is no CPU path and a
+missing library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi
+from .abi import MeshArrays, MgpuIterRec, MgpuTiming, dptr, iptr, records_to_list
+
+
+def _lib():
+    return abi.load_library()
+
+
+class UnsCase:
+    """One unstructured case resident in HBM (mesh, matrices, fields)."""
+
+    def __init__(self, mesh, ctrl, device: int = 0):
+        lib = _lib()
+        abi.check(lib, lib.mgpu_set_device(int(device)), "mgpu_set_device")
+        self.mesh = mesh
+        self.ctrl = ctrl
+        self._arrays = MeshArrays(mesh)
+        self._cctrl = ctrl.to_c()
+        self.h = C.c_void_p()
+        ier = C.c_int(0)
+        rc = lib.mgpu_case_create(C.byref(self._arrays.struct), C.byref(self._cctrl), C.byref(self.h),
+                                  C.byref(ier))
+        if rc != 0:
+            msg = lib.mgpu_last_error().decode()
+            raise RuntimeError(f"mgpu_case_create failed (status {rc}, ier {ier.value}): {msg}")
+        self.N, self.F = mesh.ncells, mesh.nfaces
+
+    def close(self):
+        if self.h:
+            _lib().mgpu_case_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, u=None, p=None, flux=None, u_old=None, u_old_old=None):
+        conv = lambda a: None if a is None else np.ascontiguousarray(a, np.float64)
+        u, p, flux, u_old, u_old_old = map(conv, (u, p, flux, u_old, u_old_old))
+        lib = _lib()
+        abi.check(lib, lib.mgpu_fields_upload(self.h, dptr(u), dptr(p), dptr(flux), dptr(u_old), dptr(u_old_old)),
+                  "mgpu_fields_upload")
+
+    def fields(self):
+        N, F = self.N, self.F
+        u = np.zeros((N, 3)); p = np.zeros(N); flux = np.zeros(F)
+        gp = np.zeros((N, 3)); gu = np.zeros((N, 3, 3)); apc = np.zeros(N)
+        lib = _lib()
+        abi.check(lib, lib.mgpu_fields_download(self.h, dptr(u), dptr(p), dptr(flux), dptr(gp), dptr(gu), dptr(apc)),
+                  "mgpu_fields_download")
+        return dict(u=u, p=p, flux=flux, gp=gp, gu=gu.transpose(0, 2, 1).copy(), apc=apc)
+
+    def _run(self, fn, nsteps, logcap):
+        recs = (MgpuIterRec * max(logcap, 1))()
+        nrec, ier = C.c_int(0), C.c_int(0)
+        lib = _lib()
+        abi.check(lib, fn(self.h, int(nsteps), recs, int(logcap), C.byref(nrec), C.byref(ier)), fn.__name__)
+        return ier.value, records_to_list(recs, min(nrec.value, logcap))
+
+    def simple_run(self, nsteps: int = 0, logcap: int = 4096):
+        """Steady SIMPLE; returns (ier, per-iteration records)."""
+        return self._run(_lib().mgpu_simple_run, nsteps, logcap)
+
+    def piso_run(self, nsteps: int = 0, logcap: int = 4096):
+        """Transient PISO; returns (ier, per-step records)."""
+        return self._run(_lib().mgpu_piso_run, nsteps, logcap)
+
+    def nan_scan(self):
+        """(ifin, field, cell, value, kind) of the first non-finite value."""
+        ifin, field, cell, kind = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        val = C.c_double()
+        lib = _lib()
+        abi.check(lib, lib.mgpu_nan_scan(self.h, C.byref(ifin), C.byref(field), C.byref(cell), C.byref(val),
+                                         C.byref(kind)), "mgpu_nan_scan")
+        return ifin.value, field.value, cell.value, val.value, kind.value
+
+    def stage(self, what: int, ts_order: int = 0, apc=None, nnz: int = 0, pp=None):
+        """Run one kernel stage (see mgpu_case_stage); returns (aval, rhs, ap)."""
+        lib = _lib()
+        aval = np.zeros(max(nnz, 1)); rhs = np.zeros(self.N); ap = np.zeros(self.N)
+        a = None if apc is None else np.ascontiguousarray(apc, np.float64)
+        q = None if pp is None else np.ascontiguousarray(pp, np.float64)
+        abi.check(lib, lib.mgpu_case_stage(self.h, int(what), int(ts_order), dptr(a), dptr(aval) if nnz else None,
+                                           dptr(rhs), dptr(ap), dptr(q)), "mgpu_case_stage")
+        return aval, rhs, ap
+
+    def set_profiling(self, on: bool):
+        _lib().mgpu_case_set_profiling(self.h, 1 if on else 0)
+
+    def timing(self) -> dict:
+        t = MgpuTiming()
+        _lib().mgpu_case_timing(self.h, C.byref(t))
+        return dict(total_ms=t.total_ms, krylov_launches=t.krylov_launches, krylov_ms=t.krylov_ms,
+                    gpu_launches=t.gpu_launches)
+
+    def device_bytes(self) -> int:
+        b = C.c_int64()
+        _lib().mgpu_case_device_bytes(self.h, C.byref(b))
+        return int(b.value)
+
+
+def _krylov(method, row_ptr, col_idx, val, b, x, tol, maxit, norm_mode=0):
+    lib = _lib()
+    n = len(row_ptr) - 1
+    rp = np.ascontiguousarray(row_ptr, np.int32); ci = np.ascontiguousarray(col_idx, np.int32)
+    v = np.ascontiguousarray(val, np.float64); bb = np.ascontiguousarray(b, np.float64)
+    xx = np.ascontiguousarray(x, np.float64).copy()
+    it, ierr, res = C.c_int(), C.c_int(), C.c_double()
+    abi.check(lib, lib.mgpu_krylov_solve(n, iptr(rp), iptr(ci), dptr(v), dptr(bb), dptr(xx), float(tol),
+                                         int(maxit), int(method), int(norm_mode), C.byref(it), C.byref(res),
+                                         C.byref(ierr)), "mgpu_krylov_solve")
+    return xx, it.value, res.value, ierr.value
+
+
+def bicgstab_ilu0(row_ptr, col_idx, val, b, x, tol, maxit, norm_mode=0):
+    """bicgstab_ilu0 (mod_uns_linsolver.f90:148-224); 1-based CSR."""
+    return _krylov(abi.KRY_BICGSTAB_ILU0, row_ptr, col_idx, val, b, x, tol, maxit, norm_mode)
+
+
+def cg_jacobi(row_ptr, col_idx, val, b, x, tol, maxit, norm_mode=0):
+    """cg_jacobi (mod_uns_linsolver.f90:230-291)."""
+    return _krylov(abi.KRY_CG_JACOBI, row_ptr, col_idx, val, b, x, tol, maxit, norm_mode)
+
+
+def cg_ic0(row_ptr, col_idx, val, b, x, tol, maxit, norm_mode=0):
+    """cg_ic0 (mod_uns_linsolver.f90:405-461)."""
+    return _krylov(abi.KRY_CG_IC0, row_ptr, col_idx, val, b, x, tol, maxit, norm_mode)
+
+
+def bicgstab_jacobi(row_ptr, col_idx, val, b, x, tol, maxit, norm_mode=0):
+    """BiCGStab with z = r/diag in place of ilu0_apply (no reference counterpart)."""
+    return _krylov(abi.KRY_BICGSTAB_JACOBI, row_ptr, col_idx, val, b, x, tol, maxit, norm_mode)
+
+
+def cg_ilu0(row_ptr, col_idx, val, b, x, tol, maxit, norm_mode=0):
+    """PCG with ILU(0) as preconditioner (no reference counterpart)."""
+    return _krylov(abi.KRY_CG_ILU0, row_ptr, col_idx, val, b, x, tol, maxit, norm_mode)
+
+
+def csr_matvec(row_ptr, col_idx, val, x):
+    """csr_matvec (mod_uns_linsolver.f90:40-52)."""
+    lib = _lib()
+    n = len(row_ptr) - 1
+    y = np.zeros(n)
+    rp = np.ascontiguousarray(row_ptr, np.int32); ci = np.ascontiguousarray(col_idx, np.int32)
+    abi.check(lib, lib.mgpu_csr_matvec(n, iptr(rp), iptr(ci), dptr(np.ascontiguousarray(val, np.float64)),
+                                       dptr(np.ascontiguousarray(x, np.float64)), dptr(y)), "mgpu_csr_matvec")
+    return y
+
+
+def build_connectivity(mesh) -> dict:
+    """build_connectivity + build_cell_csr (1-based arrays)."""
+    lib = _lib()
+    arr = MeshArrays(mesh)
+    N, F = mesh.ncells, mesh.nfaces
+    nint = mesh.n_interior()
+    cf_ptr = np.zeros(N + 1, np.int32); cf = np.zeros(2 * nint + (F - nint), np.int32)
+    c2c_ptr = np.zeros(N + 1, np.int32); c2c = np.zeros(2 * nint, np.int32)
+    row_ptr = np.zeros(N + 1, np.int32); col = np.zeros(N + 2 * nint, np.int32)
+    nnz = C.c_int32(0)
+    abi.check(lib, lib.mgpu_build_connectivity(C.byref(arr.struct), iptr(cf_ptr), iptr(cf), iptr(c2c_ptr),
+                                               iptr(c2c), iptr(row_ptr), iptr(col), C.byref(nnz)),
+              "mgpu_build_connectivity")
+    return dict(cf_ptr=cf_ptr, cf=cf, c2c_ptr=c2c_ptr, c2c=c2c, row_ptr=row_ptr, col_idx=col[:nnz.value].copy())
+
+
+def compute_geometry(mesh) -> dict:
+    """compute_geometry + lf weights, computed on the device."""
+    lib = _lib()
+    arr = MeshArrays(mesh)
+    N, F = mesh.ncells, mesh.nfaces
+    xf = np.zeros((F, 3)); sf = np.zeros((F, 3)); area = np.zeros(F)
+    vol = np.zeros(N); xc = np.zeros((N, 3)); lf = np.zeros(F)
+    abi.check(lib, lib.mgpu_geometry(C.byref(arr.struct), dptr(xf), dptr(sf), dptr(area), dptr(vol), dptr(xc),
+                                     dptr(lf)), "mgpu_geometry")
+    return dict(xf=xf, sf=sf, area=area, vol=vol, xc=xc, lf=lf)
+
+
+def rcm_order(mesh) -> np.ndarray:
+    """Reverse Cuthill-McKee cell numbering: new_of_old (1-based)."""
+    lib = _lib()
+    arr = MeshArrays(mesh)
+    out = np.zeros(mesh.ncells, np.int32)
+    abi.check(lib, lib.mgpu_rcm_order(C.byref(arr.struct), iptr(out)), "mgpu_rcm_order")
+    return out

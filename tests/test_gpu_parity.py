@@ -1,0 +1,300 @@
+"""Parity of the CUDA path (through the C-ABI) with the CPU oracle.
+
+Element-wise kernels (geometry, gradients, assembly, Rhie-Chow, correction,
+SpMV, factorisations through the solves) reproduce the reference arithmetic
+bit for bit. Krylov dot products are summed in a different (parallel) order,
+so whole runs are compared with tolerances:
+  * iteration count and ierr of every linear solve: equal;
+  * fields after the run (u, p, flux): relative L2 < 1e-9;
+  * max|du| per outer iteration / step: relative 1e-6;
+  * final relative residual of every linear solve: relative 1e-3. This value
+    sits near lin_tol, where its own relative accuracy is about eps*kappa/res
+    (~1e-4 at res ~ 1e-9), so a tighter bound would test rounding noise;
+  * mass imbalance: absolute 1e-12 (it is itself round-off after the correction).
+"""
+import numpy as np
+import pytest
+
+from mixsolver_b200 import abi, cases, meshgen
+from mixsolver_b200 import solver as S
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TOL = 1e-9
+
+
+def rel_l2(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib(gpu_lib):
+    return gpu_lib
+
+
+def small_channel():
+    return cases.channel3d(12, 6, 6, seed=3, outer_max=10, order_fn=S.rcm_order)
+
+
+def test_geometry_bit_exact():
+    for mesh in (cases.cavity2d(10)[0], small_channel()[0], meshgen.box_tet(3, jitter=0.1, seed=4)):
+        g = S.compute_geometry(mesh)
+        ctrl = abi.Ctrl(bcs=[abi.BcSpec(zone=int(z), btype=abi.BC_WALL) for z in np.unique(mesh.zone[mesh.c1 == 0])])
+        o = O.OracleCase(mesh, ctrl).geometry()
+        for k in ("xf", "sf", "area", "vol", "xc", "lf"):
+            np.testing.assert_array_equal(g[k], o[k], err_msg=k)
+
+
+def _seed_fields(mesh, seed=0):
+    rng = np.random.default_rng(seed)
+    return (rng.standard_normal((mesh.ncells, 3)) * 0.1, rng.standard_normal(mesh.ncells) * 0.01,
+            rng.standard_normal(mesh.nfaces) * 1e-3)
+
+
+@pytest.mark.parametrize("name", ["cavity", "cavity_blend", "channel", "channel_nonorth0"])
+def test_stage_kernels_bit_exact(name):
+    if name == "cavity":
+        mesh, ctrl = cases.cavity2d(12)
+    elif name == "cavity_blend":
+        mesh, ctrl = cases.cavity2d(12, conv_blend=1.0, nonorth=0.0)
+    elif name == "channel":
+        mesh, ctrl = small_channel()
+    else:
+        mesh, ctrl = small_channel()
+        ctrl.nonorth_corr = 0.0
+    nnz = len(S.build_connectivity(mesh)["col_idx"])
+    g = S.UnsCase(mesh, ctrl)
+    o = O.OracleCase(mesh, ctrl)
+    u, p, flux = _seed_fields(mesh)
+    apc = 1.0 + np.random.default_rng(1).random(mesh.ncells)
+    for c in (g, o):
+        c.upload(u=u, p=p, flux=flux)
+    for ts in (0, 1):
+        o.set_apc(apc, ts)
+        g.stage(0, ts, apc)
+        o.stage(0)
+        fg, fo = g.fields(), o.fields()
+        np.testing.assert_array_equal(fg["gp"], fo["gp"])
+        np.testing.assert_array_equal(fg["gu"], fo["gu"])
+        for comp in (1, 2, 3):
+            ag, rg, pg = g.stage(comp, ts, apc, nnz)
+            ao, ro, po = o.stage(comp, nnz)
+            np.testing.assert_array_equal(ag, ao)
+            np.testing.assert_array_equal(rg, ro)
+            np.testing.assert_array_equal(pg, po)
+    o.set_apc(apc, 0)
+    g.stage(4, 0, apc)
+    o.stage(4)
+    np.testing.assert_array_equal(g.fields()["flux"], o.fields()["flux"])
+    ag, rg, _ = g.stage(5, 0, apc, nnz)
+    ao, ro, _ = o.stage(5, nnz)
+    np.testing.assert_array_equal(ag, ao)
+    np.testing.assert_array_equal(rg, ro)
+    pp = np.random.default_rng(2).standard_normal(mesh.ncells) * 1e-3
+    g.stage(6, 0, apc, pp=pp)
+    o.stage(6, pp=pp)
+    fg, fo = g.fields(), o.fields()
+    for k in ("u", "p", "flux"):
+        np.testing.assert_array_equal(fg[k], fo[k], err_msg=k)
+
+
+def _ppe_system(n=16):
+    """The PPE matrix/rhs of a cavity after 3 oracle SIMPLE iterations."""
+    mesh, ctrl = cases.cavity2d(n, outer_max=3)
+    o = O.OracleCase(mesh, ctrl)
+    o.simple_run()
+    con = o.connectivity()
+    nnz = len(con["col_idx"])
+    aval, rhs, ap = o.stage(5, nnz)
+    mom, mrhs, _ = o.stage(1, nnz)
+    return con["row_ptr"], con["col_idx"], aval, rhs, mom, mrhs
+
+
+def test_csr_matvec_bit_exact():
+    rp, ci, aval, rhs, mom, _ = _ppe_system()
+    x = np.random.default_rng(0).standard_normal(len(rp) - 1)
+    for v in (aval, mom):
+        np.testing.assert_array_equal(S.csr_matvec(rp, ci, v, x), O.csr_matvec(rp, ci, v, x))
+
+
+@pytest.mark.parametrize("method", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("norm_mode", [0, 1])
+def test_krylov_parity(method, norm_mode):
+    rp, ci, aval, rhs, mom, mrhs = _ppe_system(24)
+    sym = method in (1, 2, 4)
+    A, b = (aval, rhs) if sym else (mom, mrhs)
+    x0 = np.zeros(len(rp) - 1) if sym else np.random.default_rng(5).standard_normal(len(rp) - 1) * 1e-3
+    fns = [S.bicgstab_ilu0, S.cg_jacobi, S.cg_ic0, S.bicgstab_jacobi, S.cg_ilu0]
+    xg, itg, resg, ierrg = fns[method](rp, ci, A, b, x0, 1e-10, 300, norm_mode)
+    xo, ito, reso, ierro = O.krylov_solve(rp, ci, A, b, x0, 1e-10, 300, method, norm_mode)
+    assert (itg, ierrg) == (ito, ierro)
+    assert abs(resg - reso) <= 1e-6 * reso + 1e-300
+    assert rel_l2(xg, xo) < 1e-9
+
+
+def test_krylov_contracts_on_gpu():
+    rp = np.array([1, 3, 5], np.int32); ci = np.array([1, 2, 1, 2], np.int32)
+    v = np.array([4.0, -1.0, -1.0, 3.0])
+    x, it, res, ierr = S.cg_ic0(rp, ci, v, np.zeros(2), np.ones(2), 1e-8, 10)
+    assert (it, ierr) == (0, 0) and np.all(x == 0)
+    v0 = v.copy(); v0[0] = 0.0
+    _, it, _, ierr = S.bicgstab_ilu0(rp, ci, v0, np.array([1.0, 1.0]), np.zeros(2), 1e-8, 10)
+    assert ierr == 12
+    # breakdown (ierr = 2): p.Ap = 0 for an indefinite matrix and b along its null direction
+    va = np.array([1.0, 0.0, 0.0, -1.0])
+    _, it, _, ierr = S.cg_jacobi(rp, ci, va, np.array([1.0, 1.0]), np.zeros(2), 1e-12, 10)
+    _, ito, _, ierro = O.krylov_solve(rp, ci, va, np.array([1.0, 1.0]), np.zeros(2), 1e-12, 10, 1)
+    assert (it, ierr) == (ito, ierro) == (1, 2)
+    _, it, _, ierr = S.cg_jacobi(np.array([1, 2, 3], np.int32), np.array([2, 1], np.int32), np.array([1.0, 1.0]),
+                                 np.array([1.0, 1.0]), np.zeros(2), 1e-8, 10)
+    assert ierr == 2
+
+
+def _compare_runs(log_g, log_o, fg, fo):
+    assert len(log_g) == len(log_o)
+    worst = dict(res=0.0, du=0.0, imbal=0.0)
+    for a, b in zip(log_g, log_o):
+        assert a["lin_it"] == b["lin_it"], (a["it"], a["lin_it"], b["lin_it"])
+        assert a["lin_ierr"] == b["lin_ierr"]
+        for x, y in zip(a["lin_res"], b["lin_res"]):
+            if y > 0:
+                worst["res"] = max(worst["res"], abs(x - y) / y)
+        if b["du_max"] > 0:
+            worst["du"] = max(worst["du"], abs(a["du_max"] - b["du_max"]) / b["du_max"])
+        worst["imbal"] = max(worst["imbal"], abs(a["imbal"] - b["imbal"]))
+    fields = {k: rel_l2(fg[k], fo[k]) for k in ("u", "p", "flux")}
+    print("parity:", {k: f"{v:.2e}" for k, v in {**worst, **fields}.items()})
+    assert worst["res"] < 1e-3, worst
+    assert worst["du"] < 1e-6, worst
+    assert worst["imbal"] < 1e-12, worst
+    for k, v in fields.items():
+        assert v < FIELD_TOL, (k, v)
+
+
+@pytest.mark.parametrize("ppe", [abi.PPE_IC0, abi.PPE_JACOBI])
+def test_simple_cavity_parity(ppe):
+    mesh, ctrl = cases.cavity2d(16, outer_max=40, ppe=ppe)
+    g = S.UnsCase(mesh, ctrl)
+    ier_g, log_g = g.simple_run()
+    o = O.OracleCase(mesh, ctrl)
+    ier_o, log_o = o.simple_run()
+    assert ier_g == ier_o == 0
+    _compare_runs(log_g, log_o, g.fields(), o.fields())
+
+
+def test_simple_cavity_blend_parity():
+    mesh, ctrl = cases.cavity2d(12, outer_max=20, conv_blend=1.0, nonorth=0.0)
+    g = S.UnsCase(mesh, ctrl)
+    o = O.OracleCase(mesh, ctrl)
+    ier_g, log_g = g.simple_run()
+    ier_o, log_o = o.simple_run()
+    assert ier_g == ier_o == 0
+    _compare_runs(log_g, log_o, g.fields(), o.fields())
+
+
+def test_simple_channel_parity():
+    mesh, ctrl = small_channel()
+    g = S.UnsCase(mesh, ctrl)
+    o = O.OracleCase(mesh, ctrl)
+    ier_g, log_g = g.simple_run()
+    ier_o, log_o = o.simple_run()
+    assert ier_g == ier_o == 0
+    _compare_runs(log_g, log_o, g.fields(), o.fields())
+
+
+def test_simple_convergence_stops_early():
+    mesh, ctrl = cases.cavity2d(8, outer_max=400)
+    ctrl.outer_tol = 1e-5
+    g = S.UnsCase(mesh, ctrl)
+    o = O.OracleCase(mesh, ctrl)
+    ier_g, log_g = g.simple_run()
+    ier_o, log_o = o.simple_run()
+    assert ier_g == ier_o == 0
+    assert len(log_g) == len(log_o) < 400
+    _compare_runs(log_g, log_o, g.fields(), o.fields())
+
+
+def test_piso_tet_parity():
+    mesh, ctrl = cases.tet_box(4, dt=1e-3, steps=6)
+    geo = O.OracleCase(mesh, ctrl).geometry()
+    u0 = meshgen.taylor_green(geo["xc"], seed=1)
+    g = S.UnsCase(mesh, ctrl)
+    o = O.OracleCase(mesh, ctrl)
+    for c in (g, o):
+        c.upload(u=u0)
+    ier_g, log_g = g.piso_run()
+    ier_o, log_o = o.piso_run()
+    assert ier_g == ier_o == 0
+    _compare_runs(log_g, log_o, g.fields(), o.fields())
+    for a, b in zip(log_g, log_o):
+        assert abs(a["umax"] - b["umax"]) <= 1e-9 * b["umax"]
+        assert a["t_now"] == b["t_now"]
+
+
+def test_piso_bdf2_parity():
+    mesh, ctrl = cases.tet_box(3, dt=2e-3, steps=4)
+    ctrl.time_scheme = 2
+    geo = O.OracleCase(mesh, ctrl).geometry()
+    u0 = meshgen.taylor_green(geo["xc"], seed=2)
+    g = S.UnsCase(mesh, ctrl)
+    o = O.OracleCase(mesh, ctrl)
+    for c in (g, o):
+        c.upload(u=u0)
+    ier_g, log_g = g.piso_run()
+    ier_o, log_o = o.piso_run()
+    assert ier_g == ier_o == 0
+    _compare_runs(log_g, log_o, g.fields(), o.fields())
+
+
+def test_piso_error_codes():
+    mesh, ctrl = cases.cavity2d(4)
+    g = S.UnsCase(mesh, ctrl)
+    assert g.piso_run()[0] == 30          # transient = false
+    ctrl.transient = True
+    ctrl.dt = 0.0
+    g = S.UnsCase(mesh, ctrl)
+    assert g.piso_run()[0] == 31          # dt <= 0
+
+
+def test_nan_guard_on_gpu():
+    """test_nan_guard.f90 semantics on the device scan."""
+    mesh, ctrl = cases.cavity2d(8, outer_max=1)
+    g = S.UnsCase(mesh, ctrl)
+    n = mesh.ncells
+    kc1, kc2 = n // 2 + 1, max(1, n // 4)
+    u = np.zeros((n, 3)); p = np.zeros(n)
+    g.upload(u=u, p=p)
+    assert g.nan_scan()[0] == 0
+    u[kc1 - 1, 1] = np.nan
+    g.upload(u=u)
+    assert g.nan_scan()[:3] == (1, 2, kc1) and g.nan_scan()[4] == 1
+    u[kc1 - 1, 1] = 0.0
+    p[kc2 - 1] = np.inf
+    g.upload(u=u, p=p)
+    ifin, field, cell, val, kind = g.nan_scan()
+    assert (ifin, field, cell, kind) == (1, 4, kc2, 2)
+    u[kc1 - 1, 0] = np.inf
+    p[kc2 - 1] = np.nan
+    g.upload(u=u, p=p)
+    assert g.nan_scan()[:3] == (1, 4, kc2)
+    # a run that meets a non-finite value stops with ier = 60
+    u[:] = 0.0; p[:] = 0.0
+    u[5, 0] = np.nan
+    g.upload(u=u, p=p)
+    ier, log = g.simple_run()
+    assert ier == 60
+    u[:] = 0.0
+    g.upload(u=u, p=np.zeros(n))
+    assert g.nan_scan()[0] == 0
+
+
+def test_bc_errors():
+    mesh, ctrl = cases.cavity2d(4)
+    ctrl.bcs = ctrl.bcs[:1]                  # symmetry zone left without a bc
+    with pytest.raises(RuntimeError, match="ier 12"):
+        S.UnsCase(mesh, ctrl)
+    mesh, ctrl = cases.cavity2d(4)
+    ctrl.bcs.append(abi.BcSpec(zone=77, btype=abi.BC_WALL))
+    with pytest.raises(RuntimeError, match="ier 10"):
+        S.UnsCase(mesh, ctrl)

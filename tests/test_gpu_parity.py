@@ -215,21 +215,53 @@ def test_simple_convergence_stops_early():
     _compare_runs(log_g, log_o, g.fields(), o.fields())
 
 
+def _piso_ensemble(mesh, ctrl, u0):
+    """Oracle PISO runs from u0 scaled by (1 + e), e in {0, +-3e-16, +-1e-15}.
+
+    From the second corrector on, a PISO pressure solve starts from the
+    imbalance the previous corrector left, i.e. from that solve's final
+    residual, so its iteration count follows round-off: the oracle itself
+    moves between e.g. 28, 29 and 34 iterations under a 1e-15 relative change
+    of the initial field. The GPU is held to the spread of these runs."""
+    runs = []
+    for e in (0.0, 3e-16, -3e-16, 1e-15, -1e-15):
+        o = O.OracleCase(mesh, ctrl)
+        o.upload(u=u0 * (1.0 + e))
+        ier, log = o.piso_run()
+        assert ier == 0
+        runs.append((log, o.fields()))
+    return runs
+
+
+def _compare_piso(log_g, fg, runs):
+    log_o, fo = runs[0]
+    assert len(log_g) == len(log_o)
+    for k, a in enumerate(log_g):
+        ens = np.array([r[0][k]["lin_it"] for r in runs])
+        lo, hi = ens.min(0), ens.max(0)
+        got = np.array(a["lin_it"])
+        assert np.all((got >= lo) & (got <= hi)), (k + 1, got, lo, hi)
+        same = lo == hi
+        assert np.all(got[same] == lo[same])
+        assert a["lin_ierr"] == log_o[k]["lin_ierr"]
+        assert a["t_now"] == log_o[k]["t_now"]
+        assert abs(a["umax"] - log_o[k]["umax"]) <= 1e-9 * log_o[k]["umax"]
+    for key in ("u", "p", "flux"):
+        err = rel_l2(fg[key], fo[key])
+        spread = max(rel_l2(r[1][key], fo[key]) for r in runs)
+        print(f"piso {key}: gpu {err:.2e}, oracle spread {spread:.2e}")
+        assert err < FIELD_TOL, (key, err)
+
+
 def test_piso_tet_parity():
     mesh, ctrl = cases.tet_box(4, dt=1e-3, steps=6)
     geo = O.OracleCase(mesh, ctrl).geometry()
     u0 = meshgen.taylor_green(geo["xc"], seed=1)
     g = S.UnsCase(mesh, ctrl)
-    o = O.OracleCase(mesh, ctrl)
-    for c in (g, o):
-        c.upload(u=u0)
+    g.upload(u=u0)
     ier_g, log_g = g.piso_run()
-    ier_o, log_o = o.piso_run()
-    assert ier_g == ier_o == 0
-    _compare_runs(log_g, log_o, g.fields(), o.fields())
-    for a, b in zip(log_g, log_o):
-        assert abs(a["umax"] - b["umax"]) <= 1e-9 * b["umax"]
-        assert a["t_now"] == b["t_now"]
+    assert ier_g == 0
+    _compare_piso(log_g, g.fields(), _piso_ensemble(mesh, ctrl, u0))
 
 
 def test_piso_bdf2_parity():
@@ -238,13 +270,10 @@ def test_piso_bdf2_parity():
     geo = O.OracleCase(mesh, ctrl).geometry()
     u0 = meshgen.taylor_green(geo["xc"], seed=2)
     g = S.UnsCase(mesh, ctrl)
-    o = O.OracleCase(mesh, ctrl)
-    for c in (g, o):
-        c.upload(u=u0)
+    g.upload(u=u0)
     ier_g, log_g = g.piso_run()
-    ier_o, log_o = o.piso_run()
-    assert ier_g == ier_o == 0
-    _compare_runs(log_g, log_o, g.fields(), o.fields())
+    assert ier_g == 0
+    _compare_piso(log_g, g.fields(), _piso_ensemble(mesh, ctrl, u0))
 
 
 def test_piso_error_codes():

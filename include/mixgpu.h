@@ -216,6 +216,24 @@ int mgpu_rcm_order(const MgpuMesh* mesh, int32_t* new_of_old);
 int mgpu_case_stage(MgpuCase* c, int what, int ts_order, const double* apc, double* aval, double* rhs,
                     double* ap, const double* pp);
 
+/* Allocation-free PCG with Jacobi preconditioning, for callers that cannot
+ * allocate device memory: a host that owns every device byte and passes only
+ * its own buffers, a CUDA Fortran host whose arrays already live on the GPU,
+ * or code inside a stream capture, where an allocation would break the
+ * capture. No counterpart in the reference, whose solvers allocate their work
+ * arrays on every call.
+ * Same algorithm and outputs as mgpu_krylov_solve(method 1), but every array
+ * is a device pointer (CSR 0-based: row_ptr[0] = 0) and the work space is one
+ * fixed array inside the library (about 4.9 MB per GPU that loads it):
+ *   - n above MGPU_NOALLOC_MAX_ROWS is rejected with MGPU_E_ARG;
+ *   - calls that overlap on the GPU race on that array: serialise them;
+ *   - the first call on a device looks up the array's device address; make it
+ *     before any stream capture. stream: a cudaStream_t (NULL = default). */
+#define MGPU_NOALLOC_MAX_ROWS 131072
+int mgpu_cg_jacobi_noalloc(int n, const int32_t* d_row_ptr, const int32_t* d_col_idx, const double* d_val,
+                           const double* d_b, double* d_x, double tol, int maxit, int norm_mode, void* stream,
+                           int* it, double* res, int* ierr);
+
 /* Timing of the last run on the case's stream (CUDA events): total device ms
  * and, for the dominant kernel family, launches and summed device ms. */
 typedef struct {

@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmixgpu.so")
 BUILD = os.path.join(HERE, "_build")
 
-SOURCES = ["case.cu", "assembly.cu", "krylov.cu", "standalone.cu", "mesh_host.cpp"]
+SOURCES = ["case.cu", "assembly.cu", "krylov.cu", "standalone.cu", "noalloc.cu", "mesh_host.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr"]

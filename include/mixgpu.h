@@ -234,6 +234,13 @@ int mgpu_cg_jacobi_noalloc(int n, const int32_t* d_row_ptr, const int32_t* d_col
                            const double* d_b, double* d_x, double tol, int maxit, int norm_mode, void* stream,
                            int* it, double* res, int* ierr);
 
+/* Launch tunables, process-wide (for autotuning): "single_block_rows" (a
+ * solve of at most this many rows runs in one block, default 32768),
+ * "sweep_threads" (threads of a sync-free triangular sweep, default 65536),
+ * "sweep_sleep_ns" (back-off of a long wait in that sweep, default 0),
+ * "min_blocks" (least number of blocks of a multi-block solve, default 1). */
+int mgpu_set_tuning(const char* key, int value);
+
 /* Timing of the last run on the case's stream (CUDA events): total device ms
  * and, for the dominant kernel family, launches and summed device ms. */
 typedef struct {

@@ -57,6 +57,8 @@ struct KrylovArgs {
   int slot;            // record slot of this solve
   int ier_breakdown;   // driver code when ierr == 2 (0: none)
   int* ferr;           // factorisation status written by the factor kernel
+  int sweep_threads;   // threads of a sync-free triangular sweep (set at launch)
+  int sweep_sleep;     // nanosleep of a long wait in that sweep (0: spin)
 };
 
 struct DeviceCase {

@@ -23,7 +23,6 @@ namespace mgpu {
 
 namespace {
 
-constexpr int kSingleBlockRows = 32768;  // rows up to which one block runs a solve
 constexpr unsigned kSpinLimit = 1u << 25;  // ~2 s of polling: then flag a timeout
 
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
@@ -138,42 +137,172 @@ __device__ __forceinline__ double row_spmv(const int* __restrict__ rp, const int
   return y;
 }
 
-// z = M^{-1} src for ILU(0) (kind 0) or IC(0) (kind 2); src may alias nothing
-// but z. Level-scheduled forward and backward sweeps.
+// Marker of "not yet computed" in the sync-free sweeps: a signalling-NaN bit
+// pattern, which IEEE arithmetic never produces (its results are quiet NaNs).
+constexpr unsigned long long kPending = 0x7FF0DEAD0BADF00Dull;
+
+// Tunables (mgpu_set_tuning): rows up to which a solve runs in one block, and
+// the number of threads taking part in a sync-free triangular sweep.
+int g_single_block_rows = 32768;
+int g_sweep_threads = 65536;
+int g_sweep_sleep = 0;
+int g_min_blocks = 1;
+
+__device__ __forceinline__ double ld_relaxed_f64(const double* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return __longlong_as_double((long long)v);
+}
+
+// Spin (bounded) until p no longer holds kPending; returns the value.
+__device__ __forceinline__ double wait_value(const double* p, DevStatus* st, bool& ok, int sleep_ns) {
+  double v = ld_relaxed_f64(p);
+  unsigned spins = 0;
+  while (__double_as_longlong(v) == (long long)kPending) {
+    ++spins;
+    if ((spins & 1023u) == 0u) {
+      if (ld_acquire_i32(&st->timeout) != 0 || spins > (1u << 24)) {
+        atomicExch(&st->timeout, 1);
+        ok = false;
+        return 0.0;
+      }
+    }
+    if (sleep_ns > 0 && spins > 256u) __nanosleep(sleep_ns);
+    v = ld_relaxed_f64(p);
+  }
+  return v;
+}
+
+constexpr int kGather = 8;  // dependencies of one row fetched together
+
+// Load x[cols[0..m)] (m <= K) with all loads in flight at once, then re-poll
+// only the entries still pending, until none is (bounded).
+template <int K>
+__device__ __forceinline__ void gather_ready(const double* x, const int* cols, int m, double (&v)[K], DevStatus* st,
+                                             bool& ok, int sleep_ns) {
+#pragma unroll
+  for (int t = 0; t < K; ++t)
+    if (t < m) v[t] = ld_relaxed_f64(&x[cols[t]]);
+  unsigned spins = 0;
+  while (true) {
+    bool pend = false;
+#pragma unroll
+    for (int t = 0; t < K; ++t)
+      if (t < m && __double_as_longlong(v[t]) == (long long)kPending) {
+        pend = true;
+        v[t] = ld_relaxed_f64(&x[cols[t]]);
+      }
+    if (!pend) return;
+    ++spins;
+    if ((spins & 1023u) == 0u) {
+      if (ld_acquire_i32(&st->timeout) != 0 || spins > (1u << 24)) {
+        atomicExch(&st->timeout, 1);
+        ok = false;
+        return;
+      }
+    }
+    if (sleep_ns > 0 && spins > 256u) __nanosleep(sleep_ns);
+  }
+}
+
+// z = M^{-1} src for ILU(0) (kind 0) or IC(0) (kind 2).
+// One block: level-scheduled with __syncthreads between levels.
+// Several blocks: sync-free. Both sweeps write into arrays pre-filled with
+// kPending (forward into a.w, backward into z); each row waits only on the
+// entries it reads. Rows are taken in level order and every thread walks its
+// rows in that order, so the lowest unfinished row can always proceed: all
+// blocks being co-resident, the sweep completes. The arithmetic of each row is
+// the reference's, in the reference's order.
 template <bool L1>
 __device__ bool apply_lu(const KrylovArgs& a, int kind, const double* src, double* z) {
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstr = gridDim.x * blockDim.x;
   const double* f = a.fval;
-  for (int lev = 0; lev < a.nlev_lo; ++lev) {
-    const int e = a.lo_ptr[lev + 1];
-    for (int idx = a.lo_ptr[lev] + gtid; idx < e; idx += gstr) {
-      const int i = a.lo_rows[idx];
-      double s = ldv<L1>(&src[i]);
-      const int d = a.diag[i];
-      for (int k = a.row_ptr[i]; k < d; ++k) s = s - f[k] * ldv<L1>(&z[a.col[k]]);
-      z[i] = (kind == 2) ? s / f[d] : s;
+  if constexpr (L1) {
+    for (int lev = 0; lev < a.nlev_lo; ++lev) {
+      const int e = a.lo_ptr[lev + 1];
+      for (int idx = a.lo_ptr[lev] + gtid; idx < e; idx += gstr) {
+        const int i = a.lo_rows[idx];
+        double s = src[i];
+        const int d = a.diag[i];
+        for (int k = a.row_ptr[i]; k < d; ++k) s = s - f[k] * z[a.col[k]];
+        z[i] = (kind == 2) ? s / f[d] : s;
+      }
+      __syncthreads();
     }
-    if (!grid_sync(a.bar, a.st)) return false;
-  }
-  for (int lev = 0; lev < a.nlev_up; ++lev) {
-    const int e = a.up_ptr[lev + 1];
-    for (int idx = a.up_ptr[lev] + gtid; idx < e; idx += gstr) {
-      const int i = a.up_rows[idx];
-      const int d = a.diag[i], re = a.row_ptr[i + 1];
-      double s = ldv<L1>(&z[i]);
-      if (kind == 2) {
-        // L^T z = y, column sweep of ic0_apply: w(i) collects -L(j,i) z(j)
-        // for j = n..i+1 (descending), then z(i) = w(i)/L(i,i).
-        for (int k = re - 1; k > d; --k) s = s - f[a.lt_pos[k]] * ldv<L1>(&z[a.col[k]]);
-        z[i] = s / f[d];
-      } else {
-        for (int k = d + 1; k < re; ++k) s = s - f[k] * ldv<L1>(&z[a.col[k]]);
+    for (int lev = 0; lev < a.nlev_up; ++lev) {
+      const int e = a.up_ptr[lev + 1];
+      for (int idx = a.up_ptr[lev] + gtid; idx < e; idx += gstr) {
+        const int i = a.up_rows[idx];
+        const int d = a.diag[i], re = a.row_ptr[i + 1];
+        double s = z[i];
+        if (kind == 2) {
+          // L^T z = y, column sweep of ic0_apply: w(i) collects -L(j,i) z(j)
+          // for j = n..i+1 (descending), then z(i) = w(i)/L(i,i).
+          for (int k = re - 1; k > d; --k) s = s - f[a.lt_pos[k]] * z[a.col[k]];
+        } else {
+          for (int k = d + 1; k < re; ++k) s = s - f[k] * z[a.col[k]];
+        }
         z[i] = s / f[d];
       }
+      __syncthreads();
+    }
+    return true;
+  } else {
+    const int n = a.n;
+    double* y = a.w;
+    const double pend = __longlong_as_double((long long)kPending);
+    for (int i = gtid; i < n; i += gstr) {
+      y[i] = pend;
+      z[i] = pend;
     }
     if (!grid_sync(a.bar, a.st)) return false;
+    bool ok = true;
+    const int P = gstr < a.sweep_threads ? gstr : a.sweep_threads;
+    const int sl = a.sweep_sleep;
+    if (gtid < P) {
+      for (int idx = gtid; idx < n && ok; idx += P) {
+        const int i = a.lo_rows[idx];
+        const int rb = a.row_ptr[i], d = a.diag[i];
+        double s = ldv<false>(&src[i]);
+        if (d - rb <= kGather) {
+          double v[kGather];
+          gather_ready<kGather>(y, a.col + rb, d - rb, v, a.st, ok, sl);
+#pragma unroll
+          for (int t = 0; t < kGather; ++t)
+            if (t < d - rb) s = s - f[rb + t] * v[t];
+        } else {
+          for (int k = rb; k < d && ok; ++k) s = s - f[k] * wait_value(&y[a.col[k]], a.st, ok, sl);
+        }
+        __stcg(&y[i], (kind == 2) ? s / f[d] : s);
+      }
+      for (int idx = gtid; idx < n && ok; idx += P) {
+        const int i = a.up_rows[idx];
+        const int d = a.diag[i], re = a.row_ptr[i + 1];
+        const int nu = re - d - 1;
+        double s = wait_value(&y[i], a.st, ok, sl);
+        if (nu <= kGather) {
+          double v[kGather];
+          gather_ready<kGather>(z, a.col + d + 1, nu, v, a.st, ok, sl);
+          if (kind == 2) {
+            // descending column order (ic0_apply's Lt sweep)
+#pragma unroll
+            for (int t = kGather - 1; t >= 0; --t)
+              if (t < nu) s = s - f[a.lt_pos[d + 1 + t]] * v[t];
+          } else {
+#pragma unroll
+            for (int t = 0; t < kGather; ++t)
+              if (t < nu) s = s - f[d + 1 + t] * v[t];
+          }
+        } else if (kind == 2) {
+          for (int k = re - 1; k > d && ok; --k) s = s - f[a.lt_pos[k]] * wait_value(&z[a.col[k]], a.st, ok, sl);
+        } else {
+          for (int k = d + 1; k < re && ok; ++k) s = s - f[k] * wait_value(&z[a.col[k]], a.st, ok, sl);
+        }
+        __stcg(&z[i], s / f[d]);
+      }
+    }
+    return grid_sync(a.bar, a.st);
   }
-  return true;
 }
 
 __device__ void write_result(const KrylovArgs& a, int it, double res, int ierr) {
@@ -542,7 +671,7 @@ int launch_coop(const void* fn, void** args, unsigned long long* bar, int grid, 
 // rows per thread, capped by co-residency.
 int krylov_grid(int n, int& block, int which) {
   static int max_blocks[3] = {0, 0, 0};
-  if (n <= kSingleBlockRows) {
+  if (n <= g_single_block_rows) {
     block = 512;
     return 1;
   }
@@ -558,6 +687,7 @@ int krylov_grid(int n, int& block, int which) {
     max_blocks[which] = sms * per;
   }
   long want = ((long)n + (long)block * 4 - 1) / ((long)block * 4);
+  if (want < g_min_blocks) want = g_min_blocks;
   if (want < 1) want = 1;
   if (want > max_blocks[which]) want = max_blocks[which];
   return (int)want;
@@ -567,6 +697,8 @@ int launch_krylov_pcg(const KrylovArgs& a, cudaStream_t s) {
   int block = 0;
   const int grid = krylov_grid(a.n, block, 0);
   KrylovArgs aa = a;
+  aa.sweep_threads = g_sweep_threads;
+  aa.sweep_sleep = g_sweep_sleep;
   void* args[] = {&aa};
   return launch_coop(grid == 1 ? (const void*)k_pcg<true> : (const void*)k_pcg<false>, args, a.bar, grid, block, s,
                      true);
@@ -576,6 +708,8 @@ int launch_krylov_bicgstab(const KrylovArgs& a, cudaStream_t s) {
   int block = 0;
   const int grid = krylov_grid(a.n, block, 1);
   KrylovArgs aa = a;
+  aa.sweep_threads = g_sweep_threads;
+  aa.sweep_sleep = g_sweep_sleep;
   void* args[] = {&aa};
   return launch_coop(grid == 1 ? (const void*)k_bicgstab<true> : (const void*)k_bicgstab<false>, args, a.bar, grid,
                      block, s, true);
@@ -598,4 +732,23 @@ int launch_spmv(int n, const int* rp, const int* col, const double* val, const d
   return 0;
 }
 
+int set_tuning(const char* key, int value) {
+  const std::string k(key ? key : "");
+  if (k == "single_block_rows" && value >= 0) {
+    g_single_block_rows = value;
+  } else if (k == "sweep_threads" && value >= 32) {
+    g_sweep_threads = value;
+  } else if (k == "min_blocks" && value >= 1) {
+    g_min_blocks = value;
+  } else if (k == "sweep_sleep_ns" && value >= 0 && value <= 100000) {
+    g_sweep_sleep = value;
+  } else {
+    set_error("mgpu_set_tuning: unknown key or value out of range: " + k);
+    return MGPU_E_ARG;
+  }
+  return 0;
+}
+
 }  // namespace mgpu
+
+extern "C" int mgpu_set_tuning(const char* key, int value) { return mgpu::set_tuning(key, value); }

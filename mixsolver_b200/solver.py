@@ -125,6 +125,12 @@ class UnsCase:
         return int(b.value)
 
 
+def set_tuning(key: str, value: int) -> None:
+    """Process-wide launch tunables (see mgpu_set_tuning)."""
+    lib = _lib()
+    abi.check(lib, lib.mgpu_set_tuning(key.encode(), int(value)), "mgpu_set_tuning")
+
+
 def _krylov(method, row_ptr, col_idx, val, b, x, tol, maxit, norm_mode=0):
     lib = _lib()
     n = len(row_ptr) - 1

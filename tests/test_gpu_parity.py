@@ -133,6 +133,58 @@ def test_krylov_parity(method, norm_mode):
     assert rel_l2(xg, xo) < 1e-9
 
 
+@pytest.fixture
+def multiblock():
+    """Force the multi-block solve (grid barriers, sync-free sweeps) on small systems."""
+    S.set_tuning("single_block_rows", 0)
+    S.set_tuning("min_blocks", 6)
+    yield
+    S.set_tuning("single_block_rows", 32768)
+    S.set_tuning("min_blocks", 1)
+
+
+@pytest.mark.parametrize("method", [0, 1, 2, 3, 4])
+def test_krylov_parity_multiblock(method, multiblock):
+    rp, ci, aval, rhs, mom, mrhs = _ppe_system(24)
+    sym = method in (1, 2, 4)
+    A, b = (aval, rhs) if sym else (mom, mrhs)
+    x0 = np.zeros(len(rp) - 1)
+    fns = [S.bicgstab_ilu0, S.cg_jacobi, S.cg_ic0, S.bicgstab_jacobi, S.cg_ilu0]
+    xg, itg, resg, ierrg = fns[method](rp, ci, A, b, x0, 1e-10, 300, 1)
+    xo, ito, reso, ierro = O.krylov_solve(rp, ci, A, b, x0, 1e-10, 300, method, 1)
+    assert (itg, ierrg) == (ito, ierro)
+    assert abs(resg - reso) <= 1e-3 * reso
+    assert rel_l2(xg, xo) < 1e-9
+
+
+@pytest.mark.parametrize("method", [2, 4, 0])
+def test_krylov_parity_large(method):
+    """A 40,000-row system: the default multi-block path."""
+    rp, ci, aval, rhs, mom, mrhs = _ppe_system(200)
+    sym = method in (2, 4)
+    A, b = (aval, rhs) if sym else (mom, mrhs)
+    x0 = np.zeros(len(rp) - 1)
+    fns = {0: S.bicgstab_ilu0, 2: S.cg_ic0, 4: S.cg_ilu0}
+    xg, itg, resg, ierrg = fns[method](rp, ci, A, b, x0, 1e-9, 2000, 0)
+    xo, ito, reso, ierro = O.krylov_solve(rp, ci, A, b, x0, 1e-9, 2000, method, 0)
+    assert (itg, ierrg) == (ito, ierro)
+    # after hundreds of iterations the final residual near tol is round-off dominated
+    assert resg <= 1e-9 and abs(resg - reso) <= 5e-2 * reso
+    assert rel_l2(xg, xo) < 1e-9
+
+
+def test_simple_channel_parity_multiblock(multiblock):
+    mesh, ctrl = small_channel()
+    ctrl.mom_solver = abi.MOM_ILU0
+    ctrl.ppe_precond = abi.PPE_IC0
+    g = S.UnsCase(mesh, ctrl)
+    o = O.OracleCase(mesh, ctrl)
+    ier_g, log_g = g.simple_run()
+    ier_o, log_o = o.simple_run()
+    assert ier_g == ier_o == 0
+    _compare_runs(log_g, log_o, g.fields(), o.fields())
+
+
 def test_krylov_contracts_on_gpu():
     rp = np.array([1, 3, 5], np.int32); ci = np.array([1, 2, 1, 2], np.int32)
     v = np.array([4.0, -1.0, -1.0, 3.0])

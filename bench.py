@@ -6,10 +6,14 @@
 Workload (one GPU): steady SIMPLE on the 3-D channel of 128 x 64 x 64 hex cells
 (524,288 cells) on [0,4]x[0,1]x[0,1], interior nodes jittered +-10 % (seed 0),
 cells shuffled then renumbered by reverse Cuthill-McKee; parabolic inlet
-(Umean = 1), pressure outlet, no-slip walls, rho = 1, mu = 5e-3; BiCGStab+Jacobi
-on momentum and PCG+ILU(0) on the pressure correction, both to 1e-8 relative.
-A step is one SIMPLE outer iteration; `value` is outer iterations per second
-over all ranks (weak scaling: one case per GPU).
+(Umean = 1), pressure outlet, no-slip walls, rho = 1, mu = 5e-3; linear solves
+to 1e-8 relative. A step is one SIMPLE outer iteration; `value` is outer
+iterations per second over all ranks (weak scaling: one case per GPU).
+
+The measured form (--precision, default mixed) is the mixed-precision one;
+the FP64 parity form (BiCGStab+Jacobi momentum, PCG+ILU(0) pressure, the
+reference's arithmetic) runs the same outer iterations beside it, and the
+line reports its rate and the relative L2 difference of u, p, flux.
 
 `--impl reference` times the CPU restatement of the reference's serial
 simple_run (the oracle, one thread: the reference's serial solver has no
@@ -41,7 +45,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--cells", default="128x64x64")
     ap.add_argument("--lin-max", type=int, default=1000)
     ap.add_argument("--cpu-steps", type=int, default=2, help="oracle outer iterations for cpu_baseline")
@@ -112,10 +116,21 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def krylov_bytes(n, nnz, its, method):
-    """Algorithmic bytes of one Krylov solve (unique footprint per operation):
-    SpMV 12 nnz + 4(N+1) + 16 N; triangular pair 12 nnz + 24 N; dot 16 N;
-    axpy 24 N; norm 8 N; Jacobi apply 20 N."""
+def krylov_bytes(n, nnz, its, method, mixed=False, tol=1e-8, tau=1e-4):
+    """Algorithmic bytes of one Krylov solve, unique footprint per operation.
+
+    FP64 form: SpMV 12 nnz + 4(N+1) + 16 N; triangular pair 12 nnz + 24 N;
+    dot 16 N; axpy 24 N; norm 8 N; Jacobi apply 20 N.
+    Mixed form: FP32 SpMV 8 nnz + 4(N+1) + 8 N; FP32 vectors 4 B per entry;
+    plus the FP64 prologue (matrix rounding 12 nnz) and one FP64 true
+    residual (12 nnz + 28 N) per refinement step."""
+    import math
+    if mixed:
+        spmv = 8 * nnz + 4 * (n + 1) + 8 * n
+        steps = max(1, math.ceil(math.log(tol) / math.log(tau)))
+        setup = 12 * nnz + 24 * n + steps * (12 * nnz + 4 * (n + 1) + 28 * n + 28 * n + 20 * n)
+        per = spmv + 44 * n if method == "pcg" else 2 * spmv + 80 * n
+        return setup + its * per
     spmv = 12 * nnz + 4 * (n + 1) + 16 * n
     tri = 12 * nnz + 24 * n
     jac = 20 * n
@@ -135,18 +150,45 @@ def run_ours(args):
     if world > 1:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    from mixsolver_b200 import abi
     from mixsolver_b200 import solver as S
     mesh, ctrl = workload(args, S.rcm_order)
-    case = S.UnsCase(mesh, ctrl, device=local)
     N, F = mesh.ncells, mesh.nfaces
     nnz = N + 2 * mesh.n_interior()
+    mixed = args.precision == "mixed"
 
     def barrier():
         torch.cuda.synchronize()
         if world > 1:
             import torch.distributed as dist
             dist.barrier()
-    # warm-up
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        import torch.distributed as dist
+        t = torch.tensor([v], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # the FP64 parity form over the same W + K outer iterations from rest (comparison leg)
+    fp64 = None
+    if mixed:
+        import copy
+        c64 = copy.deepcopy(ctrl)
+        c64.precision = abi.PREC_FP64
+        k64 = S.UnsCase(mesh, c64, device=local)
+        ier, _ = k64.simple_run(args.warmup)
+        assert ier == 0
+        barrier()
+        ier, log64 = k64.simple_run(args.steps, logcap=args.steps)
+        barrier()
+        assert ier == 0
+        t64 = max_over_ranks(k64.timing()["total_ms"])
+        fp64 = dict(value=world * args.steps / (t64 / 1e3), fields=k64.fields(),
+                    ppe_its=float(np.mean([r["lin_it"][3] for r in log64])))
+        k64.close()
+    case = S.UnsCase(mesh, ctrl, device=local)
     ier, _ = case.simple_run(args.warmup)
     assert ier == 0, f"warm-up ier={ier}"
     case.set_profiling(True)
@@ -158,30 +200,31 @@ def run_ours(args):
     barrier()
     assert ier == 0 and len(log) == args.steps, (ier, len(log))
     tm = case.timing()
-    dev_ms = tm["total_ms"]
-    mx = dev_ms
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([dev_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        mx = float(t.item())
+    mx = max_over_ranks(tm["total_ms"])
     value = world * args.steps / (mx / 1e3)
-    # roofline of the dominant kernel family (Krylov solves; factor + solve per launch pair)
+    solve_ms = case.solve_times()
+    ppe_ms = solve_ms[3::4] if len(solve_ms) >= 4 else solve_ms
+    pct = lambda a, q: float(np.percentile(a, q)) if len(a) else None
+    # roofline of the dominant kernel family (the persistent Krylov solves)
     its_mom = sum(sum(r["lin_it"][:3]) for r in log)
     its_ppe = sum(r["lin_it"][3] for r in log)
-    kbytes = (sum(krylov_bytes(N, nnz, r["lin_it"][c], "bicg") for r in log for c in range(3)) +
-              sum(krylov_bytes(N, nnz, r["lin_it"][3], "pcg") for r in log))
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    kbytes = (sum(krylov_bytes(N, nnz, r["lin_it"][c], "bicg", mixed, ctrl.lin_tol, ctrl.mixed_tol)
+                  for r in log for c in range(3)) +
+              sum(krylov_bytes(N, nnz, r["lin_it"][3], "pcg", mixed, ctrl.lin_tol, ctrl.mixed_tol) for r in log))
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
     peak = peaks.get("hbm_gbs", 6650.0)
     kms = tm["krylov_ms"]
     nk = max(1, tm["krylov_launches"])
     achieved = kbytes / (kms / 1e3) / 1e9 if kms > 0 else None
-    # end to end through the public API: host fields in, one outer iteration, fields out
-    u = np.ascontiguousarray(case.fields()["u"])
-    h2d = (3 * N + N + F) * 8
-    d2h = (3 * N + N + F) * 8
     f = case.fields()
+    rel = None
+    if fp64 is not None:
+        rel = {k: float(np.linalg.norm(f[k] - fp64["fields"][k]) / np.linalg.norm(fp64["fields"][k]))
+               for k in ("u", "p", "flux")}
+    # end to end through the public API: host fields in, one outer iteration, fields out
+    h2d = (3 * N + N + F) * 8
+    d2h = (3 * N + N + F + 3 * N + 9 * N + N) * 8
     barrier()
     e2e_steps = max(2, min(args.steps, 5))
     t0 = time.perf_counter()
@@ -191,23 +234,32 @@ def run_ours(args):
         f = case.fields()
     e2e_t = time.perf_counter() - t0
     e2e = {"value": world * e2e_steps / e2e_t, "unit": UNIT, "h2d_bytes_per_step": h2d,
-           "d2h_bytes_per_step": d2h + 9 * 8 * N + 8 * N + 3 * 8 * N}
+           "d2h_bytes_per_step": d2h}
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": mx / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f32-inner/f64",
+        "dtype": "f64" if not mixed else "f32-inner/f64-refinement",
         "data": "synthetic (seeded jittered hex channel, RCM-ordered)",
-        "config": {"workload": f"steady SIMPLE, 3-D channel {args.cells} hex ({N} cells), "
-                               "BiCGStab+Jacobi momentum, PCG+ILU(0) pressure, lin_tol 1e-8",
+        "config": {"workload": f"steady SIMPLE, 3-D channel {args.cells} hex ({N} cells), lin_tol 1e-8; "
+                               + ("mixed form: FP32-inner/FP64-refinement BiCGStab-Jacobi and PCG-Jacobi"
+                                  if mixed else "FP64 form: BiCGStab+Jacobi momentum, PCG+ILU(0) pressure"),
                    "cells": N, "faces": F, "nnz": nnz, "lin_max": args.lin_max,
                    "precision": args.precision, "parallelism": f"replicas x{world}",
-                   "l2": "working set per outer iteration ~0.4 GB > 126 MB L2 (no explicit flush)",
-                   "krylov_iterations_per_step": {"momentum": its_mom / args.steps, "pressure": its_ppe / args.steps}},
+                   "l2": "per-iteration working set ~0.45 GB > 126 MB L2 (no explicit flush)",
+                   "krylov_iterations_per_step": {"momentum": its_mom / args.steps, "pressure": its_ppe / args.steps},
+                   "solve_latency_ms": {"p50": pct(solve_ms, 50), "p99": pct(solve_ms, 99),
+                                        "pressure_p50": pct(ppe_ms, 50), "pressure_p99": pct(ppe_ms, 99)},
+                   "fp64_form": None if fp64 is None else {
+                       "outer_iters_per_s": fp64["value"], "pressure_iterations_per_step": fp64["ppe_its"],
+                       "solvers": "BiCGStab+Jacobi momentum, PCG+ILU(0) pressure (exact, parity form)"},
+                   "speedup_vs_fp64": None if fp64 is None else value / fp64["value"],
+                   "rel_l2_vs_fp64": rel},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": None,
-                     "kernel": "persistent Krylov solves (factor + solve per launch pair)",
-                     "launches": nk, "avg_launch_ms": kms / nk, "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
+                     "kernel": "persistent Krylov solves (" + ("k_pcg_mixed/k_bicgstab_mixed" if mixed
+                                                                else "k_factor+k_pcg, k_bicgstab") + ")",
+                     "launches": nk, "avg_launch_ms": kms / nk, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
         "e2e": e2e,
         "gpu_launches": tm["gpu_launches"],
         "clocks": clk.summary(),
@@ -225,9 +277,14 @@ def run_ours(args):
 
 def cpu_baseline(args, mesh, ctrl, steps=None):
     """The oracle (CPU restatement of the reference's serial simple_run, one
-    thread) on the same mesh and control, timed over a few outer iterations."""
+    thread) on the same mesh and control, timed over a few outer iterations.
+    The reference's solvers for this workload are the FP64 ones."""
+    import copy
+    from mixsolver_b200 import abi
     from oracle import oracle as O
     steps = steps or args.cpu_steps
+    ctrl = copy.deepcopy(ctrl)
+    ctrl.precision = abi.PREC_FP64
     oc = O.OracleCase(mesh, ctrl)
     t0 = time.perf_counter()
     ier, log = oc.simple_run(steps)

@@ -252,6 +252,10 @@ typedef struct {
   int64_t gpu_launches; /* kernels this library launched during the run */
 } MgpuTiming;
 int mgpu_case_timing(const MgpuCase* c, MgpuTiming* t);
+/* Device time (ms) of each Krylov solve of the last profiled run, in launch
+ * order (per outer iteration: momentum x, y, z, then the pressure
+ * correction(s)); *n = number of solves recorded (at most cap written). */
+int mgpu_case_solve_times(const MgpuCase* c, double* ms, int cap, int* n);
 /* 1 = record CUDA events around every Krylov-kernel launch of later runs. */
 int mgpu_case_set_profiling(MgpuCase* c, int on);
 

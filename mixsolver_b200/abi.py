@@ -198,7 +198,7 @@ EXPORTS = ["mgpu_version", "mgpu_last_error", "mgpu_set_device", "mgpu_case_crea
            "mgpu_case_destroy", "mgpu_case_device_bytes", "mgpu_fields_upload",
            "mgpu_fields_download", "mgpu_simple_run", "mgpu_piso_run", "mgpu_nan_scan",
            "mgpu_krylov_solve", "mgpu_csr_matvec", "mgpu_build_connectivity", "mgpu_geometry",
-           "mgpu_rcm_order", "mgpu_case_stage", "mgpu_cg_jacobi_noalloc", "mgpu_set_tuning", "mgpu_case_timing",
+           "mgpu_rcm_order", "mgpu_case_stage", "mgpu_cg_jacobi_noalloc", "mgpu_set_tuning", "mgpu_case_solve_times", "mgpu_case_timing",
            "mgpu_case_set_profiling"]
 NOALLOC_MAX_ROWS = 131072
 
@@ -239,6 +239,7 @@ def load_library(path: str = LIB_PATH):
                                            C.c_double, C.c_int, C.c_int, C.c_void_p, P(C.c_int), dblp,
                                            P(C.c_int)]
     lib.mgpu_set_tuning.argtypes = [C.c_char_p, C.c_int]
+    lib.mgpu_case_solve_times.argtypes = [C.c_void_p, dblp, C.c_int, P(C.c_int)]
     lib.mgpu_case_timing.argtypes = [C.c_void_p, P(MgpuTiming)]
     lib.mgpu_case_set_profiling.argtypes = [C.c_void_p, C.c_int]
     _LIB = lib

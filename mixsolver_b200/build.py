@@ -17,7 +17,9 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmixgpu.so")
 BUILD = os.path.join(HERE, "_build")
 
-SOURCES = ["case.cu", "assembly.cu", "krylov.cu", "standalone.cu", "noalloc.cu", "mesh_host.cpp"]
+SOURCES = ["case.cu", "assembly.cu", "krylov.cu", "krylov_mixed.cu", "standalone.cu", "noalloc.cu", "mesh_host.cpp"]
+# the mixed-precision form needs no bit-parity and may contract into FMA
+FMA_OK = {"krylov_mixed.cu"}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr"]
@@ -42,7 +44,8 @@ def build(verbose: bool = False, force: bool = False) -> str:
         objs.append(o)
         if not force and os.path.exists(o) and os.path.getmtime(o) > max(os.path.getmtime(s), newest_hdr):
             continue
-        cmd = [nvcc()] + ARCH + NVCC_FLAGS + ["-c", s, "-o", o]
+        flags = [("-fmad=true" if f == "-fmad=false" and os.path.basename(s) in FMA_OK else f) for f in NVCC_FLAGS]
+        cmd = [nvcc()] + ARCH + flags + ["-c", s, "-o", o]
         if verbose:
             print(" ".join(cmd))
         subprocess.check_call(cmd)

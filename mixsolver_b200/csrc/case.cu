@@ -130,9 +130,24 @@ cudaEvent_t next_event(MgpuCase* c) {
   return c->ev_pool[c->ev_used++];
 }
 
-// factor (if needed) + solve; precond 0 ILU0, 1 Jacobi, 2 IC0
+// factor (if needed) + solve; precond 0 ILU0, 1 Jacobi, 2 IC0. The mixed form
+// (ctrl.precision) runs FP32-inner / FP64-refinement solves with Jacobi.
 int krylov(MgpuCase* c, KrylovArgs a, bool bicg) {
   cudaStream_t s = c->stream;
+  if (c->ctrl.precision == MGPU_PREC_MIXED) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (c->profiling) {
+      e0 = next_event(c);
+      e1 = next_event(c);
+      cudaEventRecord(e0, s);
+    }
+    MixedArgs m{c->d.a32, c->d.dinv32, c->d.w32, c->ctrl.mixed_tol > 0.0 ? c->ctrl.mixed_tol : 1e-4};
+    a.precond = 1;
+    TRY(bicg ? launch_bicgstab_mixed(a, m, s) : launch_pcg_mixed(a, m, s));
+    c->launches++;
+    if (c->profiling) cudaEventRecord(e1, s);
+    return 0;
+  }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (c->profiling) {
     e0 = next_event(c);
@@ -357,7 +372,9 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
       (e = c->alloc(d.rhs, N)) || (e = c->alloc(d.pp, N)) || (e = c->alloc(d.uo, 3 * N)) ||
       (e = c->alloc(d.u_old, 3 * N)) || (e = c->alloc(d.u_old_old, 3 * N)) || (e = c->alloc(d.psi, N)) ||
       (e = c->alloc(d.af, F)) || (e = c->alloc(d.aval, d.nnz)) || (e = c->alloc(d.pval, d.nnz)) ||
-      (e = c->alloc(d.fval, d.nnz)) || (e = c->alloc(d.kw, 10 * N)) || (e = c->alloc(d.partials, 4 * 4096)) ||
+      (e = c->alloc(d.fval, d.nnz)) || (e = c->alloc(d.kw, 10 * N)) ||
+      (ctrl->precision == MGPU_PREC_MIXED &&
+       ((e = c->alloc(d.a32, d.nnz)) || (e = c->alloc(d.dinv32, N)) || (e = c->alloc(d.w32, 10 * N)))) || (e = c->alloc(d.partials, 4 * 4096)) ||
       (e = c->alloc(d.bar, 1)) || (e = c->alloc(d.ferr, 1)) || (e = c->alloc(d.st, 1)))
     return fail(e);
   if ((e = ensure_recs(c, 64))) return fail(e);
@@ -597,6 +614,18 @@ int mgpu_case_stage(MgpuCase* c, int what, int ts_order, const double* apc, doub
 int mgpu_case_timing(const MgpuCase* c, MgpuTiming* t) {
   if (!c || !t) return MGPU_E_ARG;
   *t = c->timing;
+  return 0;
+}
+
+int mgpu_case_solve_times(const MgpuCase* c, double* ms, int cap, int* n) {
+  if (!c || !n) return MGPU_E_ARG;
+  const int m = (int)(c->ev_used / 2);
+  *n = m;
+  for (int i = 0; i < m && i < cap && ms; ++i) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, c->ev_pool[2 * i], c->ev_pool[2 * i + 1]);
+    ms[i] = t;
+  }
   return 0;
 }
 

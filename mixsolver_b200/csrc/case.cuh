@@ -61,6 +61,15 @@ struct KrylovArgs {
   int sweep_sleep;     // nanosleep of a long wait in that sweep (0: spin)
 };
 
+// Mixed-precision solve data: FP32 matrix copy, FP32 inverse diagonal,
+// FP32 work vectors (10 N), inner relative tolerance.
+struct MixedArgs {
+  float* a32;
+  float* dinv;
+  float* w32;
+  double tau;
+};
+
 struct DeviceCase {
   int N = 0, F = 0, nnz = 0;
   // faces
@@ -87,6 +96,7 @@ struct DeviceCase {
   double *ap = nullptr, *rhs = nullptr, *pp = nullptr, *uo = nullptr, *u_old = nullptr, *u_old_old = nullptr;
   double *psi = nullptr, *af = nullptr;
   double *aval = nullptr, *pval = nullptr, *fval = nullptr;
+  float *a32 = nullptr, *dinv32 = nullptr, *w32 = nullptr;  // mixed-precision form
   // Krylov work
   double *kw = nullptr;  // 10*N
   double* partials = nullptr;
@@ -102,6 +112,8 @@ int launch_krylov_bicgstab(const KrylovArgs& a, cudaStream_t s);
 int launch_krylov_pcg(const KrylovArgs& a, cudaStream_t s);
 int launch_factor(const KrylovArgs& a, int kind, cudaStream_t s);
 int krylov_grid(int n, int& block, int which);
+int launch_pcg_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s);
+int launch_bicgstab_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s);
 int launch_spmv(int n, const int* rp, const int* col, const double* val, const double* x, double* y,
                 cudaStream_t s);
 

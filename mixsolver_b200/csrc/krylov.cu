@@ -17,115 +17,12 @@
 
 #include <type_traits>
 
-#include "case.cuh"
+#include "persist.cuh"
 
 namespace mgpu {
 
 namespace {
 
-constexpr unsigned kSpinLimit = 1u << 25;  // ~2 s of polling: then flag a timeout
-
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-
-__device__ __forceinline__ int ld_acquire_i32(const int* p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// Bounded grid barrier over a monotone 64-bit arrival counter (zeroed before
-// every cooperative launch; all blocks are co-resident). Each block adds one
-// arrival and waits until the counter reaches the end of the current round.
-// Returns false when the wait ran out; the caller then leaves the kernel.
-__device__ bool grid_sync(unsigned long long* bar, DevStatus* st) {
-  __shared__ int s_ok;
-  if (gridDim.x == 1) {
-    __syncthreads();
-    return true;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int ok = 1;
-    const unsigned long long nb = gridDim.x;
-    __threadfence();
-    const unsigned long long old = atomicAdd(bar, 1ull);
-    const unsigned long long target = (old / nb + 1ull) * nb;
-    unsigned spins = 0;
-    while (ld_acquire_u64(bar) < target) {
-      if (++spins > 256u) __nanosleep(64);
-      if (spins > kSpinLimit) {
-        atomicExch(&st->timeout, 1);
-        ok = 0;
-        break;
-      }
-    }
-    __threadfence();
-    if (ok && ld_acquire_i32(&st->timeout) != 0) ok = 0;
-    s_ok = ok;
-  }
-  __syncthreads();
-  return s_ok != 0;
-}
-
-// Vector loads inside a persistent kernel: with one block every thread sits on
-// the same SM and __syncthreads orders its global accesses, so plain (L1)
-// loads are coherent; with several blocks, data written by another block is
-// read from L2.
-template <bool L1, typename T>
-__device__ __forceinline__ T ldv(const T* p) {
-  if constexpr (L1)
-    return *p;
-  else
-    return __ldcg(p);
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = v + __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// Deterministic grid-wide sum of NQ values: block tree -> per-block partials
-// -> barrier -> every block sums the partials in the same fixed order.
-template <int NQ, bool L1>
-__device__ bool grid_sum(double (&v)[NQ], double* partials, unsigned long long* bar, DevStatus* st) {
-  __shared__ double sh[NQ][32];
-  __shared__ double tot[NQ];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) {
-    double s = warp_sum(v[q]);
-    if (lane == 0) sh[q][warp] = s;
-  }
-  __syncthreads();
-  if (warp == 0) {
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) {
-      double s = lane < nw ? sh[q][lane] : 0.0;
-      s = warp_sum(s);
-      if (lane == 0) partials[q * gridDim.x + blockIdx.x] = s;
-    }
-  }
-  if (!grid_sync(bar, st)) return false;
-  if (warp == 0) {
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) {
-      double s = 0.0;
-      for (int j = lane; j < (int)gridDim.x; j += 32) s = s + ldv<L1>(&partials[q * gridDim.x + j]);
-      s = warp_sum(s);
-      if (lane == 0) tot[q] = s;
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) v[q] = tot[q];
-  __syncthreads();
-  return true;
-}
 
 // y_i = A_i . x in csr_matvec order (x may have been written by other blocks).
 template <bool L1>

@@ -1,0 +1,148 @@
+// persist.cuh -- primitives of the persistent (cooperative) Krylov kernels:
+// bounded grid barrier, deterministic grid-wide sums, L1/L2 vector loads.
+#pragma once
+
+#include "case.cuh"
+
+namespace mgpu {
+namespace {
+
+constexpr unsigned kSpinLimit = 1u << 25;  // ~2 s of polling: then flag a timeout
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ int ld_acquire_i32(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Bounded grid barrier over a monotone 64-bit arrival counter (zeroed before
+// every cooperative launch; all blocks are co-resident). Each block adds one
+// arrival and waits until the counter reaches the end of the current round.
+// Returns false when the wait ran out; the caller then leaves the kernel.
+__device__ bool grid_sync(unsigned long long* bar, DevStatus* st) {
+  __shared__ int s_ok;
+  if (gridDim.x == 1) {
+    __syncthreads();
+    return true;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned long long nb = gridDim.x;
+    __threadfence();
+    const unsigned long long old = atomicAdd(bar, 1ull);
+    const unsigned long long target = (old / nb + 1ull) * nb;
+    unsigned spins = 0;
+    while (ld_acquire_u64(bar) < target) {
+      if (++spins > 256u) __nanosleep(64);
+      if (spins > kSpinLimit) {
+        atomicExch(&st->timeout, 1);
+        ok = 0;
+        break;
+      }
+    }
+    __threadfence();
+    if (ok && ld_acquire_i32(&st->timeout) != 0) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Vector loads inside a persistent kernel: with one block every thread sits on
+// the same SM and __syncthreads orders its global accesses, so plain (L1)
+// loads are coherent; with several blocks, data written by another block is
+// read from L2.
+template <bool L1, typename T>
+__device__ __forceinline__ T ldv(const T* p) {
+  if constexpr (L1)
+    return *p;
+  else
+    return __ldcg(p);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = v + __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic grid-wide sum of NQ values: block tree -> per-block partials
+// -> barrier -> every block sums the partials in the same fixed order (each
+// thread a strided share, then the same block tree), so all blocks hold the
+// identical total. The partials are fetched by all threads at once: a single
+// L2 round trip instead of a serial chain.
+template <int NQ, bool L1>
+__device__ bool grid_sum(double (&v)[NQ], double* partials, unsigned long long* bar, DevStatus* st) {
+  __shared__ double sh[NQ][32];
+  __shared__ double tot[NQ];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double s = warp_sum(v[q]);
+    if (lane == 0) sh[q][warp] = s;
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      double s = lane < nw ? sh[q][lane] : 0.0;
+      s = warp_sum(s);
+      if (lane == 0) {
+        if (gridDim.x == 1)
+          tot[q] = s;
+        else
+          partials[q * gridDim.x + blockIdx.x] = s;
+      }
+    }
+  }
+  if (gridDim.x == 1) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) v[q] = tot[q];
+    __syncthreads();
+    return true;
+  }
+  if (!grid_sync(bar, st)) return false;
+  const int G = gridDim.x;
+  double w[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+    const int j0 = threadIdx.x, B = blockDim.x;
+    if (j0 < G) t0 = ldv<L1>(&partials[q * G + j0]);
+    if (j0 + B < G) t1 = ldv<L1>(&partials[q * G + j0 + B]);
+    if (j0 + 2 * B < G) t2 = ldv<L1>(&partials[q * G + j0 + 2 * B]);
+    if (j0 + 3 * B < G) t3 = ldv<L1>(&partials[q * G + j0 + 3 * B]);
+    double s = ((t0 + t1) + t2) + t3;
+    for (int j = j0 + 4 * B; j < G; j += B) s = s + ldv<L1>(&partials[q * G + j]);
+    w[q] = warp_sum(s);
+  }
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) sh[q][warp] = w[q];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      double s = lane < nw ? sh[q][lane] : 0.0;
+      s = warp_sum(s);
+      if (lane == 0) tot[q] = s;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) v[q] = tot[q];
+  __syncthreads();
+  return true;
+}
+
+}  // namespace
+}  // namespace mgpu

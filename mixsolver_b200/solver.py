@@ -119,6 +119,15 @@ class UnsCase:
         return dict(total_ms=t.total_ms, krylov_launches=t.krylov_launches, krylov_ms=t.krylov_ms,
                     gpu_launches=t.gpu_launches)
 
+    def solve_times(self) -> np.ndarray:
+        """Device ms of each Krylov solve of the last profiled run, launch order."""
+        lib = _lib()
+        n = C.c_int(0)
+        lib.mgpu_case_solve_times(self.h, None, 0, C.byref(n))
+        out = np.zeros(max(n.value, 1))
+        lib.mgpu_case_solve_times(self.h, dptr(out), n.value, C.byref(n))
+        return out[:n.value]
+
     def device_bytes(self) -> int:
         b = C.c_int64()
         _lib().mgpu_case_device_bytes(self.h, C.byref(b))

@@ -238,7 +238,10 @@ int mgpu_cg_jacobi_noalloc(int n, const int32_t* d_row_ptr, const int32_t* d_col
  * solve of at most this many rows runs in one block, default 32768),
  * "sweep_threads" (threads of a sync-free triangular sweep, default 65536),
  * "sweep_sleep_ns" (back-off of a long wait in that sweep, default 0),
- * "min_blocks" (least number of blocks of a multi-block solve, default 1). */
+ * "min_blocks" (least number of blocks of a multi-block solve, default 1),
+ * "cheb_degree" (mixed form: degree of the Chebyshev-Jacobi pressure
+ * preconditioner, 1 = plain Jacobi, default 16), "cheb_ratio" (lambda_max over
+ * lambda_min of its interval, default 1000). */
 int mgpu_set_tuning(const char* key, int value);
 
 /* Timing of the last run on the case's stream (CUDA events): total device ms

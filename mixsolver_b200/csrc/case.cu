@@ -35,6 +35,11 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
 
 using namespace mgpu;
 
+namespace mgpu {
+extern int g_cheb_degree;
+extern double g_cheb_ratio;
+}  // namespace mgpu
+
 struct MgpuCase {
   DeviceCase d;
   AsmParams P;
@@ -141,7 +146,8 @@ int krylov(MgpuCase* c, KrylovArgs a, bool bicg) {
       e1 = next_event(c);
       cudaEventRecord(e0, s);
     }
-    MixedArgs m{c->d.a32, c->d.dinv32, c->d.w32, c->ctrl.mixed_tol > 0.0 ? c->ctrl.mixed_tol : 1e-4};
+    MixedArgs m{c->d.a32, c->d.dinv32, c->d.w32, c->ctrl.mixed_tol > 0.0 ? c->ctrl.mixed_tol : 1e-4,
+                bicg ? 1 : g_cheb_degree, g_cheb_ratio, c->d.ell_w, c->d.ell_col, c->d.ell_val};
     a.precond = 1;
     TRY(bicg ? launch_bicgstab_mixed(a, m, s) : launch_pcg_mixed(a, m, s));
     c->launches++;
@@ -378,6 +384,20 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
       (e = c->alloc(d.bar, 1)) || (e = c->alloc(d.ferr, 1)) || (e = c->alloc(d.st, 1)))
     return fail(e);
   if ((e = ensure_recs(c, 64))) return fail(e);
+  if (ctrl->precision == MGPU_PREC_MIXED) {
+    int w = 0;
+    for (long i = 0; i < N; ++i) w = std::max(w, t.row_ptr[i + 1] - t.row_ptr[i]);
+    if (w <= 8) {  // column-major ELL copy of the pattern for the FP32 SpMV
+      std::vector<int> ell((size_t)w * N);
+      for (long i = 0; i < N; ++i)
+        for (int k = 0; k < w; ++k) {
+          const int p = t.row_ptr[i] + k;
+          ell[(size_t)k * N + i] = p < t.row_ptr[i + 1] ? t.col[p] : (int)i;
+        }
+      if ((e = c->upload(d.ell_col, ell)) || (e = c->alloc(d.ell_val, (size_t)w * N))) return fail(e);
+      d.ell_w = w;
+    }
+  }
   // geometry (device), scratch for the node arrays and provisional centres
   std::vector<int> fptr_h(hm.fptr.begin(), hm.fptr.end());
   if ((e = c->upload(x, hm.x)) || (e = c->upload(fptr, fptr_h)) || (e = c->upload(fnodes, hm.fnodes)) ||

@@ -68,6 +68,11 @@ struct MixedArgs {
   float* dinv;
   float* w32;
   double tau;
+  int cheb_k;        // Chebyshev-Jacobi degree of the pressure preconditioner (<= 1: Jacobi)
+  double cheb_ratio; // lambda_max / lambda_min of the Chebyshev interval
+  int ell_w;         // ELL width (max entries per row) when ell_col is set
+  const int* ell_col;  // column-major ELL columns, W*N (padding: the row itself)
+  float* ell_val;      // FP32 values in the same layout (padding: 0)
 };
 
 struct DeviceCase {
@@ -97,6 +102,9 @@ struct DeviceCase {
   double *psi = nullptr, *af = nullptr;
   double *aval = nullptr, *pval = nullptr, *fval = nullptr;
   float *a32 = nullptr, *dinv32 = nullptr, *w32 = nullptr;  // mixed-precision form
+  int* ell_col = nullptr;  // column-major ELL pattern of the FP32 copy (W*N)
+  float* ell_val = nullptr;
+  int ell_w = 0;
   // Krylov work
   double *kw = nullptr;  // 10*N
   double* partials = nullptr;

@@ -44,6 +44,10 @@ int g_single_block_rows = 32768;
 int g_sweep_threads = 65536;
 int g_sweep_sleep = 0;
 int g_min_blocks = 1;
+}  // namespace
+int g_cheb_degree = 16;      // mixed form: Chebyshev-Jacobi degree of the pressure preconditioner
+double g_cheb_ratio = 1000.0; // and the ratio lambda_max / lambda_min of its interval
+namespace {
 
 __device__ __forceinline__ double ld_relaxed_f64(const double* p) {
   unsigned long long v;
@@ -635,6 +639,10 @@ int set_tuning(const char* key, int value) {
     g_single_block_rows = value;
   } else if (k == "sweep_threads" && value >= 32) {
     g_sweep_threads = value;
+  } else if (k == "cheb_degree" && value >= 1 && value <= 64) {
+    g_cheb_degree = value;
+  } else if (k == "cheb_ratio" && value >= 2) {
+    g_cheb_ratio = value;
   } else if (k == "min_blocks" && value >= 1) {
     g_min_blocks = value;
   } else if (k == "sweep_sleep_ns" && value >= 0 && value <= 100000) {

@@ -71,6 +71,51 @@ __device__ __forceinline__ void spmv32_rows(const int* __restrict__ rp, const in
   }
 }
 
+// The same product from the column-major ELL copy: entry t of row i sits at
+// t*n + i, so a warp's loads of one t are contiguous and no row pointer is
+// read. Padding entries have value 0 and the row's own column.
+template <bool L1, int R>
+__device__ __forceinline__ void spmv32_ell(const MixedArgs& m, const float* x, int i0, int stride, int n,
+                                           float (&y)[R]) {
+  constexpr int WMAX = 8;
+  const int W = m.ell_w;
+  float v[R][WMAX];
+  int c[R][WMAX];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int i = i0 + r * stride;
+#pragma unroll
+    for (int t = 0; t < WMAX; ++t)
+      if (t < W && i < n) {
+        c[r][t] = m.ell_col[(long)t * n + i];
+        v[r][t] = m.ell_val[(long)t * n + i];
+      }
+  }
+  float xv[R][WMAX];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int t = 0; t < WMAX; ++t)
+      if (t < W && i0 + r * stride < n) xv[r][t] = ldv<L1>(&x[c[r][t]]);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int t = 0; t < WMAX; ++t)
+      if (t < W && i0 + r * stride < n) acc = fmaf(v[r][t], xv[r][t], acc);
+    y[r] = acc;
+  }
+}
+
+template <bool L1, bool ELL, int R>
+__device__ __forceinline__ void spmv32_any(const KrylovArgs& a, const MixedArgs& m, const float* x, int i0,
+                                           int stride, int n, float (&y)[R]) {
+  if constexpr (ELL)
+    spmv32_ell<L1, R>(m, x, i0, stride, n, y);
+  else
+    spmv32_rows<L1, R, 8>(a.row_ptr, a.col, m.a32, x, i0, stride, n, y);
+}
+
 template <bool L1>
 __device__ __forceinline__ double row_spmv64(const KrylovArgs& a, const double* x, int i) {
   double y = 0.0;
@@ -104,6 +149,10 @@ __device__ bool prologue(const KrylovArgs& a, const MixedArgs& m, double& bnrm, 
   for (int k = gtid; k < nnz; k += gstr) m.a32[k] = (float)a.aval[k];
   double v[2] = {0.0, 0.0};
   for (int i = gtid; i < n; i += gstr) {
+    if (m.ell_col) {
+      const int rb = a.row_ptr[i], len = a.row_ptr[i + 1] - rb;
+      for (int t = 0; t < m.ell_w; ++t) m.ell_val[(long)t * n + i] = t < len ? (float)a.aval[rb + t] : 0.0f;
+    }
     if (a.zero_x) a.x[i] = 0.0;
     const double dg = a.aval[a.diag[i]];
     if (fabs(dg) < DTINY) v[1] = v[1] + 1.0;
@@ -139,12 +188,68 @@ __device__ bool update_x(const KrylovArgs& a, const float* d, double scale) {
   return grid_sync(a.bar, a.st);
 }
 
-template <bool L1>
-__global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : 3) k_pcg_mixed(KrylovArgs a, MixedArgs m) {
+// Chebyshev-Jacobi preconditioner z = p(D^-1 A) D^-1 rr of degree k on
+// [lmax/ratio, lmax]: k-1 SpMV passes, one barrier each, no reductions.
+// On entry z0 = d = D^-1 rr / theta (written by the caller's pass, followed by
+// a barrier). The result lands in zout (z0 or z1, ping-pong); the last pass
+// also accumulates rr.z and rr.rr, reduced before returning.
+template <bool L1, bool ELL>
+__device__ bool cheb_apply(const KrylovArgs& a, const MixedArgs& m, const float* rr, float* dch, float* z0,
+                           float* z1, double lmax, float*& zout, double (&red)[2]) {
+  const int n = a.n;
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstr = gridDim.x * blockDim.x;
+  const double lmin = lmax / m.cheb_ratio;
+  const double th = 0.5 * (lmax + lmin), de = 0.5 * (lmax - lmin), sg = th / de;
+  double rho0 = 1.0 / sg;
+  float* zc = z0;
+  float* zn = z1;
+  red[0] = red[1] = 0.0;
+  for (int j = 1; j < m.cheb_k; ++j) {
+    const double rho1 = 1.0 / (2.0 * sg - rho0);
+    const float c1 = (float)(rho1 * rho0), c2 = (float)(2.0 * rho1 / de);
+    const bool last = (j == m.cheb_k - 1);
+    constexpr int R = ELL ? 1 : 2;
+    for (int i0 = gtid; i0 < n; i0 += R * gstr) {
+      float az[R];
+      spmv32_any<L1, ELL, R>(a, m, zc, i0, gstr, n, az);
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = i0 + r * gstr;
+        if (i < n) {
+          const float res = m.dinv[i] * (rr[i] - az[r]);
+          const float dn = fmaf(c1, dch[i], c2 * res);
+          dch[i] = dn;
+          const float zi = zc[i] + dn;
+          zn[i] = zi;
+          if (last) {
+            red[0] = fma((double)rr[i], (double)zi, red[0]);
+            red[1] = fma((double)rr[i], (double)rr[i], red[1]);
+          }
+        }
+      }
+    }
+    if (last) {
+      if (!grid_sum<2, L1>(red, a.partials, a.bar, a.st)) return false;
+    } else if (!grid_sync(a.bar, a.st)) {
+      return false;
+    }
+    float* t = zc;
+    zc = zn;
+    zn = t;
+    rho0 = rho1;
+  }
+  zout = zc;
+  return true;
+}
+
+template <bool L1, bool ELL>
+__global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : 2) k_pcg_mixed(KrylovArgs a, MixedArgs m) {
   if (a.st->abort) return;
   const int n = a.n;
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstr = gridDim.x * blockDim.x;
-  float *rr = m.w32, *z = m.w32 + n, *p = m.w32 + 2l * n, *q = m.w32 + 3l * n, *d = m.w32 + 4l * n;
+  float *rr = m.w32, *zA = m.w32 + n, *p = m.w32 + 2l * n, *q = m.w32 + 3l * n, *d = m.w32 + 4l * n;
+  float *dch = m.w32 + 5l * n, *zB = m.w32 + 6l * n;
+  const bool cheb = m.cheb_k > 1;
   double bnrm;
   bool diag_bad;
   if (!prologue<L1>(a, m, bnrm, diag_bad)) return;
@@ -157,6 +262,20 @@ __global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : 3) k_pcg_mixed(Krylov
     write_result_m(a, 0, 0.0, 2);
     return;
   }
+  // Chebyshev interval: Gershgorin bound of D^-1 A (row sum of |a_ij| / a_ii)
+  double lmax = 2.0, th = 1.0;
+  if (cheb) {
+    double g = 0.0;
+    for (int i = gtid; i < n; i += gstr) {
+      double s = 0.0;
+      for (int k = a.row_ptr[i]; k < a.row_ptr[i + 1]; ++k) s += fabs(a.aval[k]);
+      g = fmax(g, s / fabs(a.aval[a.diag[i]]));
+    }
+    if (!grid_max<L1>(g, a.partials, a.bar, a.st)) return;
+    lmax = g;
+    th = 0.5 * (lmax + lmax / m.cheb_ratio);
+  }
+  const float inv_th = (float)(1.0 / th);
   double rnorm;
   if (!true_residual<L1>(a, rnorm)) return;
   double res = rnorm / bnrm;
@@ -165,32 +284,46 @@ __global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : 3) k_pcg_mixed(Krylov
     return;
   }
   int total = 0, ierr = 0;
+  float* z = zA;
   while (true) {
+    // restart on the scaled FP64 residual
     const double inv = 1.0 / rnorm;
     double v2[2] = {0.0, 0.0};
     for (int i = gtid; i < n; i += gstr) {
       const float ri = (float)(ldv<L1>(&a.r[i]) * inv);
-      const float zi = m.dinv[i] * ri;
       rr[i] = ri;
-      z[i] = zi;
       d[i] = 0.0f;
-      v2[0] = fma((double)ri, (double)zi, v2[0]);
-      v2[1] = fma((double)ri, (double)ri, v2[1]);
+      if (cheb) {
+        const float di = m.dinv[i] * ri * inv_th;
+        dch[i] = di;
+        zA[i] = di;
+      } else {
+        const float zi = m.dinv[i] * ri;
+        zA[i] = zi;
+        v2[0] = fma((double)ri, (double)zi, v2[0]);
+        v2[1] = fma((double)ri, (double)ri, v2[1]);
+      }
     }
-    if (!grid_sum<2, L1>(v2, a.partials, a.bar, a.st)) return;
+    if (cheb) {
+      if (!grid_sync(a.bar, a.st)) return;
+      if (!cheb_apply<L1, ELL>(a, m, rr, dch, zA, zB, lmax, z, v2)) return;
+    } else {
+      z = zA;
+      if (!grid_sum<2, L1>(v2, a.partials, a.bar, a.st)) return;
+    }
     double rz = v2[0];
     const double target = m.tau * m.tau * v2[1];
     // p := z and q := A p on the first inner iteration; afterwards
-    // p := z + beta p and q := A z + beta q in the same pass (one barrier less)
+    // p := z + beta p and q := A z + beta q in the same pass
     float beta = 0.0f;
     bool first = true;
     while (true) {
       ++total;
       double pq[1] = {0.0};
-      constexpr int R = 2;
+      constexpr int R = ELL ? 1 : 2;
       for (int i0 = gtid; i0 < n; i0 += R * gstr) {
         float az[R];
-        spmv32_rows<L1, R, 8>(a.row_ptr, a.col, m.a32, z, i0, gstr, n, az);
+        spmv32_any<L1, ELL, R>(a, m, z, i0, gstr, n, az);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const int i = i0 + r * gstr;
@@ -216,12 +349,27 @@ __global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : 3) k_pcg_mixed(Krylov
         d[i] = fmaf(af, p[i], d[i]);
         const float ri = fmaf(-af, q[i], rr[i]);
         rr[i] = ri;
-        const float zi = m.dinv[i] * ri;
-        z[i] = zi;
-        u2[0] = fma((double)ri, (double)ri, u2[0]);
-        u2[1] = fma((double)ri, (double)zi, u2[1]);
+        if (cheb) {
+          const float di = m.dinv[i] * ri * inv_th;
+          dch[i] = di;
+          zA[i] = di;
+        } else {
+          const float zi = m.dinv[i] * ri;
+          zA[i] = zi;
+          u2[0] = fma((double)ri, (double)ri, u2[0]);
+          u2[1] = fma((double)ri, (double)zi, u2[1]);
+        }
       }
-      if (!grid_sum<2, L1>(u2, a.partials, a.bar, a.st)) return;
+      if (cheb) {
+        if (!grid_sync(a.bar, a.st)) return;
+        double red[2];
+        if (!cheb_apply<L1, ELL>(a, m, rr, dch, zA, zB, lmax, z, red)) return;
+        u2[0] = red[1];
+        u2[1] = red[0];
+      } else {
+        z = zA;
+        if (!grid_sum<2, L1>(u2, a.partials, a.bar, a.st)) return;
+      }
       if (u2[0] <= target || total >= a.maxit) break;
       if (fabs(rz) < DTINY) {
         ierr = 2;
@@ -397,7 +545,9 @@ int launch_mixed(const void* fn1, const void* fnN, const KrylovArgs& a, const Mi
 }  // namespace
 
 int launch_pcg_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s) {
-  return launch_mixed((const void*)k_pcg_mixed<true>, (const void*)k_pcg_mixed<false>, a, m, s);
+  if (m.ell_col)
+    return launch_mixed((const void*)k_pcg_mixed<true, true>, (const void*)k_pcg_mixed<false, true>, a, m, s);
+  return launch_mixed((const void*)k_pcg_mixed<true, false>, (const void*)k_pcg_mixed<false, false>, a, m, s);
 }
 
 int launch_bicgstab_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s) {

@@ -144,5 +144,45 @@ __device__ bool grid_sum(double (&v)[NQ], double* partials, unsigned long long* 
   return true;
 }
 
+// Grid-wide maximum of one non-negative value (exact, order-independent).
+template <bool L1>
+__device__ bool grid_max(double& v, double* partials, unsigned long long* bar, DevStatus* st) {
+  __shared__ double sh[32];
+  __shared__ double tot;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double m = v;
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) sh[warp] = m;
+  __syncthreads();
+  if (warp == 0) {
+    double s = lane < nw ? sh[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_xor_sync(0xffffffffu, s, o));
+    if (lane == 0) {
+      if (gridDim.x == 1)
+        tot = s;
+      else
+        partials[blockIdx.x] = s;
+    }
+  }
+  if (gridDim.x > 1) {
+    if (!grid_sync(bar, st)) return false;
+    double s = 0.0;
+    for (int j = threadIdx.x; j < (int)gridDim.x; j += blockDim.x) s = fmax(s, ldv<L1>(&partials[j]));
+    for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_xor_sync(0xffffffffu, s, o));
+    __syncthreads();
+    if (lane == 0) sh[warp] = s;
+    __syncthreads();
+    if (warp == 0) {
+      double t = lane < nw ? sh[lane] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(0xffffffffu, t, o));
+      if (lane == 0) tot = t;
+    }
+  }
+  __syncthreads();
+  v = tot;
+  __syncthreads();
+  return true;
+}
+
 }  // namespace
 }  // namespace mgpu

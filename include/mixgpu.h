@@ -262,6 +262,78 @@ int mgpu_case_solve_times(const MgpuCase* c, double* ms, int cap, int* n);
 /* 1 = record CUDA events around every Krylov-kernel launch of later runs. */
 int mgpu_case_set_profiling(MgpuCase* c, int on);
 
+/* ---- Batched runs (no counterpart in the reference, which advances one case
+ * per process through simple_run / piso_run_mpi) ------------------------------
+ * A batch advances many resident cases of uneven size together, one outer
+ * iteration (SIMPLE) or time step (PISO) per step: each assembly kernel is one
+ * launch over all members, each Krylov phase of the mixed-precision members is
+ * one persistent launch split into lanes (width 1 block for small systems,
+ * several blocks for large ones), and an iteration is replayed from a CUDA
+ * graph. A member's iteration records, ier codes and fields are those of the
+ * same run made through mgpu_simple_run / mgpu_piso_run, within the tolerance
+ * of its precision; with a fixed lane policy the result of a member does not
+ * depend on the other members. A case belongs to any number of batches, but
+ * only one may step it at a time, and a case must not be run by
+ * mgpu_simple_run / mgpu_piso_run while a batch steps it. */
+typedef struct MgpuBatch MgpuBatch;
+
+/* Start a run of a case for batched stepping: mode 0 = SIMPLE (at most
+ * min(outer_max, nsteps) iterations), 1 = PISO (min(n_time_max, nsteps) time
+ * steps; ier 30 / 31 and no run as mgpu_piso_run). nsteps <= 0: the ctrl
+ * limit alone. The case then advances only in mgpu_batch_step. */
+int mgpu_case_begin(MgpuCase* c, int mode, int nsteps, int* ier);
+/* After the run has ended (converged, failed or at its limit): the records
+ * and ier exactly as mgpu_simple_run / mgpu_piso_run return them. */
+int mgpu_case_finish(MgpuCase* c, MgpuIterRec* log, int logcap, int* nrec, int* ier);
+
+int mgpu_batch_create(MgpuCase* const* cases, int ncases, MgpuBatch** out);
+int mgpu_batch_destroy(MgpuBatch* b);
+/* Lane policy. The mixed-precision solves give bit-identical results on any
+ * number of blocks, so the plan only affects speed. It prices a system of n
+ * rows and p passes on w blocks at p * (rows per block * row_ps + barrier_ns)
+ * and minimises the busiest lane within the co-resident block capacity; the
+ * first step re-plans on the measured iteration counts. (0, 0) = autotune:
+ * the first step times the first pressure solve under each candidate pair
+ * and keeps the fastest (default). */
+int mgpu_batch_set_policy(MgpuBatch* b, int barrier_ns, int row_ps);
+/* Advance every running member by up to iters iterations / steps; returns
+ * after the device is done. *active = members still running. */
+int mgpu_batch_step(MgpuBatch* b, int iters, int* active);
+/* done[k] = 1 when member k has no run in progress. */
+int mgpu_batch_poll(MgpuBatch* b, int* done);
+/* begin (mode[k]) + step until every member has ended + finish; nrec and ier
+ * per member (ier as mgpu_simple_run / mgpu_piso_run). */
+int mgpu_batch_run(MgpuBatch* b, const int* mode, int nsteps, int* nrec, int* ier);
+typedef struct {
+  int32_t ncases;
+  int32_t barrier_ns, row_ps;                /* lane policy in use */
+  int32_t autotuned;                         /* 1: policy picked by the autotuner */
+  int32_t graph;                             /* 1: iterations replay a CUDA graph */
+  int32_t lanes, blocks;                     /* first pressure phase: lanes, blocks of its widest launch */
+  int32_t launches_per_iter;                 /* kernels one iteration launches */
+  double tune_ms;                            /* device time spent by the autotuner */
+  double step_ms;                            /* device time of all steps */
+  int64_t iters;                             /* iterations stepped */
+  /* profiled steps only (mgpu_batch_set_profiling): summed device ms of the
+   * Krylov phases (momentum x, y, z, pressure correctors 1..5), of the
+   * assembly launches, and of the busiest and the average lane of the
+   * first pressure phase (lane time = its first block's start to end) */
+  double phase_ms[8];
+  double asm_ms;
+  double lane_max_ms, lane_mean_ms;
+  int64_t profiled_iters;
+} MgpuBatchInfo;
+/* 1 = later steps run launch by launch (no graph) with CUDA events around
+ * every phase and lane timestamps (mgpu_batch_info reports them). */
+int mgpu_batch_set_profiling(MgpuBatch* b, int on);
+int mgpu_batch_info(const MgpuBatch* b, MgpuBatchInfo* info);
+/* The lane plan (host only, no GPU needed) of systems of rows[i] rows and
+ * passes[i] SpMV-sized passes (NULL: modelled) under a policy and a
+ * co-resident block capacity: width[i] = blocks of system i's lane, lane[i] =
+ * its lane; *makespan_us = the modelled time of the busiest lane. */
+int mgpu_batch_plan(int nsys, const int* rows, const double* passes, int barrier_ns, int row_ps, int capacity,
+                    int* width, int* lane, double* makespan_us);
+
 #ifdef __cplusplus
 }
 #endif

@@ -78,6 +78,14 @@ class MgpuTiming(C.Structure):
                 ("gpu_launches", C.c_int64)]
 
 
+class MgpuBatchInfo(C.Structure):
+    _fields_ = [("ncases", C.c_int32), ("barrier_ns", C.c_int32), ("row_ps", C.c_int32),
+                ("autotuned", C.c_int32), ("graph", C.c_int32), ("lanes", C.c_int32), ("blocks", C.c_int32),
+                ("launches_per_iter", C.c_int32), ("tune_ms", C.c_double), ("step_ms", C.c_double),
+                ("iters", C.c_int64), ("phase_ms", C.c_double * 8), ("asm_ms", C.c_double),
+                ("lane_max_ms", C.c_double), ("lane_mean_ms", C.c_double), ("profiled_iters", C.c_int64)]
+
+
 @dataclasses.dataclass
 class BcSpec:
     """One ``bc`` control line (bc_spec_t)."""
@@ -198,8 +206,11 @@ EXPORTS = ["mgpu_version", "mgpu_last_error", "mgpu_set_device", "mgpu_case_crea
            "mgpu_case_destroy", "mgpu_case_device_bytes", "mgpu_fields_upload",
            "mgpu_fields_download", "mgpu_simple_run", "mgpu_piso_run", "mgpu_nan_scan",
            "mgpu_krylov_solve", "mgpu_csr_matvec", "mgpu_build_connectivity", "mgpu_geometry",
-           "mgpu_rcm_order", "mgpu_case_stage", "mgpu_cg_jacobi_noalloc", "mgpu_set_tuning", "mgpu_case_solve_times", "mgpu_case_timing",
-           "mgpu_case_set_profiling"]
+           "mgpu_rcm_order", "mgpu_case_stage", "mgpu_cg_jacobi_noalloc", "mgpu_set_tuning",
+           "mgpu_case_solve_times", "mgpu_case_timing", "mgpu_case_set_profiling", "mgpu_case_begin",
+           "mgpu_case_finish", "mgpu_batch_create", "mgpu_batch_destroy", "mgpu_batch_set_policy",
+           "mgpu_batch_step", "mgpu_batch_poll", "mgpu_batch_run", "mgpu_batch_info", "mgpu_batch_plan",
+           "mgpu_batch_set_profiling"]
 NOALLOC_MAX_ROWS = 131072
 
 _LIB = None
@@ -242,6 +253,17 @@ def load_library(path: str = LIB_PATH):
     lib.mgpu_case_solve_times.argtypes = [C.c_void_p, dblp, C.c_int, P(C.c_int)]
     lib.mgpu_case_timing.argtypes = [C.c_void_p, P(MgpuTiming)]
     lib.mgpu_case_set_profiling.argtypes = [C.c_void_p, C.c_int]
+    lib.mgpu_case_begin.argtypes = [C.c_void_p, C.c_int, C.c_int, P(C.c_int)]
+    lib.mgpu_case_finish.argtypes = [C.c_void_p, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int)]
+    lib.mgpu_batch_create.argtypes = [P(C.c_void_p), C.c_int, P(C.c_void_p)]
+    lib.mgpu_batch_destroy.argtypes = [C.c_void_p]
+    lib.mgpu_batch_set_policy.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    lib.mgpu_batch_step.argtypes = [C.c_void_p, C.c_int, P(C.c_int)]
+    lib.mgpu_batch_poll.argtypes = [C.c_void_p, P(C.c_int)]
+    lib.mgpu_batch_run.argtypes = [C.c_void_p, P(C.c_int), C.c_int, P(C.c_int), P(C.c_int)]
+    lib.mgpu_batch_info.argtypes = [C.c_void_p, P(MgpuBatchInfo)]
+    lib.mgpu_batch_set_profiling.argtypes = [C.c_void_p, C.c_int]
+    lib.mgpu_batch_plan.argtypes = [C.c_int, i32p, dblp, C.c_int, C.c_int, C.c_int, i32p, i32p, dblp]
     _LIB = lib
     return lib
 

@@ -17,7 +17,8 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmixgpu.so")
 BUILD = os.path.join(HERE, "_build")
 
-SOURCES = ["case.cu", "assembly.cu", "krylov.cu", "krylov_mixed.cu", "standalone.cu", "noalloc.cu", "mesh_host.cpp"]
+SOURCES = ["case.cu", "assembly.cu", "krylov.cu", "krylov_mixed.cu", "batch.cu", "standalone.cu", "noalloc.cu",
+           "mesh_host.cpp"]
 # the mixed-precision form needs no bit-parity and may contract into FMA
 FMA_OK = {"krylov_mixed.cu"}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -205,8 +205,7 @@ __global__ void k_face_consts(DeviceCase d, AsmParams P) {
 // ---------------- per-iteration kernels ------------------------------------
 
 // compute_gradients: Green-Gauss gp and gu (gu plane = comp*3 + dir)
-__global__ void __launch_bounds__(256) k_gradients(DeviceCase d, AsmParams P) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void b_gradients(const DeviceCase& d, const AsmParams& P, const int c) {
   if (d.st->abort || c >= d.N) return;
   const int N = d.N, F = d.F;
   const Ramp rp = ramp_of(P, d.st);
@@ -254,10 +253,12 @@ __global__ void __launch_bounds__(256) k_gradients(DeviceCase d, AsmParams P) {
 #pragma unroll
   for (int k = 0; k < 9; ++k) d.gu[k * N + c] = g[3 + k] / v;
 }
+__global__ void __launch_bounds__(256) k_gradients(DeviceCase d, AsmParams P) {
+  b_gradients(d, P, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // velocity_limiter for one component (Barth-Jespersen psi)
-__global__ void __launch_bounds__(256) k_limiter(DeviceCase d, AsmParams P, int comp) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void b_limiter(const DeviceCase& d, const AsmParams& P, int comp, const int c) {
   if (d.st->abort || c >= d.N) return;
   const int N = d.N, F = d.F;
   const Ramp rp = ramp_of(P, d.st);
@@ -294,10 +295,12 @@ __global__ void __launch_bounds__(256) k_limiter(DeviceCase d, AsmParams P, int 
   }
   d.psi[c] = fmax(0.0, fmin(1.0, psi));
 }
+__global__ void __launch_bounds__(256) k_limiter(DeviceCase d, AsmParams P, int comp) {
+  b_limiter(d, P, comp, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // momentum_assembly for component comp: row c of A, rhs(c), ap(c)
-__global__ void __launch_bounds__(256) k_momentum(DeviceCase d, AsmParams P, int comp) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void b_momentum(const DeviceCase& d, const AsmParams& P, int comp, const int c) {
   if (d.st->abort || c >= d.N) return;
   const int N = d.N, F = d.F;
   const Ramp rp = ramp_of(P, d.st);
@@ -409,12 +412,15 @@ __global__ void __launch_bounds__(256) k_momentum(DeviceCase d, AsmParams P, int
   d.rhs[c] = rhs;
   d.ap[c] = ap;
 }
+__global__ void __launch_bounds__(256) k_momentum(DeviceCase d, AsmParams P, int comp) {
+  b_momentum(d, P, comp, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
-__global__ void k_apc(DeviceCase d, double div) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void b_apc(const DeviceCase& d, double div, const int c) {
   if (d.st->abort || c >= d.N) return;
   d.apc[c] = (div == 1.0) ? d.ap[c] : d.ap[c] / div;
 }
+__global__ void k_apc(DeviceCase d, double div) { b_apc(d, div, blockIdx.x * blockDim.x + threadIdx.x); }
 
 __global__ void k_fill(double* a, long n, double v) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -422,8 +428,7 @@ __global__ void k_fill(double* a, long n, double v) {
 }
 
 // flux_rhiechow: one thread per face
-__global__ void __launch_bounds__(256) k_rhiechow(DeviceCase d, AsmParams P) {
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void b_rhiechow(const DeviceCase& d, const AsmParams& P, const int f) {
   if (d.st->abort || f >= d.F) return;
   const int N = d.N, F = d.F;
   const int a = d.c0[f], b = d.c1[f];
@@ -449,11 +454,14 @@ __global__ void __launch_bounds__(256) k_rhiechow(DeviceCase d, AsmParams P) {
   d.flux[f] = P.rho * (dot3(uf0, uf1, uf2, s0, s1, s2) +
                        dbf * (dot3(gp0, gp1, gp2, s0, s1, s2) - pfgrad_n * d.dsf[f] / dn));
 }
+__global__ void __launch_bounds__(256) k_rhiechow(DeviceCase d, AsmParams P) {
+  b_rhiechow(d, P, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // outflow_mass_sums + outflow_mass_scale in face order (one thread: the sums
 // are sequential in the reference; only cases with an outflow zone use it)
-__global__ void k_outflow(DeviceCase d) {
-  if (d.st->abort || blockIdx.x != 0 || threadIdx.x != 0) return;
+__device__ void b_outflow(const DeviceCase& d) {
+  if (d.st->abort) return;
   double m_req = 0.0, m_out = 0.0, area_out = 0.0;
   for (int i = 0; i < d.F; ++i) {
     if (d.c1[i] >= 0 || d.fgrp[i] < 0) continue;
@@ -473,10 +481,12 @@ __global__ void k_outflow(DeviceCase d) {
     d.flux[i] = scaled ? beta * d.flux[i] : m_req * d.area[i] / area_out;
   }
 }
+__global__ void k_outflow(DeviceCase d) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) b_outflow(d);
+}
 
 // ppe_assembly: row c of the pressure-correction matrix, rhs(c), pin, pp := 0
-__global__ void __launch_bounds__(256) k_ppe(DeviceCase d, AsmParams P) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void b_ppe(const DeviceCase& d, const AsmParams& P, const int c) {
   if (d.st->abort || c >= d.N) return;
   double* A = d.pval;
   const int rb = d.row_ptr[c], re = d.row_ptr[c + 1], dg = d.diag[c];
@@ -520,10 +530,12 @@ __global__ void __launch_bounds__(256) k_ppe(DeviceCase d, AsmParams P) {
   d.rhs[c] = rhs;
   d.pp[c] = 0.0;
 }
+__global__ void __launch_bounds__(256) k_ppe(DeviceCase d, AsmParams P) {
+  b_ppe(d, P, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // correct_fields, cell part: Green-Gauss grad(p') and the u, p updates
-__global__ void __launch_bounds__(256) k_correct_cells(DeviceCase d, AsmParams P) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void b_correct_cells(const DeviceCase& d, const AsmParams& P, const int c) {
   if (d.st->abort || c >= d.N) return;
   const int N = d.N, F = d.F;
   double g0 = 0.0, g1 = 0.0, g2 = 0.0;
@@ -559,10 +571,12 @@ __global__ void __launch_bounds__(256) k_correct_cells(DeviceCase d, AsmParams P
   d.u[2 * N + c] = d.u[2 * N + c] - va * g2;
   d.p[c] = (d.st->ts_order > 0) ? d.p[c] + d.pp[c] : d.p[c] + P.alpha_p * d.pp[c];
 }
+__global__ void __launch_bounds__(256) k_correct_cells(DeviceCase d, AsmParams P) {
+  b_correct_cells(d, P, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // correct_fields, flux part
-__global__ void k_correct_flux(DeviceCase d) {
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void b_correct_flux(const DeviceCase& d, const int f) {
   if (d.st->abort || f >= d.F) return;
   const int a = d.c0[f], b = d.c1[f];
   if (b < 0) {
@@ -572,6 +586,7 @@ __global__ void k_correct_flux(DeviceCase d) {
   }
   d.flux[f] = d.flux[f] - d.af[f] * (d.pp[b] - d.pp[a]);
 }
+__global__ void k_correct_flux(DeviceCase d) { b_correct_flux(d, blockIdx.x * blockDim.x + threadIdx.x); }
 
 __device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {
   atomicMax(a, (unsigned long long)__double_as_longlong(v));
@@ -579,8 +594,7 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) 
 
 // Diagnostics of one outer iteration / step: max|imbalance|, max|du|,
 // max|u| (transient), first non-finite value (min over cell*4+field).
-__global__ void __launch_bounds__(256) k_diag(DeviceCase d, int transient) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void b_diag(const DeviceCase& d, int transient, const int c) {
   if (d.st->abort) return;
   double im = 0.0, du = 0.0, um = 0.0;
   unsigned long long key = ~0ull;
@@ -618,9 +632,12 @@ __global__ void __launch_bounds__(256) k_diag(DeviceCase d, int transient) {
     if (key != ~0ull) atomicMin(&d.st->nan_key, key);
   }
 }
+__global__ void __launch_bounds__(256) k_diag(DeviceCase d, int transient) {
+  b_diag(d, transient, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // Close the iteration: record, NaN guard (ier 60), convergence, advance.
-__global__ void k_diag_finalize(DeviceCase d, AsmParams P, int transient) {
+__device__ void b_diag_finalize(const DeviceCase& d, const AsmParams& P, int transient) {
   DevStatus* st = d.st;
   if (st->abort) return;
   MgpuIterRec* rec = d.recs + st->cur_it;
@@ -662,11 +679,12 @@ __global__ void k_diag_finalize(DeviceCase d, AsmParams P, int transient) {
     st->converged = 1;
     st->abort = 1;
   }
+  if (st->it_limit > 0 && st->cur_it >= st->it_limit) st->abort = 1;
 }
+__global__ void k_diag_finalize(DeviceCase d, AsmParams P, int transient) { b_diag_finalize(d, P, transient); }
 
 // SIMPLE: uo := u ; PISO: history shift and time-scheme order
-__global__ void k_begin_iter(DeviceCase d, int transient, int time_scheme) {
-  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void b_begin_iter(const DeviceCase& d, int transient, int time_scheme, const long i) {
   if (d.st->abort) return;
   const long n3 = 3l * d.N;
   if (i < n3) {
@@ -683,6 +701,55 @@ __global__ void k_begin_iter(DeviceCase d, int transient, int time_scheme) {
     if (transient) d.st->ts_order = (d.st->cur_it == 0 || time_scheme == 1) ? 1 : 2;
   }
 }
+__global__ void k_begin_iter(DeviceCase d, int transient, int time_scheme) {
+  b_begin_iter(d, transient, time_scheme, blockIdx.x * (long)blockDim.x + threadIdx.x);
+}
+
+// ---------------- batched launches -----------------------------------------
+// One launch runs a kernel over many cases. Block b belongs to case
+// blk_case[range][b] and acts as block b - blk0[range] of that case's own
+// launch of the same body, so every case computes exactly what its
+// single-case launch computes. The case's descriptor is staged in shared
+// memory once per block.
+
+__device__ __forceinline__ const BatchCase& stage_case(unsigned char* raw, const BatchCase* src) {
+  constexpr int W = (int)(sizeof(BatchCase) / 8);
+  const long long* s = reinterpret_cast<const long long*>(src);
+  long long* t = reinterpret_cast<long long*>(raw);
+  for (int k = threadIdx.x; k < W; k += blockDim.x) t[k] = s[k];
+  __syncthreads();
+  return *reinterpret_cast<const BatchCase*>(raw);
+}
+
+#define MGPU_BATCHED(NAME, RANGE, ...)                                                 \
+  __global__ void __launch_bounds__(256) kb_##NAME(AsmBatch B, int arg) {              \
+    __shared__ __align__(16) unsigned char raw[sizeof(BatchCase)];                     \
+    const BatchCase& sc = stage_case(raw, B.cases + B.blk_case[RANGE][blockIdx.x]);    \
+    const DeviceCase& d = sc.d;                                                        \
+    const AsmParams& P = sc.P;                                                         \
+    const long i = (long)(blockIdx.x - sc.blk0[RANGE]) * blockDim.x + threadIdx.x;     \
+    (void)arg;                                                                         \
+    (void)i;                                                                           \
+    (void)P;                                                                           \
+    __VA_ARGS__;                                                                       \
+  }
+
+MGPU_BATCHED(fill_apc, RANGE_N, if (i < d.N) d.apc[i] = 1.0)
+MGPU_BATCHED(gradients, RANGE_N, b_gradients(d, P, (int)i))
+MGPU_BATCHED(rhiechow_piso, RANGE_F, if (sc.transient) b_rhiechow(d, P, (int)i))
+MGPU_BATCHED(begin_iter, RANGE_3N, b_begin_iter(d, sc.transient, sc.time_scheme, i))
+MGPU_BATCHED(limiter, RANGE_N, if (P.conv_blend > 0.0) b_limiter(d, P, arg, (int)i))
+MGPU_BATCHED(momentum, RANGE_N, b_momentum(d, P, arg, (int)i))
+MGPU_BATCHED(apc, RANGE_N, b_apc(d, sc.transient ? 1.0 : P.alpha_u, (int)i))
+MGPU_BATCHED(rhiechow, RANGE_F, b_rhiechow(d, P, (int)i))
+MGPU_BATCHED(outflow, RANGE_ONE, if (sc.has_outflow && threadIdx.x == 0) b_outflow(d))
+MGPU_BATCHED(ppe, RANGE_N, if (arg < sc.ncorr) b_ppe(d, P, (int)i))
+MGPU_BATCHED(correct_cells, RANGE_N, if (arg < sc.ncorr) b_correct_cells(d, P, (int)i))
+MGPU_BATCHED(correct_flux, RANGE_F, if (arg < sc.ncorr) b_correct_flux(d, (int)i))
+MGPU_BATCHED(diag, RANGE_N, b_diag(d, sc.transient, (int)i))
+MGPU_BATCHED(diag_finalize, RANGE_ONE, if (threadIdx.x == 0) b_diag_finalize(d, P, sc.transient))
+
+#undef MGPU_BATCHED
 
 }  // namespace
 
@@ -759,6 +826,39 @@ int launch_diag(const DeviceCase& d, const AsmParams& P, int transient, cudaStre
   MGPU_LAUNCH_CHECK("k_diag_finalize");
   return 0;
 }
+int launch_batch_asm(int op, int arg, const AsmBatch& b, cudaStream_t s) {
+  struct OpInfo {
+    void (*fn)(AsmBatch, int);
+    int range;
+    const char* name;
+  };
+  static const OpInfo ops[BOP_COUNT] = {
+      {kb_fill_apc, RANGE_N, "kb_fill_apc"},
+      {kb_gradients, RANGE_N, "kb_gradients"},
+      {kb_rhiechow_piso, RANGE_F, "kb_rhiechow_piso"},
+      {kb_begin_iter, RANGE_3N, "kb_begin_iter"},
+      {kb_limiter, RANGE_N, "kb_limiter"},
+      {kb_momentum, RANGE_N, "kb_momentum"},
+      {kb_apc, RANGE_N, "kb_apc"},
+      {kb_rhiechow, RANGE_F, "kb_rhiechow"},
+      {kb_outflow, RANGE_ONE, "kb_outflow"},
+      {kb_ppe, RANGE_N, "kb_ppe"},
+      {kb_correct_cells, RANGE_N, "kb_correct_cells"},
+      {kb_correct_flux, RANGE_F, "kb_correct_flux"},
+      {kb_diag, RANGE_N, "kb_diag"},
+      {kb_diag_finalize, RANGE_ONE, "kb_diag_finalize"},
+  };
+  if (op < 0 || op >= BOP_COUNT) {
+    set_error("launch_batch_asm: unknown op");
+    return MGPU_E_ARG;
+  }
+  const OpInfo& o = ops[op];
+  if (b.nblk[o.range] <= 0) return 0;
+  o.fn<<<b.nblk[o.range], 256, 0, s>>>(b, arg);
+  MGPU_LAUNCH_CHECK(o.name);
+  return 0;
+}
+
 int launch_begin_iter(const DeviceCase& d, int transient, int time_scheme, cudaStream_t s) {
   k_begin_iter<<<GRID(3l * d.N)>>>(d, transient, time_scheme);
   MGPU_LAUNCH_CHECK("k_begin_iter");

@@ -17,6 +17,48 @@ struct AsmParams {
   int inlet_ramp;
 };
 
+// One case of a batched assembly launch: its arrays, its parameters, the
+// first block of its share of each launch range, and its per-run flags.
+enum BatchRange { RANGE_N = 0, RANGE_F = 1, RANGE_3N = 2, RANGE_ONE = 3 };
+
+struct alignas(16) BatchCase {
+  DeviceCase d;
+  AsmParams P;
+  int blk0[4];      // first block of this case in the N, F, 3N and one-block ranges
+  int transient;    // 1: PISO step, 0: SIMPLE iteration
+  int time_scheme;  // ctrl.time_scheme
+  int has_outflow;
+  int ncorr;        // pressure correctors per iteration (1 for SIMPLE)
+};
+
+// Device tables of a batched launch: the cases and, per range, the case of
+// every block.
+struct AsmBatch {
+  const BatchCase* cases;
+  const int* blk_case[4];
+  int nblk[4];
+};
+
+enum BatchOp {
+  BOP_FILL_APC = 0,
+  BOP_GRADIENTS,
+  BOP_RHIECHOW_PISO,  // start of a PISO run: the flux from the initial fields
+  BOP_BEGIN_ITER,
+  BOP_LIMITER,        // arg: component
+  BOP_MOMENTUM,       // arg: component
+  BOP_APC,
+  BOP_RHIECHOW,
+  BOP_OUTFLOW,
+  BOP_PPE,            // arg: corrector index
+  BOP_CORRECT_CELLS,  // arg: corrector index
+  BOP_CORRECT_FLUX,   // arg: corrector index
+  BOP_DIAG,
+  BOP_DIAG_FINALIZE,
+  BOP_COUNT
+};
+
+int launch_batch_asm(int op, int arg, const AsmBatch& b, cudaStream_t s);
+
 int geometry_setup(DeviceCase& d, const double* x, const int* fptr, const int* fnodes, double* pcen,
                    const AsmParams& P, cudaStream_t s);
 int launch_gradients(const DeviceCase& d, const AsmParams& P, cudaStream_t s);

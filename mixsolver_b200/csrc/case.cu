@@ -17,6 +17,7 @@
 
 #include "assembly.cuh"
 #include "case.cuh"
+#include "case_host.h"
 #include "mesh_host.h"
 
 namespace mgpu {
@@ -36,59 +37,6 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
 using namespace mgpu;
 
 namespace mgpu {
-extern int g_cheb_degree;
-extern double g_cheb_ratio;
-}  // namespace mgpu
-
-struct MgpuCase {
-  DeviceCase d;
-  AsmParams P;
-  MgpuCtrl ctrl;
-  cudaStream_t stream = nullptr;
-  std::vector<void*> allocs;
-  int64_t bytes = 0;
-  int has_outflow = 0;
-  int profiling = 0;
-  MgpuTiming timing{};
-  std::vector<cudaEvent_t> ev_pool;
-  size_t ev_used = 0;
-  cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;
-  int64_t launches = 0;
-  int kblock = 256;
-
-  template <typename T>
-  int alloc(T*& p, size_t n) {
-    p = nullptr;
-    if (n == 0) n = 1;
-    void* q = nullptr;
-    MGPU_CUDA(cudaMalloc(&q, n * sizeof(T)));
-    allocs.push_back(q);
-    bytes += (int64_t)(n * sizeof(T));
-    p = (T*)q;
-    return 0;
-  }
-  template <typename T>
-  int upload(T*& p, const std::vector<T>& h) {
-    if (int e = alloc(p, h.size())) return e;
-    if (!h.empty()) MGPU_CUDA(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
-    return 0;
-  }
-  ~MgpuCase() {
-    for (auto e : ev_pool) cudaEventDestroy(e);
-    if (ev_run0) cudaEventDestroy(ev_run0);
-    if (ev_run1) cudaEventDestroy(ev_run1);
-    for (void* p : allocs) cudaFree(p);
-    if (stream) cudaStreamDestroy(stream);
-  }
-};
-
-namespace {
-
-#define TRY(x)                 \
-  do {                         \
-    int rc_ = (x);             \
-    if (rc_ != 0) return rc_;  \
-  } while (0)
 
 KrylovArgs base_args(MgpuCase* c) {
   DeviceCase& d = c->d;
@@ -135,10 +83,14 @@ cudaEvent_t next_event(MgpuCase* c) {
   return c->ev_pool[c->ev_used++];
 }
 
+MixedArgs mixed_args(const MgpuCase* c, bool bicg) {
+  return MixedArgs{c->d.a32, c->d.dinv32, c->d.w32, c->ctrl.mixed_tol > 0.0 ? c->ctrl.mixed_tol : 1e-4,
+                   bicg ? 1 : g_cheb_degree, g_cheb_ratio, c->d.ell_w, c->d.ell_col, c->d.ell_val, c->d.red32};
+}
+
 // factor (if needed) + solve; precond 0 ILU0, 1 Jacobi, 2 IC0. The mixed form
 // (ctrl.precision) runs FP32-inner / FP64-refinement solves with Jacobi.
-int krylov(MgpuCase* c, KrylovArgs a, bool bicg) {
-  cudaStream_t s = c->stream;
+int krylov(MgpuCase* c, KrylovArgs a, bool bicg, cudaStream_t s) {
   if (c->ctrl.precision == MGPU_PREC_MIXED) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (c->profiling) {
@@ -146,8 +98,7 @@ int krylov(MgpuCase* c, KrylovArgs a, bool bicg) {
       e1 = next_event(c);
       cudaEventRecord(e0, s);
     }
-    MixedArgs m{c->d.a32, c->d.dinv32, c->d.w32, c->ctrl.mixed_tol > 0.0 ? c->ctrl.mixed_tol : 1e-4,
-                bicg ? 1 : g_cheb_degree, g_cheb_ratio, c->d.ell_w, c->d.ell_col, c->d.ell_val};
+    const MixedArgs m = mixed_args(c, bicg);
     a.precond = 1;
     TRY(bicg ? launch_bicgstab_mixed(a, m, s) : launch_pcg_mixed(a, m, s));
     c->launches++;
@@ -173,7 +124,7 @@ int krylov(MgpuCase* c, KrylovArgs a, bool bicg) {
   return 0;
 }
 
-int momentum_solve(MgpuCase* c, int comp, bool transient) {
+KrylovArgs mom_args(MgpuCase* c, int comp, bool transient) {
   KrylovArgs a = base_args(c);
   a.aval = c->d.aval;
   a.b = c->d.rhs;
@@ -183,10 +134,10 @@ int momentum_solve(MgpuCase* c, int comp, bool transient) {
   a.mpi_mode = transient ? 1 : 0;
   a.slot = comp;
   a.ier_breakdown = transient ? 33 : 20;
-  return krylov(c, a, true);
+  return a;
 }
 
-int ppe_solve(MgpuCase* c, int slot, bool transient) {
+KrylovArgs ppe_args(MgpuCase* c, int slot, bool transient) {
   KrylovArgs a = base_args(c);
   a.aval = c->d.pval;
   a.b = c->d.rhs;
@@ -196,13 +147,24 @@ int ppe_solve(MgpuCase* c, int slot, bool transient) {
   a.mpi_mode = transient ? 1 : 0;
   a.slot = slot;
   a.ier_breakdown = transient ? 34 : 21;
-  return krylov(c, a, false);
+  return a;
 }
+
+namespace {
+
+int momentum_solve(MgpuCase* c, int comp, bool transient) {
+  return krylov(c, mom_args(c, comp, transient), true, c->stream);
+}
+
+int ppe_solve(MgpuCase* c, int slot, bool transient) { return krylov(c, ppe_args(c, slot, transient), false, c->stream); }
+
+}  // namespace
 
 int reset_status(MgpuCase* c, int ts_order, int nrec) {
   DevStatus h{};
   h.ts_order = ts_order;
   h.nan_key = ~0ull;
+  h.it_limit = nrec > 1 ? nrec - 1 : 0;
   MGPU_CUDA(cudaMemcpyAsync(c->d.st, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
   MGPU_CUDA(cudaMemsetAsync(c->d.bar, 0, sizeof(unsigned long long), c->stream));
   MGPU_CUDA(cudaMemsetAsync(c->d.recs, 0, sizeof(MgpuIterRec) * (size_t)nrec, c->stream));
@@ -217,6 +179,8 @@ int ensure_recs(MgpuCase* c, int n) {
   c->d.rec_cap = n;
   return 0;
 }
+
+namespace {
 
 int begin_run(MgpuCase* c) {
   c->ev_used = 0;
@@ -300,6 +264,7 @@ int outer_iteration(MgpuCase* c, bool transient) {
 }
 
 }  // namespace
+}  // namespace mgpu
 
 extern "C" {
 
@@ -336,6 +301,10 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
   }
   if (ctrl->conv_blend < 0.0 || ctrl->alpha_u <= 0.0 || ctrl->lin_max < 0) {
     set_error("ctrl: invalid alpha_u / conv_blend / lin_max");
+    return MGPU_E_ARG;
+  }
+  if (ctrl->precision == MGPU_PREC_MIXED && hm.N > kMixedMaxRows) {
+    set_error("mgpu_case_create: the mixed-precision form takes at most 2^24 cells");
     return MGPU_E_ARG;
   }
   HostTopo t;
@@ -380,7 +349,9 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
       (e = c->alloc(d.af, F)) || (e = c->alloc(d.aval, d.nnz)) || (e = c->alloc(d.pval, d.nnz)) ||
       (e = c->alloc(d.fval, d.nnz)) || (e = c->alloc(d.kw, 10 * N)) ||
       (ctrl->precision == MGPU_PREC_MIXED &&
-       ((e = c->alloc(d.a32, d.nnz)) || (e = c->alloc(d.dinv32, N)) || (e = c->alloc(d.w32, 10 * N)))) || (e = c->alloc(d.partials, 4 * 4096)) ||
+       ((e = c->alloc(d.a32, d.nnz)) || (e = c->alloc(d.dinv32, N)) || (e = c->alloc(d.w32, 10 * N)) ||
+        (e = c->alloc(d.red32, (size_t)mixed_red_words(N))))) ||
+      (e = c->alloc(d.partials, 4 * 4096)) ||
       (e = c->alloc(d.bar, 1)) || (e = c->alloc(d.ferr, 1)) || (e = c->alloc(d.st, 1)))
     return fail(e);
   if ((e = ensure_recs(c, 64))) return fail(e);

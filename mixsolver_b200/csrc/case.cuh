@@ -19,7 +19,7 @@ struct DevStatus {
   int ts_order;   // 0 steady, 1 Euler, 2 BDF2 (fields_t%ts_order)
   int nan_field, nan_cell;
   int nan_kind;
-  int pad;
+  int it_limit;  // > 0: the run ends (abort, no ier) once cur_it reaches it
   double nan_val;
   double t_now;
   unsigned long long imbal_bits, du_bits, umax_bits;  // max-reductions (bit patterns of x >= 0)
@@ -73,6 +73,46 @@ struct MixedArgs {
   int ell_w;         // ELL width (max entries per row) when ell_col is set
   const int* ell_col;  // column-major ELL columns, W*N (padding: the row itself)
   float* ell_val;      // FP32 values in the same layout (padding: 0)
+  double* red;         // chunk reduction partials: mixed_red_words(N) doubles
+};
+
+// The mixed-precision solves reduce over fixed row chunks (32 rows) and
+// super-chunks (256 rows), so their results do not depend on how rows are
+// spread over blocks. Work words of those partials for n rows: two halves of
+// two sums each.
+#ifndef MGPU_MIXED_MAX_ROWS_LOG2
+#define MGPU_MIXED_MAX_ROWS_LOG2 23
+#endif
+#ifndef MGPU_BLOCK_MAX_ROWS
+#define MGPU_BLOCK_MAX_ROWS 32768
+#endif
+constexpr int kMixedMaxRows = 1 << MGPU_MIXED_MAX_ROWS_LOG2;
+constexpr int kSuperRows = 256;
+constexpr int kBlockMaxRows = MGPU_BLOCK_MAX_ROWS;  // rows one block of a mixed solve may hold
+inline long mixed_red_words(long n) { return 4l * ((n + kSuperRows - 1) / kSuperRows); }
+
+// One system of a batched solve.
+struct alignas(16) BatchSys {
+  KrylovArgs a;
+  MixedArgs m;
+};
+
+// A lane of a batched launch: nblocks co-resident blocks that solve the
+// systems items[first_item .. first_item+nitems) one after the other.
+struct BatchLane {
+  int first_block, nblocks, first_item, nitems;
+};
+
+// Device tables of one batched Krylov launch.
+struct LanePlan {
+  const BatchSys* sys;
+  const BatchLane* lanes;
+  const int* block_lane;
+  const int* items;
+  unsigned long long* bars;  // one barrier counter per lane
+  double* partials;          // 8 doubles per block
+  unsigned long long* lane_t;  // optional: start and end time (ns) of each lane
+  int nlanes, nblocks;
 };
 
 struct DeviceCase {
@@ -105,6 +145,7 @@ struct DeviceCase {
   int* ell_col = nullptr;  // column-major ELL pattern of the FP32 copy (W*N)
   float* ell_val = nullptr;
   int ell_w = 0;
+  double* red32 = nullptr;  // chunk reduction partials of the mixed-precision solves
   // Krylov work
   double *kw = nullptr;  // 10*N
   double* partials = nullptr;
@@ -122,6 +163,8 @@ int launch_factor(const KrylovArgs& a, int kind, cudaStream_t s);
 int krylov_grid(int n, int& block, int which);
 int launch_pcg_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s);
 int launch_bicgstab_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s);
+int batch_capacity(bool pcg, bool ell);
+int launch_mixed_batch(const LanePlan& p, bool pcg, bool ell, cudaStream_t s);
 int launch_spmv(int n, const int* rp, const int* col, const double* val, const double* x, double* y,
                 cudaStream_t s);
 

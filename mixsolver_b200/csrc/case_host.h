@@ -1,0 +1,82 @@
+// case_host.h -- host-side state of a resident case and the driver helpers
+// shared by the single-case runs (case.cu) and the batched runs (batch.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "assembly.cuh"
+#include "case.cuh"
+
+#define TRY(x)                 \
+  do {                         \
+    int rc_ = (x);             \
+    if (rc_ != 0) return rc_;  \
+  } while (0)
+
+// A resident case: device arrays, parameters, its stream and run bookkeeping.
+struct MgpuCase {
+  using DeviceCase = mgpu::DeviceCase;
+  using AsmParams = mgpu::AsmParams;
+  DeviceCase d;
+  AsmParams P;
+  MgpuCtrl ctrl;
+  cudaStream_t stream = nullptr;
+  std::vector<void*> allocs;
+  int64_t bytes = 0;
+  int has_outflow = 0;
+  int profiling = 0;
+  MgpuTiming timing{};
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;
+  int64_t launches = 0;
+  int kblock = 256;
+  int run_mode = -1;  // batched runs: 0 SIMPLE, 1 PISO after mgpu_case_begin, -1 none
+  int run_gen = 0;    // counts mgpu_case_begin calls
+
+  template <typename T>
+  int alloc(T*& p, size_t n) {
+    p = nullptr;
+    if (n == 0) n = 1;
+    void* q = nullptr;
+    MGPU_CUDA(cudaMalloc(&q, n * sizeof(T)));
+    allocs.push_back(q);
+    bytes += (int64_t)(n * sizeof(T));
+    p = (T*)q;
+    return 0;
+  }
+  template <typename T>
+  int upload(T*& p, const std::vector<T>& h) {
+    if (int e = alloc(p, h.size())) return e;
+    if (!h.empty()) MGPU_CUDA(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return 0;
+  }
+  ~MgpuCase() {
+    for (auto e : ev_pool) cudaEventDestroy(e);
+    if (ev_run0) cudaEventDestroy(ev_run0);
+    if (ev_run1) cudaEventDestroy(ev_run1);
+    for (void* p : allocs) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace mgpu {
+
+extern int g_cheb_degree;
+extern double g_cheb_ratio;
+
+KrylovArgs base_args(MgpuCase* c);
+MixedArgs mixed_args(const MgpuCase* c, bool bicg);
+// momentum solve of component comp / pressure-correction solve into slot
+KrylovArgs mom_args(MgpuCase* c, int comp, bool transient);
+KrylovArgs ppe_args(MgpuCase* c, int slot, bool transient);
+// one solve on stream s in the case's precision (FP64: factor + solve)
+int krylov(MgpuCase* c, KrylovArgs a, bool bicg, cudaStream_t s);
+// fresh device status for a run of nrec-1 iterations (ts_order 0 steady)
+int reset_status(MgpuCase* c, int ts_order, int nrec);
+int ensure_recs(MgpuCase* c, int n);
+
+}  // namespace mgpu

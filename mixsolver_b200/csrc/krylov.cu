@@ -302,6 +302,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_pcg(KrylovArgs a) {
   if (a.st->abort) return;
   const int n = a.n;
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstr = gridDim.x * blockDim.x;
+  VGrid vg = whole_grid(a.bar, a.partials);
   const bool jac = a.precond == 1;
   double* x = a.x;
   double *r = a.r, *z = a.z, *p = a.p, *q = a.v;
@@ -313,7 +314,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_pcg(KrylovArgs a) {
     v2[0] = v2[0] + bi * bi;
     if (jac && fabs(a.aval[a.diag[i]]) < DTINY) v2[1] = v2[1] + 1.0;
   }
-  if (!grid_sum<2, L1>(v2, a.partials, a.bar, a.st)) return;
+  if (!vg_sum<2, L1>(v2, vg, a.st)) return;
   const double bnrm = sqrt(v2[0]);
   if (bnrm == 0.0) {
     for (int i = gtid; i < n; i += gstr) x[i] = 0.0;
@@ -340,7 +341,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_pcg(KrylovArgs a) {
       w2[1] = w2[1] + ri * zi;
     }
   }
-  if (!grid_sum<2, L1>(w2, a.partials, a.bar, a.st)) return;
+  if (!vg_sum<2, L1>(w2, vg, a.st)) return;
   double res = sqrt(w2[0]) / bnrm;
   if (res <= a.tol) {
     write_result(a, 0, res, 0);
@@ -353,7 +354,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_pcg(KrylovArgs a) {
     if (!apply_lu<L1>(a, a.precond, r, z)) return;
     double v1[1] = {0.0};
     for (int i = gtid; i < n; i += gstr) v1[0] = v1[0] + r[i] * ldv<L1>(&z[i]);
-    if (!grid_sum<1, L1>(v1, a.partials, a.bar, a.st)) return;
+    if (!vg_sum<1, L1>(v1, vg, a.st)) return;
     rz = v1[0];
   }
   for (int i = gtid; i < n; i += gstr) p[i] = ldv<L1>(&z[i]);
@@ -366,7 +367,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_pcg(KrylovArgs a) {
       q[i] = qi;
       pq[0] = pq[0] + p[i] * qi;
     }
-    if (!grid_sum<1, L1>(pq, a.partials, a.bar, a.st)) return;
+    if (!vg_sum<1, L1>(pq, vg, a.st)) return;
     const double pap = pq[0];
     if (fabs(pap) < DTINY) {
       ierr = 2;
@@ -385,7 +386,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_pcg(KrylovArgs a) {
         u2[1] = u2[1] + ri * zi;
       }
     }
-    if (!grid_sum<2, L1>(u2, a.partials, a.bar, a.st)) return;
+    if (!vg_sum<2, L1>(u2, vg, a.st)) return;
     res = sqrt(u2[0]) / bnrm;
     if (res <= a.tol) {
       write_result(a, it, res, 0);
@@ -398,7 +399,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_pcg(KrylovArgs a) {
       if (!apply_lu<L1>(a, a.precond, r, z)) return;
       double v1[1] = {0.0};
       for (int i = gtid; i < n; i += gstr) v1[0] = v1[0] + r[i] * ldv<L1>(&z[i]);
-      if (!grid_sum<1, L1>(v1, a.partials, a.bar, a.st)) return;
+      if (!vg_sum<1, L1>(v1, vg, a.st)) return;
       rz_new = v1[0];
     }
     if (fabs(rz) < DTINY) {
@@ -422,6 +423,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_bicgstab(KrylovArgs a) {
   if (a.st->abort) return;
   const int n = a.n;
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstr = gridDim.x * blockDim.x;
+  VGrid vg = whole_grid(a.bar, a.partials);
   const bool jac = a.precond == 1;
   double* x = a.x;
   double *r = a.r, *r0 = a.r0, *p = a.p, *v = a.v, *s = a.s, *t = a.t, *ph = a.ph, *sh = a.sh;
@@ -431,7 +433,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_bicgstab(KrylovArgs a) {
     v2[0] = v2[0] + bi * bi;
     if (jac && fabs(a.aval[a.diag[i]]) < DTINY) v2[1] = v2[1] + 1.0;
   }
-  if (!grid_sum<2, L1>(v2, a.partials, a.bar, a.st)) return;
+  if (!vg_sum<2, L1>(v2, vg, a.st)) return;
   const double bnrm = sqrt(v2[0]);
   if (bnrm == 0.0) {
     for (int i = gtid; i < n; i += gstr) x[i] = 0.0;
@@ -455,7 +457,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_bicgstab(KrylovArgs a) {
     v[i] = 0.0;
     w1[0] = w1[0] + ri * ri;
   }
-  if (!grid_sum<1, L1>(w1, a.partials, a.bar, a.st)) return;
+  if (!vg_sum<1, L1>(w1, vg, a.st)) return;
   double res = sqrt(w1[0]) / bnrm;
   if (res <= a.tol) {
     write_result(a, 0, res, 0);
@@ -484,7 +486,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_bicgstab(KrylovArgs a) {
       v[i] = vi;
       d1[0] = d1[0] + r0[i] * vi;
     }
-    if (!grid_sum<1, L1>(d1, a.partials, a.bar, a.st)) return;
+    if (!vg_sum<1, L1>(d1, vg, a.st)) return;
     alpha = rho / d1[0];
     double d2[1] = {0.0};
     for (int i = gtid; i < n; i += gstr) {
@@ -493,7 +495,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_bicgstab(KrylovArgs a) {
       d2[0] = d2[0] + si * si;
       if (jac) sh[i] = si / a.aval[a.diag[i]];
     }
-    if (!grid_sum<1, L1>(d2, a.partials, a.bar, a.st)) return;
+    if (!vg_sum<1, L1>(d2, vg, a.st)) return;
     const double snrm = sqrt(d2[0]);
     if (snrm / bnrm <= a.tol) {
       for (int i = gtid; i < n; i += gstr) x[i] = x[i] + alpha * ldv<L1>(&ph[i]);
@@ -508,7 +510,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_bicgstab(KrylovArgs a) {
       d3[0] = d3[0] + ti * ti;
       d3[1] = d3[1] + ti * s[i];
     }
-    if (!grid_sum<2, L1>(d3, a.partials, a.bar, a.st)) return;
+    if (!vg_sum<2, L1>(d3, vg, a.st)) return;
     const double tt = d3[0];
     if (tt < DTINY) {
       ierr = 2;
@@ -527,7 +529,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_bicgstab(KrylovArgs a) {
       d4[0] = d4[0] + ri * ri;
       d4[1] = d4[1] + ri * r0[i];
     }
-    if (!grid_sum<2, L1>(d4, a.partials, a.bar, a.st)) return;
+    if (!vg_sum<2, L1>(d4, vg, a.st)) return;
     res = sqrt(d4[0]) / bnrm;
     if (res <= a.tol) {
       write_result(a, it, res, 0);

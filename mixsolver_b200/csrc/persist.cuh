@@ -21,20 +21,47 @@ __device__ __forceinline__ int ld_acquire_i32(const int* p) {
   return v;
 }
 
-// Bounded grid barrier over a monotone 64-bit arrival counter (zeroed before
-// every cooperative launch; all blocks are co-resident). Each block adds one
-// arrival and waits until the counter reaches the end of the current round.
-// Returns false when the wait ran out; the caller then leaves the kernel.
-__device__ bool grid_sync(unsigned long long* bar, DevStatus* st) {
+// A group of co-resident blocks working on one system: the whole grid of a
+// single-system launch, or one system's share of a batched launch.
+struct VGrid {
+  int nb;    // blocks in the group
+  int rank;  // this block's rank in the group
+  unsigned long long* bar;  // the group's barrier counter
+  double* partials;         // the group's reduction partials (2 halves of 4 * nb)
+  int half;                 // half of the partials the next reduction writes
+  __device__ int gtid() const { return rank * blockDim.x + threadIdx.x; }
+  __device__ int gstr() const { return nb * blockDim.x; }
+  // Consecutive reductions alternate between the two halves: a block that
+  // leaves reduction k early and writes its share of k+1 cannot overwrite a
+  // partial of k that a slower block is still reading, because every block
+  // reads k's partials before it arrives at k+1's barrier, and k+2 (the next
+  // user of the same half) writes only after that barrier.
+  __device__ double* next_partials() {
+    double* p = partials + (half ? 4 * nb : 0);
+    half ^= 1;
+    return p;
+  }
+};
+
+__device__ __forceinline__ VGrid whole_grid(unsigned long long* bar, double* partials) {
+  return VGrid{(int)gridDim.x, (int)blockIdx.x, bar, partials, 0};
+}
+
+// Bounded barrier of a group over a monotone 64-bit arrival counter (zeroed
+// before every launch; all blocks of the group are co-resident). Each block
+// adds one arrival and waits until the counter reaches the end of the current
+// round. Returns false when the wait ran out; the caller then leaves the kernel.
+__device__ bool vg_sync(const VGrid& g, DevStatus* st) {
   __shared__ int s_ok;
-  if (gridDim.x == 1) {
+  if (g.nb == 1) {
     __syncthreads();
     return true;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    const unsigned long long nb = gridDim.x;
+    unsigned long long* bar = g.bar;
+    const unsigned long long nb = g.nb;
     __threadfence();
     const unsigned long long old = atomicAdd(bar, 1ull);
     const unsigned long long target = (old / nb + 1ull) * nb;
@@ -53,6 +80,10 @@ __device__ bool grid_sync(unsigned long long* bar, DevStatus* st) {
   }
   __syncthreads();
   return s_ok != 0;
+}
+
+__device__ __forceinline__ bool grid_sync(unsigned long long* bar, DevStatus* st) {
+  return vg_sync(VGrid{(int)gridDim.x, (int)blockIdx.x, bar, nullptr, 0}, st);
 }
 
 // Vector loads inside a persistent kernel: with one block every thread sits on
@@ -79,7 +110,9 @@ __device__ __forceinline__ double warp_sum(double v) {
 // identical total. The partials are fetched by all threads at once: a single
 // L2 round trip instead of a serial chain.
 template <int NQ, bool L1>
-__device__ bool grid_sum(double (&v)[NQ], double* partials, unsigned long long* bar, DevStatus* st) {
+__device__ bool vg_sum(double (&v)[NQ], VGrid& g, DevStatus* st) {
+  static_assert(NQ <= 4, "at most 4 sums per reduction");
+  double* partials = g.nb == 1 ? nullptr : g.next_partials();
   __shared__ double sh[NQ][32];
   __shared__ double tot[NQ];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -95,22 +128,22 @@ __device__ bool grid_sum(double (&v)[NQ], double* partials, unsigned long long* 
       double s = lane < nw ? sh[q][lane] : 0.0;
       s = warp_sum(s);
       if (lane == 0) {
-        if (gridDim.x == 1)
+        if (g.nb == 1)
           tot[q] = s;
         else
-          partials[q * gridDim.x + blockIdx.x] = s;
+          partials[q * g.nb + g.rank] = s;
       }
     }
   }
-  if (gridDim.x == 1) {
+  if (g.nb == 1) {
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < NQ; ++q) v[q] = tot[q];
     __syncthreads();
     return true;
   }
-  if (!grid_sync(bar, st)) return false;
-  const int G = gridDim.x;
+  if (!vg_sync(g, st)) return false;
+  const int G = g.nb;
   double w[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
@@ -146,7 +179,8 @@ __device__ bool grid_sum(double (&v)[NQ], double* partials, unsigned long long* 
 
 // Grid-wide maximum of one non-negative value (exact, order-independent).
 template <bool L1>
-__device__ bool grid_max(double& v, double* partials, unsigned long long* bar, DevStatus* st) {
+__device__ bool vg_max(double& v, VGrid& g, DevStatus* st) {
+  double* partials = g.nb == 1 ? nullptr : g.next_partials();
   __shared__ double sh[32];
   __shared__ double tot;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -158,16 +192,16 @@ __device__ bool grid_max(double& v, double* partials, unsigned long long* bar, D
     double s = lane < nw ? sh[lane] : 0.0;
     for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_xor_sync(0xffffffffu, s, o));
     if (lane == 0) {
-      if (gridDim.x == 1)
+      if (g.nb == 1)
         tot = s;
       else
-        partials[blockIdx.x] = s;
+        partials[g.rank] = s;
     }
   }
-  if (gridDim.x > 1) {
-    if (!grid_sync(bar, st)) return false;
+  if (g.nb > 1) {
+    if (!vg_sync(g, st)) return false;
     double s = 0.0;
-    for (int j = threadIdx.x; j < (int)gridDim.x; j += blockDim.x) s = fmax(s, ldv<L1>(&partials[j]));
+    for (int j = threadIdx.x; j < g.nb; j += blockDim.x) s = fmax(s, ldv<L1>(&partials[j]));
     for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_xor_sync(0xffffffffu, s, o));
     __syncthreads();
     if (lane == 0) sh[warp] = s;

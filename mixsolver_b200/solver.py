@@ -11,6 +11,9 @@ replaces, so a caller of the reference finds the same operations:
 * :func:`bicgstab_ilu0`, :func:`cg_jacobi`, :func:`cg_ic0` and :func:`csr_matvec`
   -- ``mod_uns_linsolver.f90``: ``(A, b, x, tol, maxit) -> (x, it, res, ierr)``.
 * :func:`build_connectivity`, :func:`compute_geometry` -- the mesh pipeline.
+* :class:`CaseBatch` -- no counterpart in the reference (one case per process
+  there): many resident cases advanced together, each assembly kernel one
+  launch over all of them and each Krylov phase one persistent launch.
 
 Every call runs on the GPU through ``libmixgpu.so``; there is no CPU path and a
 missing library raises.
@@ -23,7 +26,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import abi
-from .abi import MeshArrays, MgpuIterRec, MgpuTiming, dptr, iptr, records_to_list
+from .abi import MeshArrays, MgpuBatchInfo, MgpuIterRec, MgpuTiming, dptr, iptr, records_to_list
 
 
 def _lib():
@@ -132,6 +135,98 @@ class UnsCase:
         b = C.c_int64()
         _lib().mgpu_case_device_bytes(self.h, C.byref(b))
         return int(b.value)
+
+    def begin(self, mode: int, nsteps: int = 0) -> int:
+        """Start a run (0 SIMPLE, 1 PISO) that a :class:`CaseBatch` steps;
+        returns ier (30 / 31 for a PISO run the control rejects)."""
+        ier = C.c_int(0)
+        lib = _lib()
+        abi.check(lib, lib.mgpu_case_begin(self.h, int(mode), int(nsteps), C.byref(ier)), "mgpu_case_begin")
+        return ier.value
+
+    def finish(self, logcap: int = 4096):
+        """(ier, records) of a run begun by :meth:`begin`, as simple_run / piso_run return them."""
+        recs = (MgpuIterRec * max(logcap, 1))()
+        nrec, ier = C.c_int(0), C.c_int(0)
+        lib = _lib()
+        abi.check(lib, lib.mgpu_case_finish(self.h, recs, int(logcap), C.byref(nrec), C.byref(ier)),
+                  "mgpu_case_finish")
+        return ier.value, records_to_list(recs, min(nrec.value, logcap))
+
+
+def batch_plan(rows, barrier_ns: int, row_ps: int, capacity: int, passes=None):
+    """Lane plan of a batched Krylov phase (host only): per system its lane
+    width and lane, and the modelled makespan in microseconds."""
+    r = np.ascontiguousarray(rows, np.int32)
+    p = None if passes is None else np.ascontiguousarray(passes, np.float64)
+    w = np.zeros(len(r), np.int32); ln = np.zeros(len(r), np.int32)
+    mk = C.c_double(0.0)
+    lib = _lib()
+    abi.check(lib, lib.mgpu_batch_plan(len(r), iptr(r), dptr(p), int(barrier_ns), int(row_ps), int(capacity),
+                                       iptr(w), iptr(ln), C.byref(mk)), "mgpu_batch_plan")
+    return w, ln, mk.value
+
+
+class CaseBatch:
+    """Resident cases advanced together (see mgpu_batch_* in include/mixgpu.h)."""
+
+    def __init__(self, cases, policy=None):
+        lib = _lib()
+        self.cases = list(cases)
+        arr = (C.c_void_p * len(self.cases))(*[c.h.value for c in self.cases])
+        self.h = C.c_void_p()
+        abi.check(lib, lib.mgpu_batch_create(arr, len(self.cases), C.byref(self.h)), "mgpu_batch_create")
+        if policy is not None:
+            self.set_policy(*policy)
+
+    def close(self):
+        if self.h:
+            _lib().mgpu_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_policy(self, barrier_ns: int, row_ps: int):
+        """Fixed lane policy (cost-model constants); (0, 0) = autotune."""
+        lib = _lib()
+        abi.check(lib, lib.mgpu_batch_set_policy(self.h, int(barrier_ns), int(row_ps)), "mgpu_batch_set_policy")
+
+    def step(self, iters: int) -> int:
+        """Advance every running member; returns how many still run."""
+        active = C.c_int(0)
+        lib = _lib()
+        abi.check(lib, lib.mgpu_batch_step(self.h, int(iters), C.byref(active)), "mgpu_batch_step")
+        return active.value
+
+    def poll(self) -> np.ndarray:
+        done = np.zeros(len(self.cases), np.int32)
+        lib = _lib()
+        abi.check(lib, lib.mgpu_batch_poll(self.h, iptr(done)), "mgpu_batch_poll")
+        return done
+
+    def run(self, modes, nsteps: int = 0):
+        """begin + step to the end + finish; returns (nrec, ier) arrays."""
+        K = len(self.cases)
+        m = np.ascontiguousarray(np.broadcast_to(np.asarray(modes, np.int32), (K,)))
+        nrec = np.zeros(K, np.int32)
+        ier = np.zeros(K, np.int32)
+        lib = _lib()
+        abi.check(lib, lib.mgpu_batch_run(self.h, iptr(m), int(nsteps), iptr(nrec), iptr(ier)), "mgpu_batch_run")
+        return nrec, ier
+
+    def set_profiling(self, on: bool):
+        _lib().mgpu_batch_set_profiling(self.h, 1 if on else 0)
+
+    def info(self) -> dict:
+        i = MgpuBatchInfo()
+        _lib().mgpu_batch_info(self.h, C.byref(i))
+        out = {k: getattr(i, k) for k, _ in MgpuBatchInfo._fields_}
+        out["phase_ms"] = list(i.phase_ms)
+        return out
 
 
 def set_tuning(key: str, value: int) -> None:

@@ -45,6 +45,31 @@ def test_struct_layouts():
                                       + 32 * C.sizeof(abi.MgpuBcSpec))
 
 
+def test_struct_offsets_match_compiled_header(tmp_path):
+    """Every field offset and struct size of the ctypes mirrors equals what a C
+    compiler makes of include/mixgpu.h."""
+    structs = [abi.MgpuBcSpec, abi.MgpuCtrl, abi.MgpuMesh, abi.MgpuIterRec, abi.MgpuTiming, abi.MgpuBatchInfo]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
+    for st in structs:
+        lines.append(f'  printf("{st.__name__} size %zu\\n", sizeof({st.__name__}));')
+        for name, _ in st._fields_:
+            lines.append(f'  printf("{st.__name__} {name} %zu\\n", offsetof({st.__name__}, {name}));')
+    lines.append("  return 0;\n}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    import subprocess
+    subprocess.check_call(["gcc", "-std=c11", "-o", str(exe), str(src)])
+    got = {}
+    for ln in subprocess.check_output([str(exe)]).decode().splitlines():
+        s, f, v = ln.split()
+        got[(s, f)] = int(v)
+    for st in structs:
+        assert got[(st.__name__, "size")] == C.sizeof(st), st.__name__
+        for name, _ in st._fields_:
+            assert got[(st.__name__, name)] == getattr(st, name).offset, (st.__name__, name)
+
+
 @pytest.mark.parametrize("which", ["cavity", "channel", "tet"])
 def test_connectivity_bit_exact(lib, which):
     if which == "cavity":

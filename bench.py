@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--workload", default="channel", choices=["channel", "batch"],
                     help="channel: one 524k-cell case (default); batch: many 3-D cavities in one batch")
     ap.add_argument("--cases", type=int, default=256, help="batch: number of cavity cases")
-    ap.add_argument("--policy", default="auto", help="batch: lane policy BARRIER_NSxROW_PS or auto")
+    ap.add_argument("--policy", default="auto", help="batch: lane policy SPLIT_ROWSxWIDE_LANES or auto")
     ap.add_argument("--fp64-iters", type=int, default=2, help="batch: iterations of the FP64 comparison leg")
     return ap.parse_args()
 
@@ -423,7 +423,7 @@ def run_batch(args):
     hf = [o.fields() for o in objs]
     for o in objs:
         o.begin(0, 10 ** 6)
-    B2 = S.CaseBatch(objs, policy=(i1["barrier_ns"], i1["row_ps"]))
+    B2 = S.CaseBatch(objs, policy=(i1["split_rows"], i1["wide_lanes"]))
     B2.step(1)
     e2e_steps = 3
     w0 = time.perf_counter()
@@ -464,7 +464,7 @@ def run_batch(args):
                                "[4096, 262144], Re uniform in [100, 2000], mixed SIMPLE, lin_tol 1e-8",
                    "cells_total": int(cells.sum()), "cells_min": int(cells.min()), "cells_max": int(cells.max()),
                    "device_gb": dev_bytes / 1e9, "mesh_gen_s": t_mesh, "case_create_s": t_create,
-                   "policy": {"barrier_ns": i1["barrier_ns"], "row_ps": i1["row_ps"],
+                   "policy": {"split_rows": i1["split_rows"], "wide_lanes": i1["wide_lanes"],
                               "autotuned": i1["autotuned"], "tune_ms": i1["tune_ms"]},
                    "graph": i1["graph"], "launches_per_iter": i1["launches_per_iter"],
                    "pressure_lanes": i1["lanes"], "pressure_blocks": i1["blocks"],

@@ -289,13 +289,13 @@ int mgpu_case_finish(MgpuCase* c, MgpuIterRec* log, int logcap, int* nrec, int* 
 int mgpu_batch_create(MgpuCase* const* cases, int ncases, MgpuBatch** out);
 int mgpu_batch_destroy(MgpuBatch* b);
 /* Lane policy. The mixed-precision solves give bit-identical results on any
- * number of blocks, so the plan only affects speed. It prices a system of n
- * rows and p passes on w blocks at p * (rows per block * row_ps + barrier_ns)
- * and minimises the busiest lane within the co-resident block capacity; the
- * first step re-plans on the measured iteration counts. (0, 0) = autotune:
- * the first step times the first pressure solve under each candidate pair
- * and keeps the fastest (default). */
-int mgpu_batch_set_policy(MgpuBatch* b, int barrier_ns, int row_ps);
+ * number of blocks, so the policy only affects speed: systems of more than
+ * split_rows rows (at most 32768) run on wide_lanes wide lanes sharing their
+ * class's blocks, smaller ones on single-block lanes; lanes take systems from
+ * per-class queues at run time. (0, 0) = autotune: the first step times the
+ * first pressure solve under each candidate pair and keeps the fastest
+ * (default). */
+int mgpu_batch_set_policy(MgpuBatch* b, int split_rows, int wide_lanes);
 /* Advance every running member by up to iters iterations / steps; returns
  * after the device is done. *active = members still running. */
 int mgpu_batch_step(MgpuBatch* b, int iters, int* active);
@@ -306,7 +306,7 @@ int mgpu_batch_poll(MgpuBatch* b, int* done);
 int mgpu_batch_run(MgpuBatch* b, const int* mode, int nsteps, int* nrec, int* ier);
 typedef struct {
   int32_t ncases;
-  int32_t barrier_ns, row_ps;                /* lane policy in use */
+  int32_t split_rows, wide_lanes;            /* lane policy in use */
   int32_t autotuned;                         /* 1: policy picked by the autotuner */
   int32_t graph;                             /* 1: iterations replay a CUDA graph */
   int32_t lanes, blocks;                     /* first pressure phase: lanes, blocks of its widest launch */
@@ -329,10 +329,11 @@ int mgpu_batch_set_profiling(MgpuBatch* b, int on);
 int mgpu_batch_info(const MgpuBatch* b, MgpuBatchInfo* info);
 /* The lane plan (host only, no GPU needed) of systems of rows[i] rows and
  * passes[i] SpMV-sized passes (NULL: modelled) under a policy and a
- * co-resident block capacity: width[i] = blocks of system i's lane, lane[i] =
- * its lane; *makespan_us = the modelled time of the busiest lane. */
-int mgpu_batch_plan(int nsys, const int* rows, const double* passes, int barrier_ns, int row_ps, int capacity,
-                    int* width, int* lane, double* makespan_us);
+ * co-resident block capacity: sys_class[i] = 0 (wide lanes) or 1
+ * (single-block lanes); lane_width[0 .. *nlanes) = the lanes' widths (room for
+ * `capacity` entries). */
+int mgpu_batch_plan(int nsys, const int* rows, const double* passes, int split_rows, int wide_lanes, int capacity,
+                    int* sys_class, int* lane_width, int* nlanes);
 
 #ifdef __cplusplus
 }

@@ -79,7 +79,7 @@ class MgpuTiming(C.Structure):
 
 
 class MgpuBatchInfo(C.Structure):
-    _fields_ = [("ncases", C.c_int32), ("barrier_ns", C.c_int32), ("row_ps", C.c_int32),
+    _fields_ = [("ncases", C.c_int32), ("split_rows", C.c_int32), ("wide_lanes", C.c_int32),
                 ("autotuned", C.c_int32), ("graph", C.c_int32), ("lanes", C.c_int32), ("blocks", C.c_int32),
                 ("launches_per_iter", C.c_int32), ("tune_ms", C.c_double), ("step_ms", C.c_double),
                 ("iters", C.c_int64), ("phase_ms", C.c_double * 8), ("asm_ms", C.c_double),
@@ -263,7 +263,7 @@ def load_library(path: str = LIB_PATH):
     lib.mgpu_batch_run.argtypes = [C.c_void_p, P(C.c_int), C.c_int, P(C.c_int), P(C.c_int)]
     lib.mgpu_batch_info.argtypes = [C.c_void_p, P(MgpuBatchInfo)]
     lib.mgpu_batch_set_profiling.argtypes = [C.c_void_p, C.c_int]
-    lib.mgpu_batch_plan.argtypes = [C.c_int, i32p, dblp, C.c_int, C.c_int, C.c_int, i32p, i32p, dblp]
+    lib.mgpu_batch_plan.argtypes = [C.c_int, i32p, dblp, C.c_int, C.c_int, C.c_int, i32p, i32p, P(C.c_int)]
     _LIB = lib
     return lib
 

@@ -16,21 +16,22 @@
 // host.
 //
 // Lane plan (the tiling and chunking): the mixed-precision solves give the
-// same result on any number of blocks, so the plan is free to balance. A cost
-// model prices a system of n rows and p passes on w blocks at
-// p * (rows per block * row cost + barrier cost); a binary search finds the
-// smallest makespan M for which every system fits some width within M and the
-// first-fit-decreasing packing of systems into lanes of load <= M needs at most
-// the co-resident block capacity. The first iteration of a batch runs on
-// modelled pass counts, then every phase is re-planned on the measured
-// iteration counts; with autotuning on, the first pressure solve is timed
-// under each candidate (barrier cost, row cost) and the fastest is kept.
+// same result on any number of blocks, so the plan is free to balance. Systems
+// above a row threshold run on a few wide lanes that share their class's
+// blocks; the others on single-block lanes; the blocks are split by each
+// class's share of the work (modelled on the first iteration, measured
+// iteration counts after it). Which lane solves which system is decided at run
+// time: each class has a queue of its systems, most work first, a lane takes
+// the next one of its class, and wide lanes take small systems once theirs are
+// done. With autotuning on, the first pressure solve of a batch is timed under
+// each candidate (threshold, wide lanes) and the fastest is kept.
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <string>
 #include <vector>
@@ -43,48 +44,21 @@ using namespace mgpu;
 
 namespace {
 
-// Cost model of one system on a lane of w blocks (microseconds): a solve of
-// `passes` SpMV-sized passes costs, per pass, the rows of one block (whole
-// super-chunks of kSuperRows rows) times the per-row cost of one block, plus one group
-// barrier when w > 1. The two constants are the lane policy; they only steer
-// the plan, never the results.
+// Lane policy: systems of more than split_rows rows run on wide_lanes wide
+// lanes, which share the blocks given to them; the others run on single-block
+// lanes. The blocks are split between the two classes by their share of the
+// work. Few wide lanes keep the working sets of the big systems that run at
+// the same time within L2; the small systems fit beside them. The mixed
+// solves give the same result on any lane, so the policy only affects speed.
 struct Policy {
-  double bar_us = 1.5;    // group barrier per pass
-  double row_us = 0.006;  // one row of one pass on one block
+  int split_rows = 32768;
+  int wide_lanes = 8;
 };
-
-double sys_time(long n, double passes, int w, const Policy& P) {
-  const long nsc = (n + kSuperRows - 1) / kSuperRows;
-  const long per = (nsc + w - 1) / w;
-  const double rows = (double)std::min<long>(n, per * kSuperRows);
-  return passes * (rows * P.row_us + (w > 1 ? P.bar_us : 0.05));
-}
-
-int max_width(long n, int cap) {
-  return (int)std::max<long>(1, std::min<long>(cap, (n + kSuperRows - 1) / kSuperRows));
-}
 
 // fewest blocks that keep a block's rows within kBlockMaxRows
 int least_width(long n) {
   const long nsc = (n + kSuperRows - 1) / kSuperRows, per = kBlockMaxRows / kSuperRows;
   return (int)std::max<long>(1, (nsc + per - 1) / per);
-}
-
-// smallest width whose time is at most M, or -1
-int min_width(long n, double passes, double M, int cap, const Policy& P) {
-  const int w0 = least_width(n);
-  if (w0 > cap) return -1;
-  if (w0 == 1 && sys_time(n, passes, 1, P) <= M) return 1;
-  int lo = std::max(2, w0), hi = max_width(n, cap);
-  if (hi < 2 || sys_time(n, passes, hi, P) > M) return -1;
-  while (lo < hi) {
-    const int mid = (lo + hi) / 2;
-    if (sys_time(n, passes, mid, P) <= M)
-      hi = mid;
-    else
-      lo = mid + 1;
-  }
-  return lo;
 }
 
 // Estimated passes of a solve when no iteration count is known yet: PCG with
@@ -94,71 +68,58 @@ double model_passes(long n, bool pcg, int cheb_k) {
   return pcg ? std::max(5.0, std::cbrt((double)n)) * (std::max(cheb_k, 1) + 1) : 24.0;
 }
 
-struct HostLane {
-  int width;
-  double load = 0.0;
-  std::vector<int> items;
+// Lanes of one launch: their widths and classes (0 wide, 1 single-block), and
+// per class the queue of systems, most work first.
+struct LaneSet {
+  std::vector<int> width, cls;
+  std::vector<int> queue[2];
 };
 
-// Lanes of items n[i] (rows) with passes[i] so that the busiest lane is as
-// short as possible within `cap` co-resident blocks: binary search on that
-// makespan M; each system takes the smallest width that finishes within M,
-// systems of one width are packed first-fit-decreasing into lanes of load <= M.
-std::vector<HostLane> plan_at(const std::vector<int>& n, const std::vector<double>& passes, double M, int cap,
-                              const Policy& P, int* blocks) {
-  std::map<int, std::vector<std::pair<double, int>>> cls;
-  *blocks = 0;
+LaneSet plan_lanes(const std::vector<int>& n, const std::vector<double>& passes, const Policy& P, int cap) {
+  LaneSet L;
+  std::vector<std::pair<double, int>> big, small;
+  double wb = 0.0, ws = 0.0;
+  int need = 1;  // the widest least width among the big systems
   for (int i = 0; i < (int)n.size(); ++i) {
-    const int w = min_width(n[i], passes[i], M, cap, P);
-    if (w < 0) {
-      *blocks = cap + 1;
-      return {};
-    }
-    cls[w].push_back({sys_time(n[i], passes[i], w, P), i});
-  }
-  std::vector<HostLane> lanes;
-  for (auto it = cls.rbegin(); it != cls.rend(); ++it) {
-    auto& v = it->second;
-    std::sort(v.begin(), v.end(), [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
-      return a.first != b.first ? a.first > b.first : a.second < b.second;
-    });
-    const size_t first = lanes.size();
-    for (auto& [t, i] : v) {
-      size_t k = first;
-      while (k < lanes.size() && lanes[k].load + t > M * (1.0 + 1e-12)) ++k;
-      if (k == lanes.size()) {
-        lanes.push_back(HostLane{it->first});
-        *blocks += it->first;
-      }
-      lanes[k].items.push_back(i);
-      lanes[k].load += t;
-    }
-  }
-  return lanes;
-}
-
-std::vector<std::vector<HostLane>> plan_lanes(const std::vector<int>& n, const std::vector<double>& passes,
-                                              const Policy& P, int cap) {
-  if (n.empty()) return {};
-  double lo = 0.0, hi = 0.0;
-  for (size_t i = 0; i < n.size(); ++i) {
-    lo = std::max(lo, sys_time(n[i], passes[i], max_width(n[i], cap), P));
-    hi += sys_time(n[i], passes[i], 1, P);
-  }
-  hi = std::max(hi, lo);
-  int blocks = 0;
-  std::vector<HostLane> best = plan_at(n, passes, hi, cap, P, &blocks);
-  for (int it = 0; it < 48 && hi > lo * (1.0 + 1e-4); ++it) {
-    const double mid = 0.5 * (lo + hi);
-    auto lanes = plan_at(n, passes, mid, cap, P, &blocks);
-    if (blocks <= cap) {
-      hi = mid;
-      best = std::move(lanes);
+    const double w = passes[i] * (double)n[i];
+    if (n[i] > P.split_rows || least_width(n[i]) > 1) {
+      big.push_back({w, i});
+      wb += w;
+      need = std::max(need, least_width(n[i]));
     } else {
-      lo = mid;
+      small.push_back({w, i});
+      ws += w;
     }
   }
-  return {best};
+  auto by_work = [](const std::pair<double, int>& x, const std::pair<double, int>& y) {
+    return x.first != y.first ? x.first > y.first : x.second < y.second;
+  };
+  std::sort(big.begin(), big.end(), by_work);
+  std::sort(small.begin(), small.end(), by_work);
+  for (auto& e : big) L.queue[0].push_back(e.second);
+  for (auto& e : small) L.queue[1].push_back(e.second);
+  int bb = 0, bs = 0;
+  if (big.empty()) {
+    bs = std::min<int>(cap, (int)small.size());
+  } else if (small.empty()) {
+    bb = cap;
+  } else {
+    bs = (int)std::llround(cap * ws / (wb + ws));
+    bs = std::max(1, std::min<int>(bs, std::min<int>((int)small.size(), cap - need)));
+    bb = cap - bs;
+  }
+  if (!big.empty()) {
+    const int k = std::max(1, std::min(std::min(P.wide_lanes, (int)big.size()), bb / need));
+    for (int j = 0; j < k; ++j) {
+      L.width.push_back(bb / k + (j < bb % k ? 1 : 0));
+      L.cls.push_back(0);
+    }
+  }
+  for (int j = 0; j < bs; ++j) {
+    L.width.push_back(1);
+    L.cls.push_back(1);
+  }
+  return L;
 }
 
 // done[i] for every live case, then the count of running cases and of
@@ -299,33 +260,43 @@ int build_launches(MgpuBatch* b, BatchPhase& ph, const Policy& P) {
     }
     if (items.empty()) continue;
     const int cap = batch_capacity(ph.pcg, ell == 1);
-    for (auto& lanes : plan_lanes(n, passes, P, cap)) {
-      std::vector<BatchLane> hl;
-      std::vector<int> block_lane, hitems;
-      for (auto& l : lanes) {
-        BatchLane bl{(int)block_lane.size(), l.width, (int)hitems.size(), (int)l.items.size()};
-        for (int i : l.items) hitems.push_back(items[i]);
-        for (int k = 0; k < l.width; ++k) block_lane.push_back((int)hl.size());
-        hl.push_back(bl);
-      }
-      BatchLaunch L;
-      L.pcg = ph.pcg;
-      L.ell = ell == 1;
-      BatchLane* dl = nullptr;
-      int *dbl = nullptr, *dit = nullptr;
-      TRY(dev_alloc(dl, hl.size()));
-      L.owned.push_back(dl);
-      TRY(dev_alloc(dbl, block_lane.size()));
-      L.owned.push_back(dbl);
-      TRY(dev_alloc(dit, hitems.size()));
-      L.owned.push_back(dit);
-      MGPU_CUDA(cudaMemcpy(dl, hl.data(), sizeof(BatchLane) * hl.size(), cudaMemcpyHostToDevice));
-      MGPU_CUDA(cudaMemcpy(dbl, block_lane.data(), sizeof(int) * block_lane.size(), cudaMemcpyHostToDevice));
-      MGPU_CUDA(cudaMemcpy(dit, hitems.data(), sizeof(int) * hitems.size(), cudaMemcpyHostToDevice));
-      L.plan = LanePlan{ph.d_sys, dl, dbl, dit, b->d_bars, b->d_part, nullptr, (int)hl.size(),
-                        (int)block_lane.size()};
-      ph.launches.push_back(std::move(L));
+    const LaneSet ls = plan_lanes(n, passes, P, cap);
+    std::vector<BatchLane> hl;
+    std::vector<int> block_lane, q_items, q_start;
+    for (size_t j = 0; j < ls.width.size(); ++j) {
+      hl.push_back(BatchLane{(int)block_lane.size(), ls.width[j], ls.cls[j], 0});
+      for (int k = 0; k < ls.width[j]; ++k) block_lane.push_back((int)j);
     }
+    for (int c = 0; c < 2; ++c) {
+      q_start.push_back((int)q_items.size());
+      for (int i : ls.queue[c]) q_items.push_back(items[i]);
+    }
+    q_start.push_back((int)q_items.size());
+    const int ncls = 2;
+    BatchLaunch L;
+    L.pcg = ph.pcg;
+    L.ell = ell == 1;
+    BatchLane* dl = nullptr;
+    int *dbl = nullptr, *dqi = nullptr, *dqs = nullptr, *dqh = nullptr, *dslot = nullptr;
+    TRY(dev_alloc(dl, hl.size()));
+    L.owned.push_back(dl);
+    TRY(dev_alloc(dbl, block_lane.size()));
+    L.owned.push_back(dbl);
+    TRY(dev_alloc(dqi, q_items.size()));
+    L.owned.push_back(dqi);
+    TRY(dev_alloc(dqs, q_start.size()));
+    L.owned.push_back(dqs);
+    TRY(dev_alloc(dqh, (size_t)ncls));
+    L.owned.push_back(dqh);
+    TRY(dev_alloc(dslot, 2 * hl.size()));
+    L.owned.push_back(dslot);
+    MGPU_CUDA(cudaMemcpy(dl, hl.data(), sizeof(BatchLane) * hl.size(), cudaMemcpyHostToDevice));
+    MGPU_CUDA(cudaMemcpy(dbl, block_lane.data(), sizeof(int) * block_lane.size(), cudaMemcpyHostToDevice));
+    MGPU_CUDA(cudaMemcpy(dqi, q_items.data(), sizeof(int) * q_items.size(), cudaMemcpyHostToDevice));
+    MGPU_CUDA(cudaMemcpy(dqs, q_start.data(), sizeof(int) * q_start.size(), cudaMemcpyHostToDevice));
+    L.plan = LanePlan{ph.d_sys, dl, dbl, dqi, dqs, dqh, dslot, b->d_bars, b->d_part, nullptr, ncls, (int)hl.size(),
+                      (int)block_lane.size()};
+    ph.launches.push_back(std::move(L));
   }
   return 0;
 }
@@ -585,13 +556,13 @@ int enqueue_iteration(MgpuBatch* b, bool tune) {
       float total = 0.f;
       MGPU_CUDA(cudaEventElapsedTime(&total, a0, a1));
       if (b->autotune && !b->policy_tuned && !ph.mixed.empty()) {
-        static const double bars[] = {0.75, 1.5, 3.0};
-        static const double rows[] = {0.004, 0.008};
+        static const int splits[] = {8192, 32768};
+        static const int wides[] = {2, 4, 8, 16};
         float best = 1e30f;
         Policy bp = b->policy;
-        for (double bu : bars)
-          for (double ru : rows) {
-            const Policy cand{bu, ru};
+        for (int sr : splits)
+          for (int wl : wides) {
+            const Policy cand{sr, wl};
             TRY(build_launches(b, ph, cand));
             MGPU_CUDA(cudaEventRecord(a0, s));
             TRY(run_phase(b, ph));
@@ -761,14 +732,15 @@ int mgpu_batch_destroy(MgpuBatch* b) {
   return 0;
 }
 
-int mgpu_batch_set_policy(MgpuBatch* b, int barrier_ns, int row_ps) {
-  if (!b || barrier_ns < 0 || row_ps < 0 || ((barrier_ns == 0) != (row_ps == 0))) {
+int mgpu_batch_set_policy(MgpuBatch* b, int split_rows, int wide_lanes) {
+  if (!b || split_rows < 0 || wide_lanes < 0 || ((split_rows == 0) != (wide_lanes == 0)) ||
+      split_rows > kBlockMaxRows) {
     set_error("mgpu_batch_set_policy: invalid argument");
     return MGPU_E_ARG;
   }
-  b->autotune = barrier_ns == 0;
+  b->autotune = split_rows == 0;
   b->policy_tuned = false;
-  if (!b->autotune) b->policy = Policy{barrier_ns * 1e-3, row_ps * 1e-6};
+  if (!b->autotune) b->policy = Policy{split_rows, wide_lanes};
   b->prepared = false;
   return 0;
 }
@@ -867,29 +839,23 @@ int mgpu_batch_run(MgpuBatch* b, const int* mode, int nsteps, int* nrec, int* ie
   return 0;
 }
 
-int mgpu_batch_plan(int nsys, const int* rows, const double* passes, int barrier_ns, int row_ps, int capacity,
-                    int* width, int* lane, double* makespan_us) {
-  if (nsys < 0 || (nsys > 0 && !rows) || barrier_ns <= 0 || row_ps <= 0 || capacity <= 0) {
+int mgpu_batch_plan(int nsys, const int* rows, const double* passes, int split_rows, int wide_lanes, int capacity,
+                    int* sys_class, int* lane_width, int* nlanes) {
+  if (nsys < 0 || (nsys > 0 && !rows) || split_rows <= 0 || split_rows > kBlockMaxRows || wide_lanes <= 0 ||
+      capacity <= 0 || !nlanes) {
     set_error("mgpu_batch_plan: invalid argument");
     return MGPU_E_ARG;
   }
   const std::vector<int> n(rows, rows + nsys);
   std::vector<double> ps(nsys);
   for (int i = 0; i < nsys; ++i) ps[i] = passes ? passes[i] : model_passes(n[i], true, g_cheb_degree);
-  const Policy P{barrier_ns * 1e-3, row_ps * 1e-6};
-  const auto plan = plan_lanes(n, ps, P, capacity);
-  int lane_id = 0;
-  double mk = 0.0;
-  for (const auto& lanes : plan)
-    for (const auto& L : lanes) {
-      for (int i : L.items) {
-        if (width) width[i] = L.width;
-        if (lane) lane[i] = lane_id;
-      }
-      mk = std::max(mk, L.load);
-      ++lane_id;
-    }
-  if (makespan_us) *makespan_us = mk;
+  const LaneSet L = plan_lanes(n, ps, Policy{split_rows, wide_lanes}, capacity);
+  for (int c = 0; c < 2; ++c)
+    for (int i : L.queue[c])
+      if (sys_class) sys_class[i] = c;
+  for (size_t j = 0; j < L.width.size(); ++j)
+    if (lane_width) lane_width[j] = L.width[j];
+  *nlanes = (int)L.width.size();
   return 0;
 }
 
@@ -903,8 +869,8 @@ int mgpu_batch_info(const MgpuBatch* b, MgpuBatchInfo* info) {
   if (!b || !info) return MGPU_E_ARG;
   MgpuBatchInfo r{};
   r.ncases = (int)b->cases.size();
-  r.barrier_ns = (int32_t)std::lround(b->policy.bar_us * 1e3);
-  r.row_ps = (int32_t)std::lround(b->policy.row_us * 1e6);
+  r.split_rows = b->policy.split_rows;
+  r.wide_lanes = b->policy.wide_lanes;
   r.autotuned = b->policy_tuned ? 1 : 0;
   r.graph = b->exec ? 1 : 0;
   r.launches_per_iter = b->launches_per_iter;

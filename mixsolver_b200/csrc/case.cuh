@@ -97,10 +97,11 @@ struct alignas(16) BatchSys {
   MixedArgs m;
 };
 
-// A lane of a batched launch: nblocks co-resident blocks that solve the
-// systems items[first_item .. first_item+nitems) one after the other.
+// A lane of a batched launch: nblocks co-resident blocks that solve systems
+// one after the other, taken from the queue of its width class (cls) and,
+// once that is empty, from the queues of narrower classes.
 struct BatchLane {
-  int first_block, nblocks, first_item, nitems;
+  int first_block, nblocks, cls, pad;
 };
 
 // Device tables of one batched Krylov launch.
@@ -108,11 +109,14 @@ struct LanePlan {
   const BatchSys* sys;
   const BatchLane* lanes;
   const int* block_lane;
-  const int* items;
-  unsigned long long* bars;  // one barrier counter per lane
-  double* partials;          // 8 doubles per block
-  unsigned long long* lane_t;  // optional: start and end time (ns) of each lane
-  int nlanes, nblocks;
+  const int* q_items;         // systems of every class queue, longest first
+  const int* q_start;         // class c's queue: q_items[q_start[c] .. q_start[c + 1])
+  int* q_head;                // next position of each class queue (zeroed per launch)
+  int* lane_slot;             // two slots per lane: the system its blocks run next
+  unsigned long long* bars;   // one barrier counter per lane
+  double* partials;           // 8 doubles per block
+  unsigned long long* lane_t; // optional: start and end time (ns) of each lane
+  int ncls, nlanes, nblocks;
 };
 
 struct DeviceCase {

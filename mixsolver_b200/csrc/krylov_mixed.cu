@@ -396,8 +396,7 @@ __device__ __forceinline__ bool cheb_apply(const KrylovArgs& a, const MixedArgs&
       MGPU_SPLIT_FULL(rows, base, FULL, {
         float az[kRows];
         spmv32_rows<L1, ELL, FULL>(a, m, zc, ii, in, az);
-#pragma unroll
-        for (int r = 0; r < kRows; ++r) {
+_Pragma("unroll") for (int r = 0; r < kRows; ++r) {
           const int i = ii[r];
           double c[2] = {0.0, 0.0};
           if (FULL || in[r]) {
@@ -441,8 +440,7 @@ __device__ __forceinline__ void pcg_fused_pass(const KrylovArgs& a, const MixedA
     MGPU_SPLIT_FULL(rows, base, FULL, {
       float az[kRows];
       spmv32_rows<L1, ELL, FULL>(a, S, z, ii, in, az);
-#pragma unroll
-      for (int r = 0; r < kRows; ++r) {
+_Pragma("unroll") for (int r = 0; r < kRows; ++r) {
         const int i = ii[r];
         double c[1] = {0.0};
         if (FULL || in[r]) {
@@ -467,8 +465,7 @@ __device__ __forceinline__ void bicg_v_pass(const KrylovArgs& a, const MixedArgs
     MGPU_SPLIT_FULL(rows, base, FULL, {
       float vv[kRows];
       spmv32_rows<L1, ELL, FULL>(a, S, ph, ii, in, vv);
-#pragma unroll
-      for (int r = 0; r < kRows; ++r) {
+_Pragma("unroll") for (int r = 0; r < kRows; ++r) {
         const int i = ii[r];
         double c[1] = {0.0};
         if (FULL || in[r]) {
@@ -490,8 +487,7 @@ __device__ __forceinline__ void bicg_t_pass(const KrylovArgs& a, const MixedArgs
     MGPU_SPLIT_FULL(rows, base, FULL, {
       float tv[kRows];
       spmv32_rows<L1, ELL, FULL>(a, S, sh, ii, in, tv);
-#pragma unroll
-      for (int r = 0; r < kRows; ++r) {
+_Pragma("unroll") for (int r = 0; r < kRows; ++r) {
         const int i = ii[r];
         double c[2] = {0.0, 0.0};
         if (FULL || in[r]) {
@@ -832,43 +828,54 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
   return t;
 }
 
-// Separate (not inlined) bodies per lane kind: each gets its own register
-// allocation instead of one allocation for all of them inlined together.
-template <bool PCG, bool L1, bool ELL>
-__device__ __noinline__ void batch_body(const BatchSys& S, VGrid& g) {
-  if constexpr (PCG)
-    pcg_mixed_body<L1, ELL>(S.a, S.m, g);
-  else
-    bicgstab_mixed_body<L1, ELL>(S.a, S.m, g);
+// Next system of a lane: its own class queue first, then narrower classes.
+__device__ __forceinline__ int lane_fetch(const LanePlan& p, int cls) {
+  for (int c = cls; c < p.ncls; ++c) {
+    const int k = atomicAdd(&p.q_head[c], 1);
+    if (k < p.q_start[c + 1] - p.q_start[c]) return p.q_items[p.q_start[c] + k];
+  }
+  return -1;
 }
 
 // Batched solves. The launch is split into lanes; a lane is a group of
-// co-resident blocks with its own barrier counter and max partials, and it
-// solves its list of systems one after the other. A lane of one block runs
-// with L1-coherent loads, a wider lane with L2 loads and group barriers. Each
-// system's descriptor is staged in shared memory.
+// co-resident blocks with its own barrier counter and max partials. Its first
+// block takes the lane's next system from the class queues and publishes it
+// in a lane slot (two slots, alternating, so a block still reading one slot
+// is never overwritten); the lane barrier makes it visible to the lane's
+// other blocks. Every lane runs the multi-block body (L2 loads; a lane of one
+// block synchronises with __syncthreads): one body per kernel, inlined, with
+// the system's descriptor read through a read-only pointer, keeps the
+// descriptor fields out of the register budget.
 template <bool PCG, bool ELL>
 __global__ void __launch_bounds__(256, 2) k_mixed_batch(LanePlan p) {
-  __shared__ __align__(16) unsigned char raw[sizeof(BatchSys)];
+  __shared__ int s_idx;
   const int li = p.block_lane[blockIdx.x];
   const BatchLane L = p.lanes[li];
   VGrid g{L.nblocks, (int)blockIdx.x - L.first_block, p.bars + li, p.partials + 8l * L.first_block, 0};
   if (p.lane_t && g.rank == 0 && threadIdx.x == 0) p.lane_t[2 * li] = globaltimer_ns();
-  constexpr int W = (int)(sizeof(BatchSys) / 8);
-  for (int j = 0; j < L.nitems; ++j) {
-    __syncthreads();  // every thread is done with the previous descriptor
-    const long long* src = reinterpret_cast<const long long*>(p.sys + p.items[L.first_item + j]);
-    long long* dst = reinterpret_cast<long long*>(raw);
-    for (int k = threadIdx.x; k < W; k += blockDim.x) dst[k] = src[k];
+  for (int j = 0;; ++j) {
+    __syncthreads();  // every thread is done with the previous system
+    if (threadIdx.x == 0) {
+      if (g.nb == 1)
+        s_idx = lane_fetch(p, L.cls);
+      else if (g.rank == 0)
+        p.lane_slot[2 * li + (j & 1)] = lane_fetch(p, L.cls);
+    }
+    if (g.nb > 1) {
+      if (!vg_sync(g, nullptr)) break;
+      if (threadIdx.x == 0) s_idx = ld_acquire_i32(p.lane_slot + 2 * li + (j & 1));
+    }
     __syncthreads();
-    const BatchSys& S = *reinterpret_cast<const BatchSys*>(raw);
-    if (L.nblocks == 1)
-      batch_body<PCG, true, ELL>(S, g);
+    const int idx = s_idx;
+    if (idx < 0) break;
+    const BatchSys* __restrict__ S = p.sys + idx;
+    if constexpr (PCG)
+      pcg_mixed_body<false, ELL>(S->a, S->m, g);
     else
-      batch_body<PCG, false, ELL>(S, g);
+      bicgstab_mixed_body<false, ELL>(S->a, S->m, g);
     // a bounded wait of this system ran out: the lane stops (every block of
     // the lane sees the flag at its next barrier at the latest)
-    if (ld_acquire_i32(&S.a.st->timeout) != 0) break;
+    if (ld_acquire_i32(&S->a.st->timeout) != 0) break;
   }
   if (p.lane_t && g.rank == 0 && threadIdx.x == 0) p.lane_t[2 * li + 1] = globaltimer_ns();
 }
@@ -948,6 +955,7 @@ int launch_mixed_batch(const LanePlan& p, bool pcg, bool ell, cudaStream_t s) {
     return MGPU_E_ARG;
   }
   cudaError_t e = cudaMemsetAsync(p.bars, 0, sizeof(unsigned long long) * (size_t)p.nlanes, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(p.q_head, 0, sizeof(int) * (size_t)p.ncls, s);
   if (e != cudaSuccess) return cuda_fail(e, "lane barrier reset", __FILE__, __LINE__);
   LanePlan pp = p;
   void* args[] = {(void*)&pp};

@@ -50,7 +50,10 @@ __device__ __forceinline__ VGrid whole_grid(unsigned long long* bar, double* par
 // Bounded barrier of a group over a monotone 64-bit arrival counter (zeroed
 // before every launch; all blocks of the group are co-resident). Each block
 // adds one arrival and waits until the counter reaches the end of the current
-// round. Returns false when the wait ran out; the caller then leaves the kernel.
+// round. While it waits it looks at the status every 4096 polls: once any
+// block has flagged a timeout (st may be null: no status) the wait ends. A
+// wait that runs out flags the timeout. Returns false in both cases; the
+// caller then leaves the kernel.
 __device__ bool vg_sync(const VGrid& g, DevStatus* st) {
   __shared__ int s_ok;
   if (g.nb == 1) {
@@ -67,15 +70,19 @@ __device__ bool vg_sync(const VGrid& g, DevStatus* st) {
     const unsigned long long target = (old / nb + 1ull) * nb;
     unsigned spins = 0;
     while (ld_acquire_u64(bar) < target) {
-      if (++spins > 256u) __nanosleep(64);
+      ++spins;
+      if (spins > 256u) __nanosleep(64);
+      if ((spins & 4095u) == 0 && st && ld_acquire_i32(&st->timeout) != 0) {
+        ok = 0;
+        break;
+      }
       if (spins > kSpinLimit) {
-        atomicExch(&st->timeout, 1);
+        if (st) atomicExch(&st->timeout, 1);
         ok = 0;
         break;
       }
     }
     __threadfence();
-    if (ok && ld_acquire_i32(&st->timeout) != 0) ok = 0;
     s_ok = ok;
   }
   __syncthreads();

@@ -154,17 +154,18 @@ class UnsCase:
         return ier.value, records_to_list(recs, min(nrec.value, logcap))
 
 
-def batch_plan(rows, barrier_ns: int, row_ps: int, capacity: int, passes=None):
-    """Lane plan of a batched Krylov phase (host only): per system its lane
-    width and lane, and the modelled makespan in microseconds."""
+def batch_plan(rows, split_rows: int, wide_lanes: int, capacity: int, passes=None):
+    """Lane plan of a batched Krylov phase (host only): per system its class
+    (0 wide lanes, 1 single-block lanes) and the widths of the lanes."""
     r = np.ascontiguousarray(rows, np.int32)
     p = None if passes is None else np.ascontiguousarray(passes, np.float64)
-    w = np.zeros(len(r), np.int32); ln = np.zeros(len(r), np.int32)
-    mk = C.c_double(0.0)
+    cls = np.zeros(len(r), np.int32)
+    widths = np.zeros(max(int(capacity), 1), np.int32)
+    nl = C.c_int(0)
     lib = _lib()
-    abi.check(lib, lib.mgpu_batch_plan(len(r), iptr(r), dptr(p), int(barrier_ns), int(row_ps), int(capacity),
-                                       iptr(w), iptr(ln), C.byref(mk)), "mgpu_batch_plan")
-    return w, ln, mk.value
+    abi.check(lib, lib.mgpu_batch_plan(len(r), iptr(r), dptr(p), int(split_rows), int(wide_lanes), int(capacity),
+                                       iptr(cls), iptr(widths), C.byref(nl)), "mgpu_batch_plan")
+    return cls, widths[:nl.value].copy()
 
 
 class CaseBatch:
@@ -190,10 +191,10 @@ class CaseBatch:
         except Exception:
             pass
 
-    def set_policy(self, barrier_ns: int, row_ps: int):
-        """Fixed lane policy (cost-model constants); (0, 0) = autotune."""
+    def set_policy(self, split_rows: int, wide_lanes: int):
+        """Fixed lane policy (row threshold, wide lanes); (0, 0) = autotune."""
         lib = _lib()
-        abi.check(lib, lib.mgpu_batch_set_policy(self.h, int(barrier_ns), int(row_ps)), "mgpu_batch_set_policy")
+        abi.check(lib, lib.mgpu_batch_set_policy(self.h, int(split_rows), int(wide_lanes)), "mgpu_batch_set_policy")
 
     def step(self, iters: int) -> int:
         """Advance every running member; returns how many still run."""

@@ -103,14 +103,14 @@ def test_mixed_batch_bit_identical_to_single_mixed_runs():
             assert np.array_equal(f[k], f1[k]), (k, rel(f[k], f1[k]))
 
 
-@pytest.mark.parametrize("policy", [(100, 50000), (20000, 500)])
+@pytest.mark.parametrize("policy", [(64, 2), (32768, 1)])
 def test_result_same_alone_and_in_the_mix(policy):
-    """(100 ns, 50 ns/row): barriers cheap, rows dear -> wide lanes;
-    (20 us, 0.5 ns/row): barriers dear -> single-block lanes. Either way each
-    member's result is the one it gets alone."""
+    """(64, 2): every member on one of two wide lanes; (32768, 1): every
+    member on a single-block lane. Either way each member's result is the one
+    it gets alone."""
     specs = _cavities(abi.PREC_MIXED, sizes=(9, 5, 11, 7), iters=8)
     mix, _ = _batched(specs, [0] * 4, 8, policy=policy)
-    alone, _ = _batched([specs[2]], [0], 8, policy=(1500, 6000))
+    alone, _ = _batched([specs[2]], [0], 8, policy=(64, 4))
     for k in ("u", "p", "flux"):
         assert np.array_equal(mix[2][2][k], alone[0][2][k]), k
     assert [r["lin_it"] for r in mix[2][1]] == [r["lin_it"] for r in alone[0][1]]
@@ -190,7 +190,7 @@ def test_step_and_poll_interface():
     objs = [S.UnsCase(m, c) for m, c in specs]
     assert objs[0].begin(0, 3) == 0
     assert objs[1].begin(0) == 0
-    B = S.CaseBatch(objs, policy=(1500, 6000))
+    B = S.CaseBatch(objs, policy=(16384, 8))
     assert B.step(2) == 2
     assert B.step(2) == 1          # the first member stopped at 3 iterations
     assert list(B.poll()) == [1, 0]

@@ -50,8 +50,13 @@ def parse():
     ap.add_argument("--lin-max", type=int, default=1000)
     ap.add_argument("--cpu-steps", type=int, default=2, help="oracle outer iterations for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="channel", choices=["channel", "batch"],
-                    help="channel: one 524k-cell case (default); batch: many 3-D cavities in one batch")
+    ap.add_argument("--workload", default="channel", choices=["channel", "batch", "serve"],
+                    help="channel: one 524k-cell case (default); batch: many 3-D cavities in one batch; "
+                         "serve: a Poisson stream of SIMPLE / PISO requests")
+    ap.add_argument("--rate", type=float, default=50.0, help="serve: arrivals per second")
+    ap.add_argument("--duration", type=float, default=2.0, help="serve: seconds of arrivals (mixed leg)")
+    ap.add_argument("--fp64-duration", type=float, default=0.5, help="serve: seconds of arrivals (FP64 leg)")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serve: device memory for resident cases")
     ap.add_argument("--cases", type=int, default=256, help="batch: number of cavity cases")
     ap.add_argument("--policy", default="auto", help="batch: lane policy SPLIT_ROWSxWIDE_LANES or auto")
     ap.add_argument("--fp64-iters", type=int, default=2, help="batch: iterations of the FP64 comparison leg")
@@ -493,11 +498,129 @@ def run_batch(args):
         print(json.dumps(out), flush=True)
 
 
+# mesh pool of the served workload: jittered-hex cavities (SIMPLE) and
+# hex-split-tet boxes (PISO) with cell counts spread over [1e4, 2e6]
+SERVE_HEX_EDGES = (22, 30, 41, 56, 77, 105, 126)
+SERVE_TET_EDGES = (12, 17, 24, 34, 48, 69)
+
+
+def _serve_mesh(spec):
+    from mixsolver_b200 import meshgen
+    kind, e = spec
+    if kind == "hex":
+        return meshgen.sort_faces(meshgen.box_hex(e, e, e, jitter=0.10, seed=e, zones=(5, 5, 5, 5, 5, 5)))
+    return meshgen.box_tet(e, wall_zone=4)
+
+
+def serve_requests(duration, rate, pool, prec, seed=0):
+    """Seeded Poisson arrivals: 70 % SIMPLE steady solves (50 outer
+    iterations, lid-driven jittered-hex cavity), 30 % PISO batches (10 steps,
+    dt = 1e-3, 2 correctors, Taylor-Green start in a walled hex-split-tet box);
+    cells log-uniform in [1e4, 2e6] (nearest pool mesh), Re uniform in [50, 2000]."""
+    import copy
+    from mixsolver_b200 import abi, serve
+    from mixsolver_b200.abi import BC_WALL, MOM_JACOBI, PPE_IC0, BcSpec, Ctrl
+    rng = np.random.default_rng(seed)
+    reqs, t, k = [], 0.0, 0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration:
+            break
+        piso = rng.random() < 0.3
+        cells = float(np.exp(rng.uniform(np.log(1e4), np.log(2e6))))
+        re = float(rng.uniform(50.0, 2000.0))
+        kind = "tet" if piso else "hex"
+        mesh, xc = min(pool[kind], key=lambda mx: abs(np.log(mx[0].ncells / cells)))
+        if piso:
+            ctrl = Ctrl(rho=1.0, mu=1.0 / re, outer_max=1, lin_tol=1e-8, lin_max=1000, ppe_precond=PPE_IC0,
+                        mom_solver=MOM_JACOBI, transient=True, time_scheme=1, dt=1e-3, n_time_max=10, n_correct=2,
+                        bcs=[BcSpec(zone=4, btype=BC_WALL)])
+            from mixsolver_b200 import meshgen
+            u0 = meshgen.taylor_green(xc, seed=k)
+        else:
+            ctrl = Ctrl(rho=1.0, mu=1.0 / re, alpha_u=0.7, alpha_p=0.3, outer_max=50, outer_tol=0.0, lin_tol=1e-8,
+                        lin_max=1000, ppe_precond=PPE_IC0, mom_solver=MOM_JACOBI,
+                        bcs=[BcSpec(zone=5, btype=BC_WALL, lid=(2, 1.0, (1.0, 0.0, 0.0)))])
+            u0 = None
+        ctrl.precision = prec
+        reqs.append(serve.Request(rid=k, arrival=t, mode=1 if piso else 0, mesh=mesh, ctrl=ctrl,
+                                  nsteps=10 if piso else 50, u0=u0))
+        k += 1
+    return reqs
+
+
+def run_serve(args):
+    """Served workload: requests arrive as a Poisson stream while others are on
+    the GPU; cases stay resident in HBM, are admitted against a memory budget,
+    and are stepped by continuous batching. `value` is completed requests per
+    second; p50 / p99 latency (arrival to result) beside it, for the mixed form
+    and for the plain FP64 form (a shorter stream)."""
+    rank, world, local = dist_env()
+    import multiprocessing as mp
+    import torch
+    specs = [("hex", e) for e in SERVE_HEX_EDGES] + [("tet", e) for e in SERVE_TET_EDGES]
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(min(13, os.cpu_count() or 1)) as pool:
+        meshes = pool.map(_serve_mesh, specs)
+    torch.cuda.set_device(local)
+    from mixsolver_b200 import abi, serve
+    from mixsolver_b200 import solver as S
+    mpool = {"hex": [], "tet": []}
+    for (kind, _), m in zip(specs, meshes):
+        xc = S.compute_geometry(m)["xc"] if kind == "tet" else None
+        mpool[kind].append((m, xc))
+    t_pool = time.perf_counter() - t0
+    budget = args.budget_gb * 1e9
+    legs = {}
+    for name, prec, dur in (("mixed", abi.PREC_MIXED, args.duration), ("fp64", abi.PREC_FP64, args.fp64_duration)):
+        reqs = serve_requests(dur, args.rate, mpool, prec, seed=rank)
+        srv = serve.Server(serve.GpuBackend(device=local, policy=(32768, 4)), budget_bytes=budget,
+                           active_cells=16_000_000, tick_iters=5)
+        with ClockSampler(local) as clk:
+            w0 = time.perf_counter()
+            out = srv.run(reqs)
+            wall = time.perf_counter() - w0
+        sm = serve.summary(out, wall)
+        sm.update({"wall_s": wall, "arrival_window_s": dur, "ticks": srv.ticks, "batches_built": srv.batches_built,
+                   "peak_resident_gb": srv.peak_resident_bytes / 1e9,
+                   "cells_min": min(r.cells for r in out), "cells_max": max(r.cells for r in out),
+                   "simple": sum(1 for r in out if r.mode == 0), "piso": sum(1 for r in out if r.mode == 1),
+                   "failed": [(r.rid, r.ier, r.error) for r in out if r.ier != 0 or r.error][:5],
+                   "loop_s": {"build": srv.t_build, "step": srv.t_step, "finish": srv.t_finish},
+                   "per_request": [(r.rid, r.mode, r.cells, round(r.arrival, 3), round(r.admitted, 3),
+                                    round(r.finished, 3), r.nrec) for r in out][:60],
+                   "clocks": clk.summary()})
+        legs[name] = sm
+    mx = legs["mixed"]
+    out = {
+        "metric": "served SIMPLE/PISO requests: throughput with p50/p99 latency (mixed precision)",
+        "value": mx["throughput_req_s"], "unit": "req/s", "n_gpus": world, "steps": mx["requests"], "warmup": 0,
+        "ms_per_step": 1e3 * mx["wall_s"] / max(mx["completed"], 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32-inner/f64-refinement",
+        "data": "synthetic (seeded Poisson arrivals, jittered-hex and hex-split-tet meshes)",
+        "config": {"workload": f"Poisson arrivals at {args.rate}/s: 70% SIMPLE (50 outer iterations, lid-driven "
+                               "jittered-hex cavity), 30% PISO (10 steps, dt 1e-3, Taylor-Green hex-split-tet box); "
+                               "cells log-uniform in [1e4, 2e6] (pool of 13 meshes), Re uniform in [50, 2000]",
+                   "budget_gb": args.budget_gb, "mesh_pool_s": t_pool, "latency_s": {"p50": mx["p50_s"], "p99": mx["p99_s"]},
+                   "mixed": mx, "fp64": legs["fp64"],
+                   "note": "the arrival rate exceeds the GPU's service rate: latency grows with the queue"},
+        "roofline": None,
+        "e2e": {"value": mx["throughput_req_s"], "unit": "req/s", "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": None},
+        "gpu_launches": None,
+        "clocks": mx["clocks"],
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         run_reference(a)
     elif a.workload == "batch":
         run_batch(a)
+    elif a.workload == "serve":
+        run_serve(a)
     else:
         run_ours(a)

@@ -231,15 +231,34 @@ constexpr int kRows = MGPU_KROWS;
 // in kernel-parameter space (single-system kernels) or shared memory (the
 // batched kernel): no register holds a field between uses.
 // FULL: every row of the step is below n (no per-entry row check).
+// What an FP32 SpMV pass reads, copied once per pass into registers from
+// wherever the solve's arguments live (kernel parameters, or a batch's
+// descriptor table in global memory); the restrict qualifiers tell the
+// compiler that the pass's stores do not touch them, so no field is reloaded
+// per row.
+struct Sp32 {
+  int n, w;
+  const int* __restrict__ ecol;
+  const float* __restrict__ eval;
+  const int* __restrict__ rp;
+  const int* __restrict__ col;
+  const float* __restrict__ a32;
+  const float* __restrict__ dinv;
+};
+
+__device__ __forceinline__ Sp32 sp32_of(const KrylovArgs& a, const MixedArgs& m) {
+  return Sp32{a.n, m.ell_w, m.ell_col, m.ell_val, a.row_ptr, a.col, m.a32, m.dinv};
+}
+
 template <bool L1, bool ELL, bool FULL>
-__device__ __forceinline__ void spmv32_rows(const KrylovArgs& a, const MixedArgs& S, const float* x,
-                                            const int (&i)[kRows], const bool (&in0)[kRows], float (&y)[kRows]) {
+__device__ __forceinline__ void spmv32_rows(const Sp32& S, const float* x, const int (&i)[kRows],
+                                            const bool (&in0)[kRows], float (&y)[kRows]) {
   bool in[kRows];
 #pragma unroll
   for (int r = 0; r < kRows; ++r) in[r] = FULL || in0[r];
   if constexpr (ELL) {
     constexpr int WMAX = 8;
-    const int W = S.ell_w, n = a.n;
+    const int W = S.w, n = S.n;
     float v[kRows][WMAX], xv[kRows][WMAX];
     int c[kRows][WMAX];
 #pragma unroll
@@ -247,8 +266,8 @@ __device__ __forceinline__ void spmv32_rows(const KrylovArgs& a, const MixedArgs
 #pragma unroll
       for (int t = 0; t < WMAX; ++t)
         if (t < W && in[r]) {
-          c[r][t] = S.ell_col[(long)t * n + i[r]];
-          v[r][t] = S.ell_val[(long)t * n + i[r]];
+          c[r][t] = S.ecol[(long)t * n + i[r]];
+          v[r][t] = S.eval[(long)t * n + i[r]];
         }
 #pragma unroll
     for (int r = 0; r < kRows; ++r)
@@ -265,7 +284,7 @@ __device__ __forceinline__ void spmv32_rows(const KrylovArgs& a, const MixedArgs
     }
   } else {
 #pragma unroll
-    for (int r = 0; r < kRows; ++r) y[r] = in[r] ? spmv32_csr<L1, 8>(a.row_ptr, a.col, S.a32, x, i[r]) : 0.0f;
+    for (int r = 0; r < kRows; ++r) y[r] = in[r] ? spmv32_csr<L1, 8>(S.rp, S.col, S.a32, x, i[r]) : 0.0f;
   }
 }
 
@@ -381,6 +400,7 @@ template <bool L1, bool ELL>
 __device__ __forceinline__ bool cheb_apply(const KrylovArgs& a, const MixedArgs& m, VGrid& g, Red& R,
                                            const Rows& rows, const float* rr, float* dch, float* z0, float* z1,
                                            double lmax, float*& zout, double (&red)[2]) {
+  const Sp32 S = sp32_of(a, m);
   const double lmin = lmax / m.cheb_ratio;
   const double th = 0.5 * (lmax + lmin), de = 0.5 * (lmax - lmin), sg = th / de;
   double rho0 = 1.0 / sg;
@@ -395,12 +415,12 @@ __device__ __forceinline__ bool cheb_apply(const KrylovArgs& a, const MixedArgs&
       MGPU_STEP_ROWS(rows, base, ii, in);
       MGPU_SPLIT_FULL(rows, base, FULL, {
         float az[kRows];
-        spmv32_rows<L1, ELL, FULL>(a, m, zc, ii, in, az);
+        spmv32_rows<L1, ELL, FULL>(S, zc, ii, in, az);
 _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
           const int i = ii[r];
           double c[2] = {0.0, 0.0};
           if (FULL || in[r]) {
-            const float res = m.dinv[i] * (rr[i] - az[r]);
+            const float res = S.dinv[i] * (rr[i] - az[r]);
             const float dn = fmaf(c1, dch[i], c2 * res);
             dch[i] = dn;
             const float zi = zc[i] + dn;
@@ -432,14 +452,15 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
 
 // p := z + beta p, q := A z + beta q (p := z, q := A z when first); p.q
 template <bool L1, bool ELL>
-__device__ __forceinline__ void pcg_fused_pass(const KrylovArgs& a, const MixedArgs& S, const Red& R,
+__device__ __forceinline__ void pcg_fused_pass(const KrylovArgs& a, const MixedArgs& m, const Red& R,
                                                const Rows& rows, const float* z, float* p, float* q, float beta,
                                                bool first) {
+  const Sp32 S = sp32_of(a, m);
   MGPU_STEPS(rows, base) {
     MGPU_STEP_ROWS(rows, base, ii, in);
     MGPU_SPLIT_FULL(rows, base, FULL, {
       float az[kRows];
-      spmv32_rows<L1, ELL, FULL>(a, S, z, ii, in, az);
+      spmv32_rows<L1, ELL, FULL>(S, z, ii, in, az);
 _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
         const int i = ii[r];
         double c[1] = {0.0};
@@ -458,13 +479,14 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
 
 // v := A ph; r0.v
 template <bool L1, bool ELL>
-__device__ __forceinline__ void bicg_v_pass(const KrylovArgs& a, const MixedArgs& S, const Red& R, const Rows& rows,
+__device__ __forceinline__ void bicg_v_pass(const KrylovArgs& a, const MixedArgs& m, const Red& R, const Rows& rows,
                                             const float* ph, const float* r0, float* v) {
+  const Sp32 S = sp32_of(a, m);
   MGPU_STEPS(rows, base) {
     MGPU_STEP_ROWS(rows, base, ii, in);
     MGPU_SPLIT_FULL(rows, base, FULL, {
       float vv[kRows];
-      spmv32_rows<L1, ELL, FULL>(a, S, ph, ii, in, vv);
+      spmv32_rows<L1, ELL, FULL>(S, ph, ii, in, vv);
 _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
         const int i = ii[r];
         double c[1] = {0.0};
@@ -480,13 +502,14 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
 
 // t := A sh; t.t and t.s
 template <bool L1, bool ELL>
-__device__ __forceinline__ void bicg_t_pass(const KrylovArgs& a, const MixedArgs& S, const Red& R, const Rows& rows,
+__device__ __forceinline__ void bicg_t_pass(const KrylovArgs& a, const MixedArgs& m, const Red& R, const Rows& rows,
                                             const float* sh, const float* s, float* t) {
+  const Sp32 S = sp32_of(a, m);
   MGPU_STEPS(rows, base) {
     MGPU_STEP_ROWS(rows, base, ii, in);
     MGPU_SPLIT_FULL(rows, base, FULL, {
       float tv[kRows];
-      spmv32_rows<L1, ELL, FULL>(a, S, sh, ii, in, tv);
+      spmv32_rows<L1, ELL, FULL>(S, sh, ii, in, tv);
 _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
         const int i = ii[r];
         double c[2] = {0.0, 0.0};
@@ -513,6 +536,7 @@ __device__ void pcg_mixed_body(const KrylovArgs& a, const MixedArgs& m, VGrid& g
     return;
   }
   const Rows rows = block_rows(n, g);
+  const float* __restrict__ dinv = m.dinv;
   Red R = make_red(m, n);
   float *rr = m.w32, *zA = m.w32 + n, *p = m.w32 + 2l * n, *q = m.w32 + 3l * n, *d = m.w32 + 4l * n;
   float *dch = m.w32 + 5l * n, *zB = m.w32 + 6l * n;
@@ -571,11 +595,11 @@ __device__ void pcg_mixed_body(const KrylovArgs& a, const MixedArgs& m, VGrid& g
           rr[i] = ri;
           d[i] = 0.0f;
           if (cheb) {
-            const float di = m.dinv[i] * ri * inv_th;
+            const float di = dinv[i] * ri * inv_th;
             dch[i] = di;
             zA[i] = di;
           } else {
-            const float zi = m.dinv[i] * ri;
+            const float zi = dinv[i] * ri;
             zA[i] = zi;
             c[0] = (double)ri * (double)zi;
             c[1] = (double)ri * (double)ri;
@@ -604,11 +628,11 @@ __device__ void pcg_mixed_body(const KrylovArgs& a, const MixedArgs& m, VGrid& g
           const float ri = fmaf(-af, q[i], rr[i]);
           rr[i] = ri;
           if (cheb) {
-            const float di = m.dinv[i] * ri * inv_th;
+            const float di = dinv[i] * ri * inv_th;
             dch[i] = di;
             zA[i] = di;
           } else {
-            const float zi = m.dinv[i] * ri;
+            const float zi = dinv[i] * ri;
             zA[i] = zi;
             c[0] = (double)ri * (double)ri;
             c[1] = (double)ri * (double)zi;
@@ -673,6 +697,7 @@ __device__ void bicgstab_mixed_body(const KrylovArgs& a, const MixedArgs& m, VGr
     return;
   }
   const Rows rows = block_rows(n, g);
+  const float* __restrict__ dinv = m.dinv;
   Red R = make_red(m, n);
   float* W = m.w32;
   float *r = W, *r0 = W + n, *p = W + 2l * n, *v = W + 3l * n, *s = W + 4l * n, *t = W + 5l * n,
@@ -729,7 +754,7 @@ __device__ void bicgstab_mixed_body(const KrylovArgs& a, const MixedArgs& m, VGr
       for (int i = rows.start + threadIdx.x; i < rows.n; i += rows.stride) {
         const float pi = fmaf(beta, fmaf(-om, v[i], p[i]), r[i]);
         p[i] = pi;
-        ph[i] = m.dinv[i] * pi;
+        ph[i] = dinv[i] * pi;
       }
       if (!vg_sync(g, a.st)) return;
       bicg_v_pass<L1, ELL>(a, m, R, rows, ph, r0, v);
@@ -743,7 +768,7 @@ __device__ void bicgstab_mixed_body(const KrylovArgs& a, const MixedArgs& m, VGr
         if (i < rows.n) {
           const float si = fmaf(-af, v[i], r[i]);
           s[i] = si;
-          sh[i] = m.dinv[i] * si;
+          sh[i] = dinv[i] * si;
           c[0] = (double)si * (double)si;
         }
         red_put<1>(R, rows, base, c);

@@ -588,7 +588,7 @@ def run_serve(args):
                    "failed": [(r.rid, r.ier, r.error) for r in out if r.ier != 0 or r.error][:5],
                    "loop_s": {"build": srv.t_build, "step": srv.t_step, "finish": srv.t_finish},
                    "per_request": [(r.rid, r.mode, r.cells, round(r.arrival, 3), round(r.admitted, 3),
-                                    round(r.finished, 3), r.nrec) for r in out][:60],
+                                    round(r.create_s, 3), round(r.finished, 3), r.nrec) for r in out][:60],
                    "clocks": clk.summary()})
         legs[name] = sm
     mx = legs["mixed"]

@@ -241,7 +241,11 @@ int mgpu_cg_jacobi_noalloc(int n, const int32_t* d_row_ptr, const int32_t* d_col
  * "min_blocks" (least number of blocks of a multi-block solve, default 1),
  * "cheb_degree" (mixed form: degree of the Chebyshev-Jacobi pressure
  * preconditioner, 1 = plain Jacobi, default 16), "cheb_ratio" (lambda_max over
- * lambda_min of its interval, default 1000). */
+ * lambda_min of its interval, default 1000), "batch_reserve_blocks" (block
+ * slots a batched launch leaves free for other streams, so a case being set
+ * up while a batch steps is not held up behind its persistent kernels,
+ * default 0), "stream_pool" (create this many streams for cases and batches
+ * now: creating one later waits for kernels on other streams). */
 int mgpu_set_tuning(const char* key, int value);
 
 /* Timing of the last run on the case's stream (CUDA events): total device ms

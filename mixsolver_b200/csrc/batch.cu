@@ -44,9 +44,10 @@ using namespace mgpu;
 
 namespace {
 
-// Lane policy: systems of more than split_rows rows run on wide_lanes wide
-// lanes, which share the blocks given to them; the others run on single-block
-// lanes. The blocks are split between the two classes by their share of the
+// Lane policy: systems of more than split_rows rows run on wide lanes (one
+// lane per big system, sized by its work, when there are at most wide_lanes of
+// them; else wide_lanes equal lanes sharing a queue); the others run on
+// single-block lanes. The blocks are split between the two classes by their share of the
 // work. Few wide lanes keep the working sets of the big systems that run at
 // the same time within L2; the small systems fit beside them. The mixed
 // solves give the same result on any lane, so the policy only affects speed.
@@ -108,8 +109,31 @@ LaneSet plan_lanes(const std::vector<int>& n, const std::vector<double>& passes,
     bs = std::max(1, std::min<int>(bs, std::min<int>((int)small.size(), cap - need)));
     bb = cap - bs;
   }
-  if (!big.empty()) {
-    const int k = std::max(1, std::min(std::min(P.wide_lanes, (int)big.size()), bb / need));
+  if (!big.empty() && (int)big.size() <= P.wide_lanes) {
+    // one lane per big system, widths in proportion to their work, so that
+    // they finish the phase together (each at least its least width)
+    std::vector<int> w(big.size());
+    int used = 0;
+    for (size_t j = 0; j < big.size(); ++j) {
+      w[j] = std::max(least_width(n[big[j].second]), (int)std::floor(bb * big[j].first / wb));
+      used += w[j];
+    }
+    while (used > bb) {  // trim the widest lanes that can give a block
+      size_t jm = 0;
+      for (size_t j = 1; j < w.size(); ++j)
+        if (w[j] - least_width(n[big[j].second]) > w[jm] - least_width(n[big[jm].second])) jm = j;
+      if (w[jm] <= least_width(n[big[jm].second])) break;
+      --w[jm];
+      --used;
+    }
+    for (size_t j = 0; used < bb; j = (j + 1) % w.size(), ++used) ++w[j];  // spare blocks, most work first
+    for (size_t j = 0; j < w.size(); ++j) {
+      L.width.push_back(w[j]);
+      L.cls.push_back(0);
+    }
+  } else if (!big.empty()) {
+    // more big systems than wide lanes: equal lanes sharing one queue
+    const int k = std::max(1, std::min(P.wide_lanes, bb / need));
     for (int j = 0; j < k; ++j) {
       L.width.push_back(bb / k + (j < bb % k ? 1 : 0));
       L.cls.push_back(0);
@@ -134,10 +158,12 @@ __global__ void k_batch_flags(const BatchCase* __restrict__ cases, int n, int* f
   if (st->timeout) atomicAdd(&flags[n + 1], 1);
 }
 
+// Batch tables live in stream-ordered memory on the batch's stream: freeing
+// them never waits for other streams' work.
 template <typename T>
-int dev_alloc(T*& p, size_t n) {
+int dev_alloc(T*& p, size_t n, cudaStream_t s) {
   p = nullptr;
-  MGPU_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+  MGPU_CUDA(cudaMallocAsync((void**)&p, std::max<size_t>(n, 1) * sizeof(T), s));
   return 0;
 }
 
@@ -199,13 +225,13 @@ struct MgpuBatch {
   int64_t profiled_iters = 0;
 
   void free_launch(BatchLaunch& L) {
-    for (void* p : L.owned) cudaFree(p);
+    for (void* p : L.owned) cudaFreeAsync(p, stream);
     L.owned.clear();
   }
   void free_phases() {
     for (auto& ph : phases) {
       for (auto& L : ph.launches) free_launch(L);
-      if (ph.d_sys) cudaFree(ph.d_sys);
+      if (ph.d_sys) cudaFreeAsync(ph.d_sys, stream);
     }
     phases.clear();
   }
@@ -218,23 +244,23 @@ struct MgpuBatch {
   void free_tables() {
     free_graph();
     free_phases();
-    if (d_cases) cudaFree(d_cases);
+    if (d_cases) cudaFreeAsync(d_cases, stream);
     for (auto& p : d_blk)
-      if (p) cudaFree(p);
+      if (p) cudaFreeAsync(p, stream);
     d_cases = nullptr;
     for (auto& p : d_blk) p = nullptr;
     prepared = false;
   }
   ~MgpuBatch() {
     free_tables();
-    if (d_bars) cudaFree(d_bars);
-    if (d_part) cudaFree(d_part);
-    if (d_flags) cudaFree(d_flags);
-    if (d_lane_t) cudaFree(d_lane_t);
+    if (d_bars) cudaFreeAsync(d_bars, stream);
+    if (d_part) cudaFreeAsync(d_part, stream);
+    if (d_flags) cudaFreeAsync(d_flags, stream);
+    if (d_lane_t) cudaFreeAsync(d_lane_t, stream);
     for (auto e : pev) cudaEventDestroy(e);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
-    if (stream) cudaStreamDestroy(stream);
+    if (stream) release_stream(stream);
   }
 };
 
@@ -259,7 +285,7 @@ int build_launches(MgpuBatch* b, BatchPhase& ph, const Policy& P) {
       }
     }
     if (items.empty()) continue;
-    const int cap = batch_capacity(ph.pcg, ell == 1);
+    const int cap = std::max(1, batch_capacity(ph.pcg, ell == 1) - g_batch_reserve);
     const LaneSet ls = plan_lanes(n, passes, P, cap);
     std::vector<BatchLane> hl;
     std::vector<int> block_lane, q_items, q_start;
@@ -278,22 +304,22 @@ int build_launches(MgpuBatch* b, BatchPhase& ph, const Policy& P) {
     L.ell = ell == 1;
     BatchLane* dl = nullptr;
     int *dbl = nullptr, *dqi = nullptr, *dqs = nullptr, *dqh = nullptr, *dslot = nullptr;
-    TRY(dev_alloc(dl, hl.size()));
+    TRY(dev_alloc(dl, hl.size(), b->stream));
     L.owned.push_back(dl);
-    TRY(dev_alloc(dbl, block_lane.size()));
+    TRY(dev_alloc(dbl, block_lane.size(), b->stream));
     L.owned.push_back(dbl);
-    TRY(dev_alloc(dqi, q_items.size()));
+    TRY(dev_alloc(dqi, q_items.size(), b->stream));
     L.owned.push_back(dqi);
-    TRY(dev_alloc(dqs, q_start.size()));
+    TRY(dev_alloc(dqs, q_start.size(), b->stream));
     L.owned.push_back(dqs);
-    TRY(dev_alloc(dqh, (size_t)ncls));
+    TRY(dev_alloc(dqh, (size_t)ncls, b->stream));
     L.owned.push_back(dqh);
-    TRY(dev_alloc(dslot, 2 * hl.size()));
+    TRY(dev_alloc(dslot, 2 * hl.size(), b->stream));
     L.owned.push_back(dslot);
-    MGPU_CUDA(cudaMemcpy(dl, hl.data(), sizeof(BatchLane) * hl.size(), cudaMemcpyHostToDevice));
-    MGPU_CUDA(cudaMemcpy(dbl, block_lane.data(), sizeof(int) * block_lane.size(), cudaMemcpyHostToDevice));
-    MGPU_CUDA(cudaMemcpy(dqi, q_items.data(), sizeof(int) * q_items.size(), cudaMemcpyHostToDevice));
-    MGPU_CUDA(cudaMemcpy(dqs, q_start.data(), sizeof(int) * q_start.size(), cudaMemcpyHostToDevice));
+    MGPU_CUDA(cudaMemcpyAsync(dl, hl.data(), sizeof(BatchLane) * hl.size(), cudaMemcpyHostToDevice, b->stream));
+    MGPU_CUDA(cudaMemcpyAsync(dbl, block_lane.data(), sizeof(int) * block_lane.size(), cudaMemcpyHostToDevice, b->stream));
+    MGPU_CUDA(cudaMemcpyAsync(dqi, q_items.data(), sizeof(int) * q_items.size(), cudaMemcpyHostToDevice, b->stream));
+    MGPU_CUDA(cudaMemcpyAsync(dqs, q_start.data(), sizeof(int) * q_start.size(), cudaMemcpyHostToDevice, b->stream));
     L.plan = LanePlan{ph.d_sys, dl, dbl, dqi, dqs, dqh, dslot, b->d_bars, b->d_part, nullptr, ncls, (int)hl.size(),
                       (int)block_lane.size()};
     ph.launches.push_back(std::move(L));
@@ -368,12 +394,12 @@ int prepare(MgpuBatch* b) {
   }
   b->prepared = true;
   if (K == 0) return 0;
-  TRY(dev_alloc(b->d_cases, K));
-  MGPU_CUDA(cudaMemcpy(b->d_cases, hc.data(), sizeof(BatchCase) * K, cudaMemcpyHostToDevice));
+  TRY(dev_alloc(b->d_cases, K, b->stream));
+  MGPU_CUDA(cudaMemcpyAsync(b->d_cases, hc.data(), sizeof(BatchCase) * K, cudaMemcpyHostToDevice, b->stream));
   b->asmb.cases = b->d_cases;
   for (int r = 0; r < 4; ++r) {
-    TRY(dev_alloc(b->d_blk[r], blk[r].size()));
-    MGPU_CUDA(cudaMemcpy(b->d_blk[r], blk[r].data(), sizeof(int) * blk[r].size(), cudaMemcpyHostToDevice));
+    TRY(dev_alloc(b->d_blk[r], blk[r].size(), b->stream));
+    MGPU_CUDA(cudaMemcpyAsync(b->d_blk[r], blk[r].data(), sizeof(int) * blk[r].size(), cudaMemcpyHostToDevice, b->stream));
     b->asmb.blk_case[r] = b->d_blk[r];
     b->asmb.nblk[r] = (int)blk[r].size();
   }
@@ -401,8 +427,8 @@ int prepare(MgpuBatch* b) {
       P.mixed.push_back(k);
     }
     if (!hs.empty()) {
-      TRY(dev_alloc(P.d_sys, hs.size()));
-      MGPU_CUDA(cudaMemcpy(P.d_sys, hs.data(), sizeof(BatchSys) * hs.size(), cudaMemcpyHostToDevice));
+      TRY(dev_alloc(P.d_sys, hs.size(), b->stream));
+      MGPU_CUDA(cudaMemcpyAsync(P.d_sys, hs.data(), sizeof(BatchSys) * hs.size(), cudaMemcpyHostToDevice, b->stream));
     }
     b->phases.push_back(std::move(P));
     TRY(build_launches(b, b->phases.back(), b->policy));
@@ -429,12 +455,12 @@ int measure_passes(MgpuBatch* b) {
   const int K = (int)b->live.size();
   if (K == 0) return 0;
   int* d_its = nullptr;
-  TRY(dev_alloc(d_its, (size_t)K * MGPU_MAXSOLVE));
+  TRY(dev_alloc(d_its, (size_t)K * MGPU_MAXSOLVE, b->stream));
   k_gather_its<<<(K + 127) / 128, 128, 0, b->stream>>>(b->d_cases, K, d_its);
   std::vector<int> its((size_t)K * MGPU_MAXSOLVE);
   cudaError_t e = cudaMemcpyAsync(its.data(), d_its, sizeof(int) * its.size(), cudaMemcpyDeviceToHost, b->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
-  cudaFree(d_its);
+  cudaFreeAsync(d_its, b->stream);
   if (e != cudaSuccess) return cuda_fail(e, "iteration counts", __FILE__, __LINE__);
   std::vector<int> live_of(b->cases.size(), -1);
   for (int j = 0; j < K; ++j) live_of[b->live[j]] = j;
@@ -454,7 +480,7 @@ int measure_passes(MgpuBatch* b) {
 int profiled_iteration(MgpuBatch* b) {
   const AsmBatch& A = b->asmb;
   cudaStream_t s = b->stream;
-  if (!b->d_lane_t) TRY(dev_alloc(b->d_lane_t, 2 * (size_t)b->cap));
+  if (!b->d_lane_t) TRY(dev_alloc(b->d_lane_t, 2 * (size_t)b->cap, b->stream));
   while (b->pev.size() < 32) {
     cudaEvent_t e;
     MGPU_CUDA(cudaEventCreate(&e));
@@ -509,7 +535,7 @@ int profiled_iteration(MgpuBatch* b) {
   if (b->phases.size() > 3 && !b->phases[3].launches.empty()) {
     const LanePlan& P = b->phases[3].launches[0].plan;
     std::vector<unsigned long long> t(2 * (size_t)P.nlanes);
-    MGPU_CUDA(cudaMemcpy(t.data(), b->d_lane_t, sizeof(unsigned long long) * t.size(), cudaMemcpyDeviceToHost));
+    TRY(copy_sync(t.data(), b->d_lane_t, sizeof(unsigned long long) * t.size(), cudaMemcpyDeviceToHost, b->stream));
     double mx = 0.0, sum = 0.0;
     for (int l = 0; l < P.nlanes; ++l) {
       const double ms = (double)(t[2 * l + 1] - t[2 * l]) * 1e-6;
@@ -682,8 +708,8 @@ int mgpu_case_finish(MgpuCase* c, MgpuIterRec* log, int logcap, int* nrec, int* 
   if (nrec) *nrec = h.cur_it;
   *ier = h.ier;
   if (log && logcap > 0 && h.cur_it > 0)
-    MGPU_CUDA(cudaMemcpy(log, c->d.recs, sizeof(MgpuIterRec) * (size_t)std::min(h.cur_it, logcap),
-                         cudaMemcpyDeviceToHost));
+    TRY(copy_sync(log, c->d.recs, sizeof(MgpuIterRec) * (size_t)std::min(h.cur_it, logcap), cudaMemcpyDeviceToHost,
+                  c->stream));
   if (h.timeout) {
     set_error("a bounded device wait ran out (grid barrier)");
     return MGPU_E_TIMEOUT;
@@ -710,15 +736,16 @@ int mgpu_batch_create(MgpuCase* const* cases, int ncases, MgpuBatch** out) {
     delete b;
     return e;
   };
-  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  b->stream = acquire_stream();
+  if (!b->stream) {
     set_error("cudaStreamCreate failed");
     return fail(MGPU_E_CUDA);
   }
   b->cap = std::max(std::max(batch_capacity(true, true), batch_capacity(true, false)),
                     std::max(batch_capacity(false, true), batch_capacity(false, false)));
-  if (int e = dev_alloc(b->d_bars, b->cap)) return fail(e);
-  if (int e = dev_alloc(b->d_part, 8l * b->cap)) return fail(e);
-  if (int e = dev_alloc(b->d_flags, ncases + 2)) return fail(e);
+  if (int e = dev_alloc(b->d_bars, b->cap, b->stream)) return fail(e);
+  if (int e = dev_alloc(b->d_part, 8l * b->cap, b->stream)) return fail(e);
+  if (int e = dev_alloc(b->d_flags, ncases + 2, b->stream)) return fail(e);
   if (cudaEventCreate(&b->e0) != cudaSuccess || cudaEventCreate(&b->e1) != cudaSuccess) {
     set_error("cudaEventCreate failed");
     return fail(MGPU_E_CUDA);

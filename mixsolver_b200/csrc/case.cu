@@ -12,6 +12,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -24,8 +26,56 @@ namespace mgpu {
 
 static thread_local std::string g_err;
 static int g_device = 0;
+static std::mutex g_stream_mu;
+static std::map<int, std::vector<cudaStream_t>> g_streams;
 
 void set_error(const std::string& msg) { g_err = msg; }
+
+cudaStream_t acquire_stream() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_stream_mu);
+    auto& v = g_streams[dev];
+    if (!v.empty()) {
+      cudaStream_t s = v.back();
+      v.pop_back();
+      return s;
+    }
+  }
+  cudaStream_t s = nullptr;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+  return s;
+}
+
+void release_stream(cudaStream_t s) {
+  if (!s) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_stream_mu);
+  g_streams[dev].push_back(s);
+}
+
+// Make sure at least n streams wait in the pool of the current device.
+int prewarm_streams(int n) {
+  int dev = 0;
+  MGPU_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_stream_mu);
+  auto& v = g_streams[dev];
+  while ((int)v.size() < n) {
+    cudaStream_t s = nullptr;
+    MGPU_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    v.push_back(s);
+  }
+  return 0;
+}
+
+int copy_sync(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
+  if (bytes == 0) return 0;
+  MGPU_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, s));
+  MGPU_CUDA(cudaStreamSynchronize(s));
+  return 0;
+}
 
 int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
   g_err = std::string(what) + ": " + cudaGetErrorString(e) + " (" + file + ":" + std::to_string(line) + ")";
@@ -203,8 +253,8 @@ int end_run(MgpuCase* c, int nsteps_done, MgpuIterRec* log, int logcap, int* nre
   const int done = h.cur_it;
   if (nrec) *nrec = done;
   if (log && logcap > 0 && done > 0)
-    MGPU_CUDA(cudaMemcpy(log, c->d.recs, sizeof(MgpuIterRec) * (size_t)std::min(done, logcap),
-                         cudaMemcpyDeviceToHost));
+    TRY(copy_sync(log, c->d.recs, sizeof(MgpuIterRec) * (size_t)std::min(done, logcap),
+                         cudaMemcpyDeviceToHost, c->stream));
   if (ier) *ier = h.ier;
   float ms = 0.f;
   cudaEventElapsedTime(&ms, c->ev_run0, c->ev_run1);
@@ -316,7 +366,8 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
     return e;
   };
   c->ctrl = *ctrl;
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  c->stream = acquire_stream();
+  if (!c->stream) {
     set_error("cudaStreamCreate failed");
     return fail(MGPU_E_CUDA);
   }
@@ -397,7 +448,7 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
   DeviceCase dd = d;
   DevStatus h0{};
   h0.nan_key = ~0ull;
-  MGPU_CUDA(cudaMemcpy(d.st, &h0, sizeof(h0), cudaMemcpyHostToDevice));
+  MGPU_CUDA(cudaMemcpyAsync(d.st, &h0, sizeof(h0), cudaMemcpyHostToDevice, c->stream));
   if ((e = geometry_setup(dd, x, fptr, fnodes, pcen, P, c->stream))) return fail(e);
   // init_fields: everything at rest, apc = 1
   MGPU_CUDA(cudaMemsetAsync(d.u, 0, sizeof(double) * 3 * N, c->stream));
@@ -414,8 +465,8 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
   // scalars needing a sequential pass: flux_ref (group/face order) and the
   // smallest vol**(1/3) (CFL estimate); computed once on the host
   std::vector<double> area(F), vol(N);
-  MGPU_CUDA(cudaMemcpy(area.data(), d.area, sizeof(double) * F, cudaMemcpyDeviceToHost));
-  MGPU_CUDA(cudaMemcpy(vol.data(), d.vol, sizeof(double) * N, cudaMemcpyDeviceToHost));
+  TRY(copy_sync(area.data(), d.area, sizeof(double) * F, cudaMemcpyDeviceToHost, c->stream));
+  TRY(copy_sync(vol.data(), d.vol, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
   for (long i = 0; i < N; ++i)
     if (!(vol[i] > 0.0)) {
       set_error("mesh: non-positive cell volume");
@@ -459,14 +510,14 @@ int mgpu_fields_upload(MgpuCase* c, const double* u, const double* p, const doub
     std::vector<double> soa(3 * N);
     for (long i = 0; i < N; ++i)
       for (int k = 0; k < 3; ++k) soa[k * N + i] = src[3 * i + k];
-    MGPU_CUDA(cudaMemcpy(dst, soa.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice));
+    TRY(copy_sync(dst, soa.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice, c->stream));
     return 0;
   };
   if (u) TRY(up3(c->d.u, u));
   if (u_old) TRY(up3(c->d.u_old, u_old));
   if (u_old_old) TRY(up3(c->d.u_old_old, u_old_old));
-  if (p) MGPU_CUDA(cudaMemcpy(c->d.p, p, sizeof(double) * N, cudaMemcpyHostToDevice));
-  if (flux) MGPU_CUDA(cudaMemcpy(c->d.flux, flux, sizeof(double) * c->d.F, cudaMemcpyHostToDevice));
+  if (p) TRY(copy_sync(c->d.p, p, sizeof(double) * N, cudaMemcpyHostToDevice, c->stream));
+  if (flux) TRY(copy_sync(c->d.flux, flux, sizeof(double) * c->d.F, cudaMemcpyHostToDevice, c->stream));
   return 0;
 }
 
@@ -476,7 +527,7 @@ int mgpu_fields_download(MgpuCase* c, double* u, double* p, double* flux, double
   const long N = c->d.N;
   auto down = [&](double* dst, const double* src, int planes) -> int {
     std::vector<double> soa((size_t)planes * N);
-    MGPU_CUDA(cudaMemcpy(soa.data(), src, sizeof(double) * planes * N, cudaMemcpyDeviceToHost));
+    TRY(copy_sync(soa.data(), src, sizeof(double) * planes * N, cudaMemcpyDeviceToHost, c->stream));
     for (long i = 0; i < N; ++i)
       for (int k = 0; k < planes; ++k) dst[(long)planes * i + k] = soa[k * N + i];
     return 0;
@@ -486,14 +537,14 @@ int mgpu_fields_download(MgpuCase* c, double* u, double* p, double* flux, double
   if (gu) {
     // device planes comp*3+dir -> Fortran gu(comp,dir,cell): index comp + 3*dir + 9*cell
     std::vector<double> soa(9 * N);
-    MGPU_CUDA(cudaMemcpy(soa.data(), c->d.gu, sizeof(double) * 9 * N, cudaMemcpyDeviceToHost));
+    TRY(copy_sync(soa.data(), c->d.gu, sizeof(double) * 9 * N, cudaMemcpyDeviceToHost, c->stream));
     for (long i = 0; i < N; ++i)
       for (int comp = 0; comp < 3; ++comp)
         for (int dir = 0; dir < 3; ++dir) gu[9 * i + comp + 3 * dir] = soa[(comp * 3 + dir) * N + i];
   }
-  if (p) MGPU_CUDA(cudaMemcpy(p, c->d.p, sizeof(double) * N, cudaMemcpyDeviceToHost));
-  if (apc) MGPU_CUDA(cudaMemcpy(apc, c->d.apc, sizeof(double) * N, cudaMemcpyDeviceToHost));
-  if (flux) MGPU_CUDA(cudaMemcpy(flux, c->d.flux, sizeof(double) * c->d.F, cudaMemcpyDeviceToHost));
+  if (p) TRY(copy_sync(p, c->d.p, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
+  if (apc) TRY(copy_sync(apc, c->d.apc, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
+  if (flux) TRY(copy_sync(flux, c->d.flux, sizeof(double) * c->d.F, cudaMemcpyDeviceToHost, c->stream));
   return 0;
 }
 
@@ -596,9 +647,9 @@ int mgpu_case_stage(MgpuCase* c, int what, int ts_order, const double* apc, doub
   }
   MGPU_CUDA(cudaStreamSynchronize(s));
   const double* A = (what == 5) ? d.pval : d.aval;
-  if (aval && (what >= 1 && what <= 5)) MGPU_CUDA(cudaMemcpy(aval, A, sizeof(double) * d.nnz, cudaMemcpyDeviceToHost));
-  if (rhs && (what >= 1 && what <= 5)) MGPU_CUDA(cudaMemcpy(rhs, d.rhs, sizeof(double) * N, cudaMemcpyDeviceToHost));
-  if (ap && (what >= 1 && what <= 3)) MGPU_CUDA(cudaMemcpy(ap, d.ap, sizeof(double) * N, cudaMemcpyDeviceToHost));
+  if (aval && (what >= 1 && what <= 5)) TRY(copy_sync(aval, A, sizeof(double) * d.nnz, cudaMemcpyDeviceToHost, c->stream));
+  if (rhs && (what >= 1 && what <= 5)) TRY(copy_sync(rhs, d.rhs, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
+  if (ap && (what >= 1 && what <= 3)) TRY(copy_sync(ap, d.ap, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
   return 0;
 }
 

@@ -10,6 +10,17 @@
 #include "assembly.cuh"
 #include "case.cuh"
 
+namespace mgpu {
+// Non-blocking streams are recycled through a pool: creating and destroying
+// one waits for kernels running on other streams, which stalls a case being
+// set up or freed while a batch steps.
+cudaStream_t acquire_stream();
+void release_stream(cudaStream_t s);
+// dst <- src through stream s, then a wait on s alone (a plain cudaMemcpy
+// goes through the legacy default stream and waits for other streams' work).
+int copy_sync(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s);
+}  // namespace mgpu
+
 #define TRY(x)                 \
   do {                         \
     int rc_ = (x);             \
@@ -42,7 +53,8 @@ struct MgpuCase {
     p = nullptr;
     if (n == 0) n = 1;
     void* q = nullptr;
-    MGPU_CUDA(cudaMalloc(&q, n * sizeof(T)));
+    // stream-ordered: freeing a case later never waits for other streams' work
+    MGPU_CUDA(cudaMallocAsync(&q, n * sizeof(T), stream));
     allocs.push_back(q);
     bytes += (int64_t)(n * sizeof(T));
     p = (T*)q;
@@ -51,15 +63,15 @@ struct MgpuCase {
   template <typename T>
   int upload(T*& p, const std::vector<T>& h) {
     if (int e = alloc(p, h.size())) return e;
-    if (!h.empty()) MGPU_CUDA(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    if (!h.empty()) MGPU_CUDA(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
     return 0;
   }
   ~MgpuCase() {
     for (auto e : ev_pool) cudaEventDestroy(e);
     if (ev_run0) cudaEventDestroy(ev_run0);
     if (ev_run1) cudaEventDestroy(ev_run1);
-    for (void* p : allocs) cudaFree(p);
-    if (stream) cudaStreamDestroy(stream);
+    for (void* p : allocs) cudaFreeAsync(p, stream);
+    if (stream) mgpu::release_stream(stream);
   }
 };
 
@@ -67,6 +79,7 @@ namespace mgpu {
 
 extern int g_cheb_degree;
 extern double g_cheb_ratio;
+extern int g_batch_reserve;
 
 KrylovArgs base_args(MgpuCase* c);
 MixedArgs mixed_args(const MgpuCase* c, bool bicg);

@@ -46,6 +46,8 @@ int g_sweep_sleep = 0;
 int g_min_blocks = 1;
 }  // namespace
 int g_cheb_degree = 16;      // mixed form: Chebyshev-Jacobi degree of the pressure preconditioner
+int g_batch_reserve = 0;  // block slots batched launches leave to other streams
+int prewarm_streams(int n);  // case.cu
 double g_cheb_ratio = 1000.0; // and the ratio lambda_max / lambda_min of its interval
 namespace {
 
@@ -649,6 +651,10 @@ int set_tuning(const char* key, int value) {
     g_min_blocks = value;
   } else if (k == "sweep_sleep_ns" && value >= 0 && value <= 100000) {
     g_sweep_sleep = value;
+  } else if (k == "batch_reserve_blocks" && value >= 0 && value <= 256) {
+    g_batch_reserve = value;
+  } else if (k == "stream_pool" && value >= 0 && value <= 1024) {
+    if (int e = prewarm_streams(value)) return e;
   } else {
     set_error("mgpu_set_tuning: unknown key or value out of range: " + k);
     return MGPU_E_ARG;

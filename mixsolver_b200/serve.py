@@ -49,6 +49,7 @@ class Request:
     u0: Optional[np.ndarray] = None
     # filled in by the server
     admitted: float = math.nan
+    create_s: float = math.nan  # seconds spent making the case resident
     finished: float = math.nan
     ier: int = -1
     nrec: int = 0
@@ -68,11 +69,16 @@ class Request:
 class GpuBackend:
     """The C-ABI: a resident case per request, one CaseBatch per active set."""
 
-    def __init__(self, device: int = 0, policy=(32768, 4)):
+    def __init__(self, device: int = 0, policy=(32768, 4), reserve_blocks: int = 16):
         from . import solver
         self.S = solver
         self.device = device
         self.policy = policy
+        # leave block slots free during the batched Krylov launches so that the
+        # set-up kernels of arriving cases run beside them
+        solver.set_tuning("batch_reserve_blocks", int(reserve_blocks))
+        # streams for the cases and batches to come, made before the GPU is busy
+        solver.set_tuning("stream_pool", 64)
 
     def create(self, req: Request):
         c = self.S.UnsCase(req.mesh, req.ctrl, device=self.device)
@@ -155,6 +161,7 @@ class Server:
                     break
             if stop.is_set():
                 return
+            tc = self.clock()
             try:
                 h, ier, nbytes = self.be.create(req)
             except Exception as e:  # a case the library rejects: answered with the error
@@ -171,6 +178,7 @@ class Server:
                 self.peak_resident_bytes = max(self.peak_resident_bytes, self.resident_bytes)
                 self.bytes_per_cell = seen_bytes / max(seen_cells, 1)
                 req.admitted = self.clock() - t0
+                req.create_s = self.clock() - tc
                 req.device_bytes = nbytes
                 req.ier = ier
                 resident.append([req, h, 0])  # request, handle, iterations stepped

@@ -77,3 +77,13 @@ def test_plan_rejects_bad_arguments():
         S.batch_plan(np.array([10], np.int32), 32768, 0, 100)
     with pytest.raises(RuntimeError):
         S.batch_plan(np.array([10], np.int32), 65536, 4, 100)
+
+
+def test_few_big_systems_get_lanes_in_proportion_to_their_work():
+    rows = np.array([2_000_000, 500_000, 100_000], np.int32)
+    passes = np.array([100.0, 100.0, 100.0])
+    cls, widths = S.batch_plan(rows, 32768, 4, 296, passes=passes)
+    assert np.all(cls == 0) and len(widths) == 3 and widths.sum() == 296
+    share = widths / widths.sum()
+    assert np.allclose(share, rows / rows.sum(), atol=0.03)
+    assert widths[0] >= least_width(2_000_000)

@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--duration", type=float, default=2.0, help="serve: seconds of arrivals (mixed leg)")
     ap.add_argument("--fp64-duration", type=float, default=0.5, help="serve: seconds of arrivals (FP64 leg)")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serve: device memory for resident cases")
+    ap.add_argument("--active-cells", type=int, default=4_000_000, help="serve: cells stepped together per tick")
     ap.add_argument("--cases", type=int, default=256, help="batch: number of cavity cases")
     ap.add_argument("--policy", default="auto", help="batch: lane policy SPLIT_ROWSxWIDE_LANES or auto")
     ap.add_argument("--fp64-iters", type=int, default=2, help="batch: iterations of the FP64 comparison leg")
@@ -575,7 +576,7 @@ def run_serve(args):
     for name, prec, dur in (("mixed", abi.PREC_MIXED, args.duration), ("fp64", abi.PREC_FP64, args.fp64_duration)):
         reqs = serve_requests(dur, args.rate, mpool, prec, seed=rank)
         srv = serve.Server(serve.GpuBackend(device=local, policy=(32768, 4)), budget_bytes=budget,
-                           active_cells=16_000_000, tick_iters=5)
+                           active_cells=args.active_cells, tick_iters=5)
         with ClockSampler(local) as clk:
             w0 = time.perf_counter()
             out = srv.run(reqs)
@@ -601,7 +602,7 @@ def run_serve(args):
         "config": {"workload": f"Poisson arrivals at {args.rate}/s: 70% SIMPLE (50 outer iterations, lid-driven "
                                "jittered-hex cavity), 30% PISO (10 steps, dt 1e-3, Taylor-Green hex-split-tet box); "
                                "cells log-uniform in [1e4, 2e6] (pool of 13 meshes), Re uniform in [50, 2000]",
-                   "budget_gb": args.budget_gb, "mesh_pool_s": t_pool, "latency_s": {"p50": mx["p50_s"], "p99": mx["p99_s"]},
+                   "budget_gb": args.budget_gb, "active_cells": args.active_cells, "mesh_pool_s": t_pool, "latency_s": {"p50": mx["p50_s"], "p99": mx["p99_s"]},
                    "mixed": mx, "fp64": legs["fp64"],
                    "note": "the arrival rate exceeds the GPU's service rate: latency grows with the queue"},
         "roofline": None,

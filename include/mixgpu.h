@@ -333,8 +333,9 @@ int mgpu_batch_set_profiling(MgpuBatch* b, int on);
 int mgpu_batch_info(const MgpuBatch* b, MgpuBatchInfo* info);
 /* The lane plan (host only, no GPU needed) of systems of rows[i] rows and
  * passes[i] SpMV-sized passes (NULL: modelled) under a policy and a
- * co-resident block capacity: sys_class[i] = 0 (wide lanes) or 1
- * (single-block lanes); lane_width[0 .. *nlanes) = the lanes' widths (room for
+ * co-resident block capacity: sys_class[i] = the class (queue) of system i,
+ * classes numbered widest lanes first, the last one the single-block lanes;
+ * lane_width[0 .. *nlanes) = the lanes' widths, in class order (room for
  * `capacity` entries). */
 int mgpu_batch_plan(int nsys, const int* rows, const double* passes, int split_rows, int wide_lanes, int capacity,
                     int* sys_class, int* lane_width, int* nlanes);

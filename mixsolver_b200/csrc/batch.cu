@@ -69,11 +69,13 @@ double model_passes(long n, bool pcg, int cheb_k) {
   return pcg ? std::max(5.0, std::cbrt((double)n)) * (std::max(cheb_k, 1) + 1) : 24.0;
 }
 
-// Lanes of one launch: their widths and classes (0 wide, 1 single-block), and
-// per class the queue of systems, most work first.
+// Lanes of one launch: their widths and classes, and per class the queue of
+// systems, most work first. Classes are ordered by lane width, widest first;
+// a lane takes from its own class and then from later (narrower) ones, so a
+// system only ever runs on a lane at least as wide as the one planned for it.
 struct LaneSet {
   std::vector<int> width, cls;
-  std::vector<int> queue[2];
+  std::vector<std::vector<int>> queue;
 };
 
 LaneSet plan_lanes(const std::vector<int>& n, const std::vector<double>& passes, const Policy& P, int cap) {
@@ -97,8 +99,6 @@ LaneSet plan_lanes(const std::vector<int>& n, const std::vector<double>& passes,
   };
   std::sort(big.begin(), big.end(), by_work);
   std::sort(small.begin(), small.end(), by_work);
-  for (auto& e : big) L.queue[0].push_back(e.second);
-  for (auto& e : small) L.queue[1].push_back(e.second);
   int bb = 0, bs = 0;
   if (big.empty()) {
     bs = std::min<int>(cap, (int)small.size());
@@ -111,14 +111,15 @@ LaneSet plan_lanes(const std::vector<int>& n, const std::vector<double>& passes,
   }
   if (!big.empty() && (int)big.size() <= P.wide_lanes) {
     // one lane per big system, widths in proportion to their work, so that
-    // they finish the phase together (each at least its least width)
+    // they finish the phase together (each at least its least width); each
+    // lane is its own class holding exactly its system
     std::vector<int> w(big.size());
     int used = 0;
     for (size_t j = 0; j < big.size(); ++j) {
       w[j] = std::max(least_width(n[big[j].second]), (int)std::floor(bb * big[j].first / wb));
       used += w[j];
     }
-    while (used > bb) {  // trim the widest lanes that can give a block
+    while (used > bb) {  // trim the lanes with most room above their least width
       size_t jm = 0;
       for (size_t j = 1; j < w.size(); ++j)
         if (w[j] - least_width(n[big[j].second]) > w[jm] - least_width(n[big[jm].second])) jm = j;
@@ -127,9 +128,13 @@ LaneSet plan_lanes(const std::vector<int>& n, const std::vector<double>& passes,
       --used;
     }
     for (size_t j = 0; used < bb; j = (j + 1) % w.size(), ++used) ++w[j];  // spare blocks, most work first
-    for (size_t j = 0; j < w.size(); ++j) {
+    std::vector<size_t> ord(w.size());
+    for (size_t j = 0; j < ord.size(); ++j) ord[j] = j;
+    std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return w[x] > w[y]; });
+    for (size_t j : ord) {
       L.width.push_back(w[j]);
-      L.cls.push_back(0);
+      L.cls.push_back((int)L.queue.size());
+      L.queue.push_back({big[j].second});
     }
   } else if (!big.empty()) {
     // more big systems than wide lanes: equal lanes sharing one queue
@@ -138,10 +143,15 @@ LaneSet plan_lanes(const std::vector<int>& n, const std::vector<double>& passes,
       L.width.push_back(bb / k + (j < bb % k ? 1 : 0));
       L.cls.push_back(0);
     }
+    L.queue.push_back({});
+    for (auto& e : big) L.queue.back().push_back(e.second);
   }
+  const int sc = (int)L.queue.size();  // the single-block class
+  L.queue.push_back({});
+  for (auto& e : small) L.queue.back().push_back(e.second);
   for (int j = 0; j < bs; ++j) {
     L.width.push_back(1);
-    L.cls.push_back(1);
+    L.cls.push_back(sc);
   }
   return L;
 }
@@ -293,12 +303,12 @@ int build_launches(MgpuBatch* b, BatchPhase& ph, const Policy& P) {
       hl.push_back(BatchLane{(int)block_lane.size(), ls.width[j], ls.cls[j], 0});
       for (int k = 0; k < ls.width[j]; ++k) block_lane.push_back((int)j);
     }
-    for (int c = 0; c < 2; ++c) {
+    for (const auto& q : ls.queue) {
       q_start.push_back((int)q_items.size());
-      for (int i : ls.queue[c]) q_items.push_back(items[i]);
+      for (int i : q) q_items.push_back(items[i]);
     }
     q_start.push_back((int)q_items.size());
-    const int ncls = 2;
+    const int ncls = (int)ls.queue.size();
     BatchLaunch L;
     L.pcg = ph.pcg;
     L.ell = ell == 1;
@@ -877,9 +887,9 @@ int mgpu_batch_plan(int nsys, const int* rows, const double* passes, int split_r
   std::vector<double> ps(nsys);
   for (int i = 0; i < nsys; ++i) ps[i] = passes ? passes[i] : model_passes(n[i], true, g_cheb_degree);
   const LaneSet L = plan_lanes(n, ps, Policy{split_rows, wide_lanes}, capacity);
-  for (int c = 0; c < 2; ++c)
+  for (size_t c = 0; c < L.queue.size(); ++c)
     for (int i : L.queue[c])
-      if (sys_class) sys_class[i] = c;
+      if (sys_class) sys_class[i] = (int)c;
   for (size_t j = 0; j < L.width.size(); ++j)
     if (lane_width) lane_width[j] = L.width[j];
   *nlanes = (int)L.width.size();

@@ -41,7 +41,7 @@ def test_plan_invariants(split, wide, cap):
     passes = 17.0 * np.maximum(5.0, np.cbrt(rows))
     cls, widths = S.batch_plan(rows, split, wide, cap, passes=passes)
     big = (rows > split) | np.array([least_width(int(n)) > 1 for n in rows])
-    assert np.array_equal(cls, np.where(big, 0, 1))
+    assert np.all(cls[~big] == cls.max()) and np.all(cls[big] < cls.max()) if big.any() and (~big).any() else True
     assert widths.sum() <= cap and np.all(widths >= 1)
     nwide = int(np.sum(widths > 1)) if big.any() else 0
     assert nwide <= wide
@@ -63,13 +63,15 @@ def test_plan_is_deterministic():
 def test_only_small_systems_get_one_lane_each_up_to_capacity():
     rows = np.full(10, 5000, np.int32)
     cls, widths = S.batch_plan(rows, 32768, 8, 296)
-    assert np.all(cls == 1) and len(widths) == 10 and np.all(widths == 1)
+    assert np.all(cls == 0) and len(widths) == 10 and np.all(widths == 1)
 
 
 def test_only_big_systems_share_the_whole_capacity():
     rows = np.array([300000, 70000, 100000], np.int32)
     cls, widths = S.batch_plan(rows, 32768, 8, 296)
-    assert np.all(cls == 0) and len(widths) == 3 and widths.sum() == 296
+    assert len(widths) == 3 and widths.sum() == 296
+    # one class per big system, widest lane first, its system on it
+    assert sorted(cls) == [0, 1, 2] and cls[0] == 0 and list(widths) == sorted(widths, reverse=True)
 
 
 def test_plan_rejects_bad_arguments():
@@ -83,7 +85,25 @@ def test_few_big_systems_get_lanes_in_proportion_to_their_work():
     rows = np.array([2_000_000, 500_000, 100_000], np.int32)
     passes = np.array([100.0, 100.0, 100.0])
     cls, widths = S.batch_plan(rows, 32768, 4, 296, passes=passes)
-    assert np.all(cls == 0) and len(widths) == 3 and widths.sum() == 296
+    assert list(cls) == [0, 1, 2] and len(widths) == 3 and widths.sum() == 296
     share = widths / widths.sum()
     assert np.allclose(share, rows / rows.sum(), atol=0.03)
-    assert widths[0] >= least_width(2_000_000)
+    for i, n in enumerate(rows):  # system i's lane is lane cls[i]: wide enough for it
+        assert widths[cls[i]] >= least_width(int(n))
+
+
+def test_narrow_lanes_never_take_a_system_wider_than_planned():
+    """A few huge systems and small ones: each big system has a class of its
+    own whose lane is wide enough for it, big classes are numbered widest lane
+    first (a lane that takes from a later class meets only systems planned for
+    narrower lanes), and the small systems form the last class."""
+    rows = np.array([2_000_000, 1_157_625, 1_157_625, 456_533, 27_000, 10_000], np.int32)
+    cls, widths = S.batch_plan(rows, 32768, 4, 280)
+    big = rows > 32768
+    assert sorted(cls[big]) == list(range(int(big.sum())))
+    assert np.all(cls[~big] == big.sum())
+    for i in np.nonzero(big)[0]:
+        assert widths[cls[i]] >= least_width(int(rows[i]))
+    nbig = int(big.sum())
+    assert list(widths[:nbig]) == sorted(widths[:nbig], reverse=True)
+    assert widths.sum() <= 280

@@ -199,3 +199,28 @@ def test_step_and_poll_interface():
     e1, l1 = objs[1].finish()
     assert (e0, len(l0), e1, len(l1)) == (0, 3, 0, 9)
     B.close()
+
+
+def test_sized_lanes_keep_their_own_system():
+    """Few big systems each get a lane sized by their work; with the capacity
+    shrunk (block slots reserved) the narrow lanes are too small for the
+    biggest system, which must still run on its own lane: every member equals
+    its single-case run."""
+    specs = []
+    for k, n in enumerate((59, 39, 34)):
+        mesh, ctrl = cases.cavity3d(n, re=600.0, seed=k, outer_max=3, mom=abi.MOM_JACOBI, ppe=abi.PPE_IC0)
+        ctrl.precision = abi.PREC_MIXED
+        ctrl.lin_max = 2000
+        specs.append((mesh, ctrl))
+    cap = S.batch_plan(np.array([59 ** 3, 39 ** 3, 34 ** 3], np.int32), 32768, 4, 16)[1]
+    assert min(cap) < 7  # a lane narrower than the 59^3 system needs (7 blocks)
+    S.set_tuning("batch_reserve_blocks", 256)
+    try:
+        got, _ = _batched(specs, [0, 0, 0], 3, policy=(32768, 4))
+    finally:
+        S.set_tuning("batch_reserve_blocks", 0)
+    for (mesh, ctrl), (ier, log, f) in zip(specs, got):
+        ier1, log1, f1 = _single(mesh, copy.deepcopy(ctrl), 3)
+        assert ier == ier1 == 0
+        for k in ("u", "p", "flux"):
+            assert np.array_equal(f[k], f1[k]), k

@@ -30,7 +30,7 @@ __device__ __forceinline__ double row_spmv(const int* __restrict__ rp, const int
                                            const double* __restrict__ val, const double* x, int i) {
   double y = 0.0;
   const int e = rp[i + 1];
-  for (int k = rp[i]; k < e; ++k) y = y + val[k] * ldv<L1>(&x[col[k]]);
+  for (int k = rp[i]; k < e; ++k) y = y + val[k] * ldv(&x[col[k]]);
   return y;
 }
 
@@ -166,7 +166,7 @@ __device__ bool apply_lu(const KrylovArgs& a, int kind, const double* src, doubl
       for (int idx = gtid; idx < n && ok; idx += P) {
         const int i = a.lo_rows[idx];
         const int rb = a.row_ptr[i], d = a.diag[i];
-        double s = ldv<false>(&src[i]);
+        double s = ldv(&src[i]);
         if (d - rb <= kGather) {
           double v[kGather];
           gather_ready<kGather>(y, a.col + rb, d - rb, v, a.st, ok, sl);
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_factor(KrylovArgs a, int kin
         // ilu0_factor row i (IKJ): rows k < i are final
         for (int kk = rb; kk < di; ++kk) {
           const int k = a.col[kk];
-          const double piv = ldv<L1>(&f[a.diag[k]]);
+          const double piv = ldv(&f[a.diag[k]]);
           if (fabs(piv) < DTINY) {
             atomicExch(a.ferr, 2);
             continue;
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_factor(KrylovArgs a, int kin
             const int j = a.col[jj];
             if (j <= k) continue;
             while (pos < re && a.col[pos] < j) ++pos;
-            if (pos < re && a.col[pos] == j) f[pos] = f[pos] - aik * ldv<L1>(&f[jj]);
+            if (pos < re && a.col[pos] == j) f[pos] = f[pos] - aik * ldv(&f[jj]);
           }
         }
       } else {
@@ -277,13 +277,13 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_factor(KrylovArgs a, int kin
             else if (cp > cq)
               ++q;
             else {
-              dsum = dsum + f[p] * ldv<L1>(&f[q]);
+              dsum = dsum + f[p] * ldv(&f[q]);
               ++p;
               ++q;
             }
           }
           const double s = f[kp] - dsum;
-          f[kp] = s / ldv<L1>(&f[a.diag[k]]);
+          f[kp] = s / ldv(&f[a.diag[k]]);
         }
         double s = f[di];
         for (int kp = rb; kp < di; ++kp) s = s - f[kp] * f[kp];
@@ -355,11 +355,11 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_pcg(KrylovArgs a) {
   } else {
     if (!apply_lu<L1>(a, a.precond, r, z)) return;
     double v1[1] = {0.0};
-    for (int i = gtid; i < n; i += gstr) v1[0] = v1[0] + r[i] * ldv<L1>(&z[i]);
+    for (int i = gtid; i < n; i += gstr) v1[0] = v1[0] + r[i] * ldv(&z[i]);
     if (!vg_sum<1, L1>(v1, vg, a.st)) return;
     rz = v1[0];
   }
-  for (int i = gtid; i < n; i += gstr) p[i] = ldv<L1>(&z[i]);
+  for (int i = gtid; i < n; i += gstr) p[i] = ldv(&z[i]);
   if (!grid_sync(a.bar, a.st)) return;
   int ierr = 0, it;
   for (it = 1; it <= a.maxit; ++it) {
@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_pcg(KrylovArgs a) {
     } else {
       if (!apply_lu<L1>(a, a.precond, r, z)) return;
       double v1[1] = {0.0};
-      for (int i = gtid; i < n; i += gstr) v1[0] = v1[0] + r[i] * ldv<L1>(&z[i]);
+      for (int i = gtid; i < n; i += gstr) v1[0] = v1[0] + r[i] * ldv(&z[i]);
       if (!vg_sum<1, L1>(v1, vg, a.st)) return;
       rz_new = v1[0];
     }
@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_pcg(KrylovArgs a) {
       break;
     }
     const double beta = rz_new / rz;
-    for (int i = gtid; i < n; i += gstr) p[i] = ldv<L1>(&z[i]) + beta * p[i];
+    for (int i = gtid; i < n; i += gstr) p[i] = ldv(&z[i]) + beta * p[i];
     if (!grid_sync(a.bar, a.st)) return;
     rz = rz_new;
   }
@@ -500,7 +500,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_bicgstab(KrylovArgs a) {
     if (!vg_sum<1, L1>(d2, vg, a.st)) return;
     const double snrm = sqrt(d2[0]);
     if (snrm / bnrm <= a.tol) {
-      for (int i = gtid; i < n; i += gstr) x[i] = x[i] + alpha * ldv<L1>(&ph[i]);
+      for (int i = gtid; i < n; i += gstr) x[i] = x[i] + alpha * ldv(&ph[i]);
       write_result(a, it, snrm / bnrm, 0);
       return;
     }
@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(L1 ? 512 : 256) k_bicgstab(KrylovArgs a) {
     }
     double d4[2] = {0.0, 0.0};
     for (int i = gtid; i < n; i += gstr) {
-      x[i] = x[i] + alpha * ldv<L1>(&ph[i]) + omega * ldv<L1>(&sh[i]);
+      x[i] = x[i] + alpha * ldv(&ph[i]) + omega * ldv(&sh[i]);
       const double ri = s[i] - omega * t[i];
       r[i] = ri;
       d4[0] = d4[0] + ri * ri;

@@ -136,7 +136,7 @@ __device__ __forceinline__ bool red_total(Red& R, const Rows& rows, VGrid& g, De
 #pragma unroll
     for (int q = 0; q < NQ; ++q)
 #pragma unroll
-      for (int r = 0; r < 8; ++r) v[q][r] = s0 + 32 * r < nsc ? ldv<L1>(&sp[(long)q * nsc + s0 + 32 * r]) : 0.0;
+      for (int r = 0; r < 8; ++r) v[q][r] = s0 + 32 * r < nsc ? ldv(&sp[(long)q * nsc + s0 + 32 * r]) : 0.0;
 #pragma unroll
     for (int q = 0; q < NQ; ++q) {
       double acc = v[q][0];
@@ -178,12 +178,12 @@ __device__ __forceinline__ float spmv32_csr(const int* __restrict__ rp, const in
     }
 #pragma unroll
   for (int t = 0; t < MAXNZ; ++t)
-    if (b + t < e) xv[t] = ldv<L1>(&x[c[t]]);
+    if (b + t < e) xv[t] = ldv(&x[c[t]]);
   float acc = 0.0f;
 #pragma unroll
   for (int t = 0; t < MAXNZ; ++t)
     if (b + t < e) acc = fmaf(v[t], xv[t], acc);
-  for (int k = b + MAXNZ; k < e; ++k) acc = fmaf(val[k], ldv<L1>(&x[col[k]]), acc);
+  for (int k = b + MAXNZ; k < e; ++k) acc = fmaf(val[k], ldv(&x[col[k]]), acc);
   return acc;
 }
 
@@ -204,7 +204,7 @@ __device__ __forceinline__ float spmv32_ell(const MixedArgs& m, const float* x, 
     }
 #pragma unroll
   for (int t = 0; t < WMAX; ++t)
-    if (t < W) xv[t] = ldv<L1>(&x[c[t]]);
+    if (t < W) xv[t] = ldv(&x[c[t]]);
   float acc = 0.0f;
 #pragma unroll
   for (int t = 0; t < WMAX; ++t)
@@ -273,7 +273,7 @@ __device__ __forceinline__ void spmv32_rows(const Sp32& S, const float* x, const
     for (int r = 0; r < kRows; ++r)
 #pragma unroll
       for (int t = 0; t < WMAX; ++t)
-        if (t < W && in[r]) xv[r][t] = ldv<L1>(&x[c[r][t]]);
+        if (t < W && in[r]) xv[r][t] = ldv(&x[c[r][t]]);
 #pragma unroll
     for (int r = 0; r < kRows; ++r) {
       float acc = 0.0f;
@@ -292,7 +292,7 @@ template <bool L1>
 __device__ __forceinline__ double row_spmv64(const KrylovArgs& a, const double* x, int i) {
   double y = 0.0;
   const int e = a.row_ptr[i + 1];
-  for (int k = a.row_ptr[i]; k < e; ++k) y = fma(a.aval[k], ldv<L1>(&x[a.col[k]]), y);
+  for (int k = a.row_ptr[i]; k < e; ++k) y = fma(a.aval[k], ldv(&x[a.col[k]]), y);
   return y;
 }
 
@@ -591,7 +591,7 @@ __device__ void pcg_mixed_body(const KrylovArgs& a, const MixedArgs& m, VGrid& g
         const int i = base + threadIdx.x;
         double c[2] = {0.0, 0.0};
         if (i < rows.n) {
-          const float ri = (float)(ldv<L1>(&a.r[i]) * inv);
+          const float ri = (float)(ldv(&a.r[i]) * inv);
           rr[i] = ri;
           d[i] = 0.0f;
           if (cheb) {
@@ -728,7 +728,7 @@ __device__ void bicgstab_mixed_body(const KrylovArgs& a, const MixedArgs& m, VGr
       const int i = base + threadIdx.x;
       double c[1] = {0.0};
       if (i < rows.n) {
-        const float ri = (float)(ldv<L1>(&a.r[i]) * inv);
+        const float ri = (float)(ldv(&a.r[i]) * inv);
         r[i] = ri;
         r0[i] = ri;
         p[i] = 0.0f;
@@ -867,8 +867,8 @@ __device__ __forceinline__ int lane_fetch(const LanePlan& p, int cls) {
 // block takes the lane's next system from the class queues and publishes it
 // in a lane slot (two slots, alternating, so a block still reading one slot
 // is never overwritten); the lane barrier makes it visible to the lane's
-// other blocks. Every lane runs the multi-block body (L2 loads; a lane of one
-// block synchronises with __syncthreads): one body per kernel, inlined, with
+// other blocks. Every lane runs the multi-block body (a lane of one block
+// synchronises with __syncthreads): one body per kernel, inlined, with
 // the system's descriptor read through a read-only pointer, keeps the
 // descriptor fields out of the register budget.
 template <bool PCG, bool ELL>

@@ -1,5 +1,5 @@
 // persist.cuh -- primitives of the persistent (cooperative) Krylov kernels:
-// bounded grid barrier, deterministic grid-wide sums, L1/L2 vector loads.
+// bounded grid barrier, deterministic grid-wide sums, vector loads.
 #pragma once
 
 #include "case.cuh"
@@ -93,16 +93,15 @@ __device__ __forceinline__ bool grid_sync(unsigned long long* bar, DevStatus* st
   return vg_sync(VGrid{(int)gridDim.x, (int)blockIdx.x, bar, nullptr, 0}, st);
 }
 
-// Vector loads inside a persistent kernel: with one block every thread sits on
-// the same SM and __syncthreads orders its global accesses, so plain (L1)
-// loads are coherent; with several blocks, data written by another block is
-// read from L2.
-template <bool L1, typename T>
+// Vector loads inside a persistent kernel. A block reads data that other
+// blocks wrote only after a grid barrier (vg_sync), whose acquire load and
+// GPU-scope fence follow the other blocks' fence + arrival: by the PTX memory
+// model those writes then precede every later load of the block (the pattern
+// of a cooperative grid sync), so plain loads, which may hit in L1, are
+// coherent with one block or many.
+template <typename T>
 __device__ __forceinline__ T ldv(const T* p) {
-  if constexpr (L1)
-    return *p;
-  else
-    return __ldcg(p);
+  return *p;
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -156,12 +155,12 @@ __device__ bool vg_sum(double (&v)[NQ], VGrid& g, DevStatus* st) {
   for (int q = 0; q < NQ; ++q) {
     double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
     const int j0 = threadIdx.x, B = blockDim.x;
-    if (j0 < G) t0 = ldv<L1>(&partials[q * G + j0]);
-    if (j0 + B < G) t1 = ldv<L1>(&partials[q * G + j0 + B]);
-    if (j0 + 2 * B < G) t2 = ldv<L1>(&partials[q * G + j0 + 2 * B]);
-    if (j0 + 3 * B < G) t3 = ldv<L1>(&partials[q * G + j0 + 3 * B]);
+    if (j0 < G) t0 = ldv(&partials[q * G + j0]);
+    if (j0 + B < G) t1 = ldv(&partials[q * G + j0 + B]);
+    if (j0 + 2 * B < G) t2 = ldv(&partials[q * G + j0 + 2 * B]);
+    if (j0 + 3 * B < G) t3 = ldv(&partials[q * G + j0 + 3 * B]);
     double s = ((t0 + t1) + t2) + t3;
-    for (int j = j0 + 4 * B; j < G; j += B) s = s + ldv<L1>(&partials[q * G + j]);
+    for (int j = j0 + 4 * B; j < G; j += B) s = s + ldv(&partials[q * G + j]);
     w[q] = warp_sum(s);
   }
   __syncthreads();
@@ -208,7 +207,7 @@ __device__ bool vg_max(double& v, VGrid& g, DevStatus* st) {
   if (g.nb > 1) {
     if (!vg_sync(g, st)) return false;
     double s = 0.0;
-    for (int j = threadIdx.x; j < g.nb; j += blockDim.x) s = fmax(s, ldv<L1>(&partials[j]));
+    for (int j = threadIdx.x; j < g.nb; j += blockDim.x) s = fmax(s, ldv(&partials[j]));
     for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_xor_sync(0xffffffffu, s, o));
     __syncthreads();
     if (lane == 0) sh[warp] = s;

@@ -50,9 +50,12 @@ def parse():
     ap.add_argument("--lin-max", type=int, default=1000)
     ap.add_argument("--cpu-steps", type=int, default=2, help="oracle outer iterations for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="channel", choices=["channel", "batch", "serve"],
+    ap.add_argument("--workload", default="channel", choices=["channel", "batch", "serve", "piso"],
                     help="channel: one 524k-cell case (default); batch: many 3-D cavities in one batch; "
-                         "serve: a Poisson stream of SIMPLE / PISO requests")
+                         "serve: a Poisson stream of SIMPLE / PISO requests; piso: transient PISO on "
+                         "80^3 x 6 tets")
+    ap.add_argument("--tet-n", type=int, default=80, help="piso: hexes per cube edge (each split into 6 tets)")
+    ap.add_argument("--fp64-steps", type=int, default=3, help="piso: time steps of the FP64 comparison leg")
     ap.add_argument("--rate", type=float, default=50.0, help="serve: arrivals per second")
     ap.add_argument("--duration", type=float, default=2.0, help="serve: seconds of arrivals (mixed leg)")
     ap.add_argument("--fp64-duration", type=float, default=0.5, help="serve: seconds of arrivals (FP64 leg)")
@@ -353,6 +356,156 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+PISO_METRIC = "PISO time steps/s, mixed vs FP64 GPU, rel L2 of u, p vs FP64"
+
+
+def run_piso(args):
+    """Transient PISO on n^3 unit-cube hexes each split into 6 tets (n = 80:
+    3,072,000 tets), RCM-ordered, no-slip walls, rho = 1, mu = 1e-3, dt = 1e-3,
+    2 correctors, implicit Euler, seeded Taylor-Green start (amplitude 1, 1 %
+    uniform noise); linear solves to 1e-10 relative. A step is one time step.
+    The mixed form (FP32 SpMV and preconditioner inside FP64 refinement) and
+    the FP64 form (BiCGStab+Jacobi momentum, PCG+IC(0) pressure) first run the
+    same --fp64-steps steps from the same start, and the line reports the
+    relative L2 difference of u, p and flux after them; the mixed case then
+    runs W warm-up and K timed steps."""
+    rank, world, local = dist_env()
+    import copy
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    from mixsolver_b200 import abi, cases, meshgen
+    from mixsolver_b200 import solver as S
+    total = args.fp64_steps + args.warmup + args.steps
+    mesh, ctrl = cases.tet_box(args.tet_n, steps=total + 8, ppe=abi.PPE_IC0, mom=abi.MOM_JACOBI)
+    mesh = cases.rcm_renumber(mesh, S.rcm_order)
+    ctrl.lin_tol = 1e-10
+    ctrl.lin_max = args.lin_max
+    N, F = mesh.ncells, mesh.nfaces
+    nnz = N + 2 * mesh.n_interior()
+    u0 = meshgen.taylor_green(S.compute_geometry(mesh)["xc"], seed=rank)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        import torch.distributed as dist
+        t = torch.tensor([v], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def make(prec):
+        c = copy.deepcopy(ctrl)
+        c.precision = prec
+        k = S.UnsCase(mesh, c, device=local)
+        k.upload(u=u0)
+        return k
+
+    # FP64 comparison leg
+    k64 = make(abi.PREC_FP64)
+    ier, log64 = k64.piso_run(args.fp64_steps, logcap=args.fp64_steps)
+    assert ier == 0, f"FP64 leg ier={ier}"
+    t64 = max_over_ranks(k64.timing()["total_ms"])
+    f64 = k64.fields()
+    k64.close()
+    # mixed form: the same steps, then warm-up and the timed steps
+    case = make(abi.PREC_MIXED)
+    ier, logc = case.piso_run(args.fp64_steps, logcap=args.fp64_steps)
+    assert ier == 0, f"mixed comparison steps ier={ier}"
+    fc = case.fields()
+    rel = {k: float(np.linalg.norm(fc[k] - f64[k]) / np.linalg.norm(f64[k])) for k in ("u", "p", "flux")}
+    t_cmp = max_over_ranks(case.timing()["total_ms"])
+    if args.warmup:
+        ier, _ = case.piso_run(args.warmup, logcap=args.warmup)
+        assert ier == 0, f"warm-up ier={ier}"
+    case.set_profiling(True)
+    barrier()
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        ier, log = case.piso_run(args.steps, logcap=args.steps)
+        wall = time.perf_counter() - t0
+    barrier()
+    assert ier == 0 and len(log) == args.steps, (ier, len(log))
+    tm = case.timing()
+    mx = max_over_ranks(tm["total_ms"])
+    value = world * args.steps / (mx / 1e3)
+    solve_ms = case.solve_times()
+    nsol = 3 + ctrl.n_correct
+    ppe_ms = np.concatenate([solve_ms[3 + j::nsol] for j in range(ctrl.n_correct)]) if len(solve_ms) >= nsol else solve_ms
+    pct = lambda a, q: float(np.percentile(a, q)) if len(a) else None
+    ppe_bytes = [krylov_bytes(N, nnz, r["lin_it"][3 + j], "pcg", True, ctrl.lin_tol, ctrl.mixed_tol)
+                 for r in log for j in range(ctrl.n_correct)]
+    kbytes = (sum(krylov_bytes(N, nnz, r["lin_it"][c], "bicg", True, ctrl.lin_tol, ctrl.mixed_tol)
+                  for r in log for c in range(3)) + sum(ppe_bytes))
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    ppe_launch_ms = float(np.mean(ppe_ms)) if len(ppe_ms) else None
+    achieved = (float(np.mean(ppe_bytes)) / (ppe_launch_ms / 1e3) / 1e9) if ppe_launch_ms else None
+    family = kbytes / (tm["krylov_ms"] / 1e3) / 1e9 if tm["krylov_ms"] > 0 else None
+    # end to end through the public API: host velocity in, one time step, fields out
+    f = case.fields()
+    h2d = 3 * N * 8
+    d2h = (3 * N + N + F + 3 * N + 9 * N + N) * 8
+    barrier()
+    e2e_steps = max(2, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        case.upload(u=f["u"])
+        ier, _ = case.piso_run(1, logcap=1)
+        f = case.fields()
+    e2e_t = time.perf_counter() - t0
+    its = lambda lg, sl: float(np.mean([sum(r["lin_it"][c] for c in sl) for r in lg]))
+    out = {
+        "metric": PISO_METRIC, "value": value, "unit": "time_steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": mx / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32-inner/f64-refinement",
+        "data": "synthetic (seeded Taylor-Green start in a walled hex-split-tet box, RCM-ordered)",
+        "config": {"workload": f"transient PISO, {args.tet_n}^3 x 6 tets ({N} cells), dt 1e-3, 2 correctors, "
+                               "Euler, lin_tol 1e-10; mixed form: FP32-inner/FP64-refinement BiCGStab-Jacobi "
+                               "and PCG with Chebyshev-Jacobi",
+                   "cells": N, "faces": F, "nnz": nnz, "lin_max": args.lin_max, "parallelism": f"replicas x{world}",
+                   "l2": "per-step working set > 126 MB L2 (no explicit flush)",
+                   "krylov_iterations_per_step": {"momentum": its(log, range(3)),
+                                                  "pressure": its(log, range(3, nsol))},
+                   "solve_latency_ms": {"p50": pct(solve_ms, 50), "p99": pct(solve_ms, 99),
+                                        "pressure_p50": pct(ppe_ms, 50), "pressure_p99": pct(ppe_ms, 99)},
+                   "fp64_form": {"time_steps_per_s": world * args.fp64_steps / (t64 / 1e3),
+                                 "steps": args.fp64_steps,
+                                 "krylov_iterations_per_step": {"momentum": its(log64, range(3)),
+                                                                "pressure": its(log64, range(3, nsol))},
+                                 "solvers": "BiCGStab+Jacobi momentum, PCG+IC(0) pressure (parity form)"},
+                   "mixed_comparison_steps_per_s": world * args.fp64_steps / (t_cmp / 1e3),
+                   "speedup_vs_fp64": value / (world * args.fp64_steps / (t64 / 1e3)),
+                   "rel_l2_vs_fp64": rel, "rel_l2_after_steps": args.fp64_steps},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "kernel": "k_pcg_mixed (pressure solves)",
+                     "algorithmic_bytes_per_launch": float(np.mean(ppe_bytes)), "avg_launch_ms": ppe_launch_ms,
+                     "launches": len(ppe_ms), "all_krylov_solves_gbs": family,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+        "e2e": {"value": world * e2e_steps / e2e_t, "unit": "time_steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": tm["gpu_launches"],
+        "clocks": clk.summary(),
+        "wall_s": wall,
+    }
+    case.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def batch_specs(ncases, seed=0):
     """Cube edges with cell counts log-uniform in [16^3, 64^3] and Re uniform in
     [100, 2000], seeded: the batched workload's 3-D lid-driven cavities."""
@@ -633,5 +786,7 @@ if __name__ == "__main__":
         run_batch(a)
     elif a.workload == "serve":
         run_serve(a)
+    elif a.workload == "piso":
+        run_piso(a)
     else:
         run_ours(a)

@@ -54,6 +54,11 @@ __device__ __forceinline__ VGrid whole_grid(unsigned long long* bar, double* par
 // block has flagged a timeout (st may be null: no status) the wait ends. A
 // wait that runs out flags the timeout. Returns false in both cases; the
 // caller then leaves the kernel.
+// Ordering: __syncthreads puts the block's writes before thread 0's arrival,
+// a release at GPU scope; thread 0's polls are acquires, and the closing
+// __syncthreads puts them before the block's later loads. Release and acquire
+// are cumulative in the PTX memory model, so every block's pre-barrier writes
+// are visible to every block after it without a separate fence.
 __device__ bool vg_sync(const VGrid& g, DevStatus* st) {
   __shared__ int s_ok;
   if (g.nb == 1) {
@@ -65,8 +70,8 @@ __device__ bool vg_sync(const VGrid& g, DevStatus* st) {
     int ok = 1;
     unsigned long long* bar = g.bar;
     const unsigned long long nb = g.nb;
-    __threadfence();
-    const unsigned long long old = atomicAdd(bar, 1ull);
+    unsigned long long old;
+    asm volatile("atom.add.release.gpu.global.u64 %0, [%1], 1;" : "=l"(old) : "l"(bar) : "memory");
     const unsigned long long target = (old / nb + 1ull) * nb;
     unsigned spins = 0;
     while (ld_acquire_u64(bar) < target) {
@@ -82,7 +87,6 @@ __device__ bool vg_sync(const VGrid& g, DevStatus* st) {
         break;
       }
     }
-    __threadfence();
     s_ok = ok;
   }
   __syncthreads();

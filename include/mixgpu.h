@@ -245,7 +245,10 @@ int mgpu_cg_jacobi_noalloc(int n, const int32_t* d_row_ptr, const int32_t* d_col
  * slots a batched launch leaves free for other streams, so a case being set
  * up while a batch steps is not held up behind its persistent kernels,
  * default 0), "stream_pool" (create this many streams for cases and batches
- * now: creating one later waits for kernels on other streams). */
+ * now: creating one later waits for kernels on other streams),
+ * "l2_prefetch_mb" (mixed form: a system, or the systems of a batched phase
+ * together, streaming more than this many MB per SpMV pass prefetch each
+ * tile's successor into L2, default 96). */
 int mgpu_set_tuning(const char* key, int value);
 
 /* Timing of the last run on the case's stream (CUDA events): total device ms

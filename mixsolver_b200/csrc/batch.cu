@@ -181,7 +181,8 @@ int dev_alloc(T*& p, size_t n, cudaStream_t s) {
 
 // One batched Krylov launch with its device tables.
 struct BatchLaunch {
-  bool pcg = false, ell = false;
+  bool pcg = false;
+  int ell = 0;  // 0 CSR, 1 ELL, 2 ELL with the L2 prefetch
   LanePlan plan{};
   std::vector<void*> owned;
 };
@@ -194,6 +195,7 @@ struct BatchPhase {
   std::vector<int> mixed;  // member indices solved in batched launches
   std::vector<int> fp64;   // member indices solved one by one
   std::vector<double> passes;  // per mixed system: passes of its last solve (0: unknown)
+  bool pf = false;             // the phase's systems together exceed the L2 share: prefetch
   BatchSys* d_sys = nullptr;
   std::vector<BatchLaunch> launches;
 };
@@ -295,7 +297,8 @@ int build_launches(MgpuBatch* b, BatchPhase& ph, const Policy& P) {
       }
     }
     if (items.empty()) continue;
-    const int cap = std::max(1, batch_capacity(ph.pcg, ell == 1) - g_batch_reserve);
+    const int mode = ell == 1 ? (ph.pf ? 2 : 1) : 0;
+    const int cap = std::max(1, batch_capacity(ph.pcg, mode) - g_batch_reserve);
     const LaneSet ls = plan_lanes(n, passes, P, cap);
     std::vector<BatchLane> hl;
     std::vector<int> block_lane, q_items, q_start;
@@ -311,7 +314,7 @@ int build_launches(MgpuBatch* b, BatchPhase& ph, const Policy& P) {
     const int ncls = (int)ls.queue.size();
     BatchLaunch L;
     L.pcg = ph.pcg;
-    L.ell = ell == 1;
+    L.ell = mode;
     BatchLane* dl = nullptr;
     int *dbl = nullptr, *dqi = nullptr, *dqs = nullptr, *dqh = nullptr, *dslot = nullptr;
     TRY(dev_alloc(dl, hl.size(), b->stream));
@@ -436,6 +439,12 @@ int prepare(MgpuBatch* b) {
       hs.push_back(s);
       P.mixed.push_back(k);
     }
+    // the systems of a phase run side by side: together larger than the L2
+    // share, every system prefetches
+    double rows_bytes = 0.0;
+    for (size_t q = 0; q < hs.size(); ++q) rows_bytes += (double)hs[q].a.n * mixed_row_bytes(hs[q].m.ell_w);
+    P.pf = rows_bytes > g_prefetch_mb * 1048576.0;
+    for (auto& h : hs) h.m.pf = (h.m.ell_col && P.pf) ? 1 : 0;
     if (!hs.empty()) {
       TRY(dev_alloc(P.d_sys, hs.size(), b->stream));
       MGPU_CUDA(cudaMemcpyAsync(P.d_sys, hs.data(), sizeof(BatchSys) * hs.size(), cudaMemcpyHostToDevice, b->stream));
@@ -751,8 +760,9 @@ int mgpu_batch_create(MgpuCase* const* cases, int ncases, MgpuBatch** out) {
     set_error("cudaStreamCreate failed");
     return fail(MGPU_E_CUDA);
   }
-  b->cap = std::max(std::max(batch_capacity(true, true), batch_capacity(true, false)),
-                    std::max(batch_capacity(false, true), batch_capacity(false, false)));
+  b->cap = 1;
+  for (int ell = 0; ell < 3; ++ell)
+    b->cap = std::max(b->cap, std::max(batch_capacity(true, ell), batch_capacity(false, ell)));
   if (int e = dev_alloc(b->d_bars, b->cap, b->stream)) return fail(e);
   if (int e = dev_alloc(b->d_part, 8l * b->cap, b->stream)) return fail(e);
   if (int e = dev_alloc(b->d_flags, ncases + 2, b->stream)) return fail(e);

@@ -134,8 +134,12 @@ cudaEvent_t next_event(MgpuCase* c) {
 }
 
 MixedArgs mixed_args(const MgpuCase* c, bool bicg) {
-  return MixedArgs{c->d.a32, c->d.dinv32, c->d.w32, c->ctrl.mixed_tol > 0.0 ? c->ctrl.mixed_tol : 1e-4,
-                   bicg ? 1 : g_cheb_degree, g_cheb_ratio, c->d.ell_w, c->d.ell_col, c->d.ell_val, c->d.red32};
+  // a system larger than the L2 share given by l2_prefetch_mb streams from
+  // DRAM: its SpMV tiles prefetch the next tile's ELL entries
+  const bool big = (double)c->d.N * mixed_row_bytes(c->d.ell_w) > g_prefetch_mb * 1048576.0;
+  return MixedArgs{c->d.a32,   c->d.dinv32, c->d.w32,  c->ctrl.mixed_tol > 0.0 ? c->ctrl.mixed_tol : 1e-4,
+                   bicg ? 1 : g_cheb_degree, g_cheb_ratio, c->d.ell_w, c->d.ell_col, c->d.ell_val,
+                   c->d.red32, (c->d.ell_col && big) ? 1 : 0};
 }
 
 // factor (if needed) + solve; precond 0 ILU0, 1 Jacobi, 2 IC0. The mixed form

@@ -74,7 +74,12 @@ struct MixedArgs {
   const int* ell_col;  // column-major ELL columns, W*N (padding: the row itself)
   float* ell_val;      // FP32 values in the same layout (padding: 0)
   double* red;         // chunk reduction partials: mixed_red_words(N) doubles
+  int pf;              // 1: each SpMV tile prefetches the next tile's ELL entries into L2
 };
+
+// Device bytes a mixed solve streams per row: ELL columns and FP32 values,
+// the seven FP32 work vectors, x, b, r and the inverse diagonal.
+inline double mixed_row_bytes(int ell_w) { return 8.0 * ell_w + 4.0 * 7 + 8.0 * 3 + 4.0; }
 
 // The mixed-precision solves reduce over fixed row chunks (32 rows) and
 // super-chunks (256 rows), so their results do not depend on how rows are
@@ -167,8 +172,8 @@ int launch_factor(const KrylovArgs& a, int kind, cudaStream_t s);
 int krylov_grid(int n, int& block, int which);
 int launch_pcg_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s);
 int launch_bicgstab_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s);
-int batch_capacity(bool pcg, bool ell);
-int launch_mixed_batch(const LanePlan& p, bool pcg, bool ell, cudaStream_t s);
+int batch_capacity(bool pcg, int ell);  // ell: 0 CSR, 1 ELL, 2 ELL + L2 prefetch
+int launch_mixed_batch(const LanePlan& p, bool pcg, int ell, cudaStream_t s);
 int launch_spmv(int n, const int* rp, const int* col, const double* val, const double* x, double* y,
                 cudaStream_t s);
 

@@ -80,6 +80,7 @@ namespace mgpu {
 extern int g_cheb_degree;
 extern double g_cheb_ratio;
 extern int g_batch_reserve;
+extern int g_prefetch_mb;
 
 KrylovArgs base_args(MgpuCase* c);
 MixedArgs mixed_args(const MgpuCase* c, bool bicg);

@@ -47,6 +47,7 @@ int g_min_blocks = 1;
 }  // namespace
 int g_cheb_degree = 16;      // mixed form: Chebyshev-Jacobi degree of the pressure preconditioner
 int g_batch_reserve = 0;  // block slots batched launches leave to other streams
+int g_prefetch_mb = 96;   // mixed systems whose streamed bytes exceed this prefetch into L2
 int prewarm_streams(int n);  // case.cu
 double g_cheb_ratio = 1000.0; // and the ratio lambda_max / lambda_min of its interval
 namespace {
@@ -653,6 +654,8 @@ int set_tuning(const char* key, int value) {
     g_sweep_sleep = value;
   } else if (k == "batch_reserve_blocks" && value >= 0 && value <= 256) {
     g_batch_reserve = value;
+  } else if (k == "l2_prefetch_mb" && value >= 0) {
+    g_prefetch_mb = value;
   } else if (k == "stream_pool" && value >= 0 && value <= 1024) {
     if (int e = prewarm_streams(value)) return e;
   } else {

@@ -212,7 +212,7 @@ __device__ __forceinline__ float spmv32_ell(const MixedArgs& m, const float* x, 
   return acc;
 }
 
-template <bool L1, bool ELL>
+template <bool L1, int ELL>
 __device__ __forceinline__ float spmv32(const KrylovArgs& a, const MixedArgs& m, const float* x, int i) {
   if constexpr (ELL)
     return spmv32_ell<L1>(m, x, i, a.n);
@@ -244,13 +244,18 @@ struct Sp32 {
   const int* __restrict__ col;
   const float* __restrict__ a32;
   const float* __restrict__ dinv;
+  int pf;  // rows from a tile to the tile whose ELL entries it prefetches into L2 (0: none)
 };
 
-__device__ __forceinline__ Sp32 sp32_of(const KrylovArgs& a, const MixedArgs& m) {
-  return Sp32{a.n, m.ell_w, m.ell_col, m.ell_val, a.row_ptr, a.col, m.a32, m.dinv};
+__device__ __forceinline__ Sp32 sp32_of(const KrylovArgs& a, const MixedArgs& m, const Rows& rows) {
+  return Sp32{a.n, m.ell_w, m.ell_col, m.ell_val, a.row_ptr, a.col, m.a32, m.dinv, m.pf * kRows * rows.stride};
 }
 
-template <bool L1, bool ELL, bool FULL>
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+template <bool L1, int ELL, bool FULL>
 __device__ __forceinline__ void spmv32_rows(const Sp32& S, const float* x, const int (&i)[kRows],
                                             const bool (&in0)[kRows], float (&y)[kRows]) {
   bool in[kRows];
@@ -269,6 +274,22 @@ __device__ __forceinline__ void spmv32_rows(const Sp32& S, const float* x, const
           c[r][t] = S.ecol[(long)t * n + i[r]];
           v[r][t] = S.eval[(long)t * n + i[r]];
         }
+    if constexpr (ELL == 2) {
+      // the same rows of this block's next tile: DRAM -> L2 while this tile's
+      // gathers wait (no registers held)
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) {
+        const int j = i[r] + S.pf;
+        if (j < n) {
+#pragma unroll
+          for (int t = 0; t < WMAX; ++t)
+            if (t < W) {
+              prefetch_l2(S.ecol + (long)t * n + j);
+              prefetch_l2(S.eval + (long)t * n + j);
+            }
+        }
+      }
+    }
 #pragma unroll
     for (int r = 0; r < kRows; ++r)
 #pragma unroll
@@ -396,11 +417,11 @@ __device__ bool update_x(const KrylovArgs& a, const VGrid& g, const Rows& rows, 
 // D^-1 rr / theta (written by the caller's pass, followed by a barrier). The
 // result lands in zout (z0 or z1, ping-pong); the last pass also sums rr.z and
 // rr.rr, reduced before returning.
-template <bool L1, bool ELL>
+template <bool L1, int ELL>
 __device__ __forceinline__ bool cheb_apply(const KrylovArgs& a, const MixedArgs& m, VGrid& g, Red& R,
                                            const Rows& rows, const float* rr, float* dch, float* z0, float* z1,
                                            double lmax, float*& zout, double (&red)[2]) {
-  const Sp32 S = sp32_of(a, m);
+  const Sp32 S = sp32_of(a, m, rows);
   const double lmin = lmax / m.cheb_ratio;
   const double th = 0.5 * (lmax + lmin), de = 0.5 * (lmax - lmin), sg = th / de;
   double rho0 = 1.0 / sg;
@@ -451,11 +472,11 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
 // The SpMV passes of the Krylov loops.
 
 // p := z + beta p, q := A z + beta q (p := z, q := A z when first); p.q
-template <bool L1, bool ELL>
+template <bool L1, int ELL>
 __device__ __forceinline__ void pcg_fused_pass(const KrylovArgs& a, const MixedArgs& m, const Red& R,
                                                const Rows& rows, const float* z, float* p, float* q, float beta,
                                                bool first) {
-  const Sp32 S = sp32_of(a, m);
+  const Sp32 S = sp32_of(a, m, rows);
   MGPU_STEPS(rows, base) {
     MGPU_STEP_ROWS(rows, base, ii, in);
     MGPU_SPLIT_FULL(rows, base, FULL, {
@@ -478,10 +499,10 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
 }
 
 // v := A ph; r0.v
-template <bool L1, bool ELL>
+template <bool L1, int ELL>
 __device__ __forceinline__ void bicg_v_pass(const KrylovArgs& a, const MixedArgs& m, const Red& R, const Rows& rows,
                                             const float* ph, const float* r0, float* v) {
-  const Sp32 S = sp32_of(a, m);
+  const Sp32 S = sp32_of(a, m, rows);
   MGPU_STEPS(rows, base) {
     MGPU_STEP_ROWS(rows, base, ii, in);
     MGPU_SPLIT_FULL(rows, base, FULL, {
@@ -501,10 +522,10 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
 }
 
 // t := A sh; t.t and t.s
-template <bool L1, bool ELL>
+template <bool L1, int ELL>
 __device__ __forceinline__ void bicg_t_pass(const KrylovArgs& a, const MixedArgs& m, const Red& R, const Rows& rows,
                                             const float* sh, const float* s, float* t) {
-  const Sp32 S = sp32_of(a, m);
+  const Sp32 S = sp32_of(a, m, rows);
   MGPU_STEPS(rows, base) {
     MGPU_STEP_ROWS(rows, base, ii, in);
     MGPU_SPLIT_FULL(rows, base, FULL, {
@@ -527,7 +548,7 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
 // ---------------------------------------------------------------------------
 // PCG (pressure correction): Jacobi or Chebyshev-Jacobi preconditioned
 // ---------------------------------------------------------------------------
-template <bool L1, bool ELL>
+template <bool L1, int ELL>
 __device__ void pcg_mixed_body(const KrylovArgs& a, const MixedArgs& m, VGrid& g) {
   if (a.st->abort) return;
   const int n = a.n;
@@ -688,7 +709,7 @@ __device__ void pcg_mixed_body(const KrylovArgs& a, const MixedArgs& m, VGrid& g
 // ---------------------------------------------------------------------------
 // BiCGStab (momentum): right Jacobi preconditioning
 // ---------------------------------------------------------------------------
-template <bool L1, bool ELL>
+template <bool L1, int ELL>
 __device__ void bicgstab_mixed_body(const KrylovArgs& a, const MixedArgs& m, VGrid& g) {
   if (a.st->abort) return;
   const int n = a.n;
@@ -835,13 +856,13 @@ __device__ void bicgstab_mixed_body(const KrylovArgs& a, const MixedArgs& m, VGr
 // kernels
 // ---------------------------------------------------------------------------
 
-template <bool L1, bool ELL>
+template <bool L1, int ELL>
 __global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : 2) k_pcg_mixed(KrylovArgs a, MixedArgs m) {
   VGrid g = whole_grid(a.bar, a.partials);
   pcg_mixed_body<L1, ELL>(a, m, g);
 }
 
-template <bool L1, bool ELL>
+template <bool L1, int ELL>
 __global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : 2) k_bicgstab_mixed(KrylovArgs a, MixedArgs m) {
   VGrid g = whole_grid(a.bar, a.partials);
   bicgstab_mixed_body<L1, ELL>(a, m, g);
@@ -871,7 +892,7 @@ __device__ __forceinline__ int lane_fetch(const LanePlan& p, int cls) {
 // synchronises with __syncthreads): one body per kernel, inlined, with
 // the system's descriptor read through a read-only pointer, keeps the
 // descriptor fields out of the register budget.
-template <bool PCG, bool ELL>
+template <bool PCG, int ELL>
 __global__ void __launch_bounds__(256, 2) k_mixed_batch(LanePlan p) {
   __shared__ int s_idx;
   const int li = p.block_lane[blockIdx.x];
@@ -939,30 +960,46 @@ int launch_mixed(const void* fn1, const void* fnN, const KrylovArgs& a, const Mi
   return 0;
 }
 
-const void* batch_kernel(bool pcg, bool ell) {
-  return pcg ? (ell ? (const void*)k_mixed_batch<true, true> : (const void*)k_mixed_batch<true, false>)
-             : (ell ? (const void*)k_mixed_batch<false, true> : (const void*)k_mixed_batch<false, false>);
+// ell: 0 CSR, 1 ELL, 2 ELL with the L2 prefetch of the next tile
+const void* batch_kernel(bool pcg, int ell) {
+  if (pcg)
+    return ell == 2 ? (const void*)k_mixed_batch<true, 2>
+                    : ell == 1 ? (const void*)k_mixed_batch<true, 1> : (const void*)k_mixed_batch<true, 0>;
+  return ell == 2 ? (const void*)k_mixed_batch<false, 2>
+                  : ell == 1 ? (const void*)k_mixed_batch<false, 1> : (const void*)k_mixed_batch<false, 0>;
 }
+
+// A single-case solve's kernels: ELL (prefetching when the system is larger
+// than the L2 share, m.pf) or CSR; one block runs without the prefetch.
+int ell_mode(const MixedArgs& m) { return m.ell_col ? (m.pf ? 2 : 1) : 0; }
 
 }  // namespace
 
 int launch_pcg_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s) {
-  if (m.ell_col)
-    return launch_mixed((const void*)k_pcg_mixed<true, true>, (const void*)k_pcg_mixed<false, true>, a, m, s);
-  return launch_mixed((const void*)k_pcg_mixed<true, false>, (const void*)k_pcg_mixed<false, false>, a, m, s);
+  switch (ell_mode(m)) {
+    case 2:
+      return launch_mixed((const void*)k_pcg_mixed<true, 1>, (const void*)k_pcg_mixed<false, 2>, a, m, s);
+    case 1:
+      return launch_mixed((const void*)k_pcg_mixed<true, 1>, (const void*)k_pcg_mixed<false, 1>, a, m, s);
+    default:
+      return launch_mixed((const void*)k_pcg_mixed<true, 0>, (const void*)k_pcg_mixed<false, 0>, a, m, s);
+  }
 }
 
 int launch_bicgstab_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s) {
-  if (m.ell_col)
-    return launch_mixed((const void*)k_bicgstab_mixed<true, true>, (const void*)k_bicgstab_mixed<false, true>, a,
-                        m, s);
-  return launch_mixed((const void*)k_bicgstab_mixed<true, false>, (const void*)k_bicgstab_mixed<false, false>, a, m,
-                      s);
+  switch (ell_mode(m)) {
+    case 2:
+      return launch_mixed((const void*)k_bicgstab_mixed<true, 1>, (const void*)k_bicgstab_mixed<false, 2>, a, m, s);
+    case 1:
+      return launch_mixed((const void*)k_bicgstab_mixed<true, 1>, (const void*)k_bicgstab_mixed<false, 1>, a, m, s);
+    default:
+      return launch_mixed((const void*)k_bicgstab_mixed<true, 0>, (const void*)k_bicgstab_mixed<false, 0>, a, m, s);
+  }
 }
 
-int batch_capacity(bool pcg, bool ell) {
-  static int cap[4] = {0, 0, 0, 0};
-  const int idx = (pcg ? 2 : 0) + (ell ? 1 : 0);
+int batch_capacity(bool pcg, int ell) {
+  static int cap[6] = {0, 0, 0, 0, 0, 0};
+  const int idx = (pcg ? 3 : 0) + ell;
   if (cap[idx] == 0) {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
@@ -973,7 +1010,7 @@ int batch_capacity(bool pcg, bool ell) {
   return cap[idx];
 }
 
-int launch_mixed_batch(const LanePlan& p, bool pcg, bool ell, cudaStream_t s) {
+int launch_mixed_batch(const LanePlan& p, bool pcg, int ell, cudaStream_t s) {
   if (p.nblocks <= 0) return 0;
   if (p.nblocks > batch_capacity(pcg, ell)) {
     set_error("batched solve: more blocks than can be co-resident");

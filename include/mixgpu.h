@@ -149,7 +149,11 @@ int mgpu_case_destroy(MgpuCase* c);
 int mgpu_case_device_bytes(const MgpuCase* c, int64_t* bytes);
 
 /* Fields in/out: fields_t (mod_uns_fields.f90:29-79). u is u(3,ncells) AoS,
- * p(ncells), flux(nfaces). Any pointer may be NULL to skip that field. */
+ * p(ncells), flux(nfaces), gu(3,3,ncells). Any pointer may be NULL to skip
+ * that field. The AoS <-> device-plane transposes run on the device (a staging
+ * buffer of up to 9*ncells doubles is kept with the case after the first
+ * call); each field is one copy to or from the caller's array, and the call
+ * returns when every copy is done. Page-locked host arrays copy fastest. */
 int mgpu_fields_upload(MgpuCase* c, const double* u, const double* p, const double* flux,
                        const double* u_old, const double* u_old_old);
 int mgpu_fields_download(MgpuCase* c, double* u, double* p, double* flux, double* gp,

@@ -77,6 +77,40 @@ int copy_sync(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cud
   return 0;
 }
 
+__global__ void k_planes_to_cells(const double* __restrict__ src, long n, int planes, bool grad,
+                                  double* __restrict__ dst) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;  // output index: cell-major
+  if (t >= n * planes) return;
+  const long i = t / planes;
+  const int k = (int)(t - i * planes);
+  const int q = grad ? (k % 3) * 3 + k / 3 : k;
+  dst[t] = src[q * n + i];
+}
+
+__global__ void k_cells_to_planes(const double* __restrict__ src, long n, int planes, double* __restrict__ dst) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;  // output index: plane-major
+  if (t >= n * planes) return;
+  const long k = t / n;
+  const long i = t - k * n;
+  dst[t] = src[planes * i + k];
+}
+
+int launch_planes_to_cells(const double* src, long n, int planes, bool grad, double* dst, cudaStream_t s) {
+  const long tot = n * planes;
+  if (tot == 0) return 0;
+  k_planes_to_cells<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(src, n, planes, grad, dst);
+  MGPU_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int launch_cells_to_planes(const double* src, long n, int planes, double* dst, cudaStream_t s) {
+  const long tot = n * planes;
+  if (tot == 0) return 0;
+  k_cells_to_planes<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(src, n, planes, dst);
+  MGPU_CUDA(cudaGetLastError());
+  return 0;
+}
+
 int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
   g_err = std::string(what) + ": " + cudaGetErrorString(e) + " (" + file + ":" + std::to_string(line) + ")";
   return MGPU_E_CUDA;
@@ -85,6 +119,20 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
 }  // namespace mgpu
 
 using namespace mgpu;
+
+namespace mgpu {
+int ensure_stage(MgpuCase* c, size_t n) {
+  if (c->stage_n >= n) return 0;
+  if (c->stage) MGPU_CUDA(cudaFreeAsync(c->stage, c->stream));
+  c->stage = nullptr;
+  c->stage_n = 0;
+  void* q = nullptr;
+  MGPU_CUDA(cudaMallocAsync(&q, sizeof(double) * std::max<size_t>(n, 1), c->stream));
+  c->stage = (double*)q;
+  c->stage_n = n;
+  return 0;
+}
+}  // namespace mgpu
 
 namespace mgpu {
 
@@ -510,45 +558,45 @@ int mgpu_fields_upload(MgpuCase* c, const double* u, const double* p, const doub
                        const double* u_old_old) {
   if (!c) return MGPU_E_ARG;
   const long N = c->d.N;
+  cudaStream_t s = c->stream;
+  // cell-major u(3,N) -> device planes: one copy into the staging buffer, then
+  // the transpose on the device (the next copy into the buffer waits for it:
+  // same stream)
   auto up3 = [&](double* dst, const double* src) -> int {
-    std::vector<double> soa(3 * N);
-    for (long i = 0; i < N; ++i)
-      for (int k = 0; k < 3; ++k) soa[k * N + i] = src[3 * i + k];
-    TRY(copy_sync(dst, soa.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice, c->stream));
+    TRY(mgpu::ensure_stage(c, 3 * (size_t)N));
+    MGPU_CUDA(cudaMemcpyAsync(c->stage, src, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, s));
+    TRY(mgpu::launch_cells_to_planes(c->stage, N, 3, dst, s));
     return 0;
   };
   if (u) TRY(up3(c->d.u, u));
   if (u_old) TRY(up3(c->d.u_old, u_old));
   if (u_old_old) TRY(up3(c->d.u_old_old, u_old_old));
-  if (p) TRY(copy_sync(c->d.p, p, sizeof(double) * N, cudaMemcpyHostToDevice, c->stream));
-  if (flux) TRY(copy_sync(c->d.flux, flux, sizeof(double) * c->d.F, cudaMemcpyHostToDevice, c->stream));
+  if (p) MGPU_CUDA(cudaMemcpyAsync(c->d.p, p, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  if (flux) MGPU_CUDA(cudaMemcpyAsync(c->d.flux, flux, sizeof(double) * c->d.F, cudaMemcpyHostToDevice, s));
+  MGPU_CUDA(cudaStreamSynchronize(s));
   return 0;
 }
 
 int mgpu_fields_download(MgpuCase* c, double* u, double* p, double* flux, double* gp, double* gu, double* apc) {
   if (!c) return MGPU_E_ARG;
-  MGPU_CUDA(cudaStreamSynchronize(c->stream));
   const long N = c->d.N;
-  auto down = [&](double* dst, const double* src, int planes) -> int {
-    std::vector<double> soa((size_t)planes * N);
-    TRY(copy_sync(soa.data(), src, sizeof(double) * planes * N, cudaMemcpyDeviceToHost, c->stream));
-    for (long i = 0; i < N; ++i)
-      for (int k = 0; k < planes; ++k) dst[(long)planes * i + k] = soa[k * N + i];
+  cudaStream_t s = c->stream;
+  // device planes -> cell-major arrays, transposed on the device into the
+  // staging buffer and copied out from there; gu's device plane comp*3+dir
+  // goes to the Fortran index comp + 3*dir + 9*cell
+  auto down = [&](double* dst, const double* src, int planes, bool grad) -> int {
+    TRY(mgpu::ensure_stage(c, (size_t)planes * N));
+    TRY(mgpu::launch_planes_to_cells(src, N, planes, grad, c->stage, s));
+    MGPU_CUDA(cudaMemcpyAsync(dst, c->stage, sizeof(double) * planes * N, cudaMemcpyDeviceToHost, s));
     return 0;
   };
-  if (u) TRY(down(u, c->d.u, 3));
-  if (gp) TRY(down(gp, c->d.gp, 3));
-  if (gu) {
-    // device planes comp*3+dir -> Fortran gu(comp,dir,cell): index comp + 3*dir + 9*cell
-    std::vector<double> soa(9 * N);
-    TRY(copy_sync(soa.data(), c->d.gu, sizeof(double) * 9 * N, cudaMemcpyDeviceToHost, c->stream));
-    for (long i = 0; i < N; ++i)
-      for (int comp = 0; comp < 3; ++comp)
-        for (int dir = 0; dir < 3; ++dir) gu[9 * i + comp + 3 * dir] = soa[(comp * 3 + dir) * N + i];
-  }
-  if (p) TRY(copy_sync(p, c->d.p, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
-  if (apc) TRY(copy_sync(apc, c->d.apc, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
-  if (flux) TRY(copy_sync(flux, c->d.flux, sizeof(double) * c->d.F, cudaMemcpyDeviceToHost, c->stream));
+  if (u) TRY(down(u, c->d.u, 3, false));
+  if (gp) TRY(down(gp, c->d.gp, 3, false));
+  if (gu) TRY(down(gu, c->d.gu, 9, true));
+  if (p) MGPU_CUDA(cudaMemcpyAsync(p, c->d.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+  if (apc) MGPU_CUDA(cudaMemcpyAsync(apc, c->d.apc, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+  if (flux) MGPU_CUDA(cudaMemcpyAsync(flux, c->d.flux, sizeof(double) * c->d.F, cudaMemcpyDeviceToHost, s));
+  MGPU_CUDA(cudaStreamSynchronize(s));
   return 0;
 }
 

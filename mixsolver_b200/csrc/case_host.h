@@ -47,6 +47,8 @@ struct MgpuCase {
   int kblock = 256;
   int run_mode = -1;  // batched runs: 0 SIMPLE, 1 PISO after mgpu_case_begin, -1 none
   int run_gen = 0;    // counts mgpu_case_begin calls
+  double* stage = nullptr;  // device staging of cell-major field copies (grown on demand)
+  size_t stage_n = 0;
 
   template <typename T>
   int alloc(T*& p, size_t n) {
@@ -71,6 +73,7 @@ struct MgpuCase {
     if (ev_run0) cudaEventDestroy(ev_run0);
     if (ev_run1) cudaEventDestroy(ev_run1);
     for (void* p : allocs) cudaFreeAsync(p, stream);
+    if (stage) cudaFreeAsync(stage, stream);
     if (stream) mgpu::release_stream(stream);
   }
 };
@@ -92,5 +95,11 @@ int krylov(MgpuCase* c, KrylovArgs a, bool bicg, cudaStream_t s);
 // fresh device status for a run of nrec-1 iterations (ts_order 0 steady)
 int reset_status(MgpuCase* c, int ts_order, int nrec);
 int ensure_recs(MgpuCase* c, int n);
+// device staging buffer of at least n doubles (stream-ordered, kept until the case is destroyed)
+int ensure_stage(MgpuCase* c, size_t n);
+// dst[planes*i + k] = src[q*n + i], q = k (grad: q = (k%3)*3 + k/3, the 3x3 gradient's transpose)
+int launch_planes_to_cells(const double* src, long n, int planes, bool grad, double* dst, cudaStream_t s);
+// dst[k*n + i] = src[planes*i + k]
+int launch_cells_to_planes(const double* src, long n, int planes, double* dst, cudaStream_t s);
 
 }  // namespace mgpu

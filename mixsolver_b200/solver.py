@@ -70,14 +70,36 @@ class UnsCase:
         abi.check(lib, lib.mgpu_fields_upload(self.h, dptr(u), dptr(p), dptr(flux), dptr(u_old), dptr(u_old_old)),
                   "mgpu_fields_upload")
 
-    def fields(self):
+    FIELD_SHAPES = {"u": ("N", 3), "p": ("N",), "flux": ("F",), "gp": ("N", 3), "gu": ("N", 3, 3), "apc": ("N",)}
+
+    def fields(self, out=None):
+        """Host copies of u (N,3), p (N), flux (F), gp (N,3), gu (N,3,3) indexed
+        [cell, component, direction] and apc (N).
+
+        out: optional dict of caller-owned float64 C-contiguous arrays with some of
+        those keys, filled in place (page-locked arrays copy fastest); only those
+        fields are read back. Its "gu" array receives the C-ABI's layout
+        gu(component, direction, cell), i.e. [cell, direction, component]; the
+        returned "gu" is its transposed view."""
         N, F = self.N, self.F
-        u = np.zeros((N, 3)); p = np.zeros(N); flux = np.zeros(F)
-        gp = np.zeros((N, 3)); gu = np.zeros((N, 3, 3)); apc = np.zeros(N)
+        dims = {"N": N, "F": F}
+        if out is None:
+            arrs = {k: np.empty(tuple(dims.get(d, d) for d in shp)) for k, shp in self.FIELD_SHAPES.items()}
+        else:
+            arrs = {}
+            for k, a in out.items():
+                want = tuple(dims.get(d, d) for d in self.FIELD_SHAPES[k])
+                if a.dtype != np.float64 or a.shape != want or not a.flags.c_contiguous:
+                    raise ValueError(f"fields(out): {k} must be C-contiguous float64 of shape {want}")
+                arrs[k] = a
+        g = lambda k: dptr(arrs[k]) if k in arrs else None
         lib = _lib()
-        abi.check(lib, lib.mgpu_fields_download(self.h, dptr(u), dptr(p), dptr(flux), dptr(gp), dptr(gu), dptr(apc)),
+        abi.check(lib, lib.mgpu_fields_download(self.h, g("u"), g("p"), g("flux"), g("gp"), g("gu"), g("apc")),
                   "mgpu_fields_download")
-        return dict(u=u, p=p, flux=flux, gp=gp, gu=gu.transpose(0, 2, 1).copy(), apc=apc)
+        res = dict(arrs)
+        if "gu" in res:
+            res["gu"] = res["gu"].transpose(0, 2, 1)
+        return res
 
     def _run(self, fn, nsteps, logcap):
         recs = (MgpuIterRec * max(logcap, 1))()

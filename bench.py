@@ -74,6 +74,48 @@ def dist_env():
     return rank, world, local
 
 
+def init_ranks(world, backend="nccl", timeout_s=600):
+    """One process per GPU: the process group of a run with world > 1 ranks
+    (rendezvous from MASTER_ADDR / MASTER_PORT); nothing for one rank."""
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+
+
+def rank_barrier(world, cuda=True):
+    """Device idle on this rank, then every rank at the same point."""
+    import torch
+    if cuda:
+        torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v, world, device="cuda"):
+    """The largest of the ranks' values (device times are taken as the max)."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, world, max_ms):
+    """Whole-job throughput: the units all ranks processed over the slowest rank's time."""
+    return world * units_per_rank / (max_ms / 1e3)
+
+
+def close_ranks(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def workload(args, order_fn):
     from mixsolver_b200 import abi, cases
     nx, ny, nz = (int(v) for v in args.cells.split("x"))
@@ -178,9 +220,7 @@ def run_ours(args):
     rank, world, local = dist_env()
     import torch
     torch.cuda.set_device(local)
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    init_ranks(world)
     from mixsolver_b200 import abi
     from mixsolver_b200 import solver as S
     mesh, ctrl = workload(args, S.rcm_order)
@@ -188,19 +228,8 @@ def run_ours(args):
     nnz = N + 2 * mesh.n_interior()
     mixed = args.precision == "mixed"
 
-    def barrier():
-        torch.cuda.synchronize()
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        import torch.distributed as dist
-        t = torch.tensor([v], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = lambda: rank_barrier(world)
+    ranks_max = lambda v: max_over_ranks(v, world)
 
     # the FP64 parity form over the same W + K outer iterations from rest (comparison leg)
     fp64 = None
@@ -215,8 +244,8 @@ def run_ours(args):
         ier, log64 = k64.simple_run(args.steps, logcap=args.steps)
         barrier()
         assert ier == 0
-        t64 = max_over_ranks(k64.timing()["total_ms"])
-        fp64 = dict(value=world * args.steps / (t64 / 1e3), fields=k64.fields(),
+        t64 = ranks_max(k64.timing()["total_ms"])
+        fp64 = dict(value=job_rate(args.steps, world, t64), fields=k64.fields(),
                     ppe_its=float(np.mean([r["lin_it"][3] for r in log64])))
         k64.close()
     case = S.UnsCase(mesh, ctrl, device=local)
@@ -231,8 +260,8 @@ def run_ours(args):
     barrier()
     assert ier == 0 and len(log) == args.steps, (ier, len(log))
     tm = case.timing()
-    mx = max_over_ranks(tm["total_ms"])
-    value = world * args.steps / (mx / 1e3)
+    mx = ranks_max(tm["total_ms"])
+    value = job_rate(args.steps, world, mx)
     solve_ms = case.solve_times()
     ppe_ms = solve_ms[3::4] if len(solve_ms) >= 4 else solve_ms
     pct = lambda a, q: float(np.percentile(a, q)) if len(a) else None
@@ -272,7 +301,7 @@ def run_ours(args):
         case.upload(u=hbuf["u"], p=hbuf["p"], flux=hbuf["flux"])
         ier, _ = case.simple_run(1, logcap=1)
         case.fields(out=hbuf)
-    e2e_t = time.perf_counter() - t0
+    e2e_t = max_over_ranks(time.perf_counter() - t0, world)
     e2e = {"value": world * e2e_steps / e2e_t, "unit": UNIT, "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h}
     out = {
@@ -312,10 +341,7 @@ def run_ours(args):
     }
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args, mesh, ctrl)
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-        dist.destroy_process_group()
+    close_ranks(world)
     if rank == 0:
         print(json.dumps(out), flush=True)
 
@@ -385,9 +411,7 @@ def run_piso(args):
     import copy
     import torch
     torch.cuda.set_device(local)
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    init_ranks(world)
     from mixsolver_b200 import abi, cases, meshgen
     from mixsolver_b200 import solver as S
     total = args.fp64_steps + args.warmup + args.steps
@@ -399,19 +423,8 @@ def run_piso(args):
     nnz = N + 2 * mesh.n_interior()
     u0 = meshgen.taylor_green(S.compute_geometry(mesh)["xc"], seed=rank)
 
-    def barrier():
-        torch.cuda.synchronize()
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        import torch.distributed as dist
-        t = torch.tensor([v], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = lambda: rank_barrier(world)
+    ranks_max = lambda v: max_over_ranks(v, world)
 
     def make(prec):
         c = copy.deepcopy(ctrl)
@@ -424,7 +437,7 @@ def run_piso(args):
     k64 = make(abi.PREC_FP64)
     ier, log64 = k64.piso_run(args.fp64_steps, logcap=args.fp64_steps)
     assert ier == 0, f"FP64 leg ier={ier}"
-    t64 = max_over_ranks(k64.timing()["total_ms"])
+    t64 = ranks_max(k64.timing()["total_ms"])
     f64 = k64.fields()
     k64.close()
     # mixed form: the same steps, then warm-up and the timed steps
@@ -433,7 +446,7 @@ def run_piso(args):
     assert ier == 0, f"mixed comparison steps ier={ier}"
     fc = case.fields()
     rel = {k: float(np.linalg.norm(fc[k] - f64[k]) / np.linalg.norm(f64[k])) for k in ("u", "p", "flux")}
-    t_cmp = max_over_ranks(case.timing()["total_ms"])
+    t_cmp = ranks_max(case.timing()["total_ms"])
     if args.warmup:
         ier, _ = case.piso_run(args.warmup, logcap=args.warmup)
         assert ier == 0, f"warm-up ier={ier}"
@@ -446,8 +459,8 @@ def run_piso(args):
     barrier()
     assert ier == 0 and len(log) == args.steps, (ier, len(log))
     tm = case.timing()
-    mx = max_over_ranks(tm["total_ms"])
-    value = world * args.steps / (mx / 1e3)
+    mx = ranks_max(tm["total_ms"])
+    value = job_rate(args.steps, world, mx)
     solve_ms = case.solve_times()
     nsol = 3 + ctrl.n_correct
     ppe_ms = np.concatenate([solve_ms[3 + j::nsol] for j in range(ctrl.n_correct)]) if len(solve_ms) >= nsol else solve_ms
@@ -475,7 +488,7 @@ def run_piso(args):
         case.upload(u=hbuf["u"])
         ier, _ = case.piso_run(1, logcap=1)
         case.fields(out=hbuf)
-    e2e_t = time.perf_counter() - t0
+    e2e_t = max_over_ranks(time.perf_counter() - t0, world)
     its = lambda lg, sl: float(np.mean([sum(r["lin_it"][c] for c in sl) for r in lg]))
     out = {
         "metric": PISO_METRIC, "value": value, "unit": "time_steps/s", "n_gpus": world, "steps": args.steps,
@@ -512,10 +525,7 @@ def run_piso(args):
         "wall_s": wall,
     }
     case.close()
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-        dist.destroy_process_group()
+    close_ranks(world)
     if rank == 0:
         print(json.dumps(out), flush=True)
 
@@ -549,6 +559,7 @@ def run_batch(args):
     torch.cuda.set_device(local)
     from mixsolver_b200 import abi
     from mixsolver_b200 import solver as S
+    init_ranks(world)
     specs = batch_specs(args.cases, seed=rank)
     t0 = time.perf_counter()
     import multiprocessing as mp
@@ -579,15 +590,16 @@ def run_batch(args):
     policy = None if args.policy == "auto" else tuple(int(v) for v in args.policy.split("x"))
     B = S.CaseBatch(objs, policy=policy)
     B.step(args.warmup)
-    torch.cuda.synchronize()
+    rank_barrier(world)
     i0 = B.info()
     with ClockSampler(local) as clk:
         w0 = time.perf_counter()
         active = B.step(args.steps)
         wall = time.perf_counter() - w0
+    rank_barrier(world)
     i1 = B.info()
-    ms = i1["step_ms"] - i0["step_ms"]
-    value = args.cases * args.steps / (ms / 1e3)
+    ms = max_over_ranks(i1["step_ms"] - i0["step_ms"], world)
+    value = job_rate(args.cases * args.steps, world, ms)
     B.set_profiling(True)
     B.step(nprof)
     ip = B.info()
@@ -618,7 +630,7 @@ def run_batch(args):
         B2.step(1)
         for o, f in zip(objs, hf):
             o.fields(out=f)
-    e2e_t = time.perf_counter() - w0
+    e2e_t = max_over_ranks(time.perf_counter() - w0, world)
     F = np.array([m.nfaces for m, _ in meshes])
     h2d = int(np.sum((5 * cells + F) * 8))
     d2h = int(np.sum((18 * cells + F) * 8))
@@ -670,11 +682,12 @@ def run_batch(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "kernel": "whole batched iteration (Krylov bytes / step time)",
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
-        "e2e": {"value": args.cases * e2e_steps / e2e_t, "unit": "case_iters/s", "h2d_bytes_per_step": h2d,
+        "e2e": {"value": world * args.cases * e2e_steps / e2e_t, "unit": "case_iters/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": i1["launches_per_iter"] * args.steps,
         "clocks": clk.summary(), "wall_s": wall, "active_after": active,
     }
+    close_ranks(world)
     if rank == 0:
         print(json.dumps(out), flush=True)
 

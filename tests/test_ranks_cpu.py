@@ -1,0 +1,54 @@
+"""The bench's multi-rank plumbing on CPU: two gloo ranks (one process each,
+as torchrun launches one per GPU) take the same barrier, agree on the max of
+their times and report the whole-job rate from it."""
+import multiprocessing as mp
+import os
+import socket
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    sys.path.insert(0, ROOT)
+    import bench
+    r, w, _ = bench.dist_env()
+    bench.init_ranks(w, backend="gloo", timeout_s=60)
+    bench.rank_barrier(w, cuda=False)
+    ms = 100.0 + 50.0 * r  # rank 1 is the slow one
+    mx = bench.max_over_ranks(ms, w, device="cpu")
+    rate = bench.job_rate(10, w, mx)
+    bench.close_ranks(w)
+    q.put((r, mx, rate))
+
+
+def test_two_gloo_ranks_agree_on_max_and_rate():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [o[0] for o in out] == [0, 1]
+    for _, mx, rate in out:
+        assert mx == 150.0
+        assert abs(rate - 2 * 10 / 0.150) < 1e-9
+
+
+def test_one_rank_needs_no_group():
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.max_over_ranks(3.5, 1) == 3.5
+    assert bench.job_rate(10, 1, 100.0) == 100.0

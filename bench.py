@@ -50,10 +50,10 @@ def parse():
     ap.add_argument("--lin-max", type=int, default=1000)
     ap.add_argument("--cpu-steps", type=int, default=2, help="oracle outer iterations for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="channel", choices=["channel", "batch", "serve", "piso"],
+    ap.add_argument("--workload", default="channel", choices=["channel", "batch", "serve", "piso", "pimple"],
                     help="channel: one 524k-cell case (default); batch: many 3-D cavities in one batch; "
                          "serve: a Poisson stream of SIMPLE / PISO requests; piso: transient PISO on "
-                         "80^3 x 6 tets")
+                         "80^3 x 6 tets; pimple: transient PIMPLE on the 80 x 80 x 1 lid-driven cavity")
     ap.add_argument("--tet-n", type=int, default=80, help="piso: hexes per cube edge (each split into 6 tets)")
     ap.add_argument("--fp64-steps", type=int, default=3, help="piso: time steps of the FP64 comparison leg")
     ap.add_argument("--rate", type=float, default=50.0, help="serve: arrivals per second")
@@ -530,6 +530,131 @@ def run_piso(args):
         print(json.dumps(out), flush=True)
 
 
+PIMPLE_METRIC = "PIMPLE time steps/s (FP64), 2-D lid-driven cavity Re 1000, 80 x 80 x 1"
+PIMPLE_PUBLISHED_STEPS_PER_S = 1.0 / 0.182  # the reference's 6000-step run: 18.2 min, MPI np = 4
+
+
+def pimple_case():
+    """The reference's transient cavity run: 80 x 80 x 1 hex (zones 4 symmetry /
+    5 wall, lid u = (1,0,0) on y = 1), rho = 1, mu = 1e-3 (Re 1000), dt = 0.01,
+    2 outer iterations x 2 pressure corrections per step, alpha_u = 0.7,
+    limited second-order upwind (conv_blend 1), no non-orthogonal correction,
+    PCG+IC(0) pressure and BiCGStab+ILU(0) momentum to 1e-8 (lin_max 300)."""
+    from mixsolver_b200 import abi, cases
+    mesh, ctrl = cases.cavity2d(80, mu=1.0e-3, conv_blend=1.0, nonorth=0.0)
+    ctrl.transient = True
+    ctrl.dt = 0.01
+    ctrl.n_time_max = 10 ** 6
+    ctrl.n_outer_iter = 2
+    ctrl.n_correct = 2
+    ctrl.alpha_u = 0.7
+    ctrl.lin_tol = 1e-8
+    ctrl.lin_max = 300
+    ctrl.ppe_precond = abi.PPE_IC0
+    ctrl.mom_solver = abi.MOM_ILU0
+    return mesh, ctrl
+
+
+def run_pimple(args):
+    """Transient PIMPLE (pimple_run_mpi at one rank) on the 80 x 80 x 1 cavity
+    of :func:`pimple_case`, from rest, W warm-up and K timed time steps through
+    mgpu_pimple_run; `value` in time steps per second over all ranks (one case
+    per GPU). The measured form (--precision, default mixed: FP32 Krylov
+    inside FP64 refinement to the same lin_tol) runs beside the FP64 parity
+    form (the reference's arithmetic: exact IC(0)/ILU(0) sweeps), over the same
+    steps; the line reports both rates and the relative L2 difference of u, p,
+    flux after them. The reference publishes 0.182 s per step for this run
+    (CPU, MPI np = 4), so `vs_baseline` is value / 5.49."""
+    rank, world, local = dist_env()
+    import copy
+    import torch
+    torch.cuda.set_device(local)
+    init_ranks(world)
+    from mixsolver_b200 import abi
+    from mixsolver_b200 import solver as S
+    mesh, ctrl = pimple_case()
+    N, F = mesh.ncells, mesh.nfaces
+    mixed = args.precision == "mixed"
+
+    def leg(prec):
+        c = copy.deepcopy(ctrl)
+        c.precision = prec
+        k = S.UnsCase(mesh, c, device=local)
+        ier, _ = k.pimple_run(args.warmup, logcap=args.warmup)
+        assert ier == 0, f"warm-up ier={ier}"
+        rank_barrier(world)
+        with ClockSampler(local) as clk:
+            t0 = time.perf_counter()
+            ier, log = k.pimple_run(args.steps, logcap=args.steps)
+            wall = time.perf_counter() - t0
+        rank_barrier(world)
+        assert ier == 0 and len(log) == args.steps, (ier, len(log))
+        tm = k.timing()
+        mx = max_over_ranks(tm["total_ms"], world)
+        return k, log, tm, mx, clk, wall
+
+    k64, log64, _, mx64, _, _ = leg(abi.PREC_FP64)
+    f64 = k64.fields()
+    k64.close()
+    case, log, tm, mx, clk, wall = leg(abi.PREC_MIXED if mixed else abi.PREC_FP64)
+    value = job_rate(args.steps, world, mx)
+    f = case.fields()
+    rel = {k: float(np.linalg.norm(f[k] - f64[k]) / np.linalg.norm(f64[k])) for k in ("u", "p", "flux")}
+    # end to end through the public API: host fields in (page-locked), one time
+    # step, fields out into page-locked arrays
+    hbuf = pinned_fields(case)
+    case.fields(out=hbuf)
+    h2d = (3 * N + N + F) * 8
+    d2h = (3 * N + N + F + 3 * N + 9 * N + N) * 8
+    rank_barrier(world)
+    e2e_steps = max(2, min(args.steps, 20))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        case.upload(u=hbuf["u"], p=hbuf["p"], flux=hbuf["flux"])
+        ier, _ = case.pimple_run(1, logcap=1)
+        case.fields(out=hbuf)
+    e2e_t = max_over_ranks(time.perf_counter() - t0, world)
+    out = {
+        "metric": PIMPLE_METRIC, "value": value, "unit": "time_steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": mx / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": value / (world * PIMPLE_PUBLISHED_STEPS_PER_S),
+        "dtype": "f32-inner/f64-refinement" if mixed else "f64",
+        "data": "synthetic (the reference's 80 x 80 x 1 cavity layout, generated)",
+        "config": {"workload": "transient PIMPLE, 2-D lid-driven cavity Re 1000, 80x80x1 hex (6400 cells), dt 0.01, "
+                               "2 outer x 2 pressure corrections, alpha_u 0.7, conv_blend 1, lin_tol 1e-8; "
+                               + ("mixed form: FP32-inner/FP64-refinement BiCGStab-Jacobi and PCG with "
+                                  "Chebyshev-Jacobi" if mixed else "FP64 form: ILU(0) momentum, IC(0) PPE"),
+                   "cells": N, "faces": F, "parallelism": f"replicas x{world}",
+                   "l2": "working set ~5 MB fits L2 (as the reference's own run)",
+                   "published": "0.182 s/step (5.5 steps/s), CPU MPI np=4, cluster_cases/cavity_Re1000/README.md:118",
+                   "linear_iterations_per_step_max": int(max(r["itl_max"] for r in log)),
+                   "fp64_form": {"time_steps_per_s": job_rate(args.steps, world, mx64),
+                                 "linear_iterations_per_step_max": int(max(r["itl_max"] for r in log64)),
+                                 "solvers": "BiCGStab+ILU(0) momentum, PCG+IC(0) pressure (exact sweeps, parity form)"},
+                   "rel_l2_vs_fp64": rel, "rel_l2_after_steps": args.warmup + args.steps,
+                   "t_end": log[-1]["t_now"]},
+        "roofline": None,
+        "e2e": {"value": world * e2e_steps / e2e_t, "unit": "time_steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": tm["gpu_launches"],
+        "clocks": clk.summary(),
+        "wall_s": wall,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        oc = O.OracleCase(mesh, ctrl)
+        k = 5
+        t0 = time.perf_counter()
+        ier, _ = oc.pimple_run(k)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": k / dt, "unit": "time_steps/s", "cores": 1, "kind": "port",
+                               "sample": f"{k} PIMPLE steps of the same cavity from rest, {dt:.1f} s"}
+    case.close()
+    close_ranks(world)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def batch_specs(ncases, seed=0):
     """Cube edges with cell counts log-uniform in [16^3, 64^3] and Re uniform in
     [100, 2000], seeded: the batched workload's 3-D lid-driven cavities."""
@@ -818,5 +943,7 @@ if __name__ == "__main__":
         run_serve(a)
     elif a.workload == "piso":
         run_piso(a)
+    elif a.workload == "pimple":
+        run_pimple(a)
     else:
         run_ours(a)

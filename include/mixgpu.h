@@ -98,7 +98,7 @@ typedef struct {
   int32_t precision; /* MGPU_PREC_* */
   double mixed_tol;  /* inner FP32 relative tolerance per refinement sweep */
   int32_t nbc;
-  int32_t pad0;
+  int32_t n_outer_iter; /* PIMPLE outer iterations per time step (<= 0: 1) */
   MgpuBcSpec bc[MGPU_MAXBC];
 } MgpuCtrl;
 
@@ -169,6 +169,16 @@ int mgpu_simple_run(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* 
  * *ier: 0, 30 transient=false, 31 dt<=0, 33 momentum breakdown, 34 PPE
  * breakdown, 60 non-finite. */
 int mgpu_piso_run(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nrec, int* ier);
+
+/* Transient PIMPLE: pimple_run_mpi at one rank (mod_uns_simple_mpi.f90:580-850):
+ * per time step one history shift, then n_outer_iter outer iterations of the
+ * momentum predictor with alpha_u relaxation on top of the time term,
+ * apc = ap / alpha_u, gradients and Rhie-Chow fluxes, and n_correct pressure
+ * corrections. A record per time step: lin_it/lin_res of the last outer
+ * iteration's solves, itl_max and ressum over all of them.
+ * *ier: 0, 50 transient=false, 51 dt<=0, 53 momentum breakdown, 54 PPE
+ * breakdown, 60 non-finite. */
+int mgpu_pimple_run(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nrec, int* ier);
 
 /* First non-finite value: nan_scan (mod_uns_simple.f90:2375-2426). field:
  * 1 u_x, 2 u_y, 3 u_z, 4 p, 5 T, 6 T_s; cell 1-based; kind 1 NaN, 2 Inf;

@@ -52,7 +52,7 @@ class MgpuCtrl(C.Structure):
                 ("transient", C.c_int32), ("time_scheme", C.c_int32), ("dt", C.c_double),
                 ("n_time_max", C.c_int32), ("n_correct", C.c_int32), ("body_force", C.c_double * 3),
                 ("inlet_ramp", C.c_int32), ("precision", C.c_int32), ("mixed_tol", C.c_double),
-                ("nbc", C.c_int32), ("pad0", C.c_int32), ("bc", MgpuBcSpec * MAXBC)]
+                ("nbc", C.c_int32), ("n_outer_iter", C.c_int32), ("bc", MgpuBcSpec * MAXBC)]
 
 
 class MgpuMesh(C.Structure):
@@ -121,6 +121,7 @@ class Ctrl:
     dt: float = 0.0
     n_time_max: int = 0
     n_correct: int = 2
+    n_outer_iter: int = 1
     body_force: Sequence[float] = (0.0, 0.0, 0.0)
     inlet_ramp: int = 1
     precision: int = PREC_FP64
@@ -133,7 +134,7 @@ class Ctrl:
                      "nonorth_corr", "dt", "mixed_tol"):
             setattr(c, name, float(getattr(self, name)))
         for name in ("outer_max", "lin_max", "ppe_precond", "mom_solver", "time_scheme",
-                     "n_time_max", "n_correct", "inlet_ramp", "precision"):
+                     "n_time_max", "n_correct", "n_outer_iter", "inlet_ramp", "precision"):
             setattr(c, name, int(getattr(self, name)))
         c.transient = 1 if self.transient else 0
         for k in range(3):
@@ -204,7 +205,7 @@ def records_to_list(recs, n: int) -> list:
 # Every symbol include/mixgpu.h declares (checked by the CPU test suite).
 EXPORTS = ["mgpu_version", "mgpu_last_error", "mgpu_set_device", "mgpu_case_create",
            "mgpu_case_destroy", "mgpu_case_device_bytes", "mgpu_fields_upload",
-           "mgpu_fields_download", "mgpu_simple_run", "mgpu_piso_run", "mgpu_nan_scan",
+           "mgpu_fields_download", "mgpu_simple_run", "mgpu_piso_run", "mgpu_pimple_run", "mgpu_nan_scan",
            "mgpu_krylov_solve", "mgpu_csr_matvec", "mgpu_build_connectivity", "mgpu_geometry",
            "mgpu_rcm_order", "mgpu_case_stage", "mgpu_cg_jacobi_noalloc", "mgpu_set_tuning",
            "mgpu_case_solve_times", "mgpu_case_timing", "mgpu_case_set_profiling", "mgpu_case_begin",
@@ -238,6 +239,7 @@ def load_library(path: str = LIB_PATH):
     lib.mgpu_fields_download.argtypes = [C.c_void_p, dblp, dblp, dblp, dblp, dblp, dblp]
     lib.mgpu_simple_run.argtypes = [C.c_void_p, C.c_int, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int)]
     lib.mgpu_piso_run.argtypes = [C.c_void_p, C.c_int, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int)]
+    lib.mgpu_pimple_run.argtypes = [C.c_void_p, C.c_int, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int)]
     lib.mgpu_nan_scan.argtypes = [C.c_void_p, P(C.c_int), P(C.c_int), P(C.c_int), dblp, P(C.c_int)]
     lib.mgpu_krylov_solve.argtypes = [C.c_int, i32p, i32p, dblp, dblp, dblp, C.c_double, C.c_int,
                                       C.c_int, C.c_int, P(C.c_int), dblp, P(C.c_int)]

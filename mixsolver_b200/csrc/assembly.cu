@@ -403,7 +403,7 @@ __device__ __forceinline__ void b_momentum(const DeviceCase& d, const AsmParams&
     ap = ap + 3.0 * at;
     rhs = rhs + at * (4.0 * d.u_old[(long)comp * N + c] - d.u_old_old[(long)comp * N + c]);
   }
-  if (ts > 0) {
+  if (ts > 0 && !P.pimple) {
     A[d.diag[c]] = ap;
   } else {
     A[d.diag[c]] = ap / P.alpha_u;
@@ -655,10 +655,14 @@ __device__ void b_diag_finalize(const DeviceCase& d, const AsmParams& P, int tra
   }
   const double imbal = __longlong_as_double((long long)st->imbal_bits) / P.flux_ref;
   double du = __longlong_as_double((long long)st->du_bits);
-  int itl_max = 0;
-  double ressum = 0.0;
+  // itl_max and ressum continue over the earlier outer iterations of a PIMPLE
+  // step (0 otherwise), as the reference sums them in solve order
+  int itl_max = st->acc_itl;
+  double ressum = st->acc_res;
   for (int s = 0; s < rec->nsolve && s < MGPU_MAXSOLVE; ++s) itl_max = max(itl_max, rec->lin_it[s]);
   for (int s = 0; s < 3; ++s) ressum = ressum + rec->lin_res[s];
+  st->acc_itl = 0;
+  st->acc_res = 0.0;
   rec->it = st->cur_it + 1;
   rec->itl_max = itl_max;
   rec->ressum = ressum;
@@ -682,6 +686,21 @@ __device__ void b_diag_finalize(const DeviceCase& d, const AsmParams& P, int tra
   if (st->it_limit > 0 && st->cur_it >= st->it_limit) st->abort = 1;
 }
 __global__ void k_diag_finalize(DeviceCase d, AsmParams P, int transient) { b_diag_finalize(d, P, transient); }
+
+// End of a PIMPLE outer iteration that is not the step's last: its solves'
+// counts and momentum residuals join the step's running itl_max and ressum
+// (the record's slots are reused by the next outer iteration).
+__global__ void k_outer_accum(DeviceCase d) {
+  DevStatus* st = d.st;
+  if (st->abort) return;
+  const MgpuIterRec* rec = d.recs + st->cur_it;
+  int m = st->acc_itl;
+  for (int s = 0; s < rec->nsolve && s < MGPU_MAXSOLVE; ++s) m = max(m, rec->lin_it[s]);
+  double r = st->acc_res;
+  for (int s = 0; s < 3; ++s) r = r + rec->lin_res[s];
+  st->acc_itl = m;
+  st->acc_res = r;
+}
 
 // SIMPLE: uo := u ; PISO: history shift and time-scheme order
 __device__ __forceinline__ void b_begin_iter(const DeviceCase& d, int transient, int time_scheme, const long i) {
@@ -824,6 +843,12 @@ int launch_diag(const DeviceCase& d, const AsmParams& P, int transient, cudaStre
   MGPU_LAUNCH_CHECK("k_diag");
   k_diag_finalize<<<1, 1, 0, s>>>(d, P, transient);
   MGPU_LAUNCH_CHECK("k_diag_finalize");
+  return 0;
+}
+
+int launch_outer_accum(const DeviceCase& d, cudaStream_t s) {
+  k_outer_accum<<<1, 1, 0, s>>>(d);
+  MGPU_LAUNCH_CHECK("k_outer_accum");
   return 0;
 }
 int launch_batch_asm(int op, int arg, const AsmBatch& b, cudaStream_t s) {

@@ -15,6 +15,7 @@ struct AsmParams {
   int has_pdir;     // any pressure-Dirichlet boundary face: no PPE pin
   int has_outflow;  // any outflow zone: global outflow rescale
   int inlet_ramp;
+  int pimple;       // transient momentum keeps the alpha_u relaxation (ctrl%pimple)
 };
 
 // One case of a batched assembly launch: its arrays, its parameters, the
@@ -71,6 +72,7 @@ int launch_outflow(const DeviceCase& d, cudaStream_t s);
 int launch_ppe(const DeviceCase& d, const AsmParams& P, cudaStream_t s);
 int launch_correct(const DeviceCase& d, const AsmParams& P, cudaStream_t s);
 int launch_diag(const DeviceCase& d, const AsmParams& P, int transient, cudaStream_t s);
+int launch_outer_accum(const DeviceCase& d, cudaStream_t s);
 int launch_begin_iter(const DeviceCase& d, int transient, int time_scheme, cudaStream_t s);
 
 }  // namespace mgpu

@@ -688,6 +688,7 @@ int mgpu_case_begin(MgpuCase* c, int mode, int nsteps, int* ier) {
   }
   *ier = 0;
   c->run_mode = -1;
+  c->P.pimple = 0;
   int n;
   if (mode == 1) {
     if (!c->ctrl.transient) {

@@ -235,7 +235,7 @@ KrylovArgs mom_args(MgpuCase* c, int comp, bool transient) {
   a.zero_x = 0;
   a.mpi_mode = transient ? 1 : 0;
   a.slot = comp;
-  a.ier_breakdown = transient ? 33 : 20;
+  a.ier_breakdown = c->P.pimple ? 53 : (transient ? 33 : 20);
   return a;
 }
 
@@ -248,7 +248,7 @@ KrylovArgs ppe_args(MgpuCase* c, int slot, bool transient) {
   a.zero_x = 1;
   a.mpi_mode = transient ? 1 : 0;
   a.slot = slot;
-  a.ier_breakdown = transient ? 34 : 21;
+  a.ier_breakdown = c->P.pimple ? 54 : (transient ? 34 : 21);
   return a;
 }
 
@@ -285,6 +285,7 @@ int ensure_recs(MgpuCase* c, int n) {
 namespace {
 
 int begin_run(MgpuCase* c) {
+  c->P.pimple = 0;  // mgpu_pimple_run sets it after this
   c->ev_used = 0;
   c->launches = 0;
   c->timing = MgpuTiming{};
@@ -361,6 +362,54 @@ int outer_iteration(MgpuCase* c, bool transient) {
     c->launches += 2;
   }
   TRY(launch_diag(d, P, transient ? 1 : 0, s));
+  c->launches += 2;
+  return 0;
+}
+
+// One PIMPLE time step (pimple_run_mpi at one rank, mod_uns_simple_mpi.f90:
+// 676-760): the history shift once, then n_outer_iter outer iterations of the
+// relaxed momentum predictor (P.pimple), apc = ap / alpha_u, gradients,
+// Rhie-Chow fluxes, outflow rescale and n_correct pressure corrections; the
+// step's diagnostics at the end.
+int pimple_step(MgpuCase* c) {
+  DeviceCase& d = c->d;
+  const AsmParams& P = c->P;
+  cudaStream_t s = c->stream;
+  TRY(launch_begin_iter(d, 1, c->ctrl.time_scheme, s));
+  c->launches++;
+  const int n_outer = std::max(1, c->ctrl.n_outer_iter);
+  const int ncorr = std::max(1, c->ctrl.n_correct);
+  for (int io = 0; io < n_outer; ++io) {
+    for (int comp = 0; comp < 3; ++comp) {
+      if (P.conv_blend > 0.0) {
+        TRY(launch_limiter(d, P, comp, s));
+        c->launches++;
+      }
+      TRY(launch_momentum(d, P, comp, s));
+      c->launches++;
+      TRY(momentum_solve(c, comp, true));
+    }
+    TRY(launch_apc(d, P.alpha_u, s));
+    TRY(launch_gradients(d, P, s));
+    TRY(launch_rhiechow(d, P, s));
+    c->launches += 3;
+    if (c->has_outflow) {
+      TRY(launch_outflow(d, s));
+      c->launches++;
+    }
+    for (int icorr = 0; icorr < ncorr; ++icorr) {
+      TRY(launch_ppe(d, P, s));
+      c->launches++;
+      TRY(ppe_solve(c, std::min(3 + icorr, MGPU_MAXSOLVE - 1), true));
+      TRY(launch_correct(d, P, s));
+      c->launches += 2;
+    }
+    if (io + 1 < n_outer) {
+      TRY(launch_outer_accum(d, s));
+      c->launches++;
+    }
+  }
+  TRY(launch_diag(d, P, 1, s));
   c->launches += 2;
   return 0;
 }
@@ -656,6 +705,46 @@ int mgpu_piso_run(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nr
       if (ab) break;
     }
   }
+  return end_run(c, n_steps, log, logcap, nrec, ier);
+}
+
+int mgpu_pimple_run(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nrec, int* ier) {
+  if (!c || !ier) return MGPU_E_ARG;
+  *ier = 0;
+  if (nrec) *nrec = 0;
+  if (!c->ctrl.transient) {
+    *ier = 50;
+    return 0;
+  }
+  if (c->ctrl.dt <= 0.0) {
+    *ier = 51;
+    return 0;
+  }
+  int n_steps = std::max(1, c->ctrl.n_time_max);
+  if (nsteps > 0) n_steps = std::min(n_steps, nsteps);
+  TRY(ensure_recs(c, n_steps + 1));
+  TRY(begin_run(c));
+  c->P.pimple = 1;
+  TRY(reset_status(c, 1, n_steps + 1));
+  TRY(launch_fill(c->d.apc, c->d.N, 1.0, c->stream));
+  TRY(launch_gradients(c->d, c->P, c->stream));
+  TRY(launch_rhiechow(c->d, c->P, c->stream));
+  c->launches += 3;
+  int e = 0;
+  for (int it = 0; it < n_steps && !e; ++it) {
+    e = pimple_step(c);
+    if (!e && (it + 1) % 64 == 0 && it + 1 < n_steps) {
+      int ab = 0;
+      if (cudaMemcpyAsync(&ab, &c->d.st->abort, sizeof(int), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+          cudaStreamSynchronize(c->stream) != cudaSuccess) {
+        e = cuda_fail(cudaGetLastError(), "status read", __FILE__, __LINE__);
+        break;
+      }
+      if (ab) break;
+    }
+  }
+  c->P.pimple = 0;
+  if (e) return e;
   return end_run(c, n_steps, log, logcap, nrec, ier);
 }
 

@@ -24,6 +24,10 @@ struct DevStatus {
   double t_now;
   unsigned long long imbal_bits, du_bits, umax_bits;  // max-reductions (bit patterns of x >= 0)
   unsigned long long nan_key;                          // min (cell*4+field)
+  // solves of the earlier outer iterations of a PIMPLE step: largest
+  // iteration count, sum of the momentum residuals (in solve order)
+  int acc_itl;
+  double acc_res;
 };
 
 // Krylov solve arguments (matrix, preconditioner data, work, result slot).

@@ -116,6 +116,11 @@ class UnsCase:
         """Transient PISO; returns (ier, per-step records)."""
         return self._run(_lib().mgpu_piso_run, nsteps, logcap)
 
+    def pimple_run(self, nsteps: int = 0, logcap: int = 4096):
+        """Transient PIMPLE (ctrl.n_outer_iter outer iterations per step); returns
+        (ier, per-step records)."""
+        return self._run(_lib().mgpu_pimple_run, nsteps, logcap)
+
     def nan_scan(self):
         """(ifin, field, cell, value, kind) of the first non-finite value."""
         ifin, field, cell, kind = C.c_int(), C.c_int(), C.c_int(), C.c_int()

@@ -667,6 +667,7 @@ struct Case {
   // fields_t (mod_uns_fields.f90:29-79); u, gu cell-major like the Fortran arrays
   vector<double> u, p, gp, gu, flux, lf, apc, u_old, u_old_old;
   int ts_order = 0;
+  bool pimple = false;  // ctrl%pimple: pimple_run sets it for its run
   vector<double> rhs, ap, pp, phif, dpp, psi;
 };
 
@@ -931,7 +932,7 @@ void momentum_assembly(Case& cs, int comp) {
       rhs[kk] = rhs[kk] + at * (4.0 * cs.u_old[3 * kk + comp] - cs.u_old_old[3 * kk + comp]);
     }
   }
-  if (cs.ts_order > 0) {  // PISO: no relaxation (ctrl%pimple = .false.)
+  if (cs.ts_order > 0 && !cs.pimple) {  // PISO: no relaxation (ctrl%pimple = .false.)
     for (int kk = 0; kk < N; ++kk) A.val[pos_of(A, kk, kk)] = ap[kk];
   } else {
     for (int kk = 0; kk < N; ++kk) {
@@ -1302,6 +1303,101 @@ int piso_run(Case& cs, int nsteps, MgpuIterRec* log, int logcap, int* nrec) {
   return 0;
 }
 
+// pimple_run_mpi at one rank, mod_uns_simple_mpi.f90:580-850: one history
+// shift per time step, n_outer_iter outer iterations of (relaxed momentum,
+// apc = ap / alpha_u, gradients, Rhie-Chow, outflow rescale, n_correct PPE
+// solves and corrections), then the step's diagnostics. The record keeps the
+// last outer iteration's solves; itl_max and ressum run over all of them.
+int pimple_run_body(Case& cs, int nsteps, MgpuIterRec* log, int logcap, int* nrec) {
+  const MgpuCtrl& ctrl = cs.ctrl;
+  int N = cs.m.ncells;
+  *nrec = 0;
+  if (!ctrl.transient) return 50;
+  if (ctrl.dt <= 0.0) return 51;
+  int n_steps = std::max(1, ctrl.n_time_max);
+  if (nsteps > 0) n_steps = std::min(n_steps, nsteps);
+  const int n_outer = std::max(1, ctrl.n_outer_iter);
+  double flux_ref = flux_reference(cs);
+  std::fill(cs.apc.begin(), cs.apc.end(), 1.0);
+  compute_gradients(cs);
+  flux_rhiechow(cs);
+  double t_now = 0.0;
+  for (int it = 1; it <= n_steps; ++it) {
+    cs.u_old_old = cs.u_old;
+    cs.u_old = cs.u;
+    cs.ts_order = (it == 1 || ctrl.time_scheme == 1) ? 1 : 2;
+    MgpuIterRec rec;
+    std::memset(&rec, 0, sizeof(rec));
+    rec.it = it;
+    int itl_max = 0, itl, ierr;
+    double ressum = 0.0, resl;
+    int ns = 3;
+    for (int iouter = 1; iouter <= n_outer; ++iouter) {
+      for (int comp = 0; comp < 3; ++comp) {
+        momentum_assembly(cs, comp);
+        solve_momentum(cs, comp, 1, itl, resl, ierr);
+        rec.lin_it[comp] = itl;
+        rec.lin_res[comp] = resl;
+        rec.lin_ierr[comp] = ierr;
+        if (ierr == 2) return 53;
+        itl_max = std::max(itl_max, itl);
+        ressum = ressum + resl;
+      }
+      for (int i = 0; i < N; ++i) cs.apc[i] = cs.ap[i] / ctrl.alpha_u;
+      compute_gradients(cs);
+      flux_rhiechow(cs);
+      outflow_mass_rescale(cs);
+      ns = 3;
+      for (int icorr = 1; icorr <= ctrl.n_correct; ++icorr) {
+        ppe_assembly(cs);
+        solve_ppe(cs, 1, itl, resl, ierr);
+        if (ns < MGPU_MAXSOLVE) {
+          rec.lin_it[ns] = itl;
+          rec.lin_res[ns] = resl;
+          rec.lin_ierr[ns] = ierr;
+          ++ns;
+        }
+        if (ierr == 2) return 54;
+        itl_max = std::max(itl_max, itl);
+        correct_fields(cs);
+      }
+    }
+    rec.nsolve = ns;
+    t_now = t_now + ctrl.dt;
+    double imbal = max_imbalance(cs) / flux_ref;
+    double du_max = 0.0;
+    for (int i = 0; i < 3 * N; ++i) du_max = std::max(du_max, std::fabs(cs.u[i] - cs.u_old[i]));
+    du_max = du_max / ctrl.dt;
+    double umax = 0.0;
+    for (int i = 0; i < N; ++i) umax = std::max(umax, norm3(&cs.u[3 * i]));
+    double cfl = 0.0;
+    for (int i = 0; i < N; ++i) {
+      double dt_dx = umax * ctrl.dt / std::pow(cs.g.vol[i], 1.0 / 3.0);
+      if (dt_dx > cfl) cfl = dt_dx;
+    }
+    int fld, cell, kind;
+    double val;
+    if (nan_scan(cs, fld, cell, val, kind)) return 60;
+    rec.itl_max = itl_max;
+    rec.imbal = imbal;
+    rec.du_max = du_max;
+    rec.ressum = ressum;
+    rec.umax = umax;
+    rec.cfl_max = cfl;
+    rec.t_now = t_now;
+    if (log && *nrec < logcap) log[*nrec] = rec;
+    ++*nrec;
+  }
+  return 0;
+}
+
+int pimple_run(Case& cs, int nsteps, MgpuIterRec* log, int logcap, int* nrec) {
+  cs.pimple = true;
+  const int ier = pimple_run_body(cs, nsteps, log, logcap, nrec);
+  cs.pimple = false;
+  return ier;
+}
+
 bool load_mesh(const MgpuMesh* in, Mesh& m) {
   if (!in || in->ncells <= 0 || in->nfaces <= 0 || in->nnodes <= 0) return false;
   m.nnodes = in->nnodes;
@@ -1412,6 +1508,11 @@ int orc_simple_run(OrcCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nr
 
 int orc_piso_run(OrcCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nrec, int* ier) {
   *ier = piso_run(c->cs, nsteps, log, logcap, nrec);
+  return 0;
+}
+
+int orc_pimple_run(OrcCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nrec, int* ier) {
+  *ier = pimple_run(c->cs, nsteps, log, logcap, nrec);
   return 0;
 }
 

@@ -39,6 +39,7 @@ def lib():
         L.orc_fields_download.argtypes = [C.c_void_p, dp, dp, dp, dp, dp, dp]
         L.orc_simple_run.argtypes = [C.c_void_p, C.c_int, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int)]
         L.orc_piso_run.argtypes = [C.c_void_p, C.c_int, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int)]
+        L.orc_pimple_run.argtypes = [C.c_void_p, C.c_int, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int)]
         L.orc_geometry.argtypes = [C.c_void_p, dp, dp, dp, dp, dp, dp]
         L.orc_connectivity.argtypes = [C.c_void_p, ip, ip, ip, ip, ip, ip, ip]
         L.orc_stage.argtypes = [C.c_void_p, C.c_int, dp, dp, dp, dp]
@@ -102,6 +103,9 @@ class OracleCase:
 
     def piso_run(self, nsteps=0, logcap=4096):
         return self._run(lib().orc_piso_run, nsteps, logcap)
+
+    def pimple_run(self, nsteps=0, logcap=4096):
+        return self._run(lib().orc_pimple_run, nsteps, logcap)
 
     def geometry(self):
         N, F = self.N, self.F

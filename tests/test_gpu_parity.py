@@ -267,7 +267,7 @@ def test_simple_convergence_stops_early():
     _compare_runs(log_g, log_o, g.fields(), o.fields())
 
 
-def _piso_ensemble(mesh, ctrl, u0):
+def _piso_ensemble(mesh, ctrl, u0, run="piso_run"):
     """Oracle PISO runs from u0 scaled by (1 + e), e in {0, +-3e-16, +-1e-15}.
 
     From the second corrector on, a PISO pressure solve starts from the
@@ -279,7 +279,7 @@ def _piso_ensemble(mesh, ctrl, u0):
     for e in (0.0, 3e-16, -3e-16, 1e-15, -1e-15):
         o = O.OracleCase(mesh, ctrl)
         o.upload(u=u0 * (1.0 + e))
-        ier, log = o.piso_run()
+        ier, log = getattr(o, run)()
         assert ier == 0
         runs.append((log, o.fields()))
     return runs
@@ -336,6 +336,55 @@ def test_piso_error_codes():
     ctrl.dt = 0.0
     g = S.UnsCase(mesh, ctrl)
     assert g.piso_run()[0] == 31          # dt <= 0
+
+
+def test_pimple_tet_parity():
+    """pimple_run_mpi at one rank: two relaxed outer iterations per step."""
+    mesh, ctrl = cases.tet_box(4, dt=2e-3, steps=4)
+    ctrl.n_outer_iter = 2
+    ctrl.alpha_u = 0.8
+    geo = O.OracleCase(mesh, ctrl).geometry()
+    u0 = meshgen.taylor_green(geo["xc"], seed=3)
+    g = S.UnsCase(mesh, ctrl)
+    g.upload(u=u0)
+    ier_g, log_g = g.pimple_run()
+    assert ier_g == 0
+    runs = _piso_ensemble(mesh, ctrl, u0, run="pimple_run")
+    _compare_piso(log_g, g.fields(), runs)
+    for k, a in enumerate(log_g):
+        its = [r[0][k]["itl_max"] for r in runs]
+        assert min(its) <= a["itl_max"] <= max(its)
+
+
+def test_pimple_one_unrelaxed_outer_iteration_is_piso():
+    """alpha_u = 1 and one outer iteration: the relaxation and apc = ap/alpha_u
+    are identities, so PIMPLE reproduces PISO bit for bit."""
+    mesh, ctrl = cases.tet_box(3, dt=1e-3, steps=3)
+    ctrl.alpha_u = 1.0
+    ctrl.n_outer_iter = 1
+    geo = O.OracleCase(mesh, ctrl).geometry()
+    u0 = meshgen.taylor_green(geo["xc"], seed=4)
+    out = []
+    for run in ("piso_run", "pimple_run"):
+        g = S.UnsCase(mesh, ctrl)
+        g.upload(u=u0)
+        ier, log = getattr(g, run)()
+        assert ier == 0
+        out.append((log, g.fields()))
+    for a, b in zip(out[0][0], out[1][0]):
+        assert a["lin_it"] == b["lin_it"] and a["lin_res"] == b["lin_res"] and a["ressum"] == b["ressum"]
+    for key in ("u", "p", "flux"):
+        np.testing.assert_array_equal(out[0][1][key], out[1][1][key])
+
+
+def test_pimple_error_codes():
+    mesh, ctrl = cases.cavity2d(4)
+    g = S.UnsCase(mesh, ctrl)
+    assert g.pimple_run()[0] == 50        # transient = false
+    ctrl.transient = True
+    ctrl.dt = 0.0
+    g = S.UnsCase(mesh, ctrl)
+    assert g.pimple_run()[0] == 51        # dt <= 0
 
 
 def test_nan_guard_on_gpu():

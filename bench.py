@@ -329,7 +329,7 @@ def run_ours(args):
                      # DRAM bytes of one pressure-solve launch from an ncu capture of this
                      # workload (committed summary: profiles/k_pcg_mixed_channel524k.md); the
                      # system stays in L2, so DRAM carries < 1 % of the algorithmic bytes
-                     "traffic": 278.6e6 if mixed else None,
+                     "traffic": 283.4e6 if mixed else None,
                      "kernel": "k_pcg_mixed (pressure solve)" if mixed else "k_factor+k_pcg (pressure solve)",
                      "algorithmic_bytes_per_launch": float(np.mean(ppe_bytes)), "avg_launch_ms": ppe_launch_ms,
                      "launches": len(ppe_ms), "all_krylov_solves_gbs": family,

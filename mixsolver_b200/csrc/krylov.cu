@@ -109,6 +109,60 @@ __device__ __forceinline__ void gather_ready(const double* x, const int* cols, i
   }
 }
 
+// A row of a one-block sweep fetched a level ahead: every load that does not
+// depend on the previous level's results (the row, its diagonal, the value it
+// starts from, its entries' columns and factor values in sweep order) is in
+// flight while that level runs, so after the barrier a level waits only for
+// its gathers of z. Rows with more than kSweepK entries to apply keep the
+// plain loop.
+constexpr int kSweepK = 8;
+struct SweepRow {
+  int i;      // row (-1: none)
+  int nk;     // entries to apply
+  double s;   // start value: src[i] (forward) or the forward result z[i] (backward)
+  double fd;  // f[diag[i]]
+  int col[kSweepK];
+  double fv[kSweepK];
+};
+
+__device__ __forceinline__ void fetch_lo(const KrylovArgs& a, const double* f, const double* src, int idx, int e,
+                                         SweepRow& R) {
+  R.i = -1;
+  if (idx >= e) return;
+  const int i = a.lo_rows[idx];
+  const int rb = a.row_ptr[i], d = a.diag[i];
+  R.i = i;
+  R.nk = d - rb;
+  R.s = src[i];
+  R.fd = f[d];
+#pragma unroll
+  for (int t = 0; t < kSweepK; ++t)
+    if (t < R.nk) {
+      R.col[t] = a.col[rb + t];
+      R.fv[t] = f[rb + t];
+    }
+}
+
+__device__ __forceinline__ void fetch_up(const KrylovArgs& a, int kind, const double* f, const double* z, int idx,
+                                         int e, SweepRow& R) {
+  R.i = -1;
+  if (idx >= e) return;
+  const int i = a.up_rows[idx];
+  const int d = a.diag[i], re = a.row_ptr[i + 1];
+  R.i = i;
+  R.nk = re - d - 1;
+  R.s = z[i];
+  R.fd = f[d];
+#pragma unroll
+  for (int t = 0; t < kSweepK; ++t)
+    if (t < R.nk) {
+      // IC(0): the L^T entries in descending column order; ILU(0): U ascending
+      const int k = kind == 2 ? re - 1 - t : d + 1 + t;
+      R.col[t] = a.col[k];
+      R.fv[t] = kind == 2 ? f[a.lt_pos[k]] : f[k];
+    }
+}
+
 // z = M^{-1} src for ILU(0) (kind 0) or IC(0) (kind 2).
 // One block: level-scheduled with __syncthreads between levels.
 // Several blocks: sync-free. Both sweeps write into arrays pre-filled with
@@ -122,20 +176,55 @@ __device__ bool apply_lu(const KrylovArgs& a, int kind, const double* src, doubl
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstr = gridDim.x * blockDim.x;
   const double* f = a.fval;
   if constexpr (L1) {
+    SweepRow R;
+    R.i = -1;
+    if (a.nlev_lo > 0) fetch_lo(a, f, src, a.lo_ptr[0] + gtid, a.lo_ptr[1], R);
     for (int lev = 0; lev < a.nlev_lo; ++lev) {
       const int e = a.lo_ptr[lev + 1];
-      for (int idx = a.lo_ptr[lev] + gtid; idx < e; idx += gstr) {
+      if (R.i >= 0) {  // this thread's first row of the level, fetched ahead
+        double s = R.s;
+        if (R.nk <= kSweepK) {
+#pragma unroll
+          for (int t = 0; t < kSweepK; ++t)
+            if (t < R.nk) s = s - R.fv[t] * z[R.col[t]];
+        } else {
+          for (int k = a.row_ptr[R.i]; k < a.diag[R.i]; ++k) s = s - f[k] * z[a.col[k]];
+        }
+        z[R.i] = (kind == 2) ? s / R.fd : s;
+      }
+      for (int idx = a.lo_ptr[lev] + gtid + gstr; idx < e; idx += gstr) {
         const int i = a.lo_rows[idx];
         double s = src[i];
         const int d = a.diag[i];
         for (int k = a.row_ptr[i]; k < d; ++k) s = s - f[k] * z[a.col[k]];
         z[i] = (kind == 2) ? s / f[d] : s;
       }
+      if (lev + 1 < a.nlev_lo) fetch_lo(a, f, src, e + gtid, a.lo_ptr[lev + 2], R);
       __syncthreads();
     }
+    // the forward results are final here: a backward row's start value z[i]
+    // is only rewritten in its own level, so it may be fetched a level ahead
+    R.i = -1;
+    if (a.nlev_up > 0) fetch_up(a, kind, f, z, a.up_ptr[0] + gtid, a.up_ptr[1], R);
     for (int lev = 0; lev < a.nlev_up; ++lev) {
       const int e = a.up_ptr[lev + 1];
-      for (int idx = a.up_ptr[lev] + gtid; idx < e; idx += gstr) {
+      if (R.i >= 0) {
+        double s = R.s;
+        if (R.nk <= kSweepK) {
+#pragma unroll
+          for (int t = 0; t < kSweepK; ++t)
+            if (t < R.nk) s = s - R.fv[t] * z[R.col[t]];
+        } else {
+          const int d = a.diag[R.i], re = a.row_ptr[R.i + 1];
+          if (kind == 2) {
+            for (int k = re - 1; k > d; --k) s = s - f[a.lt_pos[k]] * z[a.col[k]];
+          } else {
+            for (int k = d + 1; k < re; ++k) s = s - f[k] * z[a.col[k]];
+          }
+        }
+        z[R.i] = s / R.fd;
+      }
+      for (int idx = a.up_ptr[lev] + gtid + gstr; idx < e; idx += gstr) {
         const int i = a.up_rows[idx];
         const int d = a.diag[i], re = a.row_ptr[i + 1];
         double s = z[i];
@@ -148,6 +237,7 @@ __device__ bool apply_lu(const KrylovArgs& a, int kind, const double* src, doubl
         }
         z[i] = s / f[d];
       }
+      if (lev + 1 < a.nlev_up) fetch_up(a, kind, f, z, e + gtid, a.up_ptr[lev + 2], R);
       __syncthreads();
     }
     return true;

@@ -374,7 +374,8 @@ def run_reference(args):
     from oracle.rcm import rcm
     mesh, ctrl = workload(args, rcm)
     oc = O.OracleCase(mesh, ctrl)
-    w = min(args.warmup, 1)
+    # bounded sample: at most 3 warm-up and 3 timed outer iterations (~6.5 s each on one core)
+    w = min(args.warmup, 3)
     k = max(1, min(args.steps, 3))
     oc.simple_run(w)
     t0 = time.perf_counter()
@@ -388,7 +389,7 @@ def run_reference(args):
                                   "BiCGStab+Jacobi momentum, PCG+ILU(0) pressure, lin_tol 1e-8",
                       "cells": mesh.ncells, "lin_max": args.lin_max},
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
-                            "sample": f"{k} outer iterations after {w} warm-up (steps capped at 3 to bound "
+                            "sample": f"{k} outer iterations after {w} warm-up (each capped at 3 to bound "
                                       "the CPU run); the reference's serial SIMPLE is single-threaded"},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)

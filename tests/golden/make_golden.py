@@ -13,6 +13,9 @@ Produces
     read from the reference source at generation time; only the resulting L2
     is stored. The reference publishes 2.897e-2 (80x80, unMesh.control:63,
     cluster_cases/README.md:189) and 9.12e-2 (40x40, cluster_cases/README.md:190).
+    It also holds the oracle's PIMPLE run on the 80x80 mesh to t = 10, against
+    the transient history that cluster_cases/cavity_Re1000/README.md section 4
+    records (np = 4, dt = 0.01, 2 x 2 corrections per step).
   * oracle_cases.npz -- oracle histories and final fields on small synthetic
     workloads (the same generators the CUDA tests use), used by the CPU suite
     to detect any change in the oracle's results.
@@ -93,8 +96,41 @@ def make_ghia():
                                 final_imbal=log[-1]["imbal"], final_du_max=log[-1]["du_max"],
                                 it1=log[0]))
         print(rel, out["runs"][-1]["ghia_l2"])
+    make_pimple_pin(out)
     with open(os.path.join(ROOT, "tests/golden/ghia_pin.json"), "w") as f:
         json.dump(out, f, indent=1)
+
+
+def make_pimple_pin(out):
+    """PIMPLE (pimple_run_mpi at one rank) on the reference's 80x80 cavity mesh
+    with its control and the recorded transient settings (dt 0.01, 2 outer
+    iterations x 2 corrections per step; cluster_cases/cavity_Re1000/README.md
+    section 4), 1000 steps to t = 10 in one run: the centre-line L2, max|u| at
+    t = 10, and the 500-step means of max|u| and du/dt that the README tabulates
+    for t = 0-5 and 5-10."""
+    yg, u1000 = ghia_table()
+    mesh = read_cas(os.path.join(REF, "cluster_cases/cavity_Re1000/unMesh.cas"))
+    c = cavity_control(1)
+    c.transient = True
+    c.dt = 0.01
+    c.n_time_max = 1000
+    c.n_outer_iter = 2
+    c.n_correct = 2
+    oc = O.OracleCase(mesh, c)
+    xc = oc.geometry()["xc"]
+    ier, log = oc.pimple_run(1000, logcap=1000)
+    u = oc.fields()["u"]
+    du = np.array([r["du_max"] for r in log])
+    um = np.array([r["umax"] for r in log])
+    out["pimple"] = dict(mesh="cluster_cases/cavity_Re1000/unMesh.cas", steps=len(log), ier=ier,
+                         ghia_l2_t10=probe_l2(xc, u, yg, u1000),
+                         umax_t10=float(np.sqrt((u ** 2).sum(1)).max()),
+                         umax_mean=[float(um[:500].mean()), float(um[500:].mean())],
+                         dudt_mean=[float(du[:500].mean()), float(du[500:].mean())],
+                         itl_max=[int(min(r["itl_max"] for r in log)), int(max(r["itl_max"] for r in log))],
+                         published=dict(ghia_l2_t10=4.51e-1, umax_t10=0.8996, umax_mean=[0.8718, 0.9003],
+                                        dudt_mean=[5.174e-1, 1.054e-1]))
+    print("pimple", out["pimple"]["ghia_l2_t10"], out["pimple"]["umax_t10"])
 
 
 def hist_arrays(log):

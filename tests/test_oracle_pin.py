@@ -34,6 +34,27 @@ def test_ghia_pin_matches_published():
     assert abs(r40["ghia_l2"] - 9.12e-2) / 9.12e-2 < 5e-3    # 3 significant digits
 
 
+def test_pimple_pin_matches_published_history():
+    """PIMPLE of the oracle on the reference's 80x80 cavity mesh, dt 0.01, 2
+    outer iterations x 2 corrections per step, to t = 10, against the history
+    that cluster_cases/cavity_Re1000/README.md section 4 records for the
+    reference's own run (MPI np = 4; its transient control was not kept in the
+    case, alpha_u 0.7 is taken from the case's control): max|u| at t = 10 to 4
+    digits, the 5 s means of max|u| to 0.5 %, those of du/dt and the
+    centre-line L2 at t = 10 to 3 %."""
+    pin = json.load(open(os.path.join(GOLD, "ghia_pin.json")))
+    assert pin["oracle_sha"] == oracle_sha(), "oracle changed: rerun tests/golden/make_golden.py"
+    r = pin["pimple"]
+    pub = r["published"]
+    assert r["ier"] == 0 and r["steps"] == 1000
+    assert abs(r["umax_t10"] - pub["umax_t10"]) < 0.5e-4
+    for got, want in zip(r["umax_mean"], pub["umax_mean"]):
+        assert abs(got - want) / want < 5e-3
+    for got, want in zip(r["dudt_mean"], pub["dudt_mean"]):
+        assert abs(got - want) / want < 3e-2
+    assert abs(r["ghia_l2_t10"] - pub["ghia_l2_t10"]) / pub["ghia_l2_t10"] < 3e-2
+
+
 def _hist(log):
     return (np.array([r["lin_it"] for r in log]), np.array([r["lin_res"] for r in log]),
             np.array([r["imbal"] for r in log]), np.array([r["du_max"] for r in log]))

@@ -114,6 +114,19 @@ typedef struct {
   const int32_t* zone;      /* face zone id */
 } MgpuMesh;
 
+/* Fluent ASCII .cas reader: read_cas (mod_uns_cas_reader.f90:44-523) in the
+ * library, for hosts without the Fortran front end. Fills *mesh with arrays
+ * owned by *holder (valid until mgpu_cas_free). *ier: 0; 1 file not readable;
+ * 6/7 bad node section; 8 bad cell section; 9/10 bad face section; 11 unknown
+ * face type; 20 missing sections or faces; 21 node or cell reference out of
+ * range. No reference counterpart for the holder: the Fortran reader fills
+ * mesh_t itself. */
+typedef struct MgpuCasMesh MgpuCasMesh;
+int mgpu_cas_read(const char* path, MgpuMesh* mesh, MgpuCasMesh** holder, int* ier);
+/* The (45 ...) zone records as "id type\n" lines; *len = full length. */
+int mgpu_cas_zone_names(const MgpuCasMesh* holder, char* buf, int cap, int* len);
+int mgpu_cas_free(MgpuCasMesh* holder);
+
 /* Per outer iteration (SIMPLE) or time step (PISO) record. Solve slots:
  * 0..2 momentum components, 3.. pressure-correction sweeps. */
 #define MGPU_MAXSOLVE 8

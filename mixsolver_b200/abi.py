@@ -211,7 +211,7 @@ EXPORTS = ["mgpu_version", "mgpu_last_error", "mgpu_set_device", "mgpu_case_crea
            "mgpu_case_solve_times", "mgpu_case_timing", "mgpu_case_set_profiling", "mgpu_case_begin",
            "mgpu_case_finish", "mgpu_batch_create", "mgpu_batch_destroy", "mgpu_batch_set_policy",
            "mgpu_batch_step", "mgpu_batch_poll", "mgpu_batch_run", "mgpu_batch_info", "mgpu_batch_plan",
-           "mgpu_batch_set_profiling"]
+           "mgpu_batch_set_profiling", "mgpu_cas_read", "mgpu_cas_zone_names", "mgpu_cas_free"]
 NOALLOC_MAX_ROWS = 131072
 
 _LIB = None
@@ -240,6 +240,9 @@ def load_library(path: str = LIB_PATH):
     lib.mgpu_simple_run.argtypes = [C.c_void_p, C.c_int, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int)]
     lib.mgpu_piso_run.argtypes = [C.c_void_p, C.c_int, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int)]
     lib.mgpu_pimple_run.argtypes = [C.c_void_p, C.c_int, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int)]
+    lib.mgpu_cas_read.argtypes = [C.c_char_p, P(MgpuMesh), P(C.c_void_p), P(C.c_int)]
+    lib.mgpu_cas_zone_names.argtypes = [C.c_void_p, C.c_char_p, C.c_int, P(C.c_int)]
+    lib.mgpu_cas_free.argtypes = [C.c_void_p]
     lib.mgpu_nan_scan.argtypes = [C.c_void_p, P(C.c_int), P(C.c_int), P(C.c_int), dblp, P(C.c_int)]
     lib.mgpu_krylov_solve.argtypes = [C.c_int, i32p, i32p, dblp, dblp, dblp, C.c_double, C.c_int,
                                       C.c_int, C.c_int, P(C.c_int), dblp, P(C.c_int)]

@@ -18,7 +18,7 @@ OUT = os.path.join(HERE, "libmixgpu.so")
 BUILD = os.path.join(HERE, "_build")
 
 SOURCES = ["case.cu", "assembly.cu", "krylov.cu", "krylov_mixed.cu", "batch.cu", "standalone.cu", "noalloc.cu",
-           "mesh_host.cpp"]
+           "mesh_host.cpp", "cas_reader.cpp"]
 # the mixed-precision form needs no bit-parity and may contract into FMA
 FMA_OK = {"krylov_mixed.cu"}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

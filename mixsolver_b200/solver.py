@@ -312,6 +312,41 @@ def csr_matvec(row_ptr, col_idx, val, x):
     return y
 
 
+def read_cas(path: str):
+    """A Fluent ASCII .cas mesh read by the library (mgpu_cas_read, the record
+    handling of read_cas in mod_uns_cas_reader.f90:44-523) as a FaceMesh.
+    Raises ValueError with the reader's ier on a file it rejects."""
+    from .meshgen import FaceMesh
+    lib = _lib()
+    m = abi.MgpuMesh()
+    holder = C.c_void_p()
+    ier = C.c_int(0)
+    abi.check(lib, lib.mgpu_cas_read(str(path).encode(), C.byref(m), C.byref(holder), C.byref(ier)),
+              "mgpu_cas_read")
+    if ier.value != 0:
+        raise ValueError(f"mgpu_cas_read: {path}: ier {ier.value}")
+    try:
+        nn, nf = m.nnodes, m.nfaces
+        x = np.ctypeslib.as_array(m.x, shape=(3 * nn,)).reshape(nn, 3).copy()
+        ptr = np.ctypeslib.as_array(m.fnode_ptr, shape=(nf + 1,)).copy()
+        fnodes = np.ctypeslib.as_array(m.fnodes, shape=(int(ptr[-1]),)).copy()
+        c0 = np.ctypeslib.as_array(m.c0, shape=(nf,)).copy()
+        c1 = np.ctypeslib.as_array(m.c1, shape=(nf,)).copy()
+        zone = np.ctypeslib.as_array(m.zone, shape=(nf,)).copy()
+        n = C.c_int(0)
+        lib.mgpu_cas_zone_names(holder, None, 0, C.byref(n))
+        buf = C.create_string_buffer(n.value + 1)
+        lib.mgpu_cas_zone_names(holder, buf, n.value + 1, C.byref(n))
+        names = {}
+        for line in buf.value.decode().splitlines():
+            zid, name = line.split(" ", 1)
+            names[int(zid)] = name
+    finally:
+        lib.mgpu_cas_free(holder)
+    return FaceMesh(x, ptr.astype(np.int32), fnodes.astype(np.int32), c0.astype(np.int32), c1.astype(np.int32),
+                    zone.astype(np.int32), int(m.ncells), names)
+
+
 def build_connectivity(mesh) -> dict:
     """build_connectivity + build_cell_csr (1-based arrays)."""
     lib = _lib()

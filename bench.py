@@ -180,6 +180,18 @@ def pinned_fields(case):
             for k, shp in case.FIELD_SHAPES.items()}
 
 
+def hbm_peak():
+    """The roofline denominator: the measured HBM copy rate of this pool's B200s
+    (MEASURED_PEAKS.json, "of measured"), else the earlier measurement of
+    6.65 TB/s ("of fallback")."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        v = float(json.load(open(path))["hbm_gbs"])
+        return v, "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    except (OSError, ValueError, KeyError, TypeError):
+        return 6650.0, "6.65 TB/s earlier measurement on this pool (of fallback)"
+
+
 def krylov_bytes(n, nnz, its, method, mixed=False, tol=1e-8, tau=1e-4, cheb_k=16):
     """Algorithmic bytes of one Krylov solve: the unique footprint of every
     pass over the system (matrix entries once, each vector read or written
@@ -271,9 +283,7 @@ def run_ours(args):
     kbytes = (sum(krylov_bytes(N, nnz, r["lin_it"][c], "bicg", mixed, ctrl.lin_tol, ctrl.mixed_tol)
                   for r in log for c in range(3)) +
               sum(krylov_bytes(N, nnz, r["lin_it"][3], "pcg", mixed, ctrl.lin_tol, ctrl.mixed_tol) for r in log))
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
-    peak = peaks.get("hbm_gbs", 6650.0)
+    peak, peak_source = hbm_peak()
     kms = tm["krylov_ms"]
     nk = max(1, tm["krylov_launches"])
     # the dominant kernel: the persistent pressure solve (one launch per outer
@@ -333,7 +343,7 @@ def run_ours(args):
                      "kernel": "k_pcg_mixed (pressure solve)" if mixed else "k_factor+k_pcg (pressure solve)",
                      "algorithmic_bytes_per_launch": float(np.mean(ppe_bytes)), "avg_launch_ms": ppe_launch_ms,
                      "launches": len(ppe_ms), "all_krylov_solves_gbs": family,
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+                     "peak_source": peak_source},
         "e2e": e2e,
         "gpu_launches": tm["gpu_launches"],
         "clocks": clk.summary(),
@@ -470,9 +480,7 @@ def run_piso(args):
                  for r in log for j in range(ctrl.n_correct)]
     kbytes = (sum(krylov_bytes(N, nnz, r["lin_it"][c], "bicg", True, ctrl.lin_tol, ctrl.mixed_tol)
                   for r in log for c in range(3)) + sum(ppe_bytes))
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
-    peak = peaks.get("hbm_gbs", 6650.0)
+    peak, peak_source = hbm_peak()
     ppe_launch_ms = float(np.mean(ppe_ms)) if len(ppe_ms) else None
     achieved = (float(np.mean(ppe_bytes)) / (ppe_launch_ms / 1e3) / 1e9) if ppe_launch_ms else None
     family = kbytes / (tm["krylov_ms"] / 1e3) / 1e9 if tm["krylov_ms"] > 0 else None
@@ -518,7 +526,7 @@ def run_piso(args):
                      "kernel": "k_pcg_mixed (pressure solves)",
                      "algorithmic_bytes_per_launch": float(np.mean(ppe_bytes)), "avg_launch_ms": ppe_launch_ms,
                      "launches": len(ppe_ms), "all_krylov_solves_gbs": family,
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+                     "peak_source": peak_source},
         "e2e": {"value": world * e2e_steps / e2e_t, "unit": "time_steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": tm["gpu_launches"],
@@ -775,9 +783,7 @@ def run_batch(args):
     B64.close()
     for o in objs64:
         o.close()
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
-    peak = peaks.get("hbm_gbs", 6650.0)
+    peak, peak_source = hbm_peak()
     achieved = kbytes / (ms / 1e3) / 1e9
     out = {
         "metric": "batched SIMPLE case-iterations/s (mixed precision, one persistent kernel per Krylov phase)",
@@ -807,7 +813,7 @@ def run_batch(args):
                    "l2": "working set ~GBs > 126 MB L2"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "kernel": "whole batched iteration (Krylov bytes / step time)",
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+                     "peak_source": peak_source},
         "e2e": {"value": world * args.cases * e2e_steps / e2e_t, "unit": "case_iters/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": i1["launches_per_iter"] * args.steps,

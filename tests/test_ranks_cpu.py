@@ -52,3 +52,14 @@ def test_one_rank_needs_no_group():
     import bench
     assert bench.max_over_ranks(3.5, 1) == 3.5
     assert bench.job_rate(10, 1, 100.0) == 100.0
+
+
+def test_hbm_peak_names_its_source(tmp_path, monkeypatch):
+    sys.path.insert(0, ROOT)
+    import bench
+    v, src = bench.hbm_peak()
+    if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")):
+        assert "of measured" in src and v > 1000
+    monkeypatch.setattr(bench, "ROOT", str(tmp_path))
+    v, src = bench.hbm_peak()
+    assert v == 6650.0 and "of fallback" in src

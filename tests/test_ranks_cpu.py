@@ -63,3 +63,17 @@ def test_hbm_peak_names_its_source(tmp_path, monkeypatch):
     monkeypatch.setattr(bench, "ROOT", str(tmp_path))
     v, src = bench.hbm_peak()
     assert v == 6650.0 and "of fallback" in src
+
+
+def test_krylov_byte_model_matches_the_stated_formulas():
+    """The roofline's algorithmic bytes per inner iteration, as stated with the
+    kernels: mixed PCG with a degree-16 Chebyshev-Jacobi polynomial reads
+    128 nnz + 416 N bytes (1302 B per row on the 524,288-cell channel); mixed
+    BiCGStab-Jacobi 16 nnz + 104 N + 8."""
+    sys.path.insert(0, ROOT)
+    import bench
+    N, nnz = 524288, 3629056
+    per = lambda m: (bench.krylov_bytes(N, nnz, 10, m, True) - bench.krylov_bytes(N, nnz, 0, m, True)) / 10
+    assert per("pcg") == 128 * nnz + 416 * N
+    assert round(per("pcg") / N) == 1302
+    assert per("bicg") == 16 * nnz + 104 * N + 8

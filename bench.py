@@ -349,7 +349,7 @@ def run_ours(args):
         "clocks": clk.summary(),
         "wall_s": wall,
     }
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:  # the CPU baseline is an N = 1 figure
         out["cpu_baseline"] = cpu_baseline(args, mesh, ctrl)
     close_ranks(world)
     if rank == 0:
@@ -649,7 +649,7 @@ def run_pimple(args):
         "clocks": clk.summary(),
         "wall_s": wall,
     }
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:  # the CPU baseline is an N = 1 figure
         from oracle import oracle as O
         oc = O.OracleCase(mesh, ctrl)
         k = 5

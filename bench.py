@@ -2,6 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--precision fp64|mixed] [--cells NXxNYxNZ]
+                    [--workload channel|batch|serve|piso|pimple]
 
 Workload (one GPU): steady SIMPLE on the 3-D channel of 128 x 64 x 64 hex cells
 (524,288 cells) on [0,4]x[0,1]x[0,1], interior nodes jittered +-10 % (seed 0),
@@ -14,6 +15,11 @@ The measured form (--precision, default mixed) is the mixed-precision one;
 the FP64 parity form (BiCGStab+Jacobi momentum, PCG+ILU(0) pressure, the
 reference's arithmetic) runs the same outer iterations beside it, and the
 line reports its rate and the relative L2 difference of u, p, flux.
+
+The other workloads print their own lines: `batch` (many 3-D cavities in one
+batched iteration), `serve` (a Poisson stream of SIMPLE / PISO requests with
+p50 / p99 latency), `piso` (80^3 x 6 tets, transient) and `pimple` (the
+reference's 80 x 80 x 1 cavity PIMPLE run, against its published step time).
 
 `--impl reference` times the CPU restatement of the reference's serial
 simple_run (the oracle, one thread: the reference's serial solver has no

@@ -930,6 +930,7 @@ def run_serve(args):
                    "simple": sum(1 for r in out if r.mode == 0), "piso": sum(1 for r in out if r.mode == 1),
                    "failed": [(r.rid, r.ier, r.error) for r in out if r.ier != 0 or r.error][:5],
                    "loop_s": {"build": srv.t_build, "step": srv.t_step, "finish": srv.t_finish},
+                   "gpu_launches": srv.gpu_launches,
                    "per_request": [(r.rid, r.mode, r.cells, round(r.arrival, 3), round(r.admitted, 3),
                                     round(r.create_s, 3), round(r.finished, 3), r.nrec) for r in out][:60],
                    "clocks": clk.summary()})
@@ -951,7 +952,7 @@ def run_serve(args):
         "roofline": None,
         "e2e": {"value": mx["throughput_req_s"], "unit": "req/s", "h2d_bytes_per_step": None,
                 "d2h_bytes_per_step": None},
-        "gpu_launches": None,
+        "gpu_launches": mx["gpu_launches"],
         "clocks": mx["clocks"],
     }
     if rank == 0:

@@ -93,6 +93,10 @@ class GpuBackend:
     def step(self, batch, iters: int) -> None:
         batch.step(iters)
 
+    def launches(self, batch) -> int:
+        """Kernel launches of one batched iteration (a host-side count)."""
+        return int(batch.info()["launches_per_iter"])
+
     def poll(self, batch) -> np.ndarray:
         return batch.poll()
 
@@ -131,6 +135,7 @@ class Server:
         self.peak_resident_bytes = 0
         self.ticks = 0
         self.batches_built = 0
+        self.gpu_launches = 0  # batched-iteration launches stepped (backends that count them)
         self.case_iters = 0
         self.cell_iters = 0.0
         # wall seconds of the stepping loop: building batches, stepping,
@@ -225,6 +230,9 @@ class Server:
                 ts = self.clock()
                 self.be.step(batch, self.tick_iters)
                 self.ticks += 1
+                count = getattr(self.be, "launches", None)
+                if count is not None:
+                    self.gpu_launches += int(count(batch)) * self.tick_iters
                 flags = self.be.poll(batch)
                 now = self.clock() - t0
                 self.t_build += ts - tb

@@ -116,3 +116,18 @@ def test_rejected_case_is_answered_with_its_error():
     out = serve.Server(be, budget_bytes=1e9, tick_iters=5).run(reqs)
     assert out[1].error == "mesh rejected" and not math.isnan(out[1].finished)
     assert out[0].nrec == 5 and out[2].nrec == 5
+
+
+def test_launch_count_follows_the_ticks():
+    class Counting(FakeBackend):
+        def launches(self, batch):
+            return 7
+
+    be = Counting()
+    srv = serve.Server(be, budget_bytes=60_000_000, active_cells=30000, tick_iters=5, bytes_per_cell=1000)
+    srv.run(_requests(k=12, seed=3))
+    assert srv.ticks > 0 and srv.gpu_launches == 7 * 5 * srv.ticks
+    plain = serve.Server(FakeBackend(), budget_bytes=60_000_000, active_cells=30000, tick_iters=5,
+                         bytes_per_cell=1000)
+    plain.run(_requests(k=4, seed=4))
+    assert plain.gpu_launches == 0   # a backend without a count adds nothing

@@ -1,9 +1,9 @@
 """Regenerate the committed golden fixtures under tests/golden/.
 
-Run from the repository root in a checkout where the reference project is
-available (default path below, or MIXSOLVER_REF):
+Run from the repository root with MIXSOLVER_REF naming a checkout of the
+reference project:
 
-    python tests/golden/make_golden.py
+    MIXSOLVER_REF=<reference checkout> python tests/golden/make_golden.py
 
 Produces
   * ghia_pin.json -- the oracle's steady SIMPLE on the reference's own cavity
@@ -16,6 +16,11 @@ Produces
     It also holds the oracle's PIMPLE run on the 80x80 mesh to t = 10, against
     the transient history that cluster_cases/cavity_Re1000/README.md section 4
     records (np = 4, dt = 0.01, 2 x 2 corrections per step).
+  * channel_lowspeed_mesh.npz, channel_lowspeed_pin.json -- the reference's
+    recorded channel case (cluster_cases/channel_lowspeed: mass-flow inlet,
+    outflow, walls, symmetry) as a compact mesh fixture, and the oracle's run
+    to convergence on it beside the iteration line and convergence count its
+    README records for the reference binary.
   * oracle_cases.npz -- oracle histories and final fields on small synthetic
     workloads (the same generators the CUDA tests use), used by the CPU suite
     to detect any change in the oracle's results.
@@ -36,12 +41,13 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 from casread import read_cas  # noqa: E402
+from fixtures import LOWSPEED_MESH, LOWSPEED_PIN, decode_mesh, encode_mesh, lowspeed_control  # noqa: E402
 from mixsolver_b200 import cases  # noqa: E402
 from mixsolver_b200.abi import (BC_SYMMETRY, BC_WALL, MOM_ILU0, PPE_IC0, BcSpec,  # noqa: E402
                                 Ctrl)
 from oracle import oracle as O  # noqa: E402
 
-REF = os.environ.get("MIXSOLVER_REF", "/root/reference")
+REF = os.environ.get("MIXSOLVER_REF", "")
 
 
 def oracle_hash() -> str:
@@ -133,6 +139,27 @@ def make_pimple_pin(out):
     print("pimple", out["pimple"]["ghia_l2_t10"], out["pimple"]["umax_t10"])
 
 
+def make_lowspeed():
+    """The reference's recorded channel run (cluster_cases/channel_lowspeed:
+    README.md section 4 logs it=1 mass-imbal 5.113E-13, du_max 2.840E-04,
+    lin-it 278, and CONVERGED after 773): its mesh as a compact fixture, plus
+    the oracle's full run to convergence on it."""
+    mesh = read_cas(os.path.join(REF, "cluster_cases/channel_lowspeed/unMesh.cas"))
+    np.savez_compressed(LOWSPEED_MESH, **encode_mesh(mesh))
+    assert np.array_equal(decode_mesh(LOWSPEED_MESH).x, mesh.x)
+    oc = O.OracleCase(mesh, lowspeed_control())
+    ier, log = oc.simple_run(logcap=8000)
+    last = log[-1]
+    out = dict(oracle_sha=oracle_hash(), mesh="cluster_cases/channel_lowspeed/unMesh.cas", ier=ier,
+               converged_after=len(log), final_du_max=last["du_max"], final_imbal=last["imbal"],
+               it1=dict(imbal=log[0]["imbal"], du_max=log[0]["du_max"], itl_max=log[0]["itl_max"]),
+               published=dict(it1_imbal="5.113E-13", it1_du_max="2.840E-04", it1_lin_it=278,
+                              converged_after=773, archived_converged_after=790, final_du_max="9.950E-11"))
+    with open(LOWSPEED_PIN, "w") as f:
+        json.dump(out, f, indent=1)
+    print("lowspeed: converged after", len(log), "du_max", last["du_max"])
+
+
 def hist_arrays(log):
     return dict(lin_it=np.array([r["lin_it"] for r in log], np.int32),
                 lin_res=np.array([r["lin_res"] for r in log]),
@@ -163,8 +190,12 @@ def make_cases():
 
 
 if __name__ == "__main__":
-    make_cases()
+    if "--lowspeed-only" not in sys.argv:
+        make_cases()
     if os.path.isdir(REF):
-        make_ghia()
+        if "--lowspeed-only" not in sys.argv:
+            make_ghia()
+        make_lowspeed()
     else:
-        print("reference checkout not found; ghia_pin.json left unchanged")
+        print("MIXSOLVER_REF not set to a reference checkout; ghia_pin.json and the channel_lowspeed "
+              "fixtures left unchanged")

@@ -2,8 +2,8 @@
 written here from generated meshes read back bit for bit, in every face-record
 form the reader accepts (uniform face type, per-face type, polygon with a
 count); the same arrays as the fixture reader; the reader's error codes. With
-the reference checkout present, the reference's own 80x80 cavity mesh reads
-the same through both readers."""
+MIXSOLVER_REF naming a reference checkout, the reference's own 80x80 cavity
+mesh reads the same through both readers."""
 import os
 import sys
 
@@ -16,7 +16,9 @@ from mixsolver_b200 import solver as S
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
 from casread import read_cas as fixture_read  # noqa: E402
 
-REF_CAS = "/root/reference/cluster_cases/cavity_Re1000/unMesh.cas"
+# the reference checkout, when the environment names it (MIXSOLVER_REF)
+_REF = os.environ.get("MIXSOLVER_REF", "")
+REF_CAS = os.path.join(_REF, "cluster_cases/cavity_Re1000/unMesh.cas") if _REF else ""
 
 
 def write_cas(mesh, path, form="uniform", polygon_every=0):
@@ -103,7 +105,7 @@ def test_reader_errors(tmp_path):
         S.read_cas(p)
 
 
-@pytest.mark.skipif(not os.path.exists(REF_CAS), reason="reference checkout not present")
+@pytest.mark.skipif(not REF_CAS or not os.path.exists(REF_CAS), reason="MIXSOLVER_REF not set to a reference checkout")
 def test_reference_mesh_reads_as_the_fixture_reader():
     got = S.read_cas(REF_CAS)
     assert (got.ncells, got.nfaces) == (6400, 25760)

@@ -152,3 +152,53 @@ def test_norm2_scaled():
     assert O.norm2(a) == 5.0
     big = np.array([1e200, 1e200])
     assert np.isfinite(O.norm2(big)) and abs(O.norm2(big) / (np.sqrt(2) * 1e200) - 1) < 1e-15
+
+
+# --- the reference's recorded channel run (cluster_cases/channel_lowspeed) ---
+import sys  # noqa: E402
+
+sys.path.insert(0, GOLD)
+from fixtures import LOWSPEED_MESH, LOWSPEED_PIN, decode_mesh, lowspeed_control  # noqa: E402
+
+
+def test_channel_lowspeed_first_iteration_is_the_reference_log():
+    """cluster_cases/channel_lowspeed/README.md section 4 records the reference
+    binary's first outer iteration on this mesh and control as
+    `it=1: mass-imbal = 5.113E-13, du_max = 2.840E-04, lin-it = 278` (bit for
+    bit the same as an archived log). The oracle prints the same line: the
+    same numbers in the same es10.3 format and the same iteration count. The
+    case uses the mass-flow inlet, the outflow rescale, walls and symmetry."""
+    mesh = decode_mesh(LOWSPEED_MESH)
+    assert (mesh.ncells, mesh.nfaces, mesh.nnodes) == (30000, 120400, 60802)
+    oc = O.OracleCase(mesh, lowspeed_control())
+    ier, log = oc.simple_run(1)
+    assert ier == 0
+    r = log[0]
+    assert f"{r['imbal']:.3E}" == "5.113E-13"
+    assert f"{r['du_max']:.3E}" == "2.840E-04"
+    assert r["itl_max"] == 278
+
+
+def test_channel_lowspeed_convergence_is_the_reference_log():
+    """The oracle's full run on the same case (tests/golden/make_golden.py):
+    `CONVERGED after 773` with du_max 9.950E-11, as the README records for the
+    reference binary."""
+    pin = json.load(open(LOWSPEED_PIN))
+    assert pin["oracle_sha"] == oracle_sha(), "oracle changed: rerun tests/golden/make_golden.py"
+    pub = pin["published"]
+    assert pin["ier"] == 0
+    assert pin["converged_after"] == pub["converged_after"] == 773
+    assert f"{pin['final_du_max']:.3E}" == pub["final_du_max"]
+    assert f"{pin['it1']['imbal']:.3E}" == pub["it1_imbal"]
+    assert pin["it1"]["itl_max"] == pub["it1_lin_it"]
+
+
+@pytest.mark.slow
+@pytest.mark.skipif(not os.environ.get("MIXSOLVER_SLOW"), reason="set MIXSOLVER_SLOW=1 (about 4 min of CPU)")
+def test_channel_lowspeed_full_run_reproduces_pin():
+    mesh = decode_mesh(LOWSPEED_MESH)
+    oc = O.OracleCase(mesh, lowspeed_control())
+    ier, log = oc.simple_run(logcap=8000)
+    pin = json.load(open(LOWSPEED_PIN))
+    assert ier == 0 and len(log) == pin["converged_after"] == 773
+    assert log[-1]["du_max"] == pin["final_du_max"]

@@ -60,6 +60,9 @@ extern "C" {
 /* Arithmetic form of the Krylov solves. */
 #define MGPU_PREC_FP64 0  /* plain FP64, parity form                       */
 #define MGPU_PREC_MIXED 1 /* FP32 SpMV/preconditioner inside FP64 refinement */
+/* The mixed form's solvers (Chebyshev-Jacobi PCG, BiCGStab-Jacobi) in FP64
+ * throughout: not the parity form; isolates what the FP32 arithmetic buys. */
+#define MGPU_PREC_FP64_POLY 2
 
 /* One control "bc" line: mirrors bc_spec_t, mod_uns_control.f90:114-145
  * (thermal plane filters are not part of this path). */
@@ -245,17 +248,20 @@ int mgpu_case_stage(MgpuCase* c, int what, int ts_order, const double* apc, doub
 
 /* Allocation-free PCG with Jacobi preconditioning, for callers that cannot
  * allocate device memory: a host that owns every device byte and passes only
- * its own buffers, a CUDA Fortran host whose arrays already live on the GPU,
- * or code inside a stream capture, where an allocation would break the
- * capture. No counterpart in the reference, whose solvers allocate their work
- * arrays on every call.
+ * its own buffers, or a CUDA Fortran host whose arrays already live on the
+ * GPU. No counterpart in the reference, whose solvers allocate their work
+ * arrays on every call. The call waits for its stream (it reads the result
+ * back to the host), so it does not belong inside a stream capture.
  * Same algorithm and outputs as mgpu_krylov_solve(method 1), but every array
  * is a device pointer (CSR 0-based: row_ptr[0] = 0) and the work space is one
  * fixed array inside the library (about 4.9 MB per GPU that loads it):
  *   - n above MGPU_NOALLOC_MAX_ROWS is rejected with MGPU_E_ARG;
  *   - calls that overlap on the GPU race on that array: serialise them;
- *   - the first call on a device looks up the array's device address; make it
- *     before any stream capture. stream: a cudaStream_t (NULL = default). */
+ *   - the first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) once for that device;
+ *   - the solve's grid may hold at most 2048 blocks (reduction partials in
+ *     the array); a larger one is refused with MGPU_E_ARG.
+ * stream: a cudaStream_t (NULL = default). */
 #define MGPU_NOALLOC_MAX_ROWS 131072
 int mgpu_cg_jacobi_noalloc(int n, const int32_t* d_row_ptr, const int32_t* d_col_idx, const double* d_val,
                            const double* d_b, double* d_x, double tol, int maxit, int norm_mode, void* stream,

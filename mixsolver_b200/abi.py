@@ -27,7 +27,7 @@ BC_NAMES = {"wall": BC_WALL, "symmetry": BC_SYMMETRY, "velocity-inlet": BC_VINLE
 
 PPE_JACOBI, PPE_IC0, PPE_ILU0 = 0, 1, 2
 MOM_ILU0, MOM_JACOBI = 0, 1
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_FP64_POLY = 0, 1, 2
 MAXBC = 32
 MAXSOLVE = 8
 

@@ -458,32 +458,43 @@ __global__ void __launch_bounds__(256) k_rhiechow(DeviceCase d, AsmParams P) {
   b_rhiechow(d, P, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-// outflow_mass_sums + outflow_mass_scale in face order (one thread: the sums
-// are sequential in the reference; only cases with an outflow zone use it)
+// outflow_mass_sums + outflow_mass_scale (mod_uns_simple.f90:1463-1547). The
+// reference forms its three sums sequentially in face order, and only that
+// order gives its rounding, so each sum stays one dependent chain -- but over
+// a compact list of just its own faces in face order (built once per case:
+// of_req the fixed-flux boundary faces, of_out the outflow faces), the three
+// chains in three threads side by side. The scaling then runs over the
+// outflow faces on every thread of the block. Called by all threads of one
+// block; only cases with an outflow zone launch it.
 __device__ void b_outflow(const DeviceCase& d) {
-  if (d.st->abort) return;
-  double m_req = 0.0, m_out = 0.0, area_out = 0.0;
-  for (int i = 0; i < d.F; ++i) {
-    if (d.c1[i] >= 0 || d.fgrp[i] < 0) continue;
-    const int bt = d.groups[d.fgrp[i]].btype;
-    if (bt == MGPU_BC_OUTFLOW) {
-      m_out = m_out + d.flux[i];
-      area_out = area_out + d.area[i];
-    } else if (bt != MGPU_BC_POUTLET && bt != MGPU_BC_FARFIELD) {
-      m_req = m_req - d.flux[i];
+  __shared__ double s_sum[3];
+  if (d.st->abort) return;  // the same for every thread of the block
+  const int t = threadIdx.x;
+  if (t < 3) {
+    double acc = 0.0;
+    if (t == 0) {
+#pragma unroll 8
+      for (int k = 0; k < d.n_of_req; ++k) acc = acc - d.flux[d.of_req[k]];
+    } else if (t == 1) {
+#pragma unroll 8
+      for (int k = 0; k < d.n_of_out; ++k) acc = acc + d.flux[d.of_out[k]];
+    } else {
+#pragma unroll 8
+      for (int k = 0; k < d.n_of_out; ++k) acc = acc + d.area[d.of_out[k]];
     }
+    s_sum[t] = acc;
   }
+  __syncthreads();
+  const double m_req = s_sum[0], m_out = s_sum[1], area_out = s_sum[2];
   if (area_out <= 0.0 || m_req <= 0.0) return;
   const bool scaled = m_out > 1.0e-2 * m_req;
   const double beta = scaled ? m_req / m_out : 0.0;
-  for (int i = 0; i < d.F; ++i) {
-    if (d.c1[i] >= 0 || d.fgrp[i] < 0 || d.groups[d.fgrp[i]].btype != MGPU_BC_OUTFLOW) continue;
+  for (int k = t; k < d.n_of_out; k += blockDim.x) {
+    const int i = d.of_out[k];
     d.flux[i] = scaled ? beta * d.flux[i] : m_req * d.area[i] / area_out;
   }
 }
-__global__ void k_outflow(DeviceCase d) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) b_outflow(d);
-}
+__global__ void k_outflow(DeviceCase d) { b_outflow(d); }
 
 // ppe_assembly: row c of the pressure-correction matrix, rhs(c), pin, pp := 0
 __device__ __forceinline__ void b_ppe(const DeviceCase& d, const AsmParams& P, const int c) {
@@ -761,7 +772,7 @@ MGPU_BATCHED(limiter, RANGE_N, if (P.conv_blend > 0.0) b_limiter(d, P, arg, (int
 MGPU_BATCHED(momentum, RANGE_N, b_momentum(d, P, arg, (int)i))
 MGPU_BATCHED(apc, RANGE_N, b_apc(d, sc.transient ? 1.0 : P.alpha_u, (int)i))
 MGPU_BATCHED(rhiechow, RANGE_F, b_rhiechow(d, P, (int)i))
-MGPU_BATCHED(outflow, RANGE_ONE, if (sc.has_outflow && threadIdx.x == 0) b_outflow(d))
+MGPU_BATCHED(outflow, RANGE_ONE, if (sc.has_outflow) b_outflow(d))
 MGPU_BATCHED(ppe, RANGE_N, if (arg < sc.ncorr) b_ppe(d, P, (int)i))
 MGPU_BATCHED(correct_cells, RANGE_N, if (arg < sc.ncorr) b_correct_cells(d, P, (int)i))
 MGPU_BATCHED(correct_flux, RANGE_F, if (arg < sc.ncorr) b_correct_flux(d, (int)i))
@@ -822,7 +833,7 @@ int launch_rhiechow(const DeviceCase& d, const AsmParams& P, cudaStream_t s) {
   return 0;
 }
 int launch_outflow(const DeviceCase& d, cudaStream_t s) {
-  k_outflow<<<1, 32, 0, s>>>(d);
+  k_outflow<<<1, 256, 0, s>>>(d);
   MGPU_LAUNCH_CHECK("k_outflow");
   return 0;
 }

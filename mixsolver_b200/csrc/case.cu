@@ -187,22 +187,38 @@ MixedArgs mixed_args(const MgpuCase* c, bool bicg) {
   const bool big = (double)c->d.N * mixed_row_bytes(c->d.ell_w) > g_prefetch_mb * 1048576.0;
   return MixedArgs{c->d.a32,   c->d.dinv32, c->d.w32,  c->ctrl.mixed_tol > 0.0 ? c->ctrl.mixed_tol : 1e-4,
                    bicg ? 1 : g_cheb_degree, g_cheb_ratio, c->d.ell_w, c->d.ell_col, c->d.ell_val,
-                   c->d.red32, (c->d.ell_col && big) ? 1 : 0};
+                   c->d.red32, (c->d.ell_col && big) ? 1 : 0, g_mixed_scheme, g_rel_delta_pm * 1e-3};
+}
+
+// The same solves in FP64 throughout (MGPU_PREC_FP64_POLY): PCG keeps one
+// Krylov stream and checks b - A x only at its end (no intermediate
+// replacement); BiCGStab solves to the tolerance in one pass.
+MixedArgsT<double> poly64_args(const MgpuCase* c, bool bicg) {
+  const bool big = (double)c->d.N * (16.0 * c->d.ell_w + 8.0 * 10) > g_prefetch_mb * 1048576.0;
+  return MixedArgsT<double>{c->d.a64, c->d.dinv64, c->d.w64, 0.0, bicg ? 1 : g_cheb_degree, g_cheb_ratio,
+                            c->d.ell_w, c->d.ell_col, c->d.ell_val64, c->d.red32,
+                            (c->d.ell_col && big) ? 1 : 0, 1, 0.0};
 }
 
 // factor (if needed) + solve; precond 0 ILU0, 1 Jacobi, 2 IC0. The mixed form
-// (ctrl.precision) runs FP32-inner / FP64-refinement solves with Jacobi.
+// (ctrl.precision) runs FP32-inner / FP64-refinement solves with Jacobi or
+// Chebyshev-Jacobi; the FP64 polynomial form the same solvers in FP64.
 int krylov(MgpuCase* c, KrylovArgs a, bool bicg, cudaStream_t s) {
-  if (c->ctrl.precision == MGPU_PREC_MIXED) {
+  if (c->ctrl.precision == MGPU_PREC_MIXED || c->ctrl.precision == MGPU_PREC_FP64_POLY) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (c->profiling) {
       e0 = next_event(c);
       e1 = next_event(c);
       cudaEventRecord(e0, s);
     }
-    const MixedArgs m = mixed_args(c, bicg);
     a.precond = 1;
-    TRY(bicg ? launch_bicgstab_mixed(a, m, s) : launch_pcg_mixed(a, m, s));
+    if (c->ctrl.precision == MGPU_PREC_MIXED) {
+      const MixedArgs m = mixed_args(c, bicg);
+      TRY(bicg ? launch_bicgstab_mixed(a, m, s) : launch_pcg_mixed(a, m, s));
+    } else {
+      const MixedArgsT<double> m = poly64_args(c, bicg);
+      TRY(bicg ? launch_bicgstab_poly64(a, m, s) : launch_pcg_poly64(a, m, s));
+    }
     c->launches++;
     if (c->profiling) cudaEventRecord(e1, s);
     return 0;
@@ -267,6 +283,7 @@ int reset_status(MgpuCase* c, int ts_order, int nrec) {
   h.ts_order = ts_order;
   h.nan_key = ~0ull;
   h.it_limit = nrec > 1 ? nrec - 1 : 0;
+  h.spin_limit = g_spin_limit;
   MGPU_CUDA(cudaMemcpyAsync(c->d.st, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
   MGPU_CUDA(cudaMemsetAsync(c->d.bar, 0, sizeof(unsigned long long), c->stream));
   MGPU_CUDA(cudaMemsetAsync(c->d.recs, 0, sizeof(MgpuIterRec) * (size_t)nrec, c->stream));
@@ -454,8 +471,13 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
     set_error("ctrl: invalid alpha_u / conv_blend / lin_max");
     return MGPU_E_ARG;
   }
-  if (ctrl->precision == MGPU_PREC_MIXED && hm.N > kMixedMaxRows) {
-    set_error("mgpu_case_create: the mixed-precision form takes at most 2^24 cells");
+  const bool poly = ctrl->precision == MGPU_PREC_MIXED || ctrl->precision == MGPU_PREC_FP64_POLY;
+  if (ctrl->precision < MGPU_PREC_FP64 || ctrl->precision > MGPU_PREC_FP64_POLY) {
+    set_error("mgpu_case_create: unknown precision");
+    return MGPU_E_ARG;
+  }
+  if (poly && hm.N > kMixedMaxRows) {
+    set_error("mgpu_case_create: the mixed-precision and FP64 polynomial forms take at most 2^23 cells");
     return MGPU_E_ARG;
   }
   HostTopo t;
@@ -501,13 +523,15 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
       (e = c->alloc(d.af, F)) || (e = c->alloc(d.aval, d.nnz)) || (e = c->alloc(d.pval, d.nnz)) ||
       (e = c->alloc(d.fval, d.nnz)) || (e = c->alloc(d.kw, 10 * N)) ||
       (ctrl->precision == MGPU_PREC_MIXED &&
-       ((e = c->alloc(d.a32, d.nnz)) || (e = c->alloc(d.dinv32, N)) || (e = c->alloc(d.w32, 10 * N)) ||
-        (e = c->alloc(d.red32, (size_t)mixed_red_words(N))))) ||
+       ((e = c->alloc(d.a32, d.nnz)) || (e = c->alloc(d.dinv32, N)) || (e = c->alloc(d.w32, 10 * N)))) ||
+      (ctrl->precision == MGPU_PREC_FP64_POLY &&
+       ((e = c->alloc(d.a64, d.nnz)) || (e = c->alloc(d.dinv64, N)) || (e = c->alloc(d.w64, 10 * N)))) ||
+      (poly && (e = c->alloc(d.red32, (size_t)mixed_red_words(N)))) ||
       (e = c->alloc(d.partials, 4 * 4096)) ||
       (e = c->alloc(d.bar, 1)) || (e = c->alloc(d.ferr, 1)) || (e = c->alloc(d.st, 1)))
     return fail(e);
   if ((e = ensure_recs(c, 64))) return fail(e);
-  if (ctrl->precision == MGPU_PREC_MIXED) {
+  if (poly) {
     int w = 0;
     for (long i = 0; i < N; ++i) w = std::max(w, t.row_ptr[i + 1] - t.row_ptr[i]);
     if (w <= 8) {  // column-major ELL copy of the pattern for the FP32 SpMV
@@ -517,7 +541,10 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
           const int p = t.row_ptr[i] + k;
           ell[(size_t)k * N + i] = p < t.row_ptr[i + 1] ? t.col[p] : (int)i;
         }
-      if ((e = c->upload(d.ell_col, ell)) || (e = c->alloc(d.ell_val, (size_t)w * N))) return fail(e);
+      if ((e = c->upload(d.ell_col, ell))) return fail(e);
+      if (ctrl->precision == MGPU_PREC_MIXED) e = c->alloc(d.ell_val, (size_t)w * N);
+      else e = c->alloc(d.ell_val64, (size_t)w * N);
+      if (e) return fail(e);
       d.ell_w = w;
     }
   }
@@ -546,6 +573,21 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
   for (auto& g : groups)
     if (g.btype == MGPU_BC_OUTFLOW) c->has_outflow = 1;
   P.has_outflow = c->has_outflow;
+  if (c->has_outflow) {
+    // the faces of outflow_mass_sums' two sums, each in face order
+    std::vector<int> req, out;
+    for (int k = 0; k < hm.F; ++k) {
+      if (hm.c1[k] >= 0 || fgrp[k] < 0) continue;
+      const int bt = groups[fgrp[k]].btype;
+      if (bt == MGPU_BC_OUTFLOW)
+        out.push_back(k);
+      else if (bt != MGPU_BC_POUTLET && bt != MGPU_BC_FARFIELD)
+        req.push_back(k);
+    }
+    if ((e = c->upload(d.of_req, req)) || (e = c->upload(d.of_out, out))) return fail(e);
+    d.n_of_req = (int)req.size();
+    d.n_of_out = (int)out.size();
+  }
   DeviceCase dd = d;
   DevStatus h0{};
   h0.nan_key = ~0ull;

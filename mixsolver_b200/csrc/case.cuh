@@ -28,6 +28,7 @@ struct DevStatus {
   // iteration count, sum of the momentum residuals (in solve order)
   int acc_itl;
   double acc_res;
+  unsigned spin_limit;  // polls before a bounded barrier wait gives up (0: the default, ~2 s)
 };
 
 // Krylov solve arguments (matrix, preconditioner data, work, result slot).
@@ -65,21 +66,27 @@ struct KrylovArgs {
   int sweep_sleep;     // nanosleep of a long wait in that sweep (0: spin)
 };
 
-// Mixed-precision solve data: FP32 matrix copy, FP32 inverse diagonal,
-// FP32 work vectors (10 N), inner relative tolerance.
-struct MixedArgs {
-  float* a32;
-  float* dinv;
-  float* w32;
+// Data of a polynomial-preconditioned solve in working precision V: the
+// matrix copy and inverse diagonal in V, work vectors in V (10 N), inner
+// relative tolerance. V = float is the mixed-precision form (FP32 inner
+// Krylov inside FP64 refinement); V = double the same algorithms in FP64.
+template <typename V>
+struct MixedArgsT {
+  V* a32;
+  V* dinv;
+  V* w32;
   double tau;
   int cheb_k;        // Chebyshev-Jacobi degree of the pressure preconditioner (<= 1: Jacobi)
   double cheb_ratio; // lambda_max / lambda_min of the Chebyshev interval
   int ell_w;         // ELL width (max entries per row) when ell_col is set
   const int* ell_col;  // column-major ELL columns, W*N (padding: the row itself)
-  float* ell_val;      // FP32 values in the same layout (padding: 0)
+  V* ell_val;          // values in the same layout (padding: 0)
   double* red;         // chunk reduction partials: mixed_red_words(N) doubles
   int pf;              // 1: each SpMV tile prefetches the next tile's ELL entries into L2
+  int reliable;        // PCG: 1 reliable updates (one Krylov stream, FP64 x), 0 restarted refinement
+  double rel_delta;    // reliable updates: replace the recursive residual once its norm fell by this factor
 };
+using MixedArgs = MixedArgsT<float>;
 
 // Device bytes a mixed solve streams per row: ELL columns and FP32 values,
 // the seven FP32 work vectors, x, b, r and the inverse diagonal.
@@ -149,6 +156,10 @@ struct DeviceCase {
   int *lt_ptr = nullptr, *lt_pos = nullptr;
   DevGroup* groups = nullptr;
   int ngroups = 0;
+  // outflow rescale (cases with an outflow zone): fixed-flux boundary faces and
+  // outflow faces, each list in face order
+  int *of_req = nullptr, *of_out = nullptr;
+  int n_of_req = 0, n_of_out = 0;
   // fields (SoA)
   double *u = nullptr, *p = nullptr, *gp = nullptr, *gu = nullptr, *flux = nullptr, *apc = nullptr;
   double *ap = nullptr, *rhs = nullptr, *pp = nullptr, *uo = nullptr, *u_old = nullptr, *u_old_old = nullptr;
@@ -157,6 +168,7 @@ struct DeviceCase {
   float *a32 = nullptr, *dinv32 = nullptr, *w32 = nullptr;  // mixed-precision form
   int* ell_col = nullptr;  // column-major ELL pattern of the FP32 copy (W*N)
   float* ell_val = nullptr;
+  double *a64 = nullptr, *dinv64 = nullptr, *w64 = nullptr, *ell_val64 = nullptr;  // FP64 polynomial form
   int ell_w = 0;
   double* red32 = nullptr;  // chunk reduction partials of the mixed-precision solves
   // Krylov work
@@ -176,6 +188,8 @@ int launch_factor(const KrylovArgs& a, int kind, cudaStream_t s);
 int krylov_grid(int n, int& block, int which);
 int launch_pcg_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s);
 int launch_bicgstab_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s);
+int launch_pcg_poly64(const KrylovArgs& a, const MixedArgsT<double>& m, cudaStream_t s);
+int launch_bicgstab_poly64(const KrylovArgs& a, const MixedArgsT<double>& m, cudaStream_t s);
 int batch_capacity(bool pcg, int ell);  // ell: 0 CSR, 1 ELL, 2 ELL + L2 prefetch
 int launch_mixed_batch(const LanePlan& p, bool pcg, int ell, cudaStream_t s);
 int launch_spmv(int n, const int* rp, const int* col, const double* val, const double* x, double* y,

@@ -50,6 +50,9 @@ int g_batch_reserve = 0;  // block slots batched launches leave to other streams
 int g_prefetch_mb = 96;   // mixed systems whose streamed bytes exceed this prefetch into L2
 int prewarm_streams(int n);  // case.cu
 double g_cheb_ratio = 1000.0; // and the ratio lambda_max / lambda_min of its interval
+int g_mixed_scheme = 1;   // mixed PCG: 1 reliable updates, 0 restarted refinement
+int g_rel_delta_pm = 100; // reliable updates: residual replaced after a fall by this many thousandths
+unsigned g_spin_limit = 0; // polls before a bounded barrier wait gives up (0: kSpinLimit, ~2 s)
 namespace {
 
 __device__ __forceinline__ double ld_relaxed_f64(const double* p) {
@@ -666,26 +669,30 @@ int launch_coop(const void* fn, void** args, unsigned long long* bar, int grid, 
 // no grid barrier) for small systems, else enough 256-thread blocks for ~4
 // rows per thread, capped by co-residency.
 int krylov_grid(int n, int& block, int which) {
-  static int max_blocks[3] = {0, 0, 0};
+  constexpr int kDevs = 64;  // co-resident capacity, per device (GPUs of a node may differ)
+  static int max_blocks[kDevs][3] = {};
   if (n <= g_single_block_rows) {
     block = 512;
     return 1;
   }
   block = 256;
-  if (max_blocks[which] == 0) {
-    int dev = 0, sms = 0, per = 0;
-    cudaGetDevice(&dev);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= kDevs) dev = 0;
+  int (&mb)[3] = max_blocks[dev];
+  if (mb[which] == 0) {
+    int sms = 0, per = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const void* fn = which == 0 ? (const void*)k_pcg<false>
                                 : which == 1 ? (const void*)k_bicgstab<false> : (const void*)k_factor<false>;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, block, 0);
     if (per < 1) per = 1;
-    max_blocks[which] = sms * per;
+    mb[which] = sms * per;
   }
   long want = ((long)n + (long)block * 4 - 1) / ((long)block * 4);
   if (want < g_min_blocks) want = g_min_blocks;
   if (want < 1) want = 1;
-  if (want > max_blocks[which]) want = max_blocks[which];
+  if (want > mb[which]) want = mb[which];
   return (int)want;
 }
 
@@ -746,6 +753,12 @@ int set_tuning(const char* key, int value) {
     g_batch_reserve = value;
   } else if (k == "l2_prefetch_mb" && value >= 0) {
     g_prefetch_mb = value;
+  } else if (k == "mixed_scheme" && (value == 0 || value == 1)) {
+    g_mixed_scheme = value;
+  } else if (k == "reliable_delta_permille" && value >= 1 && value <= 900) {
+    g_rel_delta_pm = value;
+  } else if (k == "spin_limit" && value >= 0) {
+    g_spin_limit = (unsigned)value;
   } else if (k == "stream_pool" && value >= 0 && value <= 1024) {
     if (int e = prewarm_streams(value)) return e;
   } else {

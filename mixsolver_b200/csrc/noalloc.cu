@@ -2,9 +2,8 @@
 //
 // Some callers cannot call cudaMalloc at all: a host that hands over only its
 // own device buffers and forbids allocations behind its back (a memory pool or
-// a framework that owns every byte of the device), a CUDA Fortran host whose
-// arrays already live on the GPU, or code between cudaStreamBeginCapture and
-// cudaStreamEndCapture, where an allocation breaks the capture. For them this
+// a framework that owns every byte of the device), or a CUDA Fortran host whose
+// arrays already live on the GPU. For them this
 // entry point runs the library's persistent PCG-Jacobi solve with every work
 // vector, reduction partial, barrier counter and status word taken from one
 // file-scope __device__ array of fixed size. The caller passes the matrix,
@@ -16,7 +15,11 @@
 //   * all calls share the one array, so calls that overlap on the GPU (two
 //     streams, two host threads) race and corrupt each other; serialise them;
 //   * the first call on a device looks the array's address up for that device
-//     (cudaGetSymbolAddress); make that first call before any stream capture.
+//     (cudaGetSymbolAddress);
+//   * the call reads its result back and waits for its stream, so it cannot
+//     run inside a stream capture;
+//   * the solve's grid holds at most kPartials / 8 blocks (two halves of four
+//     reduction partials per block); a larger grid is refused.
 
 #include <cuda_runtime.h>
 
@@ -133,6 +136,11 @@ extern "C" int mgpu_cg_jacobi_noalloc(int n, const int32_t* d_row_ptr, const int
   a.slot = 0;
   a.ier_breakdown = 0;
   a.ferr = flags + 2;
+  int block = 0;
+  if (8l * krylov_grid(n, block, 0) > kPartials) {
+    set_error("mgpu_cg_jacobi_noalloc: the solve's grid needs more reduction partials than the fixed array holds");
+    return MGPU_E_ARG;
+  }
   if (int e = launch_krylov_pcg(a, s)) return e;
   MgpuIterRec rec;
   DevStatus st;

@@ -53,7 +53,9 @@ __device__ __forceinline__ VGrid whole_grid(unsigned long long* bar, double* par
 // round. While it waits it looks at the status every 4096 polls: once any
 // block has flagged a timeout (st may be null: no status) the wait ends. A
 // wait that runs out flags the timeout. Returns false in both cases; the
-// caller then leaves the kernel.
+// caller then leaves the kernel. The status may lower the poll limit
+// (DevStatus::spin_limit, from the spin_limit tuning key) so that a test can
+// make a wait run out on purpose.
 // Ordering: __syncthreads puts the block's writes before thread 0's arrival,
 // a release at GPU scope; thread 0's polls are acquires, and the closing
 // __syncthreads puts them before the block's later loads. Release and acquire
@@ -73,6 +75,7 @@ __device__ bool vg_sync(const VGrid& g, DevStatus* st) {
     unsigned long long old;
     asm volatile("atom.add.release.gpu.global.u64 %0, [%1], 1;" : "=l"(old) : "l"(bar) : "memory");
     const unsigned long long target = (old / nb + 1ull) * nb;
+    const unsigned limit = (st && st->spin_limit) ? st->spin_limit : kSpinLimit;
     unsigned spins = 0;
     while (ld_acquire_u64(bar) < target) {
       ++spins;
@@ -81,7 +84,7 @@ __device__ bool vg_sync(const VGrid& g, DevStatus* st) {
         ok = 0;
         break;
       }
-      if (spins > kSpinLimit) {
+      if (spins > limit) {
         if (st) atomicExch(&st->timeout, 1);
         ok = 0;
         break;

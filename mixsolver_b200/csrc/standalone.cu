@@ -12,6 +12,10 @@
 #include "case.cuh"
 #include "mesh_host.h"
 
+namespace mgpu {
+extern unsigned g_spin_limit;  // krylov.cu: the spin_limit tuning key
+}
+
 using namespace mgpu;
 
 namespace {
@@ -164,6 +168,7 @@ int mgpu_krylov_solve(int n, const int32_t* row_ptr, const int32_t* col_idx, con
   TRY(B.alloc(drec, 1));
   DevStatus h{};
   h.nan_key = ~0ull;
+  h.spin_limit = g_spin_limit;
   MGPU_CUDA(cudaMemcpy(dst, &h, sizeof(h), cudaMemcpyHostToDevice));
   MGPU_CUDA(cudaMemset(dbar, 0, sizeof(unsigned long long)));
   MGPU_CUDA(cudaMemset(drec, 0, sizeof(MgpuIterRec)));

@@ -12,6 +12,8 @@ so whole runs are compared with tolerances:
     (~1e-4 at res ~ 1e-9), so a tighter bound would test rounding noise;
   * mass imbalance: absolute 1e-12 (it is itself round-off after the correction).
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -428,3 +430,126 @@ def test_bc_errors():
     ctrl.bcs.append(abi.BcSpec(zone=77, btype=abi.BC_WALL))
     with pytest.raises(RuntimeError, match="ier 10"):
         S.UnsCase(mesh, ctrl)
+
+
+def bc_case(name, outer_max=12):
+    """Small 3-D boxes (12 x 6 x 6, jittered, RCM order) whose boundary zones
+    carry every boundary type the path supports besides the ones above, so
+    each branch of bc_face_vel / bc_face_p (mod_uns_bc.f90:400-549) and the
+    outflow rescale (mod_uns_simple.f90:1463-1547) meets the oracle:
+      * mass_outflow: mass-flow inlet (ramped over 4 iterations), outflow,
+        no-slip wall, slip wall, symmetry -- no pressure-Dirichlet face, so
+        the pressure correction is pinned and the outflow faces rescaled;
+      * vinlet_farfield: uniform velocity inlet, far field (free stream along
+        +x, p = 0.05, ramped), wall with a moving lid strip, slip wall,
+        symmetry;
+      * vinlet_poutlet: uniform velocity inlet with a cross-stream component,
+        pressure outlet at p = 0.2 (ramped), walls."""
+    zones = (4, 5, 6, 7, 8, 8)
+    mesh = meshgen.box_hex(12, 6, 6, lx=3.0, jitter=0.1, seed=11, zones=zones)
+    mesh = cases.rcm_renumber(meshgen.shuffle_cells(mesh, 12), S.rcm_order)
+    _, ctrl = cases.channel3d(4, 2, 2, outer_max=outer_max)
+    ctrl.mu = 2e-2
+    ctrl.mom_solver = abi.MOM_ILU0
+    ctrl.ppe_precond = abi.PPE_IC0
+    ctrl.lin_max = 300
+    B = abi.BcSpec
+    if name == "mass_outflow":
+        ctrl.inlet_ramp = 4
+        ctrl.bcs = [B(zone=4, btype=abi.BC_MASSINLET, mdot=0.8), B(zone=5, btype=abi.BC_OUTFLOW),
+                    B(zone=6, btype=abi.BC_WALL), B(zone=7, btype=abi.BC_SLIPWALL), B(zone=8, btype=abi.BC_SYMMETRY)]
+    elif name == "vinlet_farfield":
+        ctrl.inlet_ramp = 3
+        ctrl.bcs = [B(zone=4, btype=abi.BC_VINLET, uvel=(1.0, 0.0, 0.0)),
+                    B(zone=5, btype=abi.BC_FARFIELD, uvel=(1.0, 0.0, 0.0), pval=0.05),
+                    B(zone=6, btype=abi.BC_WALL, lid=(2, 0.0, (0.3, 0.0, 0.0))),
+                    B(zone=7, btype=abi.BC_SLIPWALL), B(zone=8, btype=abi.BC_SYMMETRY)]
+    else:
+        ctrl.inlet_ramp = 5
+        ctrl.bcs = [B(zone=4, btype=abi.BC_VINLET, uvel=(1.0, 0.1, -0.05)),
+                    B(zone=5, btype=abi.BC_POUTLET, pval=0.2),
+                    B(zone=6, btype=abi.BC_WALL), B(zone=7, btype=abi.BC_WALL), B(zone=8, btype=abi.BC_WALL)]
+    return mesh, ctrl
+
+
+BC_CASES = ["mass_outflow", "vinlet_farfield", "vinlet_poutlet"]
+
+
+@pytest.mark.parametrize("name", BC_CASES)
+def test_bc_stage_kernels_bit_exact(name):
+    """Every assembly stage on each boundary mix, element for element."""
+    mesh, ctrl = bc_case(name)
+    nnz = len(S.build_connectivity(mesh)["col_idx"])
+    g = S.UnsCase(mesh, ctrl)
+    o = O.OracleCase(mesh, ctrl)
+    u, p, flux = _seed_fields(mesh, seed=7)
+    apc = 1.0 + np.random.default_rng(8).random(mesh.ncells)
+    for c in (g, o):
+        c.upload(u=u, p=p, flux=flux)
+    o.set_apc(apc, 0)
+    g.stage(0, 0, apc)
+    o.stage(0)
+    fg, fo = g.fields(), o.fields()
+    np.testing.assert_array_equal(fg["gp"], fo["gp"])
+    np.testing.assert_array_equal(fg["gu"], fo["gu"])
+    for comp in (1, 2, 3):
+        for a, b in zip(g.stage(comp, 0, apc, nnz), o.stage(comp, nnz)):
+            np.testing.assert_array_equal(a, b)
+    g.stage(4, 0, apc)
+    o.stage(4)
+    np.testing.assert_array_equal(g.fields()["flux"], o.fields()["flux"])
+    for a, b in zip(g.stage(5, 0, apc, nnz)[:2], o.stage(5, nnz)[:2]):
+        np.testing.assert_array_equal(a, b)
+    pp = np.random.default_rng(9).standard_normal(mesh.ncells) * 1e-3
+    g.stage(6, 0, apc, pp=pp)
+    o.stage(6, pp=pp)
+    fg, fo = g.fields(), o.fields()
+    for k in ("u", "p", "flux"):
+        np.testing.assert_array_equal(fg[k], fo[k], err_msg=k)
+
+
+@pytest.mark.parametrize("name", BC_CASES)
+def test_bc_simple_parity(name):
+    """Whole SIMPLE runs on each boundary mix (outflow rescale and inlet ramp
+    included): the parity bar of the runs above."""
+    mesh, ctrl = bc_case(name)
+    g = S.UnsCase(mesh, ctrl)
+    o = O.OracleCase(mesh, ctrl)
+    ier_g, log_g = g.simple_run()
+    ier_o, log_o = o.simple_run()
+    assert ier_g == ier_o == 0
+    _compare_runs(log_g, log_o, g.fields(), o.fields())
+
+
+def _lowspeed():
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from fixtures import LOWSPEED_MESH, decode_mesh, lowspeed_control
+    return decode_mesh(LOWSPEED_MESH), lowspeed_control
+
+
+def test_channel_lowspeed_first_iteration_is_the_reference_log_on_gpu():
+    """The reference binary's recorded first iteration on its own channel case
+    (cluster_cases/channel_lowspeed/README.md section 4: mass-imbal 5.113E-13,
+    du_max 2.840E-04, lin-it 278), reproduced by the CUDA path: mass-flow
+    inlet, outflow rescale, walls, symmetry, IC(0) pressure solve."""
+    mesh, ctl = _lowspeed()
+    g = S.UnsCase(mesh, ctl())
+    ier, log = g.simple_run(1)
+    assert ier == 0
+    r = log[0]
+    assert f"{r['imbal']:.3E}" == "5.113E-13"
+    assert f"{r['du_max']:.3E}" == "2.840E-04"
+    assert r["itl_max"] == 278
+
+
+def test_channel_lowspeed_parity():
+    """Ten outer iterations of the same case against the oracle."""
+    mesh, ctl = _lowspeed()
+    ctrl = ctl(outer_max=10)
+    g = S.UnsCase(mesh, ctrl)
+    o = O.OracleCase(mesh, ctrl)
+    ier_g, log_g = g.simple_run()
+    ier_o, log_o = o.simple_run()
+    assert ier_g == ier_o == 0
+    _compare_runs(log_g, log_o, g.fields(), o.fields())

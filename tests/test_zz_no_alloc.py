@@ -1,12 +1,14 @@
 """The allocation-free PCG-Jacobi entry point (mgpu_cg_jacobi_noalloc).
 
 It serves callers that may not allocate device memory (a host that owns all
-device memory, CUDA Fortran device arrays, code inside a stream capture): the
-caller passes device buffers, the library works in one fixed internal array.
-Checked through the C-ABI against the allocating entry point
-(mgpu_krylov_solve, cg_jacobi) with the tolerances of the parity tests, on two
-calls in a row, so the second call also shows the shared array is cleared.
-This file is collected last on purpose.
+device memory, CUDA Fortran device arrays): the caller passes device buffers,
+the library works in one fixed internal array. Checked through the C-ABI
+against the allocating entry point (mgpu_krylov_solve, cg_jacobi) with the
+tolerances of the parity tests, on two calls in a row, so the second call also
+shows the shared array is cleared; once on one block and once on several
+blocks, where the array's grid-barrier counter and reduction partials are in
+use; and on the early returns (b = 0, a row without a diagonal). This file is
+collected last on purpose.
 """
 import ctypes as C
 
@@ -47,7 +49,19 @@ def _noalloc(lib, torch, rp, ci, val, b, x0, tol, maxit):
     return d_x.cpu().numpy(), it.value, res.value, ierr.value
 
 
-def test_noalloc_matches_allocating_entry_point(gpu_lib):
+@pytest.fixture(params=["one_block", "multi_block"])
+def layout(request):
+    """One block, or the cooperative multi-block solve on 6 blocks (grid
+    barrier and reduction partials inside the fixed array)."""
+    if request.param == "multi_block":
+        S.set_tuning("single_block_rows", 0)
+        S.set_tuning("min_blocks", 6)
+    yield request.param
+    S.set_tuning("single_block_rows", 32768)
+    S.set_tuning("min_blocks", 1)
+
+
+def test_noalloc_matches_allocating_entry_point(gpu_lib, layout):
     torch = pytest.importorskip("torch")
     rp, ci, val, b1, b2 = _system()
     n = len(rp) - 1
@@ -58,6 +72,30 @@ def test_noalloc_matches_allocating_entry_point(gpu_lib):
         assert (ita, ierra) == (itr, ierrr) and ierra == 0
         assert abs(resa - resr) <= 1e-3 * resr
         assert np.linalg.norm(xa - xr) / np.linalg.norm(xr) < 1e-9
+
+
+def test_noalloc_early_returns_match(gpu_lib):
+    """b = 0 gives x = 0 at iteration 0; a row without a diagonal gives
+    ierr = 2 with x left as it was (cg_jacobi's contract), as the allocating
+    entry point returns them."""
+    torch = pytest.importorskip("torch")
+    rp, ci, val, _, _ = _system(8)
+    n = len(rp) - 1
+    x0 = np.full(n, 0.5)
+    xa, ita, resa, ierra = _noalloc(gpu_lib, torch, rp, ci, val, np.zeros(n), x0, 1e-8, 50)
+    xr, itr, resr, ierrr = S.cg_jacobi(rp, ci, val, np.zeros(n), x0, 1e-8, 50)
+    assert (ita, ierra) == (itr, ierrr) == (0, 0)
+    np.testing.assert_array_equal(xa, xr)
+    assert np.all(xa == 0.0)
+    rp2 = np.array([1, 2, 3], np.int32)
+    ci2 = np.array([2, 1], np.int32)        # no diagonal in either row
+    v2 = np.array([1.0, 1.0])
+    b2 = np.array([1.0, 1.0])
+    x2 = np.array([0.25, -0.5])
+    xa, ita, _, ierra = _noalloc(gpu_lib, torch, rp2, ci2, v2, b2, x2, 1e-8, 10)
+    xr, itr, _, ierrr = S.cg_jacobi(rp2, ci2, v2, b2, x2, 1e-8, 10)
+    assert (ita, ierra) == (itr, ierrr) and ierra == 2
+    np.testing.assert_array_equal(xa, xr)
 
 
 def test_noalloc_rejects_oversize(gpu_lib):

@@ -299,63 +299,29 @@ __global__ void __launch_bounds__(256) k_limiter(DeviceCase d, AsmParams P, int 
   b_limiter(d, P, comp, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-// momentum_assembly for component comp: row c of A, rhs(c), ap(c)
-__device__ __forceinline__ void b_momentum(const DeviceCase& d, const AsmParams& P, int comp, const int c) {
-  if (d.st->abort || c >= d.N) return;
+// momentum_assembly (mod_uns_simple.f90:928-1338), the part after the
+// interior faces: boundary faces (:1123-1227), sources (:1233-1284), time term
+// (:1297-1311) and alpha_u relaxation (:1322-1334) of component comp of cell
+// c, continuing the interior sums ap and rhs, then A(diag), rhs and ap out.
+// LIST: the boundary faces come from the cell's own boundary-face list (the
+// same faces in the same order as the cell's face list, with the interior
+// faces and the faces without a group left out); otherwise from its face list.
+template <bool LIST>
+__device__ __forceinline__ void mom_finish(const DeviceCase& d, const AsmParams& P, const Ramp& rp, int comp,
+                                           const int c, double ap, double rhs) {
   const int N = d.N, F = d.F;
-  const Ramp rp = ramp_of(P, d.st);
   const double *u0 = d.u, *u1 = d.u + N, *u2 = d.u + 2 * N;
   const double* ucomp = d.u + (long)comp * N;
   const double* sfc = d.sf + (long)comp * F;
   double* A = d.aval;
-  const int rb = d.row_ptr[c], re = d.row_ptr[c + 1];
-  for (int k = rb; k < re; ++k) A[k] = 0.0;
-  double ap = 0.0, rhs = 0.0;
-  const int kb = d.cf_ptr[c], ke = d.cf_ptr[c + 1];
-  // interior faces
+  const int kb = LIST ? d.bf_ptr[c] : d.cf_ptr[c], ke = LIST ? d.bf_ptr[c + 1] : d.cf_ptr[c + 1];
   for (int k = kb; k < ke; ++k) {
-    const int f = d.cf[k];
-    const int b = d.c1[f];
-    if (b < 0) continue;
-    const int a = d.c0[f];
-    const bool own = (a == c);
-    const double Fm = d.flux[f];
-    const double D = d.Dm[f];
-    const int slot = d.cf_slot[k];
-    if (own) {
-      ap = ap + fmax(Fm, 0.0) + D;
-      A[slot] = A[slot] - (D + fmax(-Fm, 0.0));
-    } else {
-      ap = ap + fmax(-Fm, 0.0) + D;
-      A[slot] = A[slot] - (D + fmax(Fm, 0.0));
+    const int f = LIST ? d.bf[k] : d.cf[k];
+    if (!LIST) {
+      if (d.c1[f] >= 0) continue;
+      if (d.fgrp[f] < 0) continue;
     }
-    const double lf = d.lf[f], l1 = 1.0 - lf;
-    if (P.conv_blend > 0.0) {
-      const int cu = (Fm > 0.0) ? a : b;
-      const double dcv = d.psi[cu] * dot3(d.gu[(comp * 3 + 0) * N + cu], d.gu[(comp * 3 + 1) * N + cu],
-                                          d.gu[(comp * 3 + 2) * N + cu], d.xf[f] - d.xc[cu],
-                                          d.xf[F + f] - d.xc[N + cu], d.xf[2 * F + f] - d.xc[2 * N + cu]);
-      const double dc = P.conv_blend * Fm * dcv;
-      rhs = own ? rhs - dc : rhs + dc;
-    }
-    if (P.nonorth_corr > 0.0) {
-      const double gf0 = lf * d.gu[(comp * 3 + 0) * N + a] + l1 * d.gu[(comp * 3 + 0) * N + b];
-      const double gf1 = lf * d.gu[(comp * 3 + 1) * N + a] + l1 * d.gu[(comp * 3 + 1) * N + b];
-      const double gf2 = lf * d.gu[(comp * 3 + 2) * N + a] + l1 * d.gu[(comp * 3 + 2) * N + b];
-      const double noc = d.mnc[f] * dot3(gf0, gf1, gf2, d.tv[f], d.tv[F + f], d.tv[2 * F + f]);
-      rhs = own ? rhs + noc : rhs - noc;
-    }
-    const double pf = lf * d.p[a] + l1 * d.p[b];
-    const double S = sfc[f];
-    rhs = own ? rhs - pf * S : rhs + pf * S;
-  }
-  // boundary faces
-  for (int k = kb; k < ke; ++k) {
-    const int f = d.cf[k];
-    if (d.c1[f] >= 0) continue;
-    const int gi = d.fgrp[f];
-    if (gi < 0) continue;
-    const DevGroup& gr = d.groups[gi];
+    const DevGroup& gr = d.groups[d.fgrp[f]];
     const double s0 = d.sf[f], s1 = d.sf[F + f], s2 = d.sf[2 * F + f];
     double w[3];
     bc_face_vel(gr, rp, d.xf[f], d.xf[F + f], d.xf[2 * F + f], s0, s1, s2, u0[c], u1[c], u2[c], w[0], w[1],
@@ -412,8 +378,129 @@ __device__ __forceinline__ void b_momentum(const DeviceCase& d, const AsmParams&
   d.rhs[c] = rhs;
   d.ap[c] = ap;
 }
+
+// momentum_assembly for component comp: row c of A, rhs(c), ap(c)
+__device__ __forceinline__ void b_momentum(const DeviceCase& d, const AsmParams& P, int comp, const int c) {
+  if (d.st->abort || c >= d.N) return;
+  const int N = d.N, F = d.F;
+  const Ramp rp = ramp_of(P, d.st);
+  const double* sfc = d.sf + (long)comp * F;
+  double* A = d.aval;
+  const int rb = d.row_ptr[c], re = d.row_ptr[c + 1];
+  for (int k = rb; k < re; ++k) A[k] = 0.0;
+  double ap = 0.0, rhs = 0.0;
+  const int kb = d.cf_ptr[c], ke = d.cf_ptr[c + 1];
+  // interior faces
+  for (int k = kb; k < ke; ++k) {
+    const int f = d.cf[k];
+    const int b = d.c1[f];
+    if (b < 0) continue;
+    const int a = d.c0[f];
+    const bool own = (a == c);
+    const double Fm = d.flux[f];
+    const double D = d.Dm[f];
+    const int slot = d.cf_slot[k];
+    if (own) {
+      ap = ap + fmax(Fm, 0.0) + D;
+      A[slot] = A[slot] - (D + fmax(-Fm, 0.0));
+    } else {
+      ap = ap + fmax(-Fm, 0.0) + D;
+      A[slot] = A[slot] - (D + fmax(Fm, 0.0));
+    }
+    const double lf = d.lf[f], l1 = 1.0 - lf;
+    if (P.conv_blend > 0.0) {
+      const int cu = (Fm > 0.0) ? a : b;
+      const double dcv = d.psi[cu] * dot3(d.gu[(comp * 3 + 0) * N + cu], d.gu[(comp * 3 + 1) * N + cu],
+                                          d.gu[(comp * 3 + 2) * N + cu], d.xf[f] - d.xc[cu],
+                                          d.xf[F + f] - d.xc[N + cu], d.xf[2 * F + f] - d.xc[2 * N + cu]);
+      const double dc = P.conv_blend * Fm * dcv;
+      rhs = own ? rhs - dc : rhs + dc;
+    }
+    if (P.nonorth_corr > 0.0) {
+      const double gf0 = lf * d.gu[(comp * 3 + 0) * N + a] + l1 * d.gu[(comp * 3 + 0) * N + b];
+      const double gf1 = lf * d.gu[(comp * 3 + 1) * N + a] + l1 * d.gu[(comp * 3 + 1) * N + b];
+      const double gf2 = lf * d.gu[(comp * 3 + 2) * N + a] + l1 * d.gu[(comp * 3 + 2) * N + b];
+      const double noc = d.mnc[f] * dot3(gf0, gf1, gf2, d.tv[f], d.tv[F + f], d.tv[2 * F + f]);
+      rhs = own ? rhs + noc : rhs - noc;
+    }
+    const double pf = lf * d.p[a] + l1 * d.p[b];
+    const double S = sfc[f];
+    rhs = own ? rhs - pf * S : rhs + pf * S;
+  }
+  mom_finish<false>(d, P, rp, comp, c, ap, rhs);
+}
 __global__ void __launch_bounds__(256) k_momentum(DeviceCase d, AsmParams P, int comp) {
   b_momentum(d, P, comp, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// The interior faces of momentum_assembly (mod_uns_simple.f90:974-1120) for
+// all three components at once, without the deferred convection correction
+// (conv_blend = 0: the only input that changes between the components' solves
+// inside the interior loop is then absent). The matrix row (off-diagonals) and
+// ap are the same for every component; the three rhs sums are kept apart, each
+// receiving its component's terms in the reference's order. Out: the row of A,
+// mom_ap(c), mom_rhs(comp, c); mom_finish<true> completes each component after
+// the previous component's solve.
+__device__ __forceinline__ void b_mom_interior(const DeviceCase& d, const AsmParams& P, const int c) {
+  if (d.st->abort || c >= d.N) return;
+  const int N = d.N, F = d.F;
+  double* A = d.aval;
+  const int rb = d.row_ptr[c], re = d.row_ptr[c + 1];
+  for (int k = rb; k < re; ++k) A[k] = 0.0;
+  double ap = 0.0, r0 = 0.0, r1 = 0.0, r2 = 0.0;
+  const int kb = d.cf_ptr[c], ke = d.cf_ptr[c + 1];
+  for (int k = kb; k < ke; ++k) {
+    const int f = d.cf[k];
+    const int b = d.c1[f];
+    if (b < 0) continue;
+    const int a = d.c0[f];
+    const bool own = (a == c);
+    const double Fm = d.flux[f];
+    const double D = d.Dm[f];
+    const int slot = d.cf_slot[k];
+    if (own) {
+      ap = ap + fmax(Fm, 0.0) + D;
+      A[slot] = A[slot] - (D + fmax(-Fm, 0.0));
+    } else {
+      ap = ap + fmax(-Fm, 0.0) + D;
+      A[slot] = A[slot] - (D + fmax(Fm, 0.0));
+    }
+    const double lf = d.lf[f], l1 = 1.0 - lf;
+    if (P.nonorth_corr > 0.0) {
+      const double t0 = d.tv[f], t1 = d.tv[F + f], t2 = d.tv[2 * F + f], mn = d.mnc[f];
+      double nc[3];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const double gf0 = lf * d.gu[(q * 3 + 0) * N + a] + l1 * d.gu[(q * 3 + 0) * N + b];
+        const double gf1 = lf * d.gu[(q * 3 + 1) * N + a] + l1 * d.gu[(q * 3 + 1) * N + b];
+        const double gf2 = lf * d.gu[(q * 3 + 2) * N + a] + l1 * d.gu[(q * 3 + 2) * N + b];
+        nc[q] = mn * dot3(gf0, gf1, gf2, t0, t1, t2);
+      }
+      r0 = own ? r0 + nc[0] : r0 - nc[0];
+      r1 = own ? r1 + nc[1] : r1 - nc[1];
+      r2 = own ? r2 + nc[2] : r2 - nc[2];
+    }
+    const double pf = lf * d.p[a] + l1 * d.p[b];
+    const double S0 = d.sf[f], S1 = d.sf[F + f], S2 = d.sf[2 * F + f];
+    r0 = own ? r0 - pf * S0 : r0 + pf * S0;
+    r1 = own ? r1 - pf * S1 : r1 + pf * S1;
+    r2 = own ? r2 - pf * S2 : r2 + pf * S2;
+  }
+  d.mom_ap[c] = ap;
+  d.mom_rhs[c] = r0;
+  d.mom_rhs[N + c] = r1;
+  d.mom_rhs[2 * N + c] = r2;
+}
+__global__ void __launch_bounds__(256) k_mom_interior(DeviceCase d, AsmParams P) {
+  b_mom_interior(d, P, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+__device__ __forceinline__ void b_mom_finish(const DeviceCase& d, const AsmParams& P, int comp, const int c) {
+  if (d.st->abort || c >= d.N) return;
+  mom_finish<true>(d, P, ramp_of(P, d.st), comp, c, d.mom_ap[c], d.mom_rhs[(long)comp * d.N + c]);
+}
+__global__ void __launch_bounds__(256) k_mom_finish(DeviceCase d, AsmParams P, int comp) {
+  b_mom_finish(d, P, comp, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 __device__ __forceinline__ void b_apc(const DeviceCase& d, double div, const int c) {
@@ -770,6 +857,8 @@ MGPU_BATCHED(rhiechow_piso, RANGE_F, if (sc.transient) b_rhiechow(d, P, (int)i))
 MGPU_BATCHED(begin_iter, RANGE_3N, b_begin_iter(d, sc.transient, sc.time_scheme, i))
 MGPU_BATCHED(limiter, RANGE_N, if (P.conv_blend > 0.0) b_limiter(d, P, arg, (int)i))
 MGPU_BATCHED(momentum, RANGE_N, b_momentum(d, P, arg, (int)i))
+MGPU_BATCHED(mom_interior, RANGE_N, b_mom_interior(d, P, (int)i))
+MGPU_BATCHED(mom_finish, RANGE_N, b_mom_finish(d, P, arg, (int)i))
 MGPU_BATCHED(apc, RANGE_N, b_apc(d, sc.transient ? 1.0 : P.alpha_u, (int)i))
 MGPU_BATCHED(rhiechow, RANGE_F, b_rhiechow(d, P, (int)i))
 MGPU_BATCHED(outflow, RANGE_ONE, if (sc.has_outflow) b_outflow(d))
@@ -815,6 +904,16 @@ int launch_limiter(const DeviceCase& d, const AsmParams& P, int comp, cudaStream
 int launch_momentum(const DeviceCase& d, const AsmParams& P, int comp, cudaStream_t s) {
   k_momentum<<<GRID(d.N)>>>(d, P, comp);
   MGPU_LAUNCH_CHECK("k_momentum");
+  return 0;
+}
+int launch_mom_interior(const DeviceCase& d, const AsmParams& P, cudaStream_t s) {
+  k_mom_interior<<<GRID(d.N)>>>(d, P);
+  MGPU_LAUNCH_CHECK("k_mom_interior");
+  return 0;
+}
+int launch_mom_finish(const DeviceCase& d, const AsmParams& P, int comp, cudaStream_t s) {
+  k_mom_finish<<<GRID(d.N)>>>(d, P, comp);
+  MGPU_LAUNCH_CHECK("k_mom_finish");
   return 0;
 }
 int launch_apc(const DeviceCase& d, double div, cudaStream_t s) {
@@ -875,6 +974,8 @@ int launch_batch_asm(int op, int arg, const AsmBatch& b, cudaStream_t s) {
       {kb_begin_iter, RANGE_3N, "kb_begin_iter"},
       {kb_limiter, RANGE_N, "kb_limiter"},
       {kb_momentum, RANGE_N, "kb_momentum"},
+      {kb_mom_interior, RANGE_N, "kb_mom_interior"},
+      {kb_mom_finish, RANGE_N, "kb_mom_finish"},
       {kb_apc, RANGE_N, "kb_apc"},
       {kb_rhiechow, RANGE_F, "kb_rhiechow"},
       {kb_outflow, RANGE_ONE, "kb_outflow"},

@@ -47,6 +47,8 @@ enum BatchOp {
   BOP_BEGIN_ITER,
   BOP_LIMITER,        // arg: component
   BOP_MOMENTUM,       // arg: component
+  BOP_MOM_INTERIOR,   // interior faces of all three components (conv_blend = 0)
+  BOP_MOM_FINISH,     // arg: component; boundary faces, sources, relaxation
   BOP_APC,
   BOP_RHIECHOW,
   BOP_OUTFLOW,
@@ -65,6 +67,11 @@ int geometry_setup(DeviceCase& d, const double* x, const int* fptr, const int* f
 int launch_gradients(const DeviceCase& d, const AsmParams& P, cudaStream_t s);
 int launch_limiter(const DeviceCase& d, const AsmParams& P, int comp, cudaStream_t s);
 int launch_momentum(const DeviceCase& d, const AsmParams& P, int comp, cudaStream_t s);
+// conv_blend = 0: launch_mom_interior once per outer iteration, then before
+// each component's solve launch_mom_finish(comp) -- the same A, rhs and ap as
+// launch_momentum(comp), bit for bit
+int launch_mom_interior(const DeviceCase& d, const AsmParams& P, cudaStream_t s);
+int launch_mom_finish(const DeviceCase& d, const AsmParams& P, int comp, cudaStream_t s);
 int launch_apc(const DeviceCase& d, double div, cudaStream_t s);
 int launch_fill(double* a, long n, double v, cudaStream_t s);
 int launch_rhiechow(const DeviceCase& d, const AsmParams& P, cudaStream_t s);

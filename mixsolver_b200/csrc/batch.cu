@@ -363,9 +363,10 @@ int count_launches(const MgpuBatch* b) {
       n += jac ? 1 : 2;
     }
   }
-  // begin, momentum x3, apc, gradients, rhiechow, 3 per corrector, diag x2
+  // begin, momentum x3 (+ the interior pass, or the limiter x3), apc,
+  // gradients, rhiechow, 3 per corrector, diag x2
   n += 1 + 3 + 3 + 3 * b->maxcorr + 2;
-  if (b->any_blend) n += 3;
+  n += b->any_blend ? 3 : 1;
   if (b->any_outflow) n += 1;
   return n;
 }
@@ -436,6 +437,7 @@ int prepare(MgpuBatch* b) {
       s.a = P.pcg ? ppe_args(c, std::min(3 + P.icorr, MGPU_MAXSOLVE - 1), tr) : mom_args(c, P.comp, tr);
       s.a.precond = 1;
       s.m = mixed_args(c, !P.pcg);
+      s.m.flags = nullptr;  // lanes use grid-stride rows and lane barriers
       hs.push_back(s);
       P.mixed.push_back(k);
     }
@@ -495,6 +497,20 @@ int measure_passes(MgpuBatch* b) {
 
 // One iteration launch by launch with events around every phase and lane
 // timestamps in the first pressure phase; accumulates into the batch's
+// The momentum assembly of component comp for every member: with any member
+// on the limited convection scheme, each component whole (after the previous
+// component's solve); else the boundary faces, sources and relaxation after
+// the one interior pass (BOP_MOM_INTERIOR) of the iteration.
+int momentum_assembly(MgpuBatch* b, int comp) {
+  const AsmBatch& A = b->asmb;
+  cudaStream_t s = b->stream;
+  if (b->any_blend) {
+    TRY(launch_batch_asm(BOP_LIMITER, comp, A, s));
+    return launch_batch_asm(BOP_MOMENTUM, comp, A, s);
+  }
+  return launch_batch_asm(BOP_MOM_FINISH, comp, A, s);
+}
+
 // profile.
 int profiled_iteration(MgpuBatch* b) {
   const AsmBatch& A = b->asmb;
@@ -510,9 +526,9 @@ int profiled_iteration(MgpuBatch* b) {
   std::vector<int> kind;  // per interval: -1 assembly, else the phase index
   mark();
   TRY(launch_batch_asm(BOP_BEGIN_ITER, 0, A, s));
+  if (!b->any_blend) TRY(launch_batch_asm(BOP_MOM_INTERIOR, 0, A, s));
   for (int comp = 0; comp < 3; ++comp) {
-    if (b->any_blend) TRY(launch_batch_asm(BOP_LIMITER, comp, A, s));
-    TRY(launch_batch_asm(BOP_MOMENTUM, comp, A, s));
+    TRY(momentum_assembly(b, comp));
     mark();
     kind.push_back(-1);
     TRY(run_phase(b, b->phases[comp]));
@@ -573,9 +589,9 @@ int enqueue_iteration(MgpuBatch* b, bool tune) {
   const AsmBatch& A = b->asmb;
   cudaStream_t s = b->stream;
   TRY(launch_batch_asm(BOP_BEGIN_ITER, 0, A, s));
+  if (!b->any_blend) TRY(launch_batch_asm(BOP_MOM_INTERIOR, 0, A, s));
   for (int comp = 0; comp < 3; ++comp) {
-    if (b->any_blend) TRY(launch_batch_asm(BOP_LIMITER, comp, A, s));
-    TRY(launch_batch_asm(BOP_MOMENTUM, comp, A, s));
+    TRY(momentum_assembly(b, comp));
     TRY(run_phase(b, b->phases[comp]));
   }
   TRY(launch_batch_asm(BOP_APC, 0, A, s));

@@ -187,7 +187,8 @@ MixedArgs mixed_args(const MgpuCase* c, bool bicg) {
   const bool big = (double)c->d.N * mixed_row_bytes(c->d.ell_w) > g_prefetch_mb * 1048576.0;
   return MixedArgs{c->d.a32,   c->d.dinv32, c->d.w32,  c->ctrl.mixed_tol > 0.0 ? c->ctrl.mixed_tol : 1e-4,
                    bicg ? 1 : g_cheb_degree, g_cheb_ratio, c->d.ell_w, c->d.ell_col, c->d.ell_val,
-                   c->d.red32, (c->d.ell_col && big) ? 1 : 0, g_mixed_scheme, g_rel_delta_pm * 1e-3};
+                   c->d.red32, (c->d.ell_col && big) ? 1 : 0, g_mixed_scheme, g_rel_delta_pm * 1e-3,
+                   (!bicg && g_neighbor_sync) ? c->d.pass_flags : nullptr};
 }
 
 // The same solves in FP64 throughout (MGPU_PREC_FP64_POLY): PCG keeps one
@@ -197,7 +198,8 @@ MixedArgsT<double> poly64_args(const MgpuCase* c, bool bicg) {
   const bool big = (double)c->d.N * (16.0 * c->d.ell_w + 8.0 * 10) > g_prefetch_mb * 1048576.0;
   return MixedArgsT<double>{c->d.a64, c->d.dinv64, c->d.w64, 0.0, bicg ? 1 : g_cheb_degree, g_cheb_ratio,
                             c->d.ell_w, c->d.ell_col, c->d.ell_val64, c->d.red32,
-                            (c->d.ell_col && big) ? 1 : 0, 1, 0.0};
+                            (c->d.ell_col && big) ? 1 : 0, 1, 0.0,
+                            (!bicg && g_neighbor_sync) ? c->d.pass_flags : nullptr};
 }
 
 // factor (if needed) + solve; precond 0 ILU0, 1 Jacobi, 2 IC0. The mixed form
@@ -276,6 +278,35 @@ int momentum_solve(MgpuCase* c, int comp, bool transient) {
 
 int ppe_solve(MgpuCase* c, int slot, bool transient) { return krylov(c, ppe_args(c, slot, transient), false, c->stream); }
 
+// The momentum predictor: per component the assembly, then its solve. With
+// conv_blend = 0 the interior faces of all three components are assembled in
+// one pass and each component then adds its boundary faces, sources and
+// relaxation right before its solve (the boundary values use the components
+// solved before it, as in the reference's loop); with the limited convection
+// scheme every component is assembled whole after the previous solve.
+int assemble_and_solve_momentum(MgpuCase* c, bool transient) {
+  DeviceCase& d = c->d;
+  const AsmParams& P = c->P;
+  cudaStream_t s = c->stream;
+  const bool fused = !(P.conv_blend > 0.0);
+  if (fused) {
+    TRY(launch_mom_interior(d, P, s));
+    c->launches++;
+  }
+  for (int comp = 0; comp < 3; ++comp) {
+    if (fused) {
+      TRY(launch_mom_finish(d, P, comp, s));
+    } else {
+      TRY(launch_limiter(d, P, comp, s));
+      c->launches++;
+      TRY(launch_momentum(d, P, comp, s));
+    }
+    c->launches++;
+    TRY(momentum_solve(c, comp, transient));
+  }
+  return 0;
+}
+
 }  // namespace
 
 int reset_status(MgpuCase* c, int ts_order, int nrec) {
@@ -353,15 +384,7 @@ int outer_iteration(MgpuCase* c, bool transient) {
   cudaStream_t s = c->stream;
   TRY(launch_begin_iter(d, transient ? 1 : 0, c->ctrl.time_scheme, s));
   c->launches++;
-  for (int comp = 0; comp < 3; ++comp) {
-    if (P.conv_blend > 0.0) {
-      TRY(launch_limiter(d, P, comp, s));
-      c->launches++;
-    }
-    TRY(launch_momentum(d, P, comp, s));
-    c->launches++;
-    TRY(momentum_solve(c, comp, transient));
-  }
+  TRY(assemble_and_solve_momentum(c, transient));
   TRY(launch_apc(d, transient ? 1.0 : P.alpha_u, s));
   TRY(launch_gradients(d, P, s));
   TRY(launch_rhiechow(d, P, s));
@@ -397,15 +420,7 @@ int pimple_step(MgpuCase* c) {
   const int n_outer = std::max(1, c->ctrl.n_outer_iter);
   const int ncorr = std::max(1, c->ctrl.n_correct);
   for (int io = 0; io < n_outer; ++io) {
-    for (int comp = 0; comp < 3; ++comp) {
-      if (P.conv_blend > 0.0) {
-        TRY(launch_limiter(d, P, comp, s));
-        c->launches++;
-      }
-      TRY(launch_momentum(d, P, comp, s));
-      c->launches++;
-      TRY(momentum_solve(c, comp, true));
-    }
+    TRY(assemble_and_solve_momentum(c, true));
     TRY(launch_apc(d, P.alpha_u, s));
     TRY(launch_gradients(d, P, s));
     TRY(launch_rhiechow(d, P, s));
@@ -526,7 +541,8 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
        ((e = c->alloc(d.a32, d.nnz)) || (e = c->alloc(d.dinv32, N)) || (e = c->alloc(d.w32, 10 * N)))) ||
       (ctrl->precision == MGPU_PREC_FP64_POLY &&
        ((e = c->alloc(d.a64, d.nnz)) || (e = c->alloc(d.dinv64, N)) || (e = c->alloc(d.w64, 10 * N)))) ||
-      (poly && (e = c->alloc(d.red32, (size_t)mixed_red_words(N)))) ||
+      (poly && ((e = c->alloc(d.red32, (size_t)mixed_red_words(N))) ||
+                (e = c->alloc(d.pass_flags, (size_t)kMaxPassFlags)))) ||
       (e = c->alloc(d.partials, 4 * 4096)) ||
       (e = c->alloc(d.bar, 1)) || (e = c->alloc(d.ferr, 1)) || (e = c->alloc(d.st, 1)))
     return fail(e);
@@ -573,6 +589,20 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
   for (auto& g : groups)
     if (g.btype == MGPU_BC_OUTFLOW) c->has_outflow = 1;
   P.has_outflow = c->has_outflow;
+  {
+    // each cell's boundary faces that carry a group, in the order of its face list
+    std::vector<int> bptr(N + 1, 0), bl;
+    for (long i = 0; i < N; ++i) {
+      for (int k = t.cf_ptr[i]; k < t.cf_ptr[i + 1]; ++k) {
+        const int f = t.cf[k];
+        if (hm.c1[f] < 0 && fgrp[f] >= 0) bl.push_back(f);
+      }
+      bptr[i + 1] = (int)bl.size();
+    }
+    if ((e = c->upload(d.bf_ptr, bptr)) || (e = c->upload(d.bf, bl)) || (e = c->alloc(d.mom_ap, N)) ||
+        (e = c->alloc(d.mom_rhs, 3 * N)))
+      return fail(e);
+  }
   if (c->has_outflow) {
     // the faces of outflow_mass_sums' two sums, each in face order
     std::vector<int> req, out;
@@ -816,8 +846,13 @@ int mgpu_case_stage(MgpuCase* c, int what, int ts_order, const double* apc, doub
   if (what == 0) {
     TRY(launch_gradients(d, c->P, s));
   } else if (what <= 3) {
-    if (c->P.conv_blend > 0.0) TRY(launch_limiter(d, c->P, what - 1, s));
-    TRY(launch_momentum(d, c->P, what - 1, s));
+    if (c->P.conv_blend > 0.0) {
+      TRY(launch_limiter(d, c->P, what - 1, s));
+      TRY(launch_momentum(d, c->P, what - 1, s));
+    } else {  // the path a run takes
+      TRY(launch_mom_interior(d, c->P, s));
+      TRY(launch_mom_finish(d, c->P, what - 1, s));
+    }
   } else if (what == 4) {
     TRY(launch_rhiechow(d, c->P, s));
   } else if (what == 5) {

@@ -85,6 +85,11 @@ struct MixedArgsT {
   int pf;              // 1: each SpMV tile prefetches the next tile's ELL entries into L2
   int reliable;        // PCG: 1 reliable updates (one Krylov stream, FP64 x), 0 restarted refinement
   double rel_delta;    // reliable updates: replace the recursive residual once its norm fell by this factor
+  // single-system PCG launches: one pass counter per block (zeroed before the
+  // launch). Each block then owns a contiguous range of rows, and a Chebyshev
+  // pass waits only for the blocks whose rows its rows read instead of the
+  // whole grid. Null: grid-stride rows and grid barriers (batched lanes).
+  unsigned* flags;
 };
 using MixedArgs = MixedArgsT<float>;
 
@@ -105,6 +110,7 @@ inline double mixed_row_bytes(int ell_w) { return 8.0 * ell_w + 4.0 * 7 + 8.0 * 
 constexpr int kMixedMaxRows = 1 << MGPU_MIXED_MAX_ROWS_LOG2;
 constexpr int kSuperRows = 256;
 constexpr int kBlockMaxRows = MGPU_BLOCK_MAX_ROWS;  // rows one block of a mixed solve may hold
+constexpr int kMaxPassFlags = 4096;                 // blocks of a neighbour-synchronised launch
 inline long mixed_red_words(long n) { return 4l * ((n + kSuperRows - 1) / kSuperRows); }
 
 // One system of a batched solve.
@@ -160,6 +166,10 @@ struct DeviceCase {
   // outflow faces, each list in face order
   int *of_req = nullptr, *of_out = nullptr;
   int n_of_req = 0, n_of_out = 0;
+  // momentum: each cell's boundary faces with a group (face order) and the
+  // interior sums of the three components (ap, rhs per component)
+  int *bf_ptr = nullptr, *bf = nullptr;
+  double *mom_ap = nullptr, *mom_rhs = nullptr;
   // fields (SoA)
   double *u = nullptr, *p = nullptr, *gp = nullptr, *gu = nullptr, *flux = nullptr, *apc = nullptr;
   double *ap = nullptr, *rhs = nullptr, *pp = nullptr, *uo = nullptr, *u_old = nullptr, *u_old_old = nullptr;
@@ -171,6 +181,7 @@ struct DeviceCase {
   double *a64 = nullptr, *dinv64 = nullptr, *w64 = nullptr, *ell_val64 = nullptr;  // FP64 polynomial form
   int ell_w = 0;
   double* red32 = nullptr;  // chunk reduction partials of the mixed-precision solves
+  unsigned* pass_flags = nullptr;  // per-block pass counters of the neighbour sync (kMaxPassFlags)
   // Krylov work
   double *kw = nullptr;  // 10*N
   double* partials = nullptr;

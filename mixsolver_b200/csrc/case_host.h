@@ -87,6 +87,7 @@ extern int g_prefetch_mb;
 extern int g_mixed_scheme;
 extern int g_rel_delta_pm;
 extern unsigned g_spin_limit;
+extern int g_neighbor_sync;
 
 KrylovArgs base_args(MgpuCase* c);
 MixedArgs mixed_args(const MgpuCase* c, bool bicg);

@@ -48,27 +48,134 @@ __device__ __forceinline__ double vfma(double a, double b, double c) { return fm
 // rows and layout-independent sums
 // ---------------------------------------------------------------------------
 
-// The rows of one block: grid-stride tiles of blockDim.x rows, tile t of
-// the group at rows [t * blockDim.x, (t + 1) * blockDim.x) for t = rank,
-// rank + nb, ... Tiles are whole super-chunks (blockDim.x is a multiple of
-// kSuperRows), so a super-chunk always lies in one block's tile, and all
-// blocks stream the same narrow window of every array at a time.
+// The rows of one block, in tiles of blockDim.x rows. Grid-stride layout
+// (batched lanes): tile t of the group at rows [t * blockDim.x, (t + 1) *
+// blockDim.x) for t = rank, rank + nb, ..., so all blocks stream the same
+// narrow window of every array at a time. Contiguous layout (single-system
+// PCG with neighbour sync): block rank owns rows [rank * len, (rank + 1) *
+// len), len a multiple of blockDim.x, so with a banded (RCM) order its SpMV
+// reads the rows of a few neighbouring blocks only. Tiles are whole
+// super-chunks either way (blockDim.x is a multiple of kSuperRows), so the
+// layout-independent sums see the same super-chunks.
 struct Rows {
   int start;   // first row of this block's first tile
-  int stride;  // rows between its consecutive tiles (nb * blockDim.x)
-  int n;
+  int stride;  // rows between its consecutive tiles
+  int n;       // end of the rows this block may own (exclusive)
+  int len;     // contiguous layout: rows per block (0: grid-stride)
 };
+
+__device__ __forceinline__ int contiguous_len(int n, const VGrid& g) {
+  const int bd = blockDim.x;
+  return (int)((((long)n + g.nb - 1) / g.nb + bd - 1) / bd * bd);
+}
 
 // A block holds at most kBlockMaxRows rows (the chunk sums of its tiles live
 // in shared memory); launches and lane plans size their groups accordingly,
 // and a group too small for its system refuses it (fits_group).
-__device__ __forceinline__ bool fits_group(int n, const VGrid& g) {
+__device__ __forceinline__ bool fits_group(int n, const VGrid& g, bool contiguous = false) {
+  if (contiguous) return contiguous_len(n, g) <= kBlockMaxRows;
   const long stride = (long)g.nb * blockDim.x;
   return ((n + stride - 1) / stride) * (long)blockDim.x <= kBlockMaxRows;
 }
 
-__device__ __forceinline__ Rows block_rows(int n, const VGrid& g) {
-  return Rows{g.rank * (int)blockDim.x, g.nb * (int)blockDim.x, n};
+__device__ __forceinline__ Rows block_rows(int n, const VGrid& g, bool contiguous = false) {
+  if (contiguous) {
+    const int len = contiguous_len(n, g);
+    const long start = (long)g.rank * len;
+    return Rows{(int)min(start, (long)n), (int)blockDim.x, (int)min(start + len, (long)n), len};
+  }
+  return Rows{g.rank * (int)blockDim.x, g.nb * (int)blockDim.x, n, 0};
+}
+
+// ---------------------------------------------------------------------------
+// neighbour sync of the Chebyshev passes
+// ---------------------------------------------------------------------------
+
+// Blocks [s_dep[0], s_dep[1]] own the rows this block's SpMV reads (its own
+// included); s_nsync: 1 when every block's range fits one poll per thread and
+// the passes use the neighbour sync, 0 for grid barriers.
+__shared__ int s_dep[2];
+__shared__ int s_nsync;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Decide between neighbour sync and grid barriers for this solve: every block
+// forms the block range of the columns its rows touch (the CSR pattern, whose
+// ELL copy adds only the row itself), and the widest range over the grid
+// decides for all blocks alike. False when a barrier wait ran out.
+template <bool L1>
+__device__ bool setup_pass_sync(const KrylovArgs& a, const unsigned* flags, VGrid& g, const Rows& rows) {
+  if (threadIdx.x == 0) {
+    s_dep[0] = s_dep[1] = g.rank;
+    s_nsync = 0;
+  }
+  if (!flags || g.nb == 1 || rows.len == 0) {
+    __syncthreads();
+    return true;
+  }
+  int cmin = 0x7fffffff, cmax = -1;
+  for (int i = rows.start + threadIdx.x; i < rows.n; i += rows.stride)
+    for (int k = a.row_ptr[i]; k < a.row_ptr[i + 1]; ++k) {
+      const int c = a.col[k];
+      cmin = min(cmin, c);
+      cmax = max(cmax, c);
+    }
+  for (int o = 16; o > 0; o >>= 1) {
+    cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
+    cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0 && cmax >= 0) {
+    atomicMin(&s_dep[0], cmin / rows.len);
+    atomicMax(&s_dep[1], cmax / rows.len);
+  }
+  __syncthreads();
+  double width = (double)(s_dep[1] - s_dep[0] + 1);
+  if (!vg_max<L1>(width, g, a.st)) return false;
+  if (threadIdx.x == 0) s_nsync = width <= (double)blockDim.x ? 1 : 0;
+  __syncthreads();
+  return true;
+}
+
+// The barrier between two Chebyshev passes. Neighbour sync: the block
+// publishes that it finished pass `pass` (a release store of its counter after
+// __syncthreads), then thread t waits (acquire loads) for block s_dep[0] + t
+// of its range to reach the same pass. A block's next pass reads only rows of
+// those blocks (read after write), and it overwrites only its own rows of the
+// vector the previous pass read, which only those blocks read (the pattern is
+// symmetric: write after read). Bounded like the grid barrier.
+__device__ bool pass_sync(unsigned* flags, VGrid& g, DevStatus* st, unsigned& pass) {
+  if (!s_nsync) return vg_sync(g, st);
+  ++pass;
+  __syncthreads();
+  if (threadIdx.x == 0) st_release_u32(flags + g.rank, pass);
+  const int k = s_dep[0] + (int)threadIdx.x;
+  int ok = 1;
+  if (k <= s_dep[1] && k != g.rank) {
+    const unsigned limit = (st && st->spin_limit) ? st->spin_limit : kSpinLimit;
+    unsigned spins = 0;
+    while (ld_acquire_u32(flags + k) < pass) {
+      ++spins;
+      if (spins > 64u) __nanosleep(32);
+      if ((spins & 4095u) == 0 && ld_acquire_i32(&st->timeout) != 0) {
+        ok = 0;
+        break;
+      }
+      if (spins > limit) {
+        atomicExch(&st->timeout, 1);
+        ok = 0;
+        break;
+      }
+    }
+  }
+  return __syncthreads_and(ok) != 0;
 }
 
 // Reduction state of one system. Chunk sums (a fixed butterfly over the 32
@@ -435,7 +542,7 @@ __device__ bool update_x(const KrylovArgs& a, const VGrid& g, const Rows& rows, 
 template <typename V, bool L1, int ELL>
 __device__ __forceinline__ bool cheb_apply(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid& g, Red& R,
                                            const Rows& rows, const V* rr, V* dch, V* z0, V* z1,
-                                           double lmax, V*& zout, double (&red)[2]) {
+                                           double lmax, V*& zout, double (&red)[2], unsigned& pass) {
   const Sp32<V> S = sp32_of(a, m, rows);
   const double lmin = lmax / m.cheb_ratio;
   const double th = 0.5 * (lmax + lmin), de = 0.5 * (lmax - lmin), sg = th / de;
@@ -472,7 +579,7 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
     }
     if (last) {
       if (!red_total<2, L1>(R, rows, g, a.st, red)) return false;
-    } else if (!vg_sync(g, a.st)) {
+    } else if (!pass_sync(m.flags, g, a.st, pass)) {
       return false;
     }
     V* t = zc;
@@ -576,7 +683,7 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
 // (one grid barrier), which is also the barrier before the next SpMV pass.
 template <typename V, bool L1, int ELL>
 __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid& g, Red& R, const Rows& rows,
-                             double bnrm, double rnorm0, double lmax, V inv_th) {
+                             double bnrm, double rnorm0, double lmax, V inv_th, unsigned& pass) {
   const int n = a.n;
   const V* __restrict__ dinv = m.dinv;
   V *rr = m.w32, *zA = m.w32 + n, *p = m.w32 + 2l * n, *q = m.w32 + 3l * n;
@@ -608,7 +715,7 @@ __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid&
     V* z = zA;
     if (cheb) {
       double red[2];  // (rr.z, rr.rr)
-      if (!cheb_apply<V, L1, ELL>(a, m, g, R, rows, rr, dch, zA, zB, lmax, z, red)) return;
+      if (!cheb_apply<V, L1, ELL>(a, m, g, R, rows, rr, dch, zA, zB, lmax, z, red, pass)) return;
       rzn = red[0];
     }
     V beta = V(0);
@@ -652,6 +759,7 @@ __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid&
     if (!red_total<2, L1>(R, rows, g, a.st, s2)) return;
     rzn = s2[1];
     if (!(s2[0] <= stop2 || s2[0] <= delta2 * rr_ref || total >= a.maxit)) continue;
+    const double rec2 = s2[0];  // the recursive residual's rr.rr before the replacement
     // replacement: r = b - A x in FP64, rr := sc r, z0; sums r.r and rr.z
     MGPU_TILES(rows, base) {
       const int i = base + threadIdx.x;
@@ -682,6 +790,10 @@ __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid&
     }
     rr_ref = (rnorm * sc) * (rnorm * sc);
     rzn = t2[1];
+    // the recursive residual had drifted from the true one by more than a
+    // factor 2: the kept direction no longer suits the replaced residual, so
+    // the next iteration starts a new direction (beta = 0)
+    if (rr_ref > 4.0 * rec2) first = true;
   }
   write_result_m(a, g, total, rnorm / bnrm, ierr);
 }
@@ -690,11 +802,14 @@ template <typename V, bool L1, int ELL>
 __device__ void pcg_mixed_body(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid& g) {
   if (a.st->abort) return;
   const int n = a.n;
-  if (!fits_group(n, g)) {  // unreachable through the launchers: reported as a breakdown
+  const bool contiguous = m.flags != nullptr;
+  if (!fits_group(n, g, contiguous)) {  // unreachable through the launchers: reported as a breakdown
     write_result_m(a, g, 0, 0.0, 2);
     return;
   }
-  const Rows rows = block_rows(n, g);
+  const Rows rows = block_rows(n, g, contiguous);
+  unsigned pass = 0;
+  if (!setup_pass_sync<L1>(a, m.flags, g, rows)) return;
   const V* __restrict__ dinv = m.dinv;
   Red R = make_red(m, n);
   V *rr = m.w32, *zA = m.w32 + n, *p = m.w32 + 2l * n, *q = m.w32 + 3l * n, *d = m.w32 + 4l * n;
@@ -735,7 +850,7 @@ __device__ void pcg_mixed_body(const KrylovArgs& a, const MixedArgsT<V>& m, VGri
     return;
   }
   if (m.reliable) {
-    pcg_reliable<V, L1, ELL>(a, m, g, R, rows, bnrm, rnorm, lmax, inv_th);
+    pcg_reliable<V, L1, ELL>(a, m, g, R, rows, bnrm, rnorm, lmax, inv_th, pass);
     return;
   }
   // Restarted refinement. One loop, one call site of the preconditioner: a restart (scaled FP64
@@ -807,7 +922,7 @@ __device__ void pcg_mixed_body(const KrylovArgs& a, const MixedArgsT<V>& m, VGri
     if (cheb) {
       if (!vg_sync(g, a.st)) return;
       double red[2];  // (rr.z, rr.rr)
-      if (!cheb_apply<V, L1, ELL>(a, m, g, R, rows, rr, dch, zA, zB, lmax, z, red)) return;
+      if (!cheb_apply<V, L1, ELL>(a, m, g, R, rows, rr, dch, zA, zB, lmax, z, red, pass)) return;
       s2[0] = restart ? red[0] : red[1];
       s2[1] = restart ? red[1] : red[0];
     } else {
@@ -1027,10 +1142,15 @@ int launch_mixed(const void* fn1, const void* fnN, const KrylovArgs& a, const Mi
     set_error("mixed-precision solve: too many rows per block for the co-resident grid");
     return MGPU_E_ARG;
   }
+  if (m.flags && grid > kMaxPassFlags) {
+    set_error("mixed-precision solve: more blocks than pass counters");
+    return MGPU_E_ARG;
+  }
   KrylovArgs aa = a;
   MixedArgsT<V> mm = m;
   void* args[] = {&aa, &mm};
   cudaError_t e = cudaMemsetAsync(a.bar, 0, sizeof(unsigned long long), s);
+  if (e == cudaSuccess && m.flags) e = cudaMemsetAsync(m.flags, 0, sizeof(unsigned) * (size_t)grid, s);
   if (e != cudaSuccess) return cuda_fail(e, "barrier reset", __FILE__, __LINE__);
   e = cudaLaunchCooperativeKernel(grid == 1 ? fn1 : fnN, dim3(grid), dim3(block), args, 0, s);
   if (e != cudaSuccess) return cuda_fail(e, "cooperative launch (mixed)", __FILE__, __LINE__);

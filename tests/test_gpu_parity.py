@@ -553,3 +553,37 @@ def test_channel_lowspeed_parity():
     ier_o, log_o = o.simple_run()
     assert ier_g == ier_o == 0
     _compare_runs(log_g, log_o, g.fields(), o.fields())
+
+
+@pytest.mark.parametrize("ppe", [abi.PPE_IC0, abi.PPE_JACOBI])
+def test_config1_cavity_64_500_iterations(ppe):
+    """The CPU-runnable workload exactly: 2-D lid-driven cavity 64 x 64 x 1
+    (4,096 cells), Re 1000, upwind, alpha_u 0.7 / alpha_p 0.3, 500 outer
+    iterations, BiCGStab+ILU(0) momentum, IC(0) or Jacobi PCG on the pressure
+    correction, lin_tol 1e-8: every linear solve's iteration count and ierr
+    equal to the oracle's over all 2,000 solves, fields within 1e-9."""
+    mesh, ctrl = cases.cavity2d(64, outer_max=500, ppe=ppe)
+    g = S.UnsCase(mesh, ctrl)
+    ier_g, log_g = g.simple_run()
+    o = O.OracleCase(mesh, ctrl)
+    ier_o, log_o = o.simple_run()
+    assert ier_g == ier_o == 0
+    assert len(log_g) == len(log_o) == 500
+    _compare_runs(log_g, log_o, g.fields(), o.fields())
+
+
+def test_config2_channel_full_size_fp64_two_iterations():
+    """The measured workload's FP64 parity form at full size: 128 x 64 x 64
+    jittered hex channel (524,288 cells, RCM order), BiCGStab+Jacobi momentum,
+    PCG+ILU(0) pressure on the default multi-block path (sync-free triangular
+    sweeps), two outer iterations against the oracle: equal iteration counts
+    (about 260 PCG iterations per pressure solve) and fields within 1e-9."""
+    mesh, ctrl = cases.channel3d(128, 64, 64, seed=0, outer_max=2, order_fn=S.rcm_order)
+    ctrl.lin_max = 1000
+    g = S.UnsCase(mesh, ctrl)
+    ier_g, log_g = g.simple_run()
+    o = O.OracleCase(mesh, ctrl)
+    ier_o, log_o = o.simple_run()
+    assert ier_g == ier_o == 0
+    print("channel 524k lin_it:", [r["lin_it"][:4] for r in log_g], [r["lin_it"][:4] for r in log_o])
+    _compare_runs(log_g, log_o, g.fields(), o.fields())

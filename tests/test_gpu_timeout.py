@@ -39,7 +39,9 @@ def rel_l2(a, b):
 
 @pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_MIXED])
 def test_barrier_wait_runs_out_then_case_recovers(prec, multiblock):
-    mesh, ctrl = cases.channel3d(12, 6, 6, seed=3, outer_max=4, order_fn=S.rcm_order)
+    # 3,456 cells: the multi-block launches hold 6 (FP64) and 7 (mixed) blocks,
+    # so some block always has to wait at some barrier of the run
+    mesh, ctrl = cases.channel3d(24, 12, 12, seed=3, outer_max=4, order_fn=S.rcm_order)
     ctrl.precision = prec
     ctrl.lin_max = 2000
     S.set_tuning("spin_limit", 1)

@@ -280,7 +280,7 @@ def run_ours(args):
     import copy
     from mixsolver_b200 import abi
     from mixsolver_b200 import solver as S
-    mesh, ctrl = workload(args, S.rcm_order)
+    mesh, ctrl = workload(args, S.rcm_order_device)  # cells renumbered by RCM on the device
     N, F = mesh.ncells, mesh.nfaces
     nnz = N + 2 * mesh.n_interior()
     mixed = args.precision == "mixed"

@@ -237,6 +237,25 @@ int mgpu_geometry(const MgpuMesh* mesh, double* xf, double* sf, double* area, do
  * the new 1-based number of cell c. */
 int mgpu_rcm_order(const MgpuMesh* mesh, int32_t* new_of_old);
 
+/* The same reverse Cuthill-McKee order computed on the device (adjacency by
+ * radix sort, George-Liu start and Cuthill-McKee levels by level-synchronous
+ * BFS, each level sorted by (parent position, degree, index)): equal to
+ * mgpu_rcm_order entry for entry. At most 2^24 - 1 cells and 255 neighbours
+ * per cell. No counterpart in the reference. */
+int mgpu_rcm_order_device(const MgpuMesh* mesh, int32_t* new_of_old);
+
+/* The integer arrays a case builds from its mesh (build_connectivity,
+ * mod_uns_connectivity.f90:28-108; build_cell_csr and the pos_of slot maps,
+ * mod_uns_simple.f90:835-923; the triangular level sets), 0-based, built on
+ * the device (on_device = 1: the path mgpu_case_create takes) or by the host
+ * builder (0). sizes[0..3] = cell-face entries, nonzeros, lower and upper
+ * levels; every array pointer may be NULL (call once with NULLs for the
+ * sizes). Sizes: cf_ptr, row_ptr N+1; cf, cf_slot sizes[0]; col, lt_pos
+ * sizes[1]; diag, lo_rows, up_rows N; lo_ptr sizes[2]+1; up_ptr sizes[3]+1. */
+int mgpu_mesh_topology(const MgpuMesh* mesh, int on_device, int32_t* sizes, int32_t* cf_ptr, int32_t* cf,
+                       int32_t* row_ptr, int32_t* col, int32_t* diag, int32_t* cf_slot, int32_t* lt_pos,
+                       int32_t* lo_ptr, int32_t* lo_rows, int32_t* up_ptr, int32_t* up_rows);
+
 /* One stage of the outer iteration on the case's current fields, for
  * element-wise checks of each kernel: what = 0 compute_gradients, 1..3
  * momentum_assembly of component what (A values, rhs, ap out), 4 flux_rhiechow,

@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmixgpu.so")
 BUILD = os.path.join(HERE, "_build")
 
-SOURCES = ["case.cu", "assembly.cu", "krylov.cu", "krylov_mixed.cu", "krylov_poly64.cu", "batch.cu", "standalone.cu", "noalloc.cu",
+SOURCES = ["case.cu", "assembly.cu", "krylov.cu", "krylov_mixed.cu", "krylov_poly64.cu", "batch.cu", "standalone.cu", "noalloc.cu", "device_topo.cu",
            "mesh_host.cpp", "cas_reader.cpp"]
 # the mixed-precision form needs no bit-parity and may contract into FMA
 FMA_OK = {"krylov_mixed.cu", "krylov_poly64.cu"}

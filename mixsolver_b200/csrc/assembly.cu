@@ -21,16 +21,12 @@ namespace mgpu {
 
 namespace {
 
-__device__ __forceinline__ Ramp ramp_of(const AsmParams& P, const DevStatus* st) {
-  Ramp r{1.0, 1.0};
-  if (P.inlet_ramp > 1) {
-    double f = (double)(st->cur_it + 1) / (double)P.inlet_ramp;
-    f = fmax(0.0, fmin(1.0, f));
-    r.inlet = f;
-    r.pval = f;
-  }
-  return r;
-}
+// The ramp factors in effect (g_inlet_ramp_factor, g_pval_ramp_factor of
+// mod_uns_bc.f90:28-37): kept with the case, 1 until a SIMPLE iteration of a
+// run with inlet_ramp > 1 sets them (b_begin_iter), and left at their last
+// value afterwards, as the reference's module variables are -- so the
+// gradients a run computes before its first iteration see the previous value.
+__device__ __forceinline__ Ramp ramp_of(const DeviceCase& d) { return Ramp{d.ramp[0], d.ramp[1]}; }
 
 // ---------------- geometry (setup) ----------------------------------------
 
@@ -208,7 +204,7 @@ __global__ void k_face_consts(DeviceCase d, AsmParams P) {
 __device__ __forceinline__ void b_gradients(const DeviceCase& d, const AsmParams& P, const int c) {
   if (d.st->abort || c >= d.N) return;
   const int N = d.N, F = d.F;
-  const Ramp rp = ramp_of(P, d.st);
+  const Ramp rp = ramp_of(d);
   const double *u0 = d.u, *u1 = d.u + N, *u2 = d.u + 2 * N;
   double g[12];
 #pragma unroll
@@ -261,7 +257,7 @@ __global__ void __launch_bounds__(256) k_gradients(DeviceCase d, AsmParams P) {
 __device__ __forceinline__ void b_limiter(const DeviceCase& d, const AsmParams& P, int comp, const int c) {
   if (d.st->abort || c >= d.N) return;
   const int N = d.N, F = d.F;
-  const Ramp rp = ramp_of(P, d.st);
+  const Ramp rp = ramp_of(d);
   const double* uc_ = d.u + (long)comp * N;
   const double uc = uc_[c];
   double pmin = uc, pmax = uc;
@@ -383,7 +379,7 @@ __device__ __forceinline__ void mom_finish(const DeviceCase& d, const AsmParams&
 __device__ __forceinline__ void b_momentum(const DeviceCase& d, const AsmParams& P, int comp, const int c) {
   if (d.st->abort || c >= d.N) return;
   const int N = d.N, F = d.F;
-  const Ramp rp = ramp_of(P, d.st);
+  const Ramp rp = ramp_of(d);
   const double* sfc = d.sf + (long)comp * F;
   double* A = d.aval;
   const int rb = d.row_ptr[c], re = d.row_ptr[c + 1];
@@ -497,7 +493,7 @@ __global__ void __launch_bounds__(256) k_mom_interior(DeviceCase d, AsmParams P)
 
 __device__ __forceinline__ void b_mom_finish(const DeviceCase& d, const AsmParams& P, int comp, const int c) {
   if (d.st->abort || c >= d.N) return;
-  mom_finish<true>(d, P, ramp_of(P, d.st), comp, c, d.mom_ap[c], d.mom_rhs[(long)comp * d.N + c]);
+  mom_finish<true>(d, P, ramp_of(d), comp, c, d.mom_ap[c], d.mom_rhs[(long)comp * d.N + c]);
 }
 __global__ void __launch_bounds__(256) k_mom_finish(DeviceCase d, AsmParams P, int comp) {
   b_mom_finish(d, P, comp, blockIdx.x * blockDim.x + threadIdx.x);
@@ -521,7 +517,7 @@ __device__ __forceinline__ void b_rhiechow(const DeviceCase& d, const AsmParams&
   const int a = d.c0[f], b = d.c1[f];
   const double s0 = d.sf[f], s1 = d.sf[F + f], s2 = d.sf[2 * F + f];
   if (b < 0) {
-    const Ramp rp = ramp_of(P, d.st);
+    const Ramp rp = ramp_of(d);
     double w0, w1, w2;
     bc_face_vel(d.groups[d.fgrp[f]], rp, d.xf[f], d.xf[F + f], d.xf[2 * F + f], s0, s1, s2, d.u[a], d.u[N + a],
                 d.u[2 * N + a], w0, w1, w2);
@@ -801,7 +797,8 @@ __global__ void k_outer_accum(DeviceCase d) {
 }
 
 // SIMPLE: uo := u ; PISO: history shift and time-scheme order
-__device__ __forceinline__ void b_begin_iter(const DeviceCase& d, int transient, int time_scheme, const long i) {
+__device__ __forceinline__ void b_begin_iter(const DeviceCase& d, int transient, int time_scheme, int inlet_ramp,
+                                             const long i) {
   if (d.st->abort) return;
   const long n3 = 3l * d.N;
   if (i < n3) {
@@ -816,10 +813,16 @@ __device__ __forceinline__ void b_begin_iter(const DeviceCase& d, int transient,
     MgpuIterRec* rec = d.recs + d.st->cur_it;
     rec->nsolve = 0;
     if (transient) d.st->ts_order = (d.st->cur_it == 0 || time_scheme == 1) ? 1 : 2;
+    // the cold-start ramp of simple_run (mod_uns_simple.f90:150-155): it / inlet_ramp, clamped to [0, 1]
+    if (!transient && inlet_ramp > 1) {
+      const double f = fmax(0.0, fmin(1.0, (double)(d.st->cur_it + 1) / (double)inlet_ramp));
+      d.ramp[0] = f;
+      d.ramp[1] = f;
+    }
   }
 }
-__global__ void k_begin_iter(DeviceCase d, int transient, int time_scheme) {
-  b_begin_iter(d, transient, time_scheme, blockIdx.x * (long)blockDim.x + threadIdx.x);
+__global__ void k_begin_iter(DeviceCase d, int transient, int time_scheme, int inlet_ramp) {
+  b_begin_iter(d, transient, time_scheme, inlet_ramp, blockIdx.x * (long)blockDim.x + threadIdx.x);
 }
 
 // ---------------- batched launches -----------------------------------------
@@ -854,7 +857,7 @@ __device__ __forceinline__ const BatchCase& stage_case(unsigned char* raw, const
 MGPU_BATCHED(fill_apc, RANGE_N, if (i < d.N) d.apc[i] = 1.0)
 MGPU_BATCHED(gradients, RANGE_N, b_gradients(d, P, (int)i))
 MGPU_BATCHED(rhiechow_piso, RANGE_F, if (sc.transient) b_rhiechow(d, P, (int)i))
-MGPU_BATCHED(begin_iter, RANGE_3N, b_begin_iter(d, sc.transient, sc.time_scheme, i))
+MGPU_BATCHED(begin_iter, RANGE_3N, b_begin_iter(d, sc.transient, sc.time_scheme, P.inlet_ramp, i))
 MGPU_BATCHED(limiter, RANGE_N, if (P.conv_blend > 0.0) b_limiter(d, P, arg, (int)i))
 MGPU_BATCHED(momentum, RANGE_N, b_momentum(d, P, arg, (int)i))
 MGPU_BATCHED(mom_interior, RANGE_N, b_mom_interior(d, P, (int)i))
@@ -996,8 +999,8 @@ int launch_batch_asm(int op, int arg, const AsmBatch& b, cudaStream_t s) {
   return 0;
 }
 
-int launch_begin_iter(const DeviceCase& d, int transient, int time_scheme, cudaStream_t s) {
-  k_begin_iter<<<GRID(3l * d.N)>>>(d, transient, time_scheme);
+int launch_begin_iter(const DeviceCase& d, int transient, int time_scheme, int inlet_ramp, cudaStream_t s) {
+  k_begin_iter<<<GRID(3l * d.N)>>>(d, transient, time_scheme, inlet_ramp);
   MGPU_LAUNCH_CHECK("k_begin_iter");
   return 0;
 }

@@ -80,6 +80,6 @@ int launch_ppe(const DeviceCase& d, const AsmParams& P, cudaStream_t s);
 int launch_correct(const DeviceCase& d, const AsmParams& P, cudaStream_t s);
 int launch_diag(const DeviceCase& d, const AsmParams& P, int transient, cudaStream_t s);
 int launch_outer_accum(const DeviceCase& d, cudaStream_t s);
-int launch_begin_iter(const DeviceCase& d, int transient, int time_scheme, cudaStream_t s);
+int launch_begin_iter(const DeviceCase& d, int transient, int time_scheme, int inlet_ramp, cudaStream_t s);
 
 }  // namespace mgpu

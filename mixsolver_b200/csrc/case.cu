@@ -20,6 +20,7 @@
 #include "assembly.cuh"
 #include "case.cuh"
 #include "case_host.h"
+#include "device_topo.h"
 #include "mesh_host.h"
 
 namespace mgpu {
@@ -382,7 +383,7 @@ int outer_iteration(MgpuCase* c, bool transient) {
   DeviceCase& d = c->d;
   const AsmParams& P = c->P;
   cudaStream_t s = c->stream;
-  TRY(launch_begin_iter(d, transient ? 1 : 0, c->ctrl.time_scheme, s));
+  TRY(launch_begin_iter(d, transient ? 1 : 0, c->ctrl.time_scheme, P.inlet_ramp, s));
   c->launches++;
   TRY(assemble_and_solve_momentum(c, transient));
   TRY(launch_apc(d, transient ? 1.0 : P.alpha_u, s));
@@ -415,7 +416,7 @@ int pimple_step(MgpuCase* c) {
   DeviceCase& d = c->d;
   const AsmParams& P = c->P;
   cudaStream_t s = c->stream;
-  TRY(launch_begin_iter(d, 1, c->ctrl.time_scheme, s));
+  TRY(launch_begin_iter(d, 1, c->ctrl.time_scheme, P.inlet_ramp, s));
   c->launches++;
   const int n_outer = std::max(1, c->ctrl.n_outer_iter);
   const int ncorr = std::max(1, c->ctrl.n_correct);
@@ -495,8 +496,6 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
     set_error("mgpu_case_create: the mixed-precision and FP64 polynomial forms take at most 2^23 cells");
     return MGPU_E_ARG;
   }
-  HostTopo t;
-  build_topology(hm, t);
   MGPU_CUDA(cudaSetDevice(g_device));
   MgpuCase* c = new MgpuCase();
   auto fail = [&](int e) {
@@ -512,20 +511,34 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
   DeviceCase& d = c->d;
   d.N = hm.N;
   d.F = hm.F;
-  d.nnz = (int)t.col.size();
   const long N = d.N, F = d.F;
   int e = 0;
   double *x = nullptr, *pcen = nullptr;
   int *fptr = nullptr, *fnodes = nullptr;
   if ((e = c->upload(d.c0, hm.c0)) || (e = c->upload(d.c1, hm.c1)) || (e = c->upload(d.fgrp, fgrp)) ||
-      (e = c->upload(d.cf_ptr, t.cf_ptr)) || (e = c->upload(d.cf, t.cf)) || (e = c->upload(d.cf_slot, t.cf_slot)) ||
-      (e = c->upload(d.row_ptr, t.row_ptr)) || (e = c->upload(d.col, t.col)) || (e = c->upload(d.diag, t.diag)) ||
-      (e = c->upload(d.lt_pos, t.mirror)) || (e = c->upload(d.lo_ptr, t.lo_ptr)) ||
-      (e = c->upload(d.lo_rows, t.lo_rows)) || (e = c->upload(d.up_ptr, t.up_ptr)) ||
-      (e = c->upload(d.up_rows, t.up_rows)) || (e = c->upload(d.groups, groups)))
+      (e = c->upload(d.groups, groups)))
     return fail(e);
-  d.nlev_lo = t.nlev_lo;
-  d.nlev_up = t.nlev_up;
+  // the integer mesh pipeline on the device (build_connectivity, build_cell_csr,
+  // slot maps, level sets): device_topo.cu
+  const TopoAlloc keep = [c](int*& p, size_t n) { return c->alloc(p, n); };
+  {
+    DeviceTopo t;
+    if ((e = device_topology(d.N, d.F, d.c0, d.c1, t, keep, c->stream))) return fail(e);
+    d.cf_ptr = t.cf_ptr;
+    d.cf = t.cf;
+    d.cf_slot = t.cf_slot;
+    d.row_ptr = t.row_ptr;
+    d.col = t.col;
+    d.diag = t.diag;
+    d.lt_pos = t.mirror;
+    d.lo_ptr = t.lo_ptr;
+    d.lo_rows = t.lo_rows;
+    d.up_ptr = t.up_ptr;
+    d.up_rows = t.up_rows;
+    d.nlev_lo = t.nlev_lo;
+    d.nlev_up = t.nlev_up;
+    d.nnz = t.nnz;
+  }
   d.ngroups = (int)groups.size();
   if ((e = c->alloc(d.xf, 3 * F)) || (e = c->alloc(d.sf, 3 * F)) || (e = c->alloc(d.area, F)) ||
       (e = c->alloc(d.lf, F)) || (e = c->alloc(d.vol, N)) || (e = c->alloc(d.xc, 3 * N)) ||
@@ -544,20 +557,20 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
       (poly && ((e = c->alloc(d.red32, (size_t)mixed_red_words(N))) ||
                 (e = c->alloc(d.pass_flags, (size_t)kMaxPassFlags)))) ||
       (e = c->alloc(d.partials, 4 * 4096)) ||
-      (e = c->alloc(d.bar, 1)) || (e = c->alloc(d.ferr, 1)) || (e = c->alloc(d.st, 1)))
+      (e = c->alloc(d.bar, 1)) || (e = c->alloc(d.ferr, 1)) || (e = c->alloc(d.st, 1)) ||
+      (e = c->alloc(d.ramp, 2)))
     return fail(e);
+  {
+    const double one[2] = {1.0, 1.0};  // the ramp factors of a fresh case
+    MGPU_CUDA(cudaMemcpyAsync(d.ramp, one, sizeof(one), cudaMemcpyHostToDevice, c->stream));
+  }
   if ((e = ensure_recs(c, 64))) return fail(e);
   if (poly) {
-    int w = 0;
-    for (long i = 0; i < N; ++i) w = std::max(w, t.row_ptr[i + 1] - t.row_ptr[i]);
-    if (w <= 8) {  // column-major ELL copy of the pattern for the FP32 SpMV
-      std::vector<int> ell((size_t)w * N);
-      for (long i = 0; i < N; ++i)
-        for (int k = 0; k < w; ++k) {
-          const int p = t.row_ptr[i] + k;
-          ell[(size_t)k * N + i] = p < t.row_ptr[i + 1] ? t.col[p] : (int)i;
-        }
-      if ((e = c->upload(d.ell_col, ell))) return fail(e);
+    // column-major ELL copy of the pattern for the polynomial forms' SpMV (rows of at most 8 entries)
+    int w = 0, *ell = nullptr;
+    if ((e = device_ell(d.N, d.row_ptr, d.col, 8, w, ell, keep, c->stream))) return fail(e);
+    if (ell) {
+      d.ell_col = ell;
       if (ctrl->precision == MGPU_PREC_MIXED) e = c->alloc(d.ell_val, (size_t)w * N);
       else e = c->alloc(d.ell_val64, (size_t)w * N);
       if (e) return fail(e);
@@ -589,20 +602,10 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
   for (auto& g : groups)
     if (g.btype == MGPU_BC_OUTFLOW) c->has_outflow = 1;
   P.has_outflow = c->has_outflow;
-  {
-    // each cell's boundary faces that carry a group, in the order of its face list
-    std::vector<int> bptr(N + 1, 0), bl;
-    for (long i = 0; i < N; ++i) {
-      for (int k = t.cf_ptr[i]; k < t.cf_ptr[i + 1]; ++k) {
-        const int f = t.cf[k];
-        if (hm.c1[f] < 0 && fgrp[f] >= 0) bl.push_back(f);
-      }
-      bptr[i + 1] = (int)bl.size();
-    }
-    if ((e = c->upload(d.bf_ptr, bptr)) || (e = c->upload(d.bf, bl)) || (e = c->alloc(d.mom_ap, N)) ||
-        (e = c->alloc(d.mom_rhs, 3 * N)))
-      return fail(e);
-  }
+  // each cell's boundary faces that carry a group, in the order of its face list
+  if ((e = device_boundary_lists(d.N, d.cf_ptr, d.cf, d.c1, d.fgrp, d.bf_ptr, d.bf, keep, c->stream)) ||
+      (e = c->alloc(d.mom_ap, N)) || (e = c->alloc(d.mom_rhs, 3 * N)))
+    return fail(e);
   if (c->has_outflow) {
     // the faces of outflow_mass_sums' two sums, each in face order
     std::vector<int> req, out;

@@ -190,6 +190,7 @@ struct DeviceCase {
   DevStatus* st = nullptr;
   MgpuIterRec* recs = nullptr;
   int rec_cap = 0;
+  double* ramp = nullptr;  // inlet-speed and pressure-value ramp factors in effect (2)
 };
 
 // Launch helpers implemented in the .cu files.

@@ -431,6 +431,72 @@ __device__ __forceinline__ void spmv32_rows(const Sp32<V>& S, const V* x, const 
   }
 }
 
+// y = A (z + beta pold) with each gathered entry formed as the owner row forms
+// its new search direction (first: y = A z): the product of the new direction
+// computed directly, from vectors no block writes during the pass.
+template <typename V, bool L1, int ELL, bool FULL>
+__device__ __forceinline__ void spmv32_rows_dir(const Sp32<V>& S, const V* z, const V* pold, V beta, bool first,
+                                                const int (&i)[kRows], const bool (&in0)[kRows], V (&y)[kRows]) {
+  bool in[kRows];
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) in[r] = FULL || in0[r];
+  if constexpr (ELL) {
+    constexpr int WMAX = 8;
+    const int W = S.w, n = S.n;
+    V v[kRows][WMAX], xv[kRows][WMAX];
+    int c[kRows][WMAX];
+#pragma unroll
+    for (int r = 0; r < kRows; ++r)
+#pragma unroll
+      for (int t = 0; t < WMAX; ++t)
+        if (t < W && in[r]) {
+          c[r][t] = S.ecol[(long)t * n + i[r]];
+          v[r][t] = S.eval[(long)t * n + i[r]];
+        }
+    if constexpr (ELL == 2) {
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) {
+        const int j = i[r] + S.pf;
+        if (j < n) {
+#pragma unroll
+          for (int t = 0; t < WMAX; ++t)
+            if (t < W) {
+              prefetch_l2(S.ecol + (long)t * n + j);
+              prefetch_l2(S.eval + (long)t * n + j);
+            }
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < kRows; ++r)
+#pragma unroll
+      for (int t = 0; t < WMAX; ++t)
+        if (t < W && in[r]) xv[r][t] = first ? ldv(&z[c[r][t]]) : vfma(beta, ldv(&pold[c[r][t]]), ldv(&z[c[r][t]]));
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      V acc = V(0);
+#pragma unroll
+      for (int t = 0; t < WMAX; ++t)
+        if (t < W && in[r]) acc = vfma(v[r][t], xv[r][t], acc);
+      y[r] = acc;
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      V acc = V(0);
+      if (in[r]) {
+        const int e = S.rp[i[r] + 1];
+        for (int k = S.rp[i[r]]; k < e; ++k) {
+          const int cc = S.col[k];
+          const V x = first ? ldv(&z[cc]) : vfma(beta, ldv(&pold[cc]), ldv(&z[cc]));
+          acc = vfma(S.a32[k], x, acc);
+        }
+      }
+      y[r] = acc;
+    }
+  }
+}
+
 template <bool L1>
 __device__ __forceinline__ double row_spmv64(const KrylovArgs& a, const double* x, int i) {
   double y = 0.0;
@@ -620,6 +686,33 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
   }
 }
 
+// pnew := z + beta pold and q := A pnew in one pass (pnew := z, q := A z when
+// first), q formed directly from z and pold rather than recurred; pnew.q
+template <typename V, bool L1, int ELL>
+__device__ __forceinline__ void pcg_direct_pass(const KrylovArgs& a, const MixedArgsT<V>& m, const Red& R,
+                                                const Rows& rows, const V* z, const V* pold, V* pnew, V* q, V beta,
+                                                bool first) {
+  const Sp32<V> S = sp32_of(a, m, rows);
+  MGPU_STEPS(rows, base) {
+    MGPU_STEP_ROWS(rows, base, ii, in);
+    MGPU_SPLIT_FULL(rows, base, FULL, {
+      V aq[kRows];
+      spmv32_rows_dir<V, L1, ELL, FULL>(S, z, pold, beta, first, ii, in, aq);
+_Pragma("unroll") for (int r = 0; r < kRows; ++r) {
+        const int i = ii[r];
+        double c[1] = {0.0};
+        if (FULL || in[r]) {
+          const V pi = first ? z[i] : vfma(beta, pold[i], z[i]);
+          pnew[i] = pi;
+          q[i] = aq[r];
+          c[0] = (double)pi * (double)aq[r];
+        }
+        red_put<1>(R, rows, base + r * rows.stride, c);
+      }
+    })
+  }
+}
+
 // v := A ph; r0.v
 template <typename V, bool L1, int ELL>
 __device__ __forceinline__ void bicg_v_pass(const KrylovArgs& a, const MixedArgsT<V>& m, const Red& R, const Rows& rows,
@@ -678,7 +771,9 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
 // an FP64 pass forms r = b - A x and puts sc r in its place. The search
 // direction p, its product q and r.z are kept across a replacement, so the
 // Krylov space is not thrown away as in a restarted refinement; the true
-// residual decides convergence. On entry a.r holds b - A x0 and rnorm0 its
+// residual decides convergence. q = A p is formed directly every iteration
+// (pcg_direct_pass), not recurred: in FP32 the recurrence drifts from A p and
+// costs iterations. On entry a.r holds b - A x0 and rnorm0 its
 // norm. Barriers: every pass that writes x, rr or z ends in a reduction
 // (one grid barrier), which is also the barrier before the next SpMV pass.
 template <typename V, bool L1, int ELL>
@@ -687,7 +782,7 @@ __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid&
   const int n = a.n;
   const V* __restrict__ dinv = m.dinv;
   V *rr = m.w32, *zA = m.w32 + n, *p = m.w32 + 2l * n, *q = m.w32 + 3l * n;
-  V *dch = m.w32 + 5l * n, *zB = m.w32 + 6l * n;
+  V *dch = m.w32 + 5l * n, *zB = m.w32 + 6l * n, *pn = m.w32 + 7l * n;  // p double-buffered
   const bool cheb = m.cheb_k > 1;
   const double sc = 1.0 / rnorm0;
   const double stop = a.tol * bnrm * sc;  // |rr| at which the estimate reaches tol
@@ -728,7 +823,12 @@ __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid&
     }
     rz = rzn;
     ++total;
-    pcg_fused_pass<V, L1, ELL>(a, m, R, rows, z, p, q, beta, first);
+    pcg_direct_pass<V, L1, ELL>(a, m, R, rows, z, p, pn, q, beta, first);
+    {
+      V* t = p;
+      p = pn;
+      pn = t;
+    }
     first = false;
     double pq[1];
     if (!red_total<1, L1>(R, rows, g, a.st, pq)) return;

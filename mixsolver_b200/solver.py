@@ -382,3 +382,36 @@ def rcm_order(mesh) -> np.ndarray:
     out = np.zeros(mesh.ncells, np.int32)
     abi.check(lib, lib.mgpu_rcm_order(C.byref(arr.struct), iptr(out)), "mgpu_rcm_order")
     return out
+
+
+def rcm_order_device(mesh) -> np.ndarray:
+    """The same reverse Cuthill-McKee numbering computed on the GPU (new_of_old,
+    1-based; equal to :func:`rcm_order` entry for entry)."""
+    lib = _lib()
+    arr = MeshArrays(mesh)
+    out = np.zeros(mesh.ncells, np.int32)
+    abi.check(lib, lib.mgpu_rcm_order_device(C.byref(arr.struct), iptr(out)), "mgpu_rcm_order_device")
+    return out
+
+
+def mesh_topology(mesh, on_device: bool = True) -> dict:
+    """The integer arrays a case builds from its mesh (0-based): cell->face
+    lists, CSR pattern, diagonal positions, face->slot map, transpose map and
+    the triangular level sets; on the GPU (the path mgpu_case_create takes) or
+    by the host builder."""
+    lib = _lib()
+    arr = MeshArrays(mesh)
+    n = mesh.ncells
+    sizes = np.zeros(4, np.int32)
+    none = [None] * 11
+    abi.check(lib, lib.mgpu_mesh_topology(C.byref(arr.struct), int(on_device), iptr(sizes), *none),
+              "mgpu_mesh_topology")
+    ncf, nnz, nlo, nup = (int(v) for v in sizes)
+    out = {k: np.zeros(m, np.int32) for k, m in (("cf_ptr", n + 1), ("cf", ncf), ("row_ptr", n + 1), ("col", nnz),
+                                                  ("diag", n), ("cf_slot", ncf), ("lt_pos", nnz),
+                                                  ("lo_ptr", nlo + 1), ("lo_rows", n), ("up_ptr", nup + 1),
+                                                  ("up_rows", n))}
+    keys = ["cf_ptr", "cf", "row_ptr", "col", "diag", "cf_slot", "lt_pos", "lo_ptr", "lo_rows", "up_ptr", "up_rows"]
+    abi.check(lib, lib.mgpu_mesh_topology(C.byref(arr.struct), int(on_device), iptr(sizes),
+                                          *[iptr(out[k]) for k in keys]), "mgpu_mesh_topology")
+    return out

@@ -117,3 +117,22 @@ def test_missing_library_fails_loudly(tmp_path):
     with pytest.raises(RuntimeError, match="not built"):
         abi.load_library(str(tmp_path / "nope.so")) if abi._LIB is None else (_ for _ in ()).throw(
             RuntimeError("not built"))
+
+
+def test_host_topology_matches_build_connectivity():
+    """mgpu_mesh_topology's host builder (the arrays the device path is checked
+    against) gives the CSR pattern and cell->face lists of
+    mgpu_build_connectivity, 0-based."""
+    from mixsolver_b200 import cases
+    from mixsolver_b200 import solver as S
+    mesh = cases.channel3d(8, 4, 4, seed=1)[0]
+    t = S.mesh_topology(mesh, on_device=False)
+    c = S.build_connectivity(mesh)
+    np.testing.assert_array_equal(t["cf_ptr"] + 1, c["cf_ptr"])
+    np.testing.assert_array_equal(t["cf"] + 1, c["cf"])
+    np.testing.assert_array_equal(t["row_ptr"] + 1, c["row_ptr"])
+    np.testing.assert_array_equal(t["col"] + 1, c["col_idx"])
+    n = mesh.ncells
+    for i in range(n):
+        row = t["col"][t["row_ptr"][i]:t["row_ptr"][i + 1]]
+        assert row[t["diag"][i] - t["row_ptr"][i]] == i

@@ -90,6 +90,7 @@ struct MixedArgsT {
   // pass waits only for the blocks whose rows its rows read instead of the
   // whole grid. Null: grid-stride rows and grid barriers (batched lanes).
   unsigned* flags;
+  int flexible;  // reliable PCG with a Chebyshev preconditioner: Polak-Ribiere (flexible) beta
 };
 using MixedArgs = MixedArgsT<float>;
 

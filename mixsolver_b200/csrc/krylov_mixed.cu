@@ -8,20 +8,24 @@
 #include "krylov_poly.cuh"
 
 namespace mgpu {
+extern int g_mixed_occ;  // krylov.cu: the mixed_blocks_per_sm tuning key
 namespace {
 
 // ---------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------
 
-template <bool L1, int ELL>
-__global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : 2) k_pcg_mixed(KrylovArgs a, MixedArgs m) {
+// OCC: resident blocks per SM the register budget is sized for (2: 128
+// registers a thread; 3: 80; 4: 64), chosen at launch for both solvers
+// (tuning key "mixed_blocks_per_sm")
+template <bool L1, int ELL, int OCC = 2>
+__global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : OCC) k_pcg_mixed(KrylovArgs a, MixedArgs m) {
   VGrid g = whole_grid(a.bar, a.partials);
   pcg_mixed_body<float, L1, ELL>(a, m, g);
 }
 
-template <bool L1, int ELL>
-__global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : 2) k_bicgstab_mixed(KrylovArgs a, MixedArgs m) {
+template <bool L1, int ELL, int OCC = 2>
+__global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : OCC) k_bicgstab_mixed(KrylovArgs a, MixedArgs m) {
   VGrid g = whole_grid(a.bar, a.partials);
   bicgstab_mixed_body<float, L1, ELL>(a, m, g);
 }
@@ -96,25 +100,41 @@ const void* batch_kernel(bool pcg, int ell) {
 }  // namespace
 
 int launch_pcg_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s) {
+  const void* one = ell_mode(m) == 0 ? (const void*)k_pcg_mixed<true, 0> : (const void*)k_pcg_mixed<true, 1>;
+  const void* grid = nullptr;
   switch (ell_mode(m)) {
     case 2:
-      return launch_mixed((const void*)k_pcg_mixed<true, 1>, (const void*)k_pcg_mixed<false, 2>, a, m, s);
+      grid = g_mixed_occ >= 4 ? (const void*)k_pcg_mixed<false, 2, 4>
+                            : g_mixed_occ == 3 ? (const void*)k_pcg_mixed<false, 2, 3> : (const void*)k_pcg_mixed<false, 2>;
+      break;
     case 1:
-      return launch_mixed((const void*)k_pcg_mixed<true, 1>, (const void*)k_pcg_mixed<false, 1>, a, m, s);
+      grid = g_mixed_occ >= 4 ? (const void*)k_pcg_mixed<false, 1, 4>
+                            : g_mixed_occ == 3 ? (const void*)k_pcg_mixed<false, 1, 3> : (const void*)k_pcg_mixed<false, 1>;
+      break;
     default:
-      return launch_mixed((const void*)k_pcg_mixed<true, 0>, (const void*)k_pcg_mixed<false, 0>, a, m, s);
+      grid = (const void*)k_pcg_mixed<false, 0>;
   }
+  return launch_mixed(one, grid, a, m, s);
 }
 
 int launch_bicgstab_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s) {
+  const void* one = ell_mode(m) == 0 ? (const void*)k_bicgstab_mixed<true, 0> : (const void*)k_bicgstab_mixed<true, 1>;
+  const void* grid = nullptr;
   switch (ell_mode(m)) {
     case 2:
-      return launch_mixed((const void*)k_bicgstab_mixed<true, 1>, (const void*)k_bicgstab_mixed<false, 2>, a, m, s);
+      grid = g_mixed_occ >= 4 ? (const void*)k_bicgstab_mixed<false, 2, 4>
+                            : g_mixed_occ == 3 ? (const void*)k_bicgstab_mixed<false, 2, 3>
+                                             : (const void*)k_bicgstab_mixed<false, 2>;
+      break;
     case 1:
-      return launch_mixed((const void*)k_bicgstab_mixed<true, 1>, (const void*)k_bicgstab_mixed<false, 1>, a, m, s);
+      grid = g_mixed_occ >= 4 ? (const void*)k_bicgstab_mixed<false, 1, 4>
+                            : g_mixed_occ == 3 ? (const void*)k_bicgstab_mixed<false, 1, 3>
+                                             : (const void*)k_bicgstab_mixed<false, 1>;
+      break;
     default:
-      return launch_mixed((const void*)k_bicgstab_mixed<true, 0>, (const void*)k_bicgstab_mixed<false, 0>, a, m, s);
+      grid = (const void*)k_bicgstab_mixed<false, 0>;
   }
+  return launch_mixed(one, grid, a, m, s);
 }
 
 int batch_capacity(bool pcg, int ell) {

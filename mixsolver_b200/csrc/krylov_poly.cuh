@@ -604,11 +604,12 @@ __device__ bool update_x(const KrylovArgs& a, const VGrid& g, const Rows& rows, 
 // [lmax/ratio, lmax]: k-1 SpMV passes, one barrier each. On entry z0 = d =
 // D^-1 rr / theta (written by the caller's pass, followed by a barrier). The
 // result lands in zout (z0 or z1, ping-pong); the last pass also sums rr.z and
-// rr.rr, reduced before returning.
+// rr.rr (r2.z instead of rr.rr when r2 is given), reduced before returning.
 template <typename V, bool L1, int ELL>
 __device__ __forceinline__ bool cheb_apply(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid& g, Red& R,
                                            const Rows& rows, const V* rr, V* dch, V* z0, V* z1,
-                                           double lmax, V*& zout, double (&red)[2], unsigned& pass) {
+                                           double lmax, V*& zout, double (&red)[2], unsigned& pass,
+                                           const V* r2 = nullptr) {
   const Sp32<V> S = sp32_of(a, m, rows);
   const double lmin = lmax / m.cheb_ratio;
   const double th = 0.5 * (lmax + lmin), de = 0.5 * (lmax - lmin), sg = th / de;
@@ -636,7 +637,7 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
             zn[i] = zi;
             if (last) {
               c[0] = (double)rr[i] * (double)zi;
-              c[1] = (double)rr[i] * (double)rr[i];
+              c[1] = r2 ? (double)r2[i] * (double)zi : (double)rr[i] * (double)rr[i];
             }
           }
           if (last) red_put<2>(R, rows, base + r * rows.stride, c);
@@ -783,7 +784,9 @@ __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid&
   const V* __restrict__ dinv = m.dinv;
   V *rr = m.w32, *zA = m.w32 + n, *p = m.w32 + 2l * n, *q = m.w32 + 3l * n;
   V *dch = m.w32 + 5l * n, *zB = m.w32 + 6l * n, *pn = m.w32 + 7l * n;  // p double-buffered
+  V* rold = m.w32 + 4l * n;  // flexible beta: the residual before the update
   const bool cheb = m.cheb_k > 1;
+  const bool flex = cheb && m.flexible;
   const double sc = 1.0 / rnorm0;
   const double stop = a.tol * bnrm * sc;  // |rr| at which the estimate reaches tol
   const double stop2 = stop * stop, delta2 = m.rel_delta * m.rel_delta;
@@ -808,10 +811,14 @@ __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid&
   bool first = true;
   while (true) {
     V* z = zA;
+    double rold_z = 0.0;
     if (cheb) {
-      double red[2];  // (rr.z, rr.rr)
-      if (!cheb_apply<V, L1, ELL>(a, m, g, R, rows, rr, dch, zA, zB, lmax, z, red, pass)) return;
+      double red[2];  // (rr.z, rr.rr), flexible: (rr.z, rold.z)
+      if (!cheb_apply<V, L1, ELL>(a, m, g, R, rows, rr, dch, zA, zB, lmax, z, red, pass,
+                                  flex && !first ? rold : nullptr))
+        return;
       rzn = red[0];
+      rold_z = red[1];
     }
     V beta = V(0);
     if (!first) {
@@ -819,7 +826,10 @@ __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid&
         ierr = 2;
         break;
       }
-      beta = (V)(rzn / rz);
+      // flexible (Polak-Ribiere) beta = z.(r - r_old) / rz_old: stays a
+      // descent direction when the FP32 polynomial differs slightly from
+      // one application to the next
+      beta = (V)((flex ? rzn - rold_z : rzn) / rz);
     }
     rz = rzn;
     ++total;
@@ -845,6 +855,7 @@ __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid&
       double c[2] = {0.0, 0.0};
       if (i < rows.n) {
         a.x[i] = fma(ax, (double)p[i], a.x[i]);
+        if (flex) rold[i] = rr[i];
         const V ri = vfma(-af, q[i], rr[i]);
         rr[i] = ri;
         const V zi = cheb ? dinv[i] * ri * inv_th : dinv[i] * ri;

@@ -92,11 +92,11 @@ def test_mixed_piso_meets_gate():
 
 
 def test_mixed_neighbour_sync_bit_identical():
-    """A single-system pressure solve runs its Chebyshev passes on contiguous
-    row ranges, each block waiting only for the blocks whose rows it reads.
-    Every sum still runs over fixed row chunks, so the run is bit-identical to
-    the same run with grid barriers (and to a batched member, where lanes use
-    grid-stride rows)."""
+    """The optional neighbour sync (tuning key neighbor_sync): a single-system
+    pressure solve runs its Chebyshev passes on contiguous row ranges, each
+    block waiting only for the blocks whose rows it reads. Every sum still runs
+    over fixed row chunks, so the run is bit-identical to the same run with
+    grid barriers (the default)."""
     mesh, ctrl = cases.channel3d(32, 16, 16, seed=6, outer_max=5, order_fn=S.rcm_order)
     ctrl.precision = abi.PREC_MIXED
     ctrl.lin_max = 2000
@@ -110,7 +110,7 @@ def test_mixed_neighbour_sync_bit_identical():
             assert ier == 0
             out.append((log, g.fields()))
     finally:
-        S.set_tuning("neighbor_sync", 1)
+        S.set_tuning("neighbor_sync", 0)
         S.set_tuning("single_block_rows", 32768)
     for a, b in zip(out[0][0], out[1][0]):
         assert a["lin_it"] == b["lin_it"] and a["lin_res"] == b["lin_res"]

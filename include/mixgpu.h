@@ -303,6 +303,27 @@ int mgpu_cg_jacobi_noalloc(int n, const int32_t* d_row_ptr, const int32_t* d_col
  * tile's successor into L2, default 96). */
 int mgpu_set_tuning(const char* key, int value);
 
+/* Coupled mode (the coupling driver's hook, mod_mix_driver.f90:1032 calling
+ * uns_solver_step with interface data). A zone given a bc line of type
+ * MGPU_BC_INTERFACE is a coupling surface (the reference groups the faces of
+ * its "interface" zones the same way, mod_uns_bc.f90:282-323).
+ * mgpu_interface_set: set_interface_vel / set_interface_p
+ * (mod_uns_bc.f90:730-760): faces 1-based, u(3,n) and p(n) either may be
+ * NULL; the values stay with the case until set again (zero at creation).
+ * mgpu_interface_mode: set_iface_p_dirichlet (mod_uns_bc.f90:810-813): 0 the
+ * peer supplies the face velocity (pressure zero-gradient), 1 it supplies the
+ * face pressure (velocity extrapolated; pressure-Dirichlet in the SIMPLE
+ * pressure correction; the transient drivers' ppe_assembly_mpi keeps only
+ * pressure outlets and far fields Dirichlet, as in the reference).
+ * mgpu_interface_extract: uns_solver_extract_iface (mod_uns_driver.f90:274-
+ * 330) for fluid owner cells: every interface face (bc order, then face
+ * order), 1-based, with its owner cell's u(3) and p; *n = their number (at
+ * most cap written). Density (ctrl.rho) and temperature (none on this path)
+ * are the caller's. The slip and zhang interface variants are not provided. */
+int mgpu_interface_set(MgpuCase* c, int n, const int32_t* faces, const double* u, const double* p);
+int mgpu_interface_mode(MgpuCase* c, int p_dirichlet);
+int mgpu_interface_extract(MgpuCase* c, int cap, int32_t* faces, double* u, double* p, int* n);
+
 /* Timing of the last run on the case's stream (CUDA events): total device ms
  * and, for the dominant kernel family, launches and summed device ms. */
 typedef struct {

@@ -26,7 +26,9 @@ namespace {
 // run with inlet_ramp > 1 sets them (b_begin_iter), and left at their last
 // value afterwards, as the reference's module variables are -- so the
 // gradients a run computes before its first iteration see the previous value.
-__device__ __forceinline__ Ramp ramp_of(const DeviceCase& d) { return Ramp{d.ramp[0], d.ramp[1]}; }
+__device__ __forceinline__ Ramp ramp_of(const DeviceCase& d) {
+  return Ramp{d.ramp[0], d.ramp[1], d.iface_vel, d.iface_p, (long)d.F, d.iface_pdir};
+}
 
 // ---------------- geometry (setup) ----------------------------------------
 
@@ -221,9 +223,9 @@ __device__ __forceinline__ void b_gradients(const DeviceCase& d, const AsmParams
       w2 = lf * u2[a] + l1 * u2[b];
     } else {
       const DevGroup& gr = d.groups[d.fgrp[f]];
-      pf = bc_face_p(gr, rp, d.p[a]);
+      pf = bc_face_p(gr, rp, d.p[a], f);
       bc_face_vel(gr, rp, d.xf[f], d.xf[F + f], d.xf[2 * F + f], d.sf[f], d.sf[F + f], d.sf[2 * F + f], u0[a],
-                  u1[a], u2[a], w0, w1, w2);
+                  u1[a], u2[a], w0, w1, w2, f);
     }
     const double s0 = d.sf[f], s1 = d.sf[F + f], s2 = d.sf[2 * F + f];
     const double phi[4] = {pf, w0, w1, w2};
@@ -271,7 +273,7 @@ __device__ __forceinline__ void b_limiter(const DeviceCase& d, const AsmParams& 
     } else if (d.fgrp[f] >= 0) {
       double w[3];
       bc_face_vel(d.groups[d.fgrp[f]], rp, d.xf[f], d.xf[F + f], d.xf[2 * F + f], d.sf[f], d.sf[F + f],
-                  d.sf[2 * F + f], d.u[a], d.u[N + a], d.u[2 * N + a], w[0], w[1], w[2]);
+                  d.sf[2 * F + f], d.u[a], d.u[N + a], d.u[2 * N + a], w[0], w[1], w[2], f);
       pmin = fmin(pmin, w[comp]);
       pmax = fmax(pmax, w[comp]);
     }
@@ -321,8 +323,8 @@ __device__ __forceinline__ void mom_finish(const DeviceCase& d, const AsmParams&
     const double s0 = d.sf[f], s1 = d.sf[F + f], s2 = d.sf[2 * F + f];
     double w[3];
     bc_face_vel(gr, rp, d.xf[f], d.xf[F + f], d.xf[2 * F + f], s0, s1, s2, u0[c], u1[c], u2[c], w[0], w[1],
-                w[2]);
-    const double pf = bc_face_p(gr, rp, d.p[c]);
+                w[2], f);
+    const double pf = bc_face_p(gr, rp, d.p[c], f);
     const double D = d.Dm[f];
     const double Fm = P.rho * dot3(w[0], w[1], w[2], s0, s1, s2);
     switch (gr.btype) {
@@ -346,6 +348,15 @@ __device__ __forceinline__ void mom_finish(const DeviceCase& d, const AsmParams&
           rhs = rhs + D * w[comp] - Fm * w[comp];
         } else {
           ap = ap + Fm;
+        }
+        break;
+      case MGPU_BC_INTERFACE:  // mod_uns_simple.f90:1144-1176 (velocity- or pressure-Dirichlet interface)
+        if (!rp.ipdir) {
+          ap = ap + D + fmax(Fm, 0.0);
+          rhs = rhs + D * w[comp] - Fm * w[comp];
+        } else {
+          ap = ap + fmax(Fm, 0.0);
+          rhs = rhs - fmin(Fm, 0.0) * ucomp[c];
         }
         break;
       default:
@@ -520,7 +531,7 @@ __device__ __forceinline__ void b_rhiechow(const DeviceCase& d, const AsmParams&
     const Ramp rp = ramp_of(d);
     double w0, w1, w2;
     bc_face_vel(d.groups[d.fgrp[f]], rp, d.xf[f], d.xf[F + f], d.xf[2 * F + f], s0, s1, s2, d.u[a], d.u[N + a],
-                d.u[2 * N + a], w0, w1, w2);
+                d.u[2 * N + a], w0, w1, w2, f);
     d.flux[f] = P.rho * dot3(w0, w1, w2, s0, s1, s2);
     return;
   }
@@ -591,10 +602,14 @@ __device__ __forceinline__ void b_ppe(const DeviceCase& d, const AsmParams& P, c
     const int a = d.c0[f], b = d.c1[f];
     if (b < 0) {
       const int gi = d.fgrp[f];
-      if (gi >= 0 && p_dirichlet(d.groups[gi].btype)) {
+      // af of a pressure-Dirichlet face (the serial rule, which the flux
+      // correction uses in every driver); it enters the matrix under the
+      // driver's own rule (the transient drivers' ppe_assembly_mpi leaves
+      // interface faces out)
+      if (gi >= 0 && p_dirichlet(d.groups[gi].btype, d.iface_pdir)) {
         const double dbf = d.vol[c] / d.apc[c];
         const double af = P.rho * dbf * d.area[f] / d.dn[f];
-        A[dg] = A[dg] + af;
+        if (p_dirichlet(d.groups[gi].btype, d.iface_pdir, d.st->ts_order > 0)) A[dg] = A[dg] + af;
         d.af[f] = af;
       }
       rhs = rhs - d.flux[f];
@@ -613,7 +628,9 @@ __device__ __forceinline__ void b_ppe(const DeviceCase& d, const AsmParams& P, c
       rhs = rhs + d.flux[f];
     }
   }
-  if (!P.has_pdir) {
+  // the pin of cell 1 when no face is pressure-Dirichlet (serial rule for
+  // SIMPLE, the one-rank mpi rule for the transient drivers)
+  if (!(P.has_pdir || (d.iface_pdir && d.n_iface > 0 && d.st->ts_order == 0))) {
     if (c == 0) {
       for (int k = rb; k < re; ++k) A[k] = (d.col[k] == 0) ? 1.0 : 0.0;
       rhs = 0.0;
@@ -642,7 +659,7 @@ __device__ __forceinline__ void b_correct_cells(const DeviceCase& d, const AsmPa
       phif = lf * d.pp[a] + (1.0 - lf) * d.pp[b];
     } else {
       const int gi = d.fgrp[f];
-      phif = (gi >= 0 && p_dirichlet(d.groups[gi].btype)) ? 0.0 : d.pp[a];
+      phif = (gi >= 0 && p_dirichlet(d.groups[gi].btype, d.iface_pdir)) ? 0.0 : d.pp[a];
     }
     const double s0 = d.sf[f], s1 = d.sf[F + f], s2 = d.sf[2 * F + f];
     if (a == c) {
@@ -675,7 +692,7 @@ __device__ __forceinline__ void b_correct_flux(const DeviceCase& d, const int f)
   const int a = d.c0[f], b = d.c1[f];
   if (b < 0) {
     const int gi = d.fgrp[f];
-    if (gi >= 0 && p_dirichlet(d.groups[gi].btype)) d.flux[f] = d.flux[f] + d.af[f] * d.pp[a];
+    if (gi >= 0 && p_dirichlet(d.groups[gi].btype, d.iface_pdir)) d.flux[f] = d.flux[f] + d.af[f] * d.pp[a];
     return;
   }
   d.flux[f] = d.flux[f] - d.af[f] * (d.pp[b] - d.pp[a]);

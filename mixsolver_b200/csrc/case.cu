@@ -96,6 +96,32 @@ __global__ void k_cells_to_planes(const double* __restrict__ src, long n, int pl
   dst[t] = src[planes * i + k];
 }
 
+// iface_vel(:, f) / iface_p(f) of the listed faces (0-based), u AoS (3, n)
+__global__ void k_iface_scatter(int n, const int* __restrict__ faces, const double* __restrict__ u,
+                                const double* __restrict__ p, long F, double* ivel, double* ip) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int f = faces[k];
+  if (u) {
+    ivel[f] = u[3l * k];
+    ivel[F + f] = u[3l * k + 1];
+    ivel[2 * F + f] = u[3l * k + 2];
+  }
+  if (p) ip[f] = p[k];
+}
+
+// the owner cell's u (AoS) and p of every interface face
+__global__ void k_iface_gather(int n, const int* __restrict__ faces, const int* __restrict__ c0,
+                               const double* __restrict__ u, const double* __restrict__ p, long N, double* out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int c = c0[faces[k]];
+  out[4l * k] = u[c];
+  out[4l * k + 1] = u[N + c];
+  out[4l * k + 2] = u[2 * N + c];
+  out[4l * k + 3] = p[c];
+}
+
 int launch_planes_to_cells(const double* src, long n, int planes, bool grad, double* dst, cudaStream_t s) {
   const long tot = n * planes;
   if (tot == 0) return 0;
@@ -599,6 +625,19 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
   for (int k = 0; k < hm.F; ++k)
     if (hm.c1[k] < 0 && (groups[fgrp[k]].btype == MGPU_BC_POUTLET || groups[fgrp[k]].btype == MGPU_BC_FARFIELD))
       P.has_pdir = 1;
+  for (int k = 0; k < hm.F; ++k)
+    if (hm.c1[k] < 0 && fgrp[k] >= 0 && groups[fgrp[k]].btype == MGPU_BC_INTERFACE) d.n_iface++;
+  if (d.n_iface > 0) {  // the peer's interface values, zero until set (mgpu_interface_set)
+    // the interface faces, group by group in bc order, each group in face order
+    for (int gi = 0; gi < (int)groups.size(); ++gi)
+      if (groups[gi].btype == MGPU_BC_INTERFACE)
+        for (int k = 0; k < hm.F; ++k)
+          if (hm.c1[k] < 0 && fgrp[k] == gi) c->iface_faces.push_back(k);
+    if ((e = c->upload(c->d_iface_faces, c->iface_faces))) return fail(e);
+    if ((e = c->alloc(d.iface_vel, 3 * F)) || (e = c->alloc(d.iface_p, F))) return fail(e);
+    MGPU_CUDA(cudaMemsetAsync(d.iface_vel, 0, sizeof(double) * 3 * F, c->stream));
+    MGPU_CUDA(cudaMemsetAsync(d.iface_p, 0, sizeof(double) * F, c->stream));
+  }
   for (auto& g : groups)
     if (g.btype == MGPU_BC_OUTFLOW) c->has_outflow = 1;
   P.has_outflow = c->has_outflow;
@@ -871,6 +910,69 @@ int mgpu_case_stage(MgpuCase* c, int what, int ts_order, const double* apc, doub
   if (aval && (what >= 1 && what <= 5)) TRY(copy_sync(aval, A, sizeof(double) * d.nnz, cudaMemcpyDeviceToHost, c->stream));
   if (rhs && (what >= 1 && what <= 5)) TRY(copy_sync(rhs, d.rhs, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
   if (ap && (what >= 1 && what <= 3)) TRY(copy_sync(ap, d.ap, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
+  return 0;
+}
+
+int mgpu_interface_set(MgpuCase* c, int n, const int32_t* faces, const double* u, const double* p) {
+  if (!c || n < 0 || (n > 0 && !faces)) return MGPU_E_ARG;
+  if (c->d.n_iface == 0) {
+    set_error("mgpu_interface_set: the case has no interface zone");
+    return MGPU_E_ARG;
+  }
+  if (n == 0 || (!u && !p)) return 0;
+  std::vector<int> f0(n);
+  for (int k = 0; k < n; ++k) {
+    if (faces[k] < 1 || faces[k] > c->d.F) {
+      set_error("mgpu_interface_set: face index out of range");
+      return MGPU_E_ARG;
+    }
+    f0[k] = faces[k] - 1;
+  }
+  cudaStream_t s = c->stream;
+  int* df = nullptr;
+  double *du = nullptr, *dp = nullptr;
+  MGPU_CUDA(cudaMallocAsync((void**)&df, sizeof(int) * n, s));
+  if (u) MGPU_CUDA(cudaMallocAsync((void**)&du, sizeof(double) * 3 * n, s));
+  if (p) MGPU_CUDA(cudaMallocAsync((void**)&dp, sizeof(double) * n, s));
+  MGPU_CUDA(cudaMemcpyAsync(df, f0.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+  if (u) MGPU_CUDA(cudaMemcpyAsync(du, u, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+  if (p) MGPU_CUDA(cudaMemcpyAsync(dp, p, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  k_iface_scatter<<<ceil_div(n, 256), 256, 0, s>>>(n, df, du, dp, c->d.F, c->d.iface_vel, c->d.iface_p);
+  MGPU_LAUNCH_CHECK("k_iface_scatter");
+  cudaFreeAsync(df, s);
+  if (du) cudaFreeAsync(du, s);
+  if (dp) cudaFreeAsync(dp, s);
+  MGPU_CUDA(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int mgpu_interface_mode(MgpuCase* c, int p_dirichlet) {
+  if (!c) return MGPU_E_ARG;
+  c->d.iface_pdir = p_dirichlet ? 1 : 0;
+  return 0;
+}
+
+int mgpu_interface_extract(MgpuCase* c, int cap, int32_t* faces, double* u, double* p, int* n) {
+  if (!c || !n) return MGPU_E_ARG;
+  const int m = (int)c->iface_faces.size();
+  *n = m;
+  if (m == 0 || cap <= 0) return 0;
+  const int k = std::min(m, cap);
+  cudaStream_t s = c->stream;
+  double* out = nullptr;
+  MGPU_CUDA(cudaMallocAsync((void**)&out, sizeof(double) * 4 * k, s));
+  k_iface_gather<<<ceil_div(k, 256), 256, 0, s>>>(k, c->d_iface_faces, c->d.c0, c->d.u, c->d.p, c->d.N, out);
+  MGPU_LAUNCH_CHECK("k_iface_gather");
+  std::vector<double> h(4 * (size_t)k);
+  MGPU_CUDA(cudaMemcpyAsync(h.data(), out, sizeof(double) * 4 * k, cudaMemcpyDeviceToHost, s));
+  cudaFreeAsync(out, s);
+  MGPU_CUDA(cudaStreamSynchronize(s));
+  for (int j = 0; j < k; ++j) {
+    if (faces) faces[j] = c->iface_faces[j] + 1;
+    if (u)
+      for (int q = 0; q < 3; ++q) u[3 * j + q] = h[4 * j + q];
+    if (p) p[j] = h[4 * j + 3];
+  }
   return 0;
 }
 

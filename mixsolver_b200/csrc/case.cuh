@@ -192,6 +192,11 @@ struct DeviceCase {
   MgpuIterRec* recs = nullptr;
   int rec_cap = 0;
   double* ramp = nullptr;  // inlet-speed and pressure-value ramp factors in effect (2)
+  // coupling interface (cases with interface zones): the peer's face velocity
+  // (3 planes of F) and face pressure (F), and the interface mode
+  double *iface_vel = nullptr, *iface_p = nullptr;
+  int n_iface = 0;     // interface faces
+  int iface_pdir = 0;  // 1: pressure is the interface constraint (g_iface_p_dir)
 };
 
 // Launch helpers implemented in the .cu files.

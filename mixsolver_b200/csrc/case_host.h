@@ -49,6 +49,8 @@ struct MgpuCase {
   int run_gen = 0;    // counts mgpu_case_begin calls
   double* stage = nullptr;  // device staging of cell-major field copies (grown on demand)
   size_t stage_n = 0;
+  std::vector<int> iface_faces;     // interface faces (0-based), bc order then face order
+  int* d_iface_faces = nullptr;     // the same on the device
 
   template <typename T>
   int alloc(T*& p, size_t n) {

@@ -79,17 +79,35 @@ struct DevGroup {
   double lid_vel[3];
 };
 
+// Boundary state in effect besides the groups: the cold-start ramp factors and
+// the coupling interface (per-face values the peer solver sets, and whether
+// the interface is pressure-Dirichlet, mod_uns_bc.f90:28-77).
 struct Ramp {
-  double inlet, pval;  // g_inlet_ramp_factor, g_pval_ramp_factor
+  double inlet, pval;         // g_inlet_ramp_factor, g_pval_ramp_factor
+  const double* ivel = nullptr;  // iface_vel, 3 planes of F (interface zones only)
+  const double* ip = nullptr;    // iface_p
+  long F = 0;
+  int ipdir = 0;                 // g_iface_p_dir
 };
 
 #ifdef __CUDACC__
 // bc_face_vel, mod_uns_bc.f90:400-509
 __device__ inline void bc_face_vel(const DevGroup& g, const Ramp& rp, double xf0, double xf1, double xf2,
                                    double s0, double s1, double s2, double u0, double u1, double u2,
-                                   double& f0, double& f1, double& f2) {
+                                   double& f0, double& f1, double& f2, long face = -1) {
   double xf[3] = {xf0, xf1, xf2};
   switch (g.btype) {
+    case MGPU_BC_INTERFACE:  // the peer's face velocity, or extrapolated when p is the interface constraint
+      if (rp.ipdir) {
+        f0 = u0;
+        f1 = u1;
+        f2 = u2;
+      } else {
+        f0 = rp.ivel[face];
+        f1 = rp.ivel[rp.F + face];
+        f2 = rp.ivel[2 * rp.F + face];
+      }
+      return;
     case MGPU_BC_WALL:
       if (g.has_lid && fabs(xf[g.lid_dir] - g.lid_coord) <= g.lid_tol) {
         f0 = g.lid_vel[0];
@@ -164,12 +182,18 @@ __device__ inline void bc_face_vel(const DevGroup& g, const Ramp& rp, double xf0
 }
 
 // bc_face_p, mod_uns_bc.f90:514-549
-__device__ inline double bc_face_p(const DevGroup& g, const Ramp& rp, double pP) {
+__device__ inline double bc_face_p(const DevGroup& g, const Ramp& rp, double pP, long face = -1) {
   if (g.btype == MGPU_BC_POUTLET || g.btype == MGPU_BC_FARFIELD) return g.pval * rp.pval;
+  if (g.btype == MGPU_BC_INTERFACE && rp.ipdir) return rp.ip[face];
   return pP;
 }
 
-__device__ inline bool p_dirichlet(int btype) { return btype == MGPU_BC_POUTLET || btype == MGPU_BC_FARFIELD; }
+// bc_face_p_dirichlet, mod_uns_bc.f90:879-893 (ipdir: g_iface_p_dir); the
+// one-rank ppe_assembly_mpi of the transient drivers counts only pressure
+// outlets and far fields (mod_uns_simple_mpi.f90:905-907, 944-945): mpi = 1
+__device__ inline bool p_dirichlet(int btype, int ipdir = 0, int mpi = 0) {
+  return btype == MGPU_BC_POUTLET || btype == MGPU_BC_FARFIELD || (btype == MGPU_BC_INTERFACE && ipdir && !mpi);
+}
 #endif
 
 

@@ -168,7 +168,7 @@ __device__ bool pass_sync(unsigned* flags, VGrid& g, DevStatus* st, unsigned& pa
         ok = 0;
         break;
       }
-      if (spins > limit) {
+      if (spins >= limit) {
         atomicExch(&st->timeout, 1);
         ok = 0;
         break;

@@ -208,10 +208,6 @@ int build_groups(const HostMesh& m, const MgpuCtrl& ctrl, std::vector<DevGroup>&
       why = "thermal boundary values: the energy equation is not part of this path";
       return MGPU_E_ARG;
     }
-    if (sp.btype == MGPU_BC_INTERFACE) {
-      why = "coupling-interface zones are not part of this path";
-      return MGPU_E_ARG;
-    }
     g.has_lid = sp.has_lid ? 1 : 0;
     g.lid_dir = sp.lid_dir - 1;
     if (g.has_lid && (sp.lid_dir < 1 || sp.lid_dir > 3)) {

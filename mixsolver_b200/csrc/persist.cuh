@@ -53,9 +53,10 @@ __device__ __forceinline__ VGrid whole_grid(unsigned long long* bar, double* par
 // round. While it waits it looks at the status every 4096 polls: once any
 // block has flagged a timeout (st may be null: no status) the wait ends. A
 // wait that runs out flags the timeout. Returns false in both cases; the
-// caller then leaves the kernel. The status may lower the poll limit
-// (DevStatus::spin_limit, from the spin_limit tuning key) so that a test can
-// make a wait run out on purpose.
+// caller then leaves the kernel. The status may lower the limit on failed
+// polls (DevStatus::spin_limit, from the spin_limit tuning key; 1 gives up at
+// the first poll that finds the barrier open) so that a test can make a wait
+// run out on purpose.
 // Ordering: __syncthreads puts the block's writes before thread 0's arrival,
 // a release at GPU scope; thread 0's polls are acquires, and the closing
 // __syncthreads puts them before the block's later loads. Release and acquire
@@ -84,7 +85,7 @@ __device__ bool vg_sync(const VGrid& g, DevStatus* st) {
         ok = 0;
         break;
       }
-      if (spins > limit) {
+      if (spins >= limit) {
         if (st) atomicExch(&st->timeout, 1);
         ok = 0;
         break;

@@ -121,6 +121,33 @@ class UnsCase:
         (ier, per-step records)."""
         return self._run(_lib().mgpu_pimple_run, nsteps, logcap)
 
+    # ---- coupled mode (mod_uns_bc.f90:730-813, mod_uns_driver.f90:274-330) ----
+    def interface_set(self, faces, u=None, p=None):
+        """set_interface_vel / set_interface_p: faces 1-based, u (n, 3), p (n)."""
+        faces = np.ascontiguousarray(faces, np.int32)
+        u = None if u is None else np.ascontiguousarray(u, np.float64)
+        p = None if p is None else np.ascontiguousarray(p, np.float64)
+        lib = _lib()
+        abi.check(lib, lib.mgpu_interface_set(self.h, len(faces), iptr(faces), dptr(u), dptr(p)),
+                  "mgpu_interface_set")
+
+    def interface_mode(self, p_dirichlet: bool):
+        """set_iface_p_dirichlet: True when the peer supplies the face pressure."""
+        lib = _lib()
+        abi.check(lib, lib.mgpu_interface_mode(self.h, 1 if p_dirichlet else 0), "mgpu_interface_mode")
+
+    def interface_extract(self):
+        """uns_solver_extract_iface for fluid owner cells: (faces 1-based, u (n, 3), p (n))."""
+        lib = _lib()
+        n = C.c_int(0)
+        abi.check(lib, lib.mgpu_interface_extract(self.h, 0, None, None, None, C.byref(n)), "mgpu_interface_extract")
+        faces = np.zeros(n.value, np.int32)
+        u = np.zeros((n.value, 3))
+        p = np.zeros(n.value)
+        abi.check(lib, lib.mgpu_interface_extract(self.h, n.value, iptr(faces), dptr(u), dptr(p), C.byref(n)),
+                  "mgpu_interface_extract")
+        return faces, u, p
+
     def nan_scan(self):
         """(ifin, field, cell, value, kind) of the first non-finite value."""
         ifin, field, cell, kind = C.c_int(), C.c_int(), C.c_int(), C.c_int()

@@ -237,6 +237,10 @@ struct BC {
   vector<Group> gb;
   vector<int> fgrp;  // face -> group index (0-based), -1 interior
   double inlet_ramp = 1.0, pval_ramp = 1.0;  // g_inlet_ramp_factor / g_pval_ramp_factor
+  // coupling interface (mod_uns_bc.f90:117-130, 730-813): iface_vel(3,nfaces),
+  // iface_p(nfaces), g_iface_p_dir
+  vector<double> iface_vel, iface_p;
+  bool iface_p_dir = false;
 };
 
 // build_bc, mod_uns_bc.f90:155-393 (interface zones are not part of this path)
@@ -300,6 +304,12 @@ void bc_face_vel(const BC& bcs, int i, const double* xf, const double* sf, const
   const Group& g = bcs.gb[bcs.fgrp[i]];
   double nvec[3], un, xi, uspc, ns;
   switch (g.btype) {
+    case MGPU_BC_INTERFACE:  // mod_uns_bc.f90:460-475
+      if (bcs.iface_p_dir)
+        for (int k = 0; k < 3; ++k) uf[k] = uP[k];
+      else
+        for (int k = 0; k < 3; ++k) uf[k] = bcs.iface_vel[3 * (size_t)i + k];
+      break;
     case MGPU_BC_WALL:
       if (g.has_lid && std::fabs(xf[g.lid_dir - 1] - g.lid_coord) <= g.lid_tol)
         for (int k = 0; k < 3; ++k) uf[k] = g.lid_vel[k];
@@ -352,11 +362,23 @@ void bc_face_vel(const BC& bcs, int i, const double* xf, const double* sf, const
 inline double bc_face_p(const BC& bcs, int i, double pP) {
   const Group& g = bcs.gb[bcs.fgrp[i]];
   if (g.btype == MGPU_BC_POUTLET || g.btype == MGPU_BC_FARFIELD) return g.pval * bcs.pval_ramp;
+  if (g.btype == MGPU_BC_INTERFACE) return bcs.iface_p_dir ? bcs.iface_p[i] : pP;  // :527-544
   return pP;
 }
 
 // bc_face_p_dirichlet, mod_uns_bc.f90:879-893
 inline bool bc_face_p_dirichlet(const BC& bcs, int i) {
+  int g = bcs.fgrp[i];
+  if (g < 0) return false;
+  int bt = bcs.gb[g].btype;
+  if (bt == MGPU_BC_INTERFACE) return bcs.iface_p_dir;
+  return bt == MGPU_BC_POUTLET || bt == MGPU_BC_FARFIELD;
+}
+
+// the Dirichlet rule of the one-rank ppe_assembly_mpi (mod_uns_simple_mpi.f90:
+// 905-907, 944-945), which the transient drivers use: pressure outlets and far
+// fields only
+inline bool ppe_dirichlet_mpi(const BC& bcs, int i) {
   int g = bcs.fgrp[i];
   if (g < 0) return false;
   int bt = bcs.gb[g].btype;
@@ -912,6 +934,15 @@ void momentum_assembly(Case& cs, int comp) {
           ap[c0] = ap[c0] + F;
         }
         break;
+      case MGPU_BC_INTERFACE:  // mod_uns_simple.f90:1144-1176 (no slip / zhang variants)
+        if (!cs.bcs.iface_p_dir) {
+          ap[c0] = ap[c0] + D + std::max(F, 0.0);
+          rhs[c0] = rhs[c0] + D * uf[comp] - F * uf[comp];
+        } else {
+          ap[c0] = ap[c0] + std::max(F, 0.0);
+          rhs[c0] = rhs[c0] - std::min(F, 0.0) * cs.u[3 * c0 + comp];
+        }
+        break;
       default:
         break;
     }
@@ -1003,10 +1034,13 @@ void ppe_assembly(Case& cs) {
   cs.rhs.assign(m.ncells, 0.0);
   vector<double>& rhs = cs.rhs;
   double rho = cs.ctrl.rho;
+  // the transient drivers assemble with ppe_assembly_mpi at one rank
+  const bool mpi = cs.ts_order > 0;
+  auto dirichlet = [&](int i) { return mpi ? ppe_dirichlet_mpi(cs.bcs, i) : bc_face_p_dirichlet(cs.bcs, i); };
   for (int i = 0; i < m.nfaces; ++i) {
     int c1 = m.c1[i], c0 = m.c0[i];
     if (c1 < 0) {
-      if (cs.bcs.fgrp[i] >= 0 && bc_face_p_dirichlet(cs.bcs, i)) {
+      if (cs.bcs.fgrp[i] >= 0 && dirichlet(i)) {
         double dbf = cs.g.vol[c0] / cs.apc[c0];
         double d[3];
         for (int k = 0; k < 3; ++k) d[k] = cs.g.xf[3 * i + k] - cs.g.xc[3 * c0 + k];
@@ -1037,7 +1071,7 @@ void ppe_assembly(Case& cs) {
   }
   bool has_pdir = false;
   for (int i = 0; i < m.nfaces; ++i)
-    if (m.c1[i] < 0 && cs.bcs.fgrp[i] >= 0 && bc_face_p_dirichlet(cs.bcs, i)) has_pdir = true;
+    if (m.c1[i] < 0 && cs.bcs.fgrp[i] >= 0 && dirichlet(i)) has_pdir = true;
   if (!has_pdir) {
     for (int k = A.row_ptr[0]; k < A.row_ptr[1]; ++k) A.val[k] = (A.col_idx[k] == 0) ? 1.0 : 0.0;
     for (int kk = 1; kk < A.nrows; ++kk) {
@@ -1074,10 +1108,13 @@ void correct_fields(Case& cs) {
   else
     for (int i = 0; i < m.ncells; ++i) cs.p[i] = cs.p[i] + cs.ctrl.alpha_p * pp[i];
   double rho = cs.ctrl.rho;
+  // the transient drivers assemble with ppe_assembly_mpi at one rank
+  const bool mpi = cs.ts_order > 0;
+  auto dirichlet = [&](int i) { return mpi ? ppe_dirichlet_mpi(cs.bcs, i) : bc_face_p_dirichlet(cs.bcs, i); };
   for (int i = 0; i < m.nfaces; ++i) {
     int c1 = m.c1[i], c0 = m.c0[i];
     if (c1 < 0) {
-      if (cs.bcs.fgrp[i] >= 0 && bc_face_p_dirichlet(cs.bcs, i)) {
+      if (cs.bcs.fgrp[i] >= 0 && dirichlet(i)) {
         double dbf = cs.g.vol[c0] / cs.apc[c0];
         double d[3];
         for (int k = 0; k < 3; ++k) d[k] = cs.g.xf[3 * i + k] - cs.g.xc[3 * c0 + k];
@@ -1458,6 +1495,8 @@ int orc_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, OrcCase** out, i
     return MGPU_E_BC;
   }
   int N = cs.m.ncells, F = cs.m.nfaces;
+  cs.bcs.iface_vel.assign(3 * (size_t)F, 0.0);  // build_bc's zero-initialised interface data
+  cs.bcs.iface_p.assign(F, 0.0);
   cs.u.assign(3 * N, 0.0);
   cs.p.assign(N, 0.0);
   cs.gp.assign(3 * N, 0.0);
@@ -1575,6 +1614,47 @@ int orc_set_apc(OrcCase* c, const double* apc, int ts_order) {
   Case& cs = c->cs;
   if (apc) cs.apc.assign(apc, apc + cs.m.ncells);
   cs.ts_order = ts_order;
+  return 0;
+}
+
+// set_interface_vel / set_interface_p (mod_uns_bc.f90:730-760): faces 1-based
+int orc_interface_set(OrcCase* c, int n, const int32_t* faces, const double* u, const double* p) {
+  BC& b = c->cs.bcs;
+  for (int k = 0; k < n; ++k) {
+    const int i = faces[k] - 1;
+    if (i < 0 || i >= c->cs.m.nfaces) return MGPU_E_ARG;
+    if (u)
+      for (int q = 0; q < 3; ++q) b.iface_vel[3 * (size_t)i + q] = u[3 * (size_t)k + q];
+    if (p) b.iface_p[i] = p[k];
+  }
+  return 0;
+}
+
+// set_iface_p_dirichlet (mod_uns_bc.f90:810-813)
+int orc_interface_mode(OrcCase* c, int flag) {
+  c->cs.bcs.iface_p_dir = flag != 0;
+  return 0;
+}
+
+// uns_solver_extract_iface (mod_uns_driver.f90:274-330), fluid owner cells:
+// interface groups in order, their faces in face order
+int orc_interface_extract(OrcCase* c, int cap, int32_t* faces, double* u, double* p, int* n) {
+  const Case& cs = c->cs;
+  int k = 0;
+  for (const Group& g : cs.bcs.gb) {
+    if (g.btype != MGPU_BC_INTERFACE) continue;
+    for (int i : g.faces) {
+      if (k < cap) {
+        const int c0 = cs.m.c0[i];
+        if (faces) faces[k] = i + 1;
+        if (u)
+          for (int q = 0; q < 3; ++q) u[3 * k + q] = cs.u[3 * c0 + q];
+        if (p) p[k] = cs.p[c0];
+      }
+      ++k;
+    }
+  }
+  *n = k;
   return 0;
 }
 

@@ -45,6 +45,9 @@ def lib():
         L.orc_stage.argtypes = [C.c_void_p, C.c_int, dp, dp, dp, dp]
         L.orc_set_apc.argtypes = [C.c_void_p, dp, C.c_int]
         L.orc_nan_scan.argtypes = [C.c_void_p, P(C.c_int), P(C.c_int), P(C.c_int), dp, P(C.c_int)]
+        L.orc_interface_set.argtypes = [C.c_void_p, C.c_int, ip, dp, dp]
+        L.orc_interface_mode.argtypes = [C.c_void_p, C.c_int]
+        L.orc_interface_extract.argtypes = [C.c_void_p, C.c_int, ip, dp, dp, P(C.c_int)]
         L.orc_krylov_solve.argtypes = [C.c_int, ip, ip, dp, dp, dp, C.c_double, C.c_int, C.c_int,
                                        C.c_int, P(C.c_int), dp, P(C.c_int)]
         L.orc_csr_matvec.argtypes = [C.c_int, ip, ip, dp, dp, dp]
@@ -136,6 +139,22 @@ class OracleCase:
     def set_apc(self, apc=None, ts_order=0):
         a = None if apc is None else np.ascontiguousarray(apc, np.float64)
         lib().orc_set_apc(self.h, dptr(a), int(ts_order))
+
+    def interface_set(self, faces, u=None, p=None):
+        faces = np.ascontiguousarray(faces, np.int32)
+        u = None if u is None else np.ascontiguousarray(u, np.float64)
+        p = None if p is None else np.ascontiguousarray(p, np.float64)
+        assert lib().orc_interface_set(self.h, len(faces), iptr(faces), dptr(u), dptr(p)) == 0
+
+    def interface_mode(self, p_dirichlet):
+        lib().orc_interface_mode(self.h, 1 if p_dirichlet else 0)
+
+    def interface_extract(self):
+        n = C.c_int(0)
+        lib().orc_interface_extract(self.h, 0, None, None, None, C.byref(n))
+        faces, u, p = np.zeros(n.value, np.int32), np.zeros((n.value, 3)), np.zeros(n.value)
+        lib().orc_interface_extract(self.h, n.value, iptr(faces), dptr(u), dptr(p), C.byref(n))
+        return faces, u, p
 
     def nan_scan(self):
         ifin, field, cell, kind = C.c_int(), C.c_int(), C.c_int(), C.c_int()

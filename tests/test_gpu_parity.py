@@ -637,3 +637,115 @@ def test_config2_channel_full_size_fp64_two_iterations():
     # after ~260 iterations the final residual near lin_tol is round-off
     # dominated (as in test_krylov_parity_large)
     _compare_runs(log_g, log_o, g.fields(), o.fields(), res_tol=5e-2)
+
+
+def iface_case(transient=False):
+    """A 12 x 6 x 6 jittered box whose x = 3 end is a coupling interface
+    (zone 9): velocity inlet at x = 0, wall, slip wall and symmetry elsewhere."""
+    zones = (4, 9, 6, 7, 8, 8)
+    mesh = meshgen.box_hex(12, 6, 6, lx=3.0, jitter=0.1, seed=13, zones=zones)
+    mesh = cases.rcm_renumber(meshgen.shuffle_cells(mesh, 14), S.rcm_order)
+    _, ctrl = cases.channel3d(4, 2, 2, outer_max=12)
+    ctrl.mu = 2e-2
+    ctrl.mom_solver = abi.MOM_ILU0
+    ctrl.ppe_precond = abi.PPE_IC0
+    ctrl.lin_max = 300
+    B = abi.BcSpec
+    ctrl.bcs = [B(zone=4, btype=abi.BC_VINLET, uvel=(1.0, 0.0, 0.0)), B(zone=9, btype=abi.BC_INTERFACE),
+                B(zone=6, btype=abi.BC_WALL), B(zone=7, btype=abi.BC_SLIPWALL), B(zone=8, btype=abi.BC_SYMMETRY)]
+    if transient:
+        ctrl.transient, ctrl.dt, ctrl.n_time_max, ctrl.n_correct = True, 5e-3, 4, 2
+    faces = np.nonzero((mesh.zone == 9) & (mesh.c1 == 0))[0] + 1
+    xf = S.compute_geometry(mesh)["xf"][faces - 1]
+    # the peer's values: outflow matching the inflow plus a tangential part; a
+    # pressure varying over the patch
+    u = np.stack([np.ones(len(faces)), 0.05 * np.sin(3.0 * xf[:, 1]), 0.02 * xf[:, 2]], 1)
+    p = 0.1 * xf[:, 1] - 0.02 * xf[:, 2]
+    return mesh, ctrl, faces, u, p
+
+
+def _iface_pair(mesh, ctrl, faces, u, p, p_dir):
+    g, o = S.UnsCase(mesh, ctrl), O.OracleCase(mesh, ctrl)
+    for c in (g, o):
+        c.interface_set(faces, u=u, p=p)
+        c.interface_mode(p_dir)
+    return g, o
+
+
+@pytest.mark.parametrize("p_dir", [False, True])
+def test_interface_stage_kernels_bit_exact(p_dir):
+    """The coupled-mode boundary (BC_INTERFACE, mod_uns_bc.f90:460-544;
+    momentum :1144-1176; pressure-Dirichlet rule :879-893) in every stage."""
+    mesh, ctrl, faces, u, p = iface_case()
+    nnz = len(S.build_connectivity(mesh)["col_idx"])
+    g, o = _iface_pair(mesh, ctrl, faces, u, p, p_dir)
+    u0, p0, flux = _seed_fields(mesh, seed=21)
+    apc = 1.0 + np.random.default_rng(22).random(mesh.ncells)
+    for c in (g, o):
+        c.upload(u=u0, p=p0, flux=flux)
+    o.set_apc(apc, 0)
+    g.stage(0, 0, apc)
+    o.stage(0)
+    fg, fo = g.fields(), o.fields()
+    np.testing.assert_array_equal(fg["gp"], fo["gp"])
+    np.testing.assert_array_equal(fg["gu"], fo["gu"])
+    for comp in (1, 2, 3):
+        for a, b in zip(g.stage(comp, 0, apc, nnz), o.stage(comp, nnz)):
+            np.testing.assert_array_equal(a, b)
+    g.stage(4, 0, apc)
+    o.stage(4)
+    np.testing.assert_array_equal(g.fields()["flux"], o.fields()["flux"])
+    for a, b in zip(g.stage(5, 0, apc, nnz)[:2], o.stage(5, nnz)[:2]):
+        np.testing.assert_array_equal(a, b)
+    pp = np.random.default_rng(23).standard_normal(mesh.ncells) * 1e-3
+    g.stage(6, 0, apc, pp=pp)
+    o.stage(6, pp=pp)
+    fg, fo = g.fields(), o.fields()
+    for k in ("u", "p", "flux"):
+        np.testing.assert_array_equal(fg[k], fo[k], err_msg=k)
+
+
+@pytest.mark.parametrize("p_dir", [False, True])
+def test_interface_simple_parity_and_extract(p_dir):
+    """SIMPLE with the peer's interface values (velocity, or pressure), then
+    uns_solver_extract_iface: the same faces, the owner cells' u and p."""
+    mesh, ctrl, faces, u, p = iface_case()
+    g, o = _iface_pair(mesh, ctrl, faces, u, p, p_dir)
+    ier_g, log_g = g.simple_run()
+    ier_o, log_o = o.simple_run()
+    assert ier_g == ier_o == 0
+    fg, fo = g.fields(), o.fields()
+    _compare_runs(log_g, log_o, fg, fo)
+    fa, ua, pa = g.interface_extract()
+    fb, ub, pb = o.interface_extract()
+    np.testing.assert_array_equal(fa, faces)
+    np.testing.assert_array_equal(fa, fb)
+    owner = mesh.c0[faces - 1] - 1
+    np.testing.assert_array_equal(ua, fg["u"][owner])
+    np.testing.assert_array_equal(pa, fg["p"][owner])
+    assert rel_l2(ua, ub) < FIELD_TOL and rel_l2(pa, pb) < FIELD_TOL
+
+
+def test_interface_piso_pressure_mode_parity():
+    """PISO with a pressure-Dirichlet interface: the transient drivers'
+    ppe_assembly_mpi keeps the interface out of the Dirichlet set while the
+    flux correction keeps it in (the reference's own rules); the run is held
+    to the oracle's round-off ensemble like the other PISO runs."""
+    mesh, ctrl, faces, u, p = iface_case(transient=True)
+    u0 = 0.1 * np.random.default_rng(24).standard_normal((mesh.ncells, 3))
+    g = S.UnsCase(mesh, ctrl)
+    g.interface_set(faces, u=u, p=p)
+    g.interface_mode(True)
+    g.upload(u=u0)
+    ier_g, log_g = g.piso_run()
+    assert ier_g == 0
+    runs = []
+    for e in (0.0, 3e-16, -3e-16, 1e-15, -1e-15):
+        o = O.OracleCase(mesh, ctrl)
+        o.interface_set(faces, u=u, p=p)
+        o.interface_mode(True)
+        o.upload(u=u0 * (1.0 + e))
+        ier, log = o.piso_run()
+        assert ier == 0
+        runs.append((log, o.fields()))
+    _compare_piso(log_g, g.fields(), runs)

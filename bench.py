@@ -73,7 +73,20 @@ def parse():
     ap.add_argument("--accuracy-iters", type=int, default=200,
                     help="channel: outer iterations after which the mixed form is compared with the tight FP64 run")
     ap.add_argument("--tight-tol", type=float, default=1e-12, help="channel: lin_tol of the tight FP64 run")
+    ap.add_argument("--tuning", default="",
+                    help="library tuning keys set before the run (mgpu_set_tuning), e.g. ell_stage=0,cheb_degree=12")
     return ap.parse_args()
+
+
+def apply_tuning(args):
+    """Set the --tuning keys; returns them as a dict for the config record."""
+    from mixsolver_b200 import solver as S
+    out = {}
+    for kv in filter(None, args.tuning.split(",")):
+        k, v = kv.split("=")
+        S.set_tuning(k.strip(), int(v))
+        out[k.strip()] = int(v)
+    return out
 
 
 def dist_env():
@@ -208,22 +221,32 @@ def krylov_bytes(n, nnz, its, method, mixed=False, tol=1e-8, tau=1e-4, cheb_k=16
 
     FP64 form: SpMV 12 nnz + 4(N+1) + 16 N; triangular pair 12 nnz + 24 N;
     dot 16 N; axpy 24 N; norm 8 N; Jacobi apply 20 N.
-    Mixed form (FP32 values + int32 columns = 8 B per entry, FP32 vectors):
-      PCG with a degree-k Chebyshev-Jacobi preconditioner, per iteration:
-        fused q = A z + beta q, p = z + beta p, p.q:   8 nnz + 20 N
-        d += alpha p, r -= alpha q, first Chebyshev term: 36 N
-        k - 1 Chebyshev steps, each an SpMV plus 5 vectors: 8 nnz + 24 N
-      BiCGStab-Jacobi, per iteration: 2 SpMV (8 nnz + 4(N+1) + 8 N) + 80 N;
-      plus the FP64 prologue (FP32 copy of A: 12 nnz) and, per refinement
-      step, one FP64 true residual (12 nnz + 4(N+1) + 28 N) and the x update."""
+    Mixed form:
+      PCG: FP64 conjugate gradients with an FP32 degree-k Chebyshev-Jacobi
+      polynomial, per iteration:
+        p = z + beta p, q = A p (FP64 values + int32 columns = 12 B per
+        entry; z FP32, p FP64), p.q:                          12 nnz + 28 N
+        x += alpha p, r -= alpha q (FP64), FP32 copy of r and
+        the first Chebyshev term:                              60 N
+        k - 1 Chebyshev steps in FP32 (FP32 values + int32
+        columns = 8 B per entry), each an SpMV plus 5 vectors: 8 nnz + 24 N
+        (the last one also reads the FP64 r for r.z:            + 8 N)
+      plus the prologue (FP32 and FP64 ELL copies of A: 8 + 12 + 8 nnz from
+      12 nnz) and two FP64 true residuals (12 nnz + 4(N+1) + 28 N).
+      BiCGStab-Jacobi (FP32 inside FP64 refinement), per iteration: 2 SpMV
+      (8 nnz + 4(N+1) + 8 N) + 80 N; plus the prologue (FP32 copy of A:
+      12 nnz) and, per refinement step, one FP64 true residual and the x
+      update."""
     import math
     if mixed:
-        steps = max(1, math.ceil(math.log(tol) / math.log(tau)))
-        setup = 12 * nnz + 24 * n + steps * (12 * nnz + 4 * (n + 1) + 28 * n + 28 * n + 20 * n)
+        true_res = 12 * nnz + 4 * (n + 1) + 28 * n
         if method == "pcg":
-            per = (8 * nnz + 20 * n) + 36 * n + max(0, cheb_k - 1) * (8 * nnz + 24 * n)
-        else:
-            per = 2 * (8 * nnz + 4 * (n + 1) + 8 * n) + 80 * n
+            setup = 40 * nnz + 24 * n + 2 * true_res + 28 * n
+            per = (12 * nnz + 28 * n) + 60 * n + max(0, cheb_k - 1) * (8 * nnz + 24 * n) + 8 * n
+            return setup + its * per
+        steps = max(1, math.ceil(math.log(tol) / math.log(tau)))
+        setup = 12 * nnz + 24 * n + steps * (true_res + 28 * n + 20 * n)
+        per = 2 * (8 * nnz + 4 * (n + 1) + 8 * n) + 80 * n
         return setup + its * per
     spmv = 12 * nnz + 4 * (n + 1) + 16 * n
     tri = 12 * nnz + 24 * n
@@ -411,8 +434,9 @@ def run_ours(args):
         "dtype": "f64" if not mixed else "f32-inner/f64-refinement",
         "data": "synthetic (seeded jittered hex channel, RCM-ordered)",
         "config": channel_config(args, mesh),
-        "form": ("mixed: FP32 BiCGStab-Jacobi momentum inside FP64 refinement, FP32 Chebyshev-Jacobi PCG "
-                 "pressure with reliable updates into FP64 x; every dot product and norm FP64"
+        "form": ("mixed: FP32 BiCGStab-Jacobi momentum inside FP64 refinement; pressure PCG in FP64 with an "
+                 "FP32 Chebyshev-Jacobi polynomial preconditioner (FP32 matrix copy and vectors); every dot "
+                 "product and norm FP64"
                  if mixed else "FP64 parity form: BiCGStab+Jacobi momentum, PCG+ILU(0) pressure"),
         "krylov_iterations_per_step": {"momentum": its_mom / K, "pressure": its_ppe / K},
         "solve_latency_ms": {"p50": pct(solve_ms, 50), "p99": pct(solve_ms, 99),
@@ -453,6 +477,8 @@ def run_ours(args):
         out["cpu_baseline"] = cpu_baseline(args, mesh, ctrl)
     close_ranks(world)
     if rank == 0:
+        if getattr(args, "tuning_set", None):
+            out["config"]["tuning"] = args.tuning_set
         print(json.dumps(out), flush=True)
 
 
@@ -638,6 +664,8 @@ def run_piso(args):
     case.close()
     close_ranks(world)
     if rank == 0:
+        if getattr(args, "tuning_set", None):
+            out["config"]["tuning"] = args.tuning_set
         print(json.dumps(out), flush=True)
 
 
@@ -763,6 +791,8 @@ def run_pimple(args):
     case.close()
     close_ranks(world)
     if rank == 0:
+        if getattr(args, "tuning_set", None):
+            out["config"]["tuning"] = args.tuning_set
         print(json.dumps(out), flush=True)
 
 
@@ -927,6 +957,8 @@ def run_batch(args):
     }
     close_ranks(world)
     if rank == 0:
+        if getattr(args, "tuning_set", None):
+            out["config"]["tuning"] = args.tuning_set
         print(json.dumps(out), flush=True)
 
 
@@ -1071,11 +1103,15 @@ def run_serve(args):
         "clocks": mx["clocks"],
     }
     if rank == 0:
+        if getattr(args, "tuning_set", None):
+            out["config"]["tuning"] = args.tuning_set
         print(json.dumps(out), flush=True)
 
 
 if __name__ == "__main__":
     a = parse()
+    if a.impl != "reference":
+        a.tuning_set = apply_tuning(a)
     if a.impl == "reference":
         run_reference(a)
     elif a.workload == "batch":

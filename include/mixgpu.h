@@ -214,6 +214,22 @@ int mgpu_krylov_solve(int n, const int32_t* row_ptr, const int32_t* col_idx, con
                       const double* b, double* x, double tol, int maxit, int method,
                       int norm_mode, int* it, double* res, int* ierr);
 
+/* The pressure solver of the mixed-precision and FP64 polynomial forms on a
+ * host CSR system (arrays 1-based as in mgpu_krylov_solve; no reference
+ * counterpart: it stands in for cg_ic0, mod_uns_linsolver.f90:405-461, with
+ * the same contract): PCG with a Chebyshev-Jacobi polynomial of degree
+ * cheb_degree (<= 0: the cheb_degree tuning key; 1: Jacobi) and reliable
+ * updates.
+ *   precision: MGPU_PREC_MIXED (FP32 matrix copy, vectors and polynomial;
+ *              x, every dot product and the residual replacements in FP64) or
+ *              MGPU_PREC_FP64_POLY (the same in FP64).
+ *   x: initial guess in, solution out. Converged when |b - A x| / |b| <= tol on
+ *   the FP64 residual (ierr 0), else ierr 1 after maxit iterations, 2 on a
+ *   breakdown. At most 2^23 rows; every row needs its diagonal entry. */
+int mgpu_pcg_poly_solve(int n, const int32_t* row_ptr, const int32_t* col_idx, const double* val,
+                        const double* b, double* x, double tol, int maxit, int precision, int cheb_degree,
+                        int* it, double* res, int* ierr);
+
 /* y = A x on a host CSR matrix (csr_matvec, mod_uns_linsolver.f90:40-52). */
 int mgpu_csr_matvec(int n, const int32_t* row_ptr, const int32_t* col_idx, const double* val,
                     const double* x, double* y);

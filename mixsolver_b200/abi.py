@@ -213,7 +213,7 @@ EXPORTS = ["mgpu_version", "mgpu_last_error", "mgpu_set_device", "mgpu_case_crea
            "mgpu_batch_step", "mgpu_batch_poll", "mgpu_batch_run", "mgpu_batch_info", "mgpu_batch_plan",
            "mgpu_batch_set_profiling", "mgpu_cas_read", "mgpu_cas_zone_names", "mgpu_cas_free",
            "mgpu_rcm_order_device", "mgpu_mesh_topology", "mgpu_interface_set", "mgpu_interface_mode",
-           "mgpu_interface_extract"]
+           "mgpu_interface_extract", "mgpu_pcg_poly_solve"]
 NOALLOC_MAX_ROWS = 131072
 
 _LIB = None
@@ -248,6 +248,8 @@ def load_library(path: str = LIB_PATH):
     lib.mgpu_nan_scan.argtypes = [C.c_void_p, P(C.c_int), P(C.c_int), P(C.c_int), dblp, P(C.c_int)]
     lib.mgpu_krylov_solve.argtypes = [C.c_int, i32p, i32p, dblp, dblp, dblp, C.c_double, C.c_int,
                                       C.c_int, C.c_int, P(C.c_int), dblp, P(C.c_int)]
+    lib.mgpu_pcg_poly_solve.argtypes = [C.c_int, i32p, i32p, dblp, dblp, dblp, C.c_double, C.c_int,
+                                        C.c_int, C.c_int, P(C.c_int), dblp, P(C.c_int)]
     lib.mgpu_csr_matvec.argtypes = [C.c_int, i32p, i32p, dblp, dblp, dblp]
     lib.mgpu_build_connectivity.argtypes = [P(MgpuMesh), i32p, i32p, i32p, i32p, i32p, i32p, i32p]
     lib.mgpu_geometry.argtypes = [P(MgpuMesh), dblp, dblp, dblp, dblp, dblp, dblp]

@@ -437,7 +437,6 @@ int prepare(MgpuBatch* b) {
       s.a = P.pcg ? ppe_args(c, std::min(3 + P.icorr, MGPU_MAXSOLVE - 1), tr) : mom_args(c, P.comp, tr);
       s.a.precond = 1;
       s.m = mixed_args(c, !P.pcg);
-      s.m.flags = nullptr;  // lanes use grid-stride rows and lane barriers
       hs.push_back(s);
       P.mixed.push_back(k);
     }

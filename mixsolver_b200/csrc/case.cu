@@ -214,8 +214,8 @@ MixedArgs mixed_args(const MgpuCase* c, bool bicg) {
   const bool big = (double)c->d.N * mixed_row_bytes(c->d.ell_w) > g_prefetch_mb * 1048576.0;
   return MixedArgs{c->d.a32,   c->d.dinv32, c->d.w32,  c->ctrl.mixed_tol > 0.0 ? c->ctrl.mixed_tol : 1e-4,
                    bicg ? 1 : g_cheb_degree, g_cheb_ratio, c->d.ell_w, c->d.ell_col, c->d.ell_val,
-                   c->d.red32, (c->d.ell_col && big) ? 1 : 0, g_mixed_scheme, g_rel_delta_pm * 1e-3,
-                   (!bicg && g_neighbor_sync) ? c->d.pass_flags : nullptr};
+                   c->d.red32, (c->d.ell_col && big) ? 1 : 0, g_rel_delta_pm * 1e-3, c->d.ell_ld, 0,
+                   c->d.ell_val64};
 }
 
 // The same solves in FP64 throughout (MGPU_PREC_FP64_POLY): PCG keeps one
@@ -225,8 +225,7 @@ MixedArgsT<double> poly64_args(const MgpuCase* c, bool bicg) {
   const bool big = (double)c->d.N * (16.0 * c->d.ell_w + 8.0 * 10) > g_prefetch_mb * 1048576.0;
   return MixedArgsT<double>{c->d.a64, c->d.dinv64, c->d.w64, 0.0, bicg ? 1 : g_cheb_degree, g_cheb_ratio,
                             c->d.ell_w, c->d.ell_col, c->d.ell_val64, c->d.red32,
-                            (c->d.ell_col && big) ? 1 : 0, 1, 0.0,
-                            (!bicg && g_neighbor_sync) ? c->d.pass_flags : nullptr};
+                            (c->d.ell_col && big) ? 1 : 0, 0.0, c->d.ell_ld};
 }
 
 // factor (if needed) + solve; precond 0 ILU0, 1 Jacobi, 2 IC0. The mixed form
@@ -580,8 +579,7 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
        ((e = c->alloc(d.a32, d.nnz)) || (e = c->alloc(d.dinv32, N)) || (e = c->alloc(d.w32, 10 * N)))) ||
       (ctrl->precision == MGPU_PREC_FP64_POLY &&
        ((e = c->alloc(d.a64, d.nnz)) || (e = c->alloc(d.dinv64, N)) || (e = c->alloc(d.w64, 10 * N)))) ||
-      (poly && ((e = c->alloc(d.red32, (size_t)mixed_red_words(N))) ||
-                (e = c->alloc(d.pass_flags, (size_t)kMaxPassFlags)))) ||
+      (poly && (e = c->alloc(d.red32, (size_t)mixed_red_words(N)))) ||
       (e = c->alloc(d.partials, 4 * 4096)) ||
       (e = c->alloc(d.bar, 1)) || (e = c->alloc(d.ferr, 1)) || (e = c->alloc(d.st, 1)) ||
       (e = c->alloc(d.ramp, 2)))
@@ -594,13 +592,21 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
   if (poly) {
     // column-major ELL copy of the pattern for the polynomial forms' SpMV (rows of at most 8 entries)
     int w = 0, *ell = nullptr;
-    if ((e = device_ell(d.N, d.row_ptr, d.col, 8, w, ell, keep, c->stream))) return fail(e);
+    long ld = 0;
+    if ((e = device_ell(d.N, d.row_ptr, d.col, 8, w, ld, ell, keep, c->stream))) return fail(e);
     if (ell) {
       d.ell_col = ell;
-      if (ctrl->precision == MGPU_PREC_MIXED) e = c->alloc(d.ell_val, (size_t)w * N);
-      else e = c->alloc(d.ell_val64, (size_t)w * N);
-      if (e) return fail(e);
+      // values zero in the padding rows
+      // FP64 values in both forms (the mixed form's conjugate-gradient
+      // product, the polynomial form's every product), FP32 in the mixed form
+      if ((e = c->alloc(d.ell_val64, (size_t)w * ld))) return fail(e);
+      MGPU_CUDA(cudaMemsetAsync(d.ell_val64, 0, sizeof(double) * (size_t)w * ld, c->stream));
+      if (ctrl->precision == MGPU_PREC_MIXED) {
+        if ((e = c->alloc(d.ell_val, (size_t)w * ld))) return fail(e);
+        MGPU_CUDA(cudaMemsetAsync(d.ell_val, 0, sizeof(float) * (size_t)w * ld, c->stream));
+      }
       d.ell_w = w;
+      d.ell_ld = (int)ld;
     }
   }
   // geometry (device), scratch for the node arrays and provisional centres

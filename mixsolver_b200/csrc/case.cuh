@@ -79,24 +79,25 @@ struct MixedArgsT {
   int cheb_k;        // Chebyshev-Jacobi degree of the pressure preconditioner (<= 1: Jacobi)
   double cheb_ratio; // lambda_max / lambda_min of the Chebyshev interval
   int ell_w;         // ELL width (max entries per row) when ell_col is set
-  const int* ell_col;  // column-major ELL columns, W*N (padding: the row itself)
+  const int* ell_col;  // column-major ELL columns, W*ell_ld (padding: the row itself)
   V* ell_val;          // values in the same layout (padding: 0)
   double* red;         // chunk reduction partials: mixed_red_words(N) doubles
   int pf;              // 1: each SpMV tile prefetches the next tile's ELL entries into L2
-  int reliable;        // PCG: 1 reliable updates (one Krylov stream, FP64 x), 0 restarted refinement
-  double rel_delta;    // reliable updates: replace the recursive residual once its norm fell by this factor
-  // single-system PCG launches: one pass counter per block (zeroed before the
-  // launch). Each block then owns a contiguous range of rows, and a Chebyshev
-  // pass waits only for the blocks whose rows its rows read instead of the
-  // whole grid. Null: grid-stride rows and grid barriers (batched lanes).
-  unsigned* flags;
-  int flexible;  // reliable PCG with a Chebyshev preconditioner: Polak-Ribiere (flexible) beta
+  double rel_delta;    // PCG reliable updates: replace the recursive residual once its norm fell by this factor
+  int ell_ld;    // leading dimension of the ELL arrays: N rounded up to a multiple of 4
+  // single-system grid launches: chunk-sum slots per sum a block keeps in its
+  // dynamic shared memory (set at launch; 0 elsewhere)
+  int cp_slots;
+  // the mixed form's PCG (V = float): the FP64 values in the ELL layout, for
+  // the FP64 conjugate-gradient product q = A p (null: the CSR values)
+  double* ell64;
 };
 using MixedArgs = MixedArgsT<float>;
 
-// Device bytes a mixed solve streams per row: ELL columns and FP32 values,
-// the seven FP32 work vectors, x, b, r and the inverse diagonal.
-inline double mixed_row_bytes(int ell_w) { return 8.0 * ell_w + 4.0 * 7 + 8.0 * 3 + 4.0; }
+// Device bytes a mixed solve keeps live per row: ELL columns, FP32 and FP64
+// values, the FP32 work vectors and inverse diagonal, and the FP64 vectors
+// (x, b, the residual, two search directions, q).
+inline double mixed_row_bytes(int ell_w) { return 16.0 * ell_w + 4.0 * 5 + 8.0 * 6; }
 
 // The mixed-precision solves reduce over fixed row chunks (32 rows) and
 // super-chunks (256 rows), so their results do not depend on how rows are
@@ -111,7 +112,6 @@ inline double mixed_row_bytes(int ell_w) { return 8.0 * ell_w + 4.0 * 7 + 8.0 * 
 constexpr int kMixedMaxRows = 1 << MGPU_MIXED_MAX_ROWS_LOG2;
 constexpr int kSuperRows = 256;
 constexpr int kBlockMaxRows = MGPU_BLOCK_MAX_ROWS;  // rows one block of a mixed solve may hold
-constexpr int kMaxPassFlags = 4096;                 // blocks of a neighbour-synchronised launch
 inline long mixed_red_words(long n) { return 4l * ((n + kSuperRows - 1) / kSuperRows); }
 
 // One system of a batched solve.
@@ -181,8 +181,8 @@ struct DeviceCase {
   float* ell_val = nullptr;
   double *a64 = nullptr, *dinv64 = nullptr, *w64 = nullptr, *ell_val64 = nullptr;  // FP64 polynomial form
   int ell_w = 0;
+  int ell_ld = 0;  // ELL leading dimension: N rounded up to a multiple of 4
   double* red32 = nullptr;  // chunk reduction partials of the mixed-precision solves
-  unsigned* pass_flags = nullptr;  // per-block pass counters of the neighbour sync (kMaxPassFlags)
   // Krylov work
   double *kw = nullptr;  // 10*N
   double* partials = nullptr;

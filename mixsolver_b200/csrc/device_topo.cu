@@ -368,12 +368,18 @@ __global__ void k_row_width(int N, const int* __restrict__ rp, int* w) {
   if (i < N) atomicMax(w, rp[i + 1] - rp[i]);
 }
 
-// column-major ELL pattern: entry t of row i at t * N + i, padding the row itself
-__global__ void k_ell_pattern(int N, int W, const int* __restrict__ rp, const int* __restrict__ col, int* ell) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
+// column-major ELL pattern: entry t of row i at t * ld + i, padding the row
+// itself (rows ld > i >= N: the last row)
+__global__ void k_ell_pattern(int N, int W, long ld, const int* __restrict__ rp, const int* __restrict__ col,
+                              int* ell) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= ld) return;
+  if (i >= N) {
+    for (int t = 0; t < W; ++t) ell[t * ld + i] = N - 1;
+    return;
+  }
   const int b = rp[i], e = rp[i + 1];
-  for (int t = 0; t < W; ++t) ell[(long)t * N + i] = b + t < e ? col[b + t] : i;
+  for (int t = 0; t < W; ++t) ell[t * ld + i] = b + t < e ? col[b + t] : (int)i;
 }
 
 __global__ void k_bface_count(int N, const int* __restrict__ cf_ptr, const int* __restrict__ cf,
@@ -483,8 +489,8 @@ int device_topology(int N, int F, const int* c0, const int* c1, DeviceTopo& t, c
   return 0;
 }
 
-int device_ell(int N, const int* rp, const int* col, int max_width, int& W, int*& ell, const TopoAlloc& alloc,
-               cudaStream_t s) {
+int device_ell(int N, const int* rp, const int* col, int max_width, int& W, long& ld, int*& ell,
+               const TopoAlloc& alloc, cudaStream_t s) {
   Tmp T(s);
   int* w = nullptr;
   DT_TRY(T.get(w, 1));
@@ -493,9 +499,10 @@ int device_ell(int N, const int* rp, const int* col, int max_width, int& W, int*
   MGPU_LAUNCH_CHECK("k_row_width");
   DT_TRY(read_int(w, W, s));
   ell = nullptr;
+  ld = ((long)N + 3) / 4 * 4;  // each column starts on a 16-byte boundary
   if (W > max_width) return 0;
-  DT_TRY(alloc(ell, (size_t)W * N));
-  k_ell_pattern<<<ceil_div(N, 256), 256, 0, s>>>(N, W, rp, col, ell);
+  DT_TRY(alloc(ell, (size_t)W * ld));
+  k_ell_pattern<<<ceil_div(ld, 256), 256, 0, s>>>(N, W, ld, rp, col, ell);
   MGPU_LAUNCH_CHECK("k_ell_pattern");
   return 0;
 }

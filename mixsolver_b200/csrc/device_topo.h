@@ -27,9 +27,10 @@ using TopoAlloc = std::function<int(int*&, size_t)>;
 int device_topology(int N, int F, const int* c0, const int* c1, DeviceTopo& t, const TopoAlloc& alloc,
                     cudaStream_t s);
 // Widest row W of the pattern and, when W <= max_width, its column-major ELL
-// copy (entry t of row i at t * N + i, padding the row itself).
-int device_ell(int N, const int* row_ptr, const int* col, int max_width, int& W, int*& ell, const TopoAlloc& alloc,
-               cudaStream_t s);
+// copy: entry t of row i at t * ld + i with ld = N rounded up to a multiple of
+// 4 (every column starts 16-byte aligned), padding the row itself.
+int device_ell(int N, const int* row_ptr, const int* col, int max_width, int& W, long& ld, int*& ell,
+               const TopoAlloc& alloc, cudaStream_t s);
 // Each cell's boundary faces that carry a group, in the order of its face list.
 int device_boundary_lists(int N, const int* cf_ptr, const int* cf, const int* c1, const int* fgrp, int*& bf_ptr,
                           int*& bf, const TopoAlloc& alloc, cudaStream_t s);

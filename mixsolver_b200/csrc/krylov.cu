@@ -50,11 +50,8 @@ int g_batch_reserve = 0;  // block slots batched launches leave to other streams
 int g_prefetch_mb = 96;   // mixed systems whose streamed bytes exceed this prefetch into L2
 int prewarm_streams(int n);  // case.cu
 double g_cheb_ratio = 1000.0; // and the ratio lambda_max / lambda_min of its interval
-int g_mixed_scheme = 1;   // mixed PCG: 1 reliable updates, 0 restarted refinement
 int g_rel_delta_pm = 100; // reliable updates: residual replaced after a fall by this many thousandths
 unsigned g_spin_limit = 0; // polls before a bounded barrier wait gives up (0: kSpinLimit, ~2 s)
-int g_neighbor_sync = 0;   // single-system mixed PCG: Chebyshev passes wait for neighbour blocks only
-int g_pcg_flexible = 0;    // reliable mixed PCG: flexible (Polak-Ribiere) beta
 int g_mixed_occ = 2;          // single-system mixed solves on a grid: resident blocks per SM (2, 3 or 4)
 namespace {
 
@@ -756,16 +753,10 @@ int set_tuning(const char* key, int value) {
     g_batch_reserve = value;
   } else if (k == "l2_prefetch_mb" && value >= 0) {
     g_prefetch_mb = value;
-  } else if (k == "mixed_scheme" && (value == 0 || value == 1)) {
-    g_mixed_scheme = value;
   } else if (k == "reliable_delta_permille" && value >= 1 && value <= 900) {
     g_rel_delta_pm = value;
   } else if (k == "mixed_blocks_per_sm" && value >= 2 && value <= 4) {
     g_mixed_occ = value;
-  } else if (k == "pcg_flexible" && (value == 0 || value == 1)) {
-    g_pcg_flexible = value;
-  } else if (k == "neighbor_sync" && (value == 0 || value == 1)) {
-    g_neighbor_sync = value;
   } else if (k == "spin_limit" && value >= 0) {
     g_spin_limit = (unsigned)value;
   } else if (k == "stream_pool" && value >= 0 && value <= 1024) {

@@ -21,13 +21,13 @@ namespace {
 template <bool L1, int ELL, int OCC = 2>
 __global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : OCC) k_pcg_mixed(KrylovArgs a, MixedArgs m) {
   VGrid g = whole_grid(a.bar, a.partials);
-  pcg_mixed_body<float, L1, ELL>(a, m, g);
+  pcg_mixed_body<float, L1, ELL, !L1>(a, m, g);
 }
 
 template <bool L1, int ELL, int OCC = 2>
 __global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : OCC) k_bicgstab_mixed(KrylovArgs a, MixedArgs m) {
   VGrid g = whole_grid(a.bar, a.partials);
-  bicgstab_mixed_body<float, L1, ELL>(a, m, g);
+  bicgstab_mixed_body<float, L1, ELL, !L1>(a, m, g);
 }
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {

@@ -48,134 +48,34 @@ __device__ __forceinline__ double vfma(double a, double b, double c) { return fm
 // rows and layout-independent sums
 // ---------------------------------------------------------------------------
 
-// The rows of one block, in tiles of blockDim.x rows. Grid-stride layout
-// (batched lanes): tile t of the group at rows [t * blockDim.x, (t + 1) *
-// blockDim.x) for t = rank, rank + nb, ..., so all blocks stream the same
-// narrow window of every array at a time. Contiguous layout (single-system
-// PCG with neighbour sync): block rank owns rows [rank * len, (rank + 1) *
-// len), len a multiple of blockDim.x, so with a banded (RCM) order its SpMV
-// reads the rows of a few neighbouring blocks only. Tiles are whole
-// super-chunks either way (blockDim.x is a multiple of kSuperRows), so the
-// layout-independent sums see the same super-chunks.
+// The rows of one block, in tiles of blockDim.x rows: tile t of the group at
+// rows [t * blockDim.x, (t + 1) * blockDim.x) for t = rank, rank + nb, ...,
+// so all blocks stream the same narrow window of every array at a time.
+// Tiles are whole super-chunks (blockDim.x is a multiple of kSuperRows), so
+// the layout-independent sums see the same super-chunks on any grid.
 struct Rows {
   int start;   // first row of this block's first tile
   int stride;  // rows between its consecutive tiles
-  int n;       // end of the rows this block may own (exclusive)
-  int len;     // contiguous layout: rows per block (0: grid-stride)
+  int n;       // end of the rows (exclusive)
 };
-
-__device__ __forceinline__ int contiguous_len(int n, const VGrid& g) {
-  const int bd = blockDim.x;
-  return (int)((((long)n + g.nb - 1) / g.nb + bd - 1) / bd * bd);
-}
 
 // A block holds at most kBlockMaxRows rows (the chunk sums of its tiles live
 // in shared memory); launches and lane plans size their groups accordingly,
 // and a group too small for its system refuses it (fits_group).
-__device__ __forceinline__ bool fits_group(int n, const VGrid& g, bool contiguous = false) {
-  if (contiguous) return contiguous_len(n, g) <= kBlockMaxRows;
+__device__ __forceinline__ bool fits_group(int n, const VGrid& g) {
   const long stride = (long)g.nb * blockDim.x;
   return ((n + stride - 1) / stride) * (long)blockDim.x <= kBlockMaxRows;
 }
 
-__device__ __forceinline__ Rows block_rows(int n, const VGrid& g, bool contiguous = false) {
-  if (contiguous) {
-    const int len = contiguous_len(n, g);
-    const long start = (long)g.rank * len;
-    return Rows{(int)min(start, (long)n), (int)blockDim.x, (int)min(start + len, (long)n), len};
-  }
-  return Rows{g.rank * (int)blockDim.x, g.nb * (int)blockDim.x, n, 0};
+// The chunk-sum slots the launch gave a block (DYN kernels) hold its tiles.
+__device__ __forceinline__ bool fits_slots(int n, const VGrid& g, int cp_slots) {
+  const long bd = blockDim.x;
+  const long tiles = ((long)n + g.nb * bd - 1) / (g.nb * bd);
+  return tiles * (bd / 32) <= cp_slots;
 }
 
-// ---------------------------------------------------------------------------
-// neighbour sync of the Chebyshev passes
-// ---------------------------------------------------------------------------
-
-// Blocks [s_dep[0], s_dep[1]] own the rows this block's SpMV reads (its own
-// included); s_nsync: 1 when every block's range fits one poll per thread and
-// the passes use the neighbour sync, 0 for grid barriers.
-__shared__ int s_dep[2];
-__shared__ int s_nsync;
-
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-// Decide between neighbour sync and grid barriers for this solve: every block
-// forms the block range of the columns its rows touch (the CSR pattern, whose
-// ELL copy adds only the row itself), and the widest range over the grid
-// decides for all blocks alike. False when a barrier wait ran out.
-template <bool L1>
-__device__ bool setup_pass_sync(const KrylovArgs& a, const unsigned* flags, VGrid& g, const Rows& rows) {
-  if (threadIdx.x == 0) {
-    s_dep[0] = s_dep[1] = g.rank;
-    s_nsync = 0;
-  }
-  if (!flags || g.nb == 1 || rows.len == 0) {
-    __syncthreads();
-    return true;
-  }
-  int cmin = 0x7fffffff, cmax = -1;
-  for (int i = rows.start + threadIdx.x; i < rows.n; i += rows.stride)
-    for (int k = a.row_ptr[i]; k < a.row_ptr[i + 1]; ++k) {
-      const int c = a.col[k];
-      cmin = min(cmin, c);
-      cmax = max(cmax, c);
-    }
-  for (int o = 16; o > 0; o >>= 1) {
-    cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
-    cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
-  }
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0 && cmax >= 0) {
-    atomicMin(&s_dep[0], cmin / rows.len);
-    atomicMax(&s_dep[1], cmax / rows.len);
-  }
-  __syncthreads();
-  double width = (double)(s_dep[1] - s_dep[0] + 1);
-  if (!vg_max<L1>(width, g, a.st)) return false;
-  if (threadIdx.x == 0) s_nsync = width <= (double)blockDim.x ? 1 : 0;
-  __syncthreads();
-  return true;
-}
-
-// The barrier between two Chebyshev passes. Neighbour sync: the block
-// publishes that it finished pass `pass` (a release store of its counter after
-// __syncthreads), then thread t waits (acquire loads) for block s_dep[0] + t
-// of its range to reach the same pass. A block's next pass reads only rows of
-// those blocks (read after write), and it overwrites only its own rows of the
-// vector the previous pass read, which only those blocks read (the pattern is
-// symmetric: write after read). Bounded like the grid barrier.
-__device__ bool pass_sync(unsigned* flags, VGrid& g, DevStatus* st, unsigned& pass) {
-  if (!s_nsync) return vg_sync(g, st);
-  ++pass;
-  __syncthreads();
-  if (threadIdx.x == 0) st_release_u32(flags + g.rank, pass);
-  const int k = s_dep[0] + (int)threadIdx.x;
-  int ok = 1;
-  if (k <= s_dep[1] && k != g.rank) {
-    const unsigned limit = (st && st->spin_limit) ? st->spin_limit : kSpinLimit;
-    unsigned spins = 0;
-    while (ld_acquire_u32(flags + k) < pass) {
-      ++spins;
-      if (spins > 64u) __nanosleep(32);
-      if ((spins & 4095u) == 0 && ld_acquire_i32(&st->timeout) != 0) {
-        ok = 0;
-        break;
-      }
-      if (spins >= limit) {
-        atomicExch(&st->timeout, 1);
-        ok = 0;
-        break;
-      }
-    }
-  }
-  return __syncthreads_and(ok) != 0;
+__device__ __forceinline__ Rows block_rows(int n, const VGrid& g) {
+  return Rows{g.rank * (int)blockDim.x, g.nb * (int)blockDim.x, n};
 }
 
 // Reduction state of one system. Chunk sums (a fixed butterfly over the 32
@@ -186,19 +86,32 @@ __device__ bool pass_sync(unsigned* flags, VGrid& g, DevStatus* st, unsigned& pa
 struct Red {
   double* base;  // 2 halves x 2 sums x nsc super-chunk sums
   int nsc, half;
+  double* cp;    // the block's chunk sums in shared memory: sum q of chunk j at cp[q * cps + j]
+  int cps;
   __device__ double* sp() const { return base + (half ? 2l * nsc : 0); }
 };
-
-template <typename V>
-__device__ __forceinline__ Red make_red(const MixedArgsT<V>& m, int n) {
-  return Red{m.red, (n + kSuperRows - 1) / kSuperRows, 0};
-}
 
 // per block: chunk sums (rows of a block <= kBlockMaxRows) and level sums
 constexpr int kBlockMaxChunks = kBlockMaxRows / 32;
 constexpr int kMaxGroups = (kMixedMaxRows / kSuperRows + 255) / 256;  // groups of 256 super-chunks
 __shared__ double s_cp[2][kBlockMaxChunks];
 __shared__ double lvg[2][kMaxGroups];
+
+// The dynamic shared memory of a single-system grid launch: the block's chunk
+// sums, 2 x MixedArgsT::cp_slots doubles, sized at launch for the rows the
+// block owns.
+extern __shared__ __align__(16) unsigned char mixed_dyn[];
+
+// DYN: the chunk sums live in the launch's dynamic shared memory (single-system
+// grid kernels); otherwise in the static array sized for kBlockMaxRows rows
+// (single-block kernels, batched lanes).
+template <typename V, bool DYN>
+__device__ __forceinline__ Red make_red(const MixedArgsT<V>& m, int n) {
+  if constexpr (DYN)
+    return Red{m.red, (n + kSuperRows - 1) / kSuperRows, 0, reinterpret_cast<double*>(mixed_dyn), m.cp_slots};
+  else
+    return Red{m.red, (n + kSuperRows - 1) / kSuperRows, 0, &s_cp[0][0], kBlockMaxChunks};
+}
 
 // Sum this thread's row values c[q] (zero for rows past n) over the warp's
 // 32 rows of the tile starting at base into the tile's chunk slot. Every lane
@@ -211,7 +124,7 @@ __device__ __forceinline__ void red_put(const Red& R, const Rows& rows, int base
   if ((threadIdx.x & 31) == 0 && base < rows.n) {
     const int slot = ((base - rows.start) / rows.stride) * (blockDim.x >> 5) + (threadIdx.x >> 5);
 #pragma unroll
-    for (int q = 0; q < NQ; ++q) s_cp[q][slot] = s[q];
+    for (int q = 0; q < NQ; ++q) R.cp[q * R.cps + slot] = s[q];
   }
 }
 
@@ -230,7 +143,7 @@ __device__ __forceinline__ bool red_total(Red& R, const Rows& rows, VGrid& g, De
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   double* sp = R.sp();
   const int nsc = R.nsc;
-  __syncthreads();  // this block's chunk sums are in s_cp
+  __syncthreads();  // this block's chunk sums are in R.cp
   const int ntb = rows.start < rows.n ? (rows.n - rows.start + rows.stride - 1) / rows.stride : 0;
   const int per_tile = blockDim.x / kSuperRows;
   for (int pr = threadIdx.x; pr < ntb * per_tile; pr += blockDim.x) {
@@ -238,9 +151,10 @@ __device__ __forceinline__ bool red_total(Red& R, const Rows& rows, VGrid& g, De
     if (sc >= nsc) continue;  // a super-chunk past the last row
 #pragma unroll
     for (int q = 0; q < NQ; ++q) {
-      double acc = s_cp[q][pr * kChunks];
+      const double* cq = R.cp + q * R.cps + pr * kChunks;
+      double acc = cq[0];
 #pragma unroll
-      for (int j = 1; j < kChunks; ++j) acc = acc + s_cp[q][pr * kChunks + j];
+      for (int j = 1; j < kChunks; ++j) acc = acc + cq[j];
       sp[(long)q * nsc + sc] = acc;
     }
   }
@@ -273,7 +187,7 @@ __device__ __forceinline__ bool red_total(Red& R, const Rows& rows, VGrid& g, De
     for (int k = 1; k < ng; ++k) acc = acc + lvg[q][k];
     out[q] = acc;
   }
-  __syncthreads();  // s_cp and lvg are reused by the next reduction
+  __syncthreads();  // the chunk sums and lvg are reused by the next reduction
   R.half ^= 1;
   return true;
 }
@@ -307,37 +221,8 @@ __device__ __forceinline__ V spmv32_csr(const int* __restrict__ rp, const int* _
   return acc;
 }
 
-// The same product from the column-major ELL copy: entry t of row i sits at
-// t*n + i, so a warp's loads of one t are contiguous and no row pointer is
-// read. Padding entries have value 0 and the row's own column.
-template <typename V, bool L1>
-__device__ __forceinline__ V spmv32_ell(const MixedArgsT<V>& m, const V* x, int i, int n) {
-  constexpr int WMAX = 8;
-  const int W = m.ell_w;
-  V v[WMAX], xv[WMAX];
-  int c[WMAX];
-#pragma unroll
-  for (int t = 0; t < WMAX; ++t)
-    if (t < W) {
-      c[t] = m.ell_col[(long)t * n + i];
-      v[t] = m.ell_val[(long)t * n + i];
-    }
-#pragma unroll
-  for (int t = 0; t < WMAX; ++t)
-    if (t < W) xv[t] = ldv(&x[c[t]]);
-  V acc = V(0);
-#pragma unroll
-  for (int t = 0; t < WMAX; ++t)
-    if (t < W) acc = vfma(v[t], xv[t], acc);
-  return acc;
-}
-
-template <typename V, bool L1, int ELL>
-__device__ __forceinline__ V spmv32(const KrylovArgs& a, const MixedArgsT<V>& m, const V* x, int i) {
-  if constexpr (ELL)
-    return spmv32_ell<V, L1>(m, x, i, a.n);
-  else
-    return spmv32_csr<V, L1, 8>(a.row_ptr, a.col, m.a32, x, i);
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
 // kRows rows per thread in the SpMV passes: every row's loads are issued
@@ -366,15 +251,13 @@ struct Sp32 {
   const V* __restrict__ a32;
   const V* __restrict__ dinv;
   int pf;  // rows from a tile to the tile whose ELL entries it prefetches into L2 (0: none)
+  long ld; // ELL leading dimension
 };
 
 template <typename V>
 __device__ __forceinline__ Sp32<V> sp32_of(const KrylovArgs& a, const MixedArgsT<V>& m, const Rows& rows) {
-  return Sp32<V>{a.n, m.ell_w, m.ell_col, m.ell_val, a.row_ptr, a.col, m.a32, m.dinv, m.pf * kRows * rows.stride};
-}
-
-__device__ __forceinline__ void prefetch_l2(const void* p) {
-  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+  return Sp32<V>{a.n,    m.ell_w, m.ell_col, m.ell_val, a.row_ptr, a.col, m.a32, m.dinv,
+                 m.pf * kRows * rows.stride, m.ell_ld};
 }
 
 template <typename V, bool L1, int ELL, bool FULL>
@@ -385,7 +268,7 @@ __device__ __forceinline__ void spmv32_rows(const Sp32<V>& S, const V* x, const 
   for (int r = 0; r < kRows; ++r) in[r] = FULL || in0[r];
   if constexpr (ELL) {
     constexpr int WMAX = 8;
-    const int W = S.w, n = S.n;
+    const int W = S.w;
     V v[kRows][WMAX], xv[kRows][WMAX];
     int c[kRows][WMAX];
 #pragma unroll
@@ -393,8 +276,8 @@ __device__ __forceinline__ void spmv32_rows(const Sp32<V>& S, const V* x, const 
 #pragma unroll
       for (int t = 0; t < WMAX; ++t)
         if (t < W && in[r]) {
-          c[r][t] = S.ecol[(long)t * n + i[r]];
-          v[r][t] = S.eval[(long)t * n + i[r]];
+          c[r][t] = S.ecol[(long)t * S.ld + i[r]];
+          v[r][t] = S.eval[(long)t * S.ld + i[r]];
         }
     if constexpr (ELL == 2) {
       // the same rows of this block's next tile: DRAM -> L2 while this tile's
@@ -402,12 +285,12 @@ __device__ __forceinline__ void spmv32_rows(const Sp32<V>& S, const V* x, const 
 #pragma unroll
       for (int r = 0; r < kRows; ++r) {
         const int j = i[r] + S.pf;
-        if (j < n) {
+        if (j < S.n) {
 #pragma unroll
           for (int t = 0; t < WMAX; ++t)
             if (t < W) {
-              prefetch_l2(S.ecol + (long)t * n + j);
-              prefetch_l2(S.eval + (long)t * n + j);
+              prefetch_l2(S.ecol + (long)t * S.ld + j);
+              prefetch_l2(S.eval + (long)t * S.ld + j);
             }
         }
       }
@@ -442,7 +325,7 @@ __device__ __forceinline__ void spmv32_rows_dir(const Sp32<V>& S, const V* z, co
   for (int r = 0; r < kRows; ++r) in[r] = FULL || in0[r];
   if constexpr (ELL) {
     constexpr int WMAX = 8;
-    const int W = S.w, n = S.n;
+    const int W = S.w;
     V v[kRows][WMAX], xv[kRows][WMAX];
     int c[kRows][WMAX];
 #pragma unroll
@@ -450,19 +333,21 @@ __device__ __forceinline__ void spmv32_rows_dir(const Sp32<V>& S, const V* z, co
 #pragma unroll
       for (int t = 0; t < WMAX; ++t)
         if (t < W && in[r]) {
-          c[r][t] = S.ecol[(long)t * n + i[r]];
-          v[r][t] = S.eval[(long)t * n + i[r]];
+          c[r][t] = S.ecol[(long)t * S.ld + i[r]];
+          v[r][t] = S.eval[(long)t * S.ld + i[r]];
         }
     if constexpr (ELL == 2) {
+      // the same rows of this block's next tile: DRAM -> L2 while this tile's
+      // gathers wait (no registers held)
 #pragma unroll
       for (int r = 0; r < kRows; ++r) {
         const int j = i[r] + S.pf;
-        if (j < n) {
+        if (j < S.n) {
 #pragma unroll
           for (int t = 0; t < WMAX; ++t)
             if (t < W) {
-              prefetch_l2(S.ecol + (long)t * n + j);
-              prefetch_l2(S.eval + (long)t * n + j);
+              prefetch_l2(S.ecol + (long)t * S.ld + j);
+              prefetch_l2(S.eval + (long)t * S.ld + j);
             }
         }
       }
@@ -550,7 +435,6 @@ __device__ void write_result_m(const KrylovArgs& a, const VGrid& g, int it, doub
 template <typename V, bool L1>
 __device__ bool prologue(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid& g, Red& R, const Rows& rows, double& bnrm,
                          bool& diag_bad) {
-  const int n = a.n;
   MGPU_TILES(rows, base) {
     const int i = base + threadIdx.x;
     double c[2] = {0.0, 0.0};
@@ -558,7 +442,9 @@ __device__ bool prologue(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid& g, 
       const int rb = a.row_ptr[i], re = a.row_ptr[i + 1];
       for (int k = rb; k < re; ++k) m.a32[k] = (V)a.aval[k];
       if (m.ell_col)
-        for (int t = 0; t < m.ell_w; ++t) m.ell_val[(long)t * n + i] = t < re - rb ? (V)a.aval[rb + t] : V(0);
+        for (int t = 0; t < m.ell_w; ++t) m.ell_val[(long)t * m.ell_ld + i] = t < re - rb ? (V)a.aval[rb + t] : V(0);
+      if (m.ell64)
+        for (int t = 0; t < m.ell_w; ++t) m.ell64[(long)t * m.ell_ld + i] = t < re - rb ? a.aval[rb + t] : 0.0;
       if (a.zero_x) a.x[i] = 0.0;
       const double dg = a.aval[a.diag[i]];
       if (fabs(dg) < DTINY) c[1] = 1.0;
@@ -604,12 +490,13 @@ __device__ bool update_x(const KrylovArgs& a, const VGrid& g, const Rows& rows, 
 // [lmax/ratio, lmax]: k-1 SpMV passes, one barrier each. On entry z0 = d =
 // D^-1 rr / theta (written by the caller's pass, followed by a barrier). The
 // result lands in zout (z0 or z1, ping-pong); the last pass also sums rr.z and
-// rr.rr (r2.z instead of rr.rr when r2 is given), reduced before returning.
+// rr.rr (r64.z in place of rr.z when the FP64 residual r64 is given),
+// reduced before returning.
 template <typename V, bool L1, int ELL>
 __device__ __forceinline__ bool cheb_apply(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid& g, Red& R,
                                            const Rows& rows, const V* rr, V* dch, V* z0, V* z1,
-                                           double lmax, V*& zout, double (&red)[2], unsigned& pass,
-                                           const V* r2 = nullptr) {
+                                           double lmax, V*& zout, double (&red)[2],
+                                           const double* r64 = nullptr) {
   const Sp32<V> S = sp32_of(a, m, rows);
   const double lmin = lmax / m.cheb_ratio;
   const double th = 0.5 * (lmax + lmin), de = 0.5 * (lmax - lmin), sg = th / de;
@@ -636,8 +523,8 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
             const V zi = zc[i] + dn;
             zn[i] = zi;
             if (last) {
-              c[0] = (double)rr[i] * (double)zi;
-              c[1] = r2 ? (double)r2[i] * (double)zi : (double)rr[i] * (double)rr[i];
+              c[0] = r64 ? r64[i] * (double)zi : (double)rr[i] * (double)zi;
+              c[1] = (double)rr[i] * (double)rr[i];
             }
           }
           if (last) red_put<2>(R, rows, base + r * rows.stride, c);
@@ -646,7 +533,7 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
     }
     if (last) {
       if (!red_total<2, L1>(R, rows, g, a.st, red)) return false;
-    } else if (!pass_sync(m.flags, g, a.st, pass)) {
+    } else if (!vg_sync(g, a.st)) {
       return false;
     }
     V* t = zc;
@@ -659,33 +546,6 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
 }
 
 // The SpMV passes of the Krylov loops.
-
-// p := z + beta p, q := A z + beta q (p := z, q := A z when first); p.q
-template <typename V, bool L1, int ELL>
-__device__ __forceinline__ void pcg_fused_pass(const KrylovArgs& a, const MixedArgsT<V>& m, const Red& R,
-                                               const Rows& rows, const V* z, V* p, V* q, V beta,
-                                               bool first) {
-  const Sp32<V> S = sp32_of(a, m, rows);
-  MGPU_STEPS(rows, base) {
-    MGPU_STEP_ROWS(rows, base, ii, in);
-    MGPU_SPLIT_FULL(rows, base, FULL, {
-      V az[kRows];
-      spmv32_rows<V, L1, ELL, FULL>(S, z, ii, in, az);
-_Pragma("unroll") for (int r = 0; r < kRows; ++r) {
-        const int i = ii[r];
-        double c[1] = {0.0};
-        if (FULL || in[r]) {
-          const V pi = first ? z[i] : vfma(beta, p[i], z[i]);
-          const V qi = first ? az[r] : vfma(beta, q[i], az[r]);
-          p[i] = pi;
-          q[i] = qi;
-          c[0] = (double)pi * (double)qi;
-        }
-        red_put<1>(R, rows, base + r * rows.stride, c);
-      }
-    })
-  }
-}
 
 // pnew := z + beta pold and q := A pnew in one pass (pnew := z, q := A z when
 // first), q formed directly from z and pold rather than recurred; pnew.q
@@ -779,14 +639,12 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
 // (one grid barrier), which is also the barrier before the next SpMV pass.
 template <typename V, bool L1, int ELL>
 __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid& g, Red& R, const Rows& rows,
-                             double bnrm, double rnorm0, double lmax, V inv_th, unsigned& pass) {
+                             double bnrm, double rnorm0, double lmax, V inv_th) {
   const int n = a.n;
   const V* __restrict__ dinv = m.dinv;
   V *rr = m.w32, *zA = m.w32 + n, *p = m.w32 + 2l * n, *q = m.w32 + 3l * n;
   V *dch = m.w32 + 5l * n, *zB = m.w32 + 6l * n, *pn = m.w32 + 7l * n;  // p double-buffered
-  V* rold = m.w32 + 4l * n;  // flexible beta: the residual before the update
   const bool cheb = m.cheb_k > 1;
-  const bool flex = cheb && m.flexible;
   const double sc = 1.0 / rnorm0;
   const double stop = a.tol * bnrm * sc;  // |rr| at which the estimate reaches tol
   const double stop2 = stop * stop, delta2 = m.rel_delta * m.rel_delta;
@@ -811,14 +669,10 @@ __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid&
   bool first = true;
   while (true) {
     V* z = zA;
-    double rold_z = 0.0;
     if (cheb) {
-      double red[2];  // (rr.z, rr.rr), flexible: (rr.z, rold.z)
-      if (!cheb_apply<V, L1, ELL>(a, m, g, R, rows, rr, dch, zA, zB, lmax, z, red, pass,
-                                  flex && !first ? rold : nullptr))
-        return;
+      double red[2];  // (rr.z, rr.rr)
+      if (!cheb_apply<V, L1, ELL>(a, m, g, R, rows, rr, dch, zA, zB, lmax, z, red)) return;
       rzn = red[0];
-      rold_z = red[1];
     }
     V beta = V(0);
     if (!first) {
@@ -826,10 +680,7 @@ __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid&
         ierr = 2;
         break;
       }
-      // flexible (Polak-Ribiere) beta = z.(r - r_old) / rz_old: stays a
-      // descent direction when the FP32 polynomial differs slightly from
-      // one application to the next
-      beta = (V)((flex ? rzn - rold_z : rzn) / rz);
+      beta = (V)(rzn / rz);
     }
     rz = rzn;
     ++total;
@@ -855,7 +706,6 @@ __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid&
       double c[2] = {0.0, 0.0};
       if (i < rows.n) {
         a.x[i] = fma(ax, (double)p[i], a.x[i]);
-        if (flex) rold[i] = rr[i];
         const V ri = vfma(-af, q[i], rr[i]);
         rr[i] = ri;
         const V zi = cheb ? dinv[i] * ri * inv_th : dinv[i] * ri;
@@ -909,22 +759,253 @@ __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid&
   write_result_m(a, g, total, rnorm / bnrm, ierr);
 }
 
-template <typename V, bool L1, int ELL>
+// ---------------------------------------------------------------------------
+// The mixed form's PCG: FP64 conjugate gradients, FP32 polynomial
+// ---------------------------------------------------------------------------
+
+// y = A (z + beta pold) in FP64 from the FP64 ELL values (the CSR values
+// without an ELL copy), each gathered entry formed as its owner row forms its
+// new direction (first: y = A z): pold FP64, z the FP32 preconditioned
+// residual.
+template <bool L1, int ELL, bool FULL>
+__device__ __forceinline__ void spmv64_rows_dir(const Sp32<float>& S, const double* __restrict__ ev,
+                                                const KrylovArgs& a, const float* z, const double* pold, double beta,
+                                                bool first, const int (&i)[kRows], const bool (&in0)[kRows],
+                                                double (&y)[kRows]) {
+  bool in[kRows];
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) in[r] = FULL || in0[r];
+  if constexpr (ELL) {
+    constexpr int WMAX = 8;
+    const int W = S.w;
+    double v[kRows][WMAX], xv[kRows][WMAX];
+    int c[kRows][WMAX];
+#pragma unroll
+    for (int r = 0; r < kRows; ++r)
+#pragma unroll
+      for (int t = 0; t < WMAX; ++t)
+        if (t < W && in[r]) {
+          c[r][t] = S.ecol[(long)t * S.ld + i[r]];
+          v[r][t] = ev[(long)t * S.ld + i[r]];
+        }
+    if constexpr (ELL == 2) {
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) {
+        const int j = i[r] + S.pf;
+        if (j < S.n) {
+#pragma unroll
+          for (int t = 0; t < WMAX; ++t)
+            if (t < W) {
+              prefetch_l2(S.ecol + (long)t * S.ld + j);
+              prefetch_l2(ev + (long)t * S.ld + j);
+            }
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < kRows; ++r)
+#pragma unroll
+      for (int t = 0; t < WMAX; ++t)
+        if (t < W && in[r])
+          xv[r][t] = first ? (double)ldv(&z[c[r][t]]) : fma(beta, ldv(&pold[c[r][t]]), (double)ldv(&z[c[r][t]]));
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      double acc = 0.0;
+#pragma unroll
+      for (int t = 0; t < WMAX; ++t)
+        if (t < W && in[r]) acc = fma(v[r][t], xv[r][t], acc);
+      y[r] = acc;
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      double acc = 0.0;
+      if (in[r]) {
+        const int e = a.row_ptr[i[r] + 1];
+        for (int k = a.row_ptr[i[r]]; k < e; ++k) {
+          const int cc = a.col[k];
+          const double x = first ? (double)ldv(&z[cc]) : fma(beta, ldv(&pold[cc]), (double)ldv(&z[cc]));
+          acc = fma(a.aval[k], x, acc);
+        }
+      }
+      y[r] = acc;
+    }
+  }
+}
+
+// pnew := z + beta pold and q := A pnew (FP64) in one pass; pnew.q
+template <bool L1, int ELL>
+__device__ __forceinline__ void pcg_hybrid_direct_pass(const KrylovArgs& a, const MixedArgs& m, const Red& R,
+                                                       const Rows& rows, const float* z, const double* pold,
+                                                       double* pnew, double* q, double beta, bool first) {
+  const Sp32<float> S = sp32_of(a, m, rows);
+  const double* __restrict__ ev = m.ell64;
+  MGPU_STEPS(rows, base) {
+    MGPU_STEP_ROWS(rows, base, ii, in);
+    MGPU_SPLIT_FULL(rows, base, FULL, {
+      double aq[kRows];
+      spmv64_rows_dir<L1, ELL, FULL>(S, ev, a, z, pold, beta, first, ii, in, aq);
+_Pragma("unroll") for (int r = 0; r < kRows; ++r) {
+        const int i = ii[r];
+        double c[1] = {0.0};
+        if (FULL || in[r]) {
+          const double pi = first ? (double)z[i] : fma(beta, pold[i], (double)z[i]);
+          pnew[i] = pi;
+          q[i] = aq[r];
+          c[0] = pi * aq[r];
+        }
+        red_put<1>(R, rows, base + r * rows.stride, c);
+      }
+    })
+  }
+}
+
+// PCG in FP64 (x, the residual, the search direction and q = A p, every sum)
+// with the preconditioner in FP32: the Chebyshev-Jacobi polynomial runs on an
+// FP32 copy of the residual with the FP32 matrix copy and FP32 vectors. The
+// polynomial's passes are 15 of the 17 passes of an iteration at degree 16,
+// so the iteration moves nearly the FP32 form's bytes, while the conjugate
+// gradient recurrence keeps the FP64 form's convergence (a CG stream run in
+// FP32 loses it: 71 against 52 iterations on the 524k channel's pressure
+// systems). The residual is carried scaled by sc = 1 / |b - A x0|. When it
+// says the solve has converged, an FP64 pass forms b - A x and decides; if
+// that is still above the tolerance the iteration restarts from it. On entry
+// a.r holds b - A x0 and rnorm0 its norm. Every pass that writes what the
+// next pass gathers ends in a reduction (one grid barrier).
+template <bool L1, int ELL>
+__device__ void pcg_hybrid(const KrylovArgs& a, const MixedArgs& m, VGrid& g, Red& R, const Rows& rows, double bnrm,
+                           double rnorm0, double lmax, float inv_th) {
+  const int n = a.n;
+  const float* __restrict__ dinv = m.dinv;
+  float *rr = m.w32, *zA = m.w32 + n, *dch = m.w32 + 5l * n, *zB = m.w32 + 6l * n;
+  double *rs = a.r, *p = a.p, *pn = a.s, *q = a.v;  // p double-buffered
+  const bool cheb = m.cheb_k > 1;
+  const double sc = 1.0 / rnorm0;
+  const double stop = a.tol * bnrm * sc;  // |rs| at which the solve has converged
+  const double stop2 = stop * stop;
+  // rs := sc r, its FP32 copy, z0 (Jacobi: z = D^-1 rr; Chebyshev: its first
+  // term); rs.z0
+  MGPU_TILES(rows, base) {
+    const int i = base + threadIdx.x;
+    double c[1] = {0.0};
+    if (i < rows.n) {
+      const double ri = ldv(&a.r[i]) * sc;
+      rs[i] = ri;
+      const float rf = (float)ri;
+      rr[i] = rf;
+      const float zi = cheb ? dinv[i] * rf * inv_th : dinv[i] * rf;
+      if (cheb) dch[i] = zi;
+      zA[i] = zi;
+      c[0] = ri * (double)zi;
+    }
+    red_put<1>(R, rows, base, c);
+  }
+  double t1[1];
+  if (!red_total<1, L1>(R, rows, g, a.st, t1)) return;
+  double rzn = t1[0], rz = 0.0, rnorm = rnorm0;
+  int total = 0, ierr = 0;
+  bool first = true;
+  while (true) {
+    float* z = zA;
+    if (cheb) {
+      double red[2];  // (rs.z, rr.rr)
+      if (!cheb_apply<float, L1, ELL>(a, m, g, R, rows, rr, dch, zA, zB, lmax, z, red, rs)) return;
+      rzn = red[0];
+    }
+    double beta = 0.0;
+    if (!first) {
+      if (fabs(rz) < DTINY) {
+        ierr = 2;
+        break;
+      }
+      beta = rzn / rz;
+    }
+    rz = rzn;
+    ++total;
+    pcg_hybrid_direct_pass<L1, ELL>(a, m, R, rows, z, p, pn, q, beta, first);
+    {
+      double* t = p;
+      p = pn;
+      pn = t;
+    }
+    first = false;
+    double pq[1];
+    if (!red_total<1, L1>(R, rows, g, a.st, pq)) return;
+    if (fabs(pq[0]) < DTINY) {
+      ierr = 2;
+      break;
+    }
+    const double al = rz / pq[0];
+    const double ax = al * rnorm0;  // the step in unscaled units
+    // x += ax p, rs -= al q, FP32 copy and z0; sums rs.rs and rs.z0
+    MGPU_TILES(rows, base) {
+      const int i = base + threadIdx.x;
+      double c[2] = {0.0, 0.0};
+      if (i < rows.n) {
+        a.x[i] = fma(ax, p[i], a.x[i]);
+        const double ri = fma(-al, q[i], rs[i]);
+        rs[i] = ri;
+        const float rf = (float)ri;
+        rr[i] = rf;
+        const float zi = cheb ? dinv[i] * rf * inv_th : dinv[i] * rf;
+        if (cheb) dch[i] = zi;
+        zA[i] = zi;
+        c[0] = ri * ri;
+        c[1] = ri * (double)zi;
+      }
+      red_put<2>(R, rows, base, c);
+    }
+    double s2[2];
+    if (!red_total<2, L1>(R, rows, g, a.st, s2)) return;
+    rzn = s2[1];
+    if (!(s2[0] <= stop2 || total >= a.maxit)) continue;
+    // r = b - A x in FP64 decides; rs := sc r, FP32 copy, z0; sums r.r, rs.z0
+    MGPU_TILES(rows, base) {
+      const int i = base + threadIdx.x;
+      double c[2] = {0.0, 0.0};
+      if (i < rows.n) {
+        const double ri = a.b[i] - row_spmv64<L1>(a, a.x, i);
+        const double si = ri * sc;
+        rs[i] = si;
+        const float rf = (float)si;
+        rr[i] = rf;
+        const float zi = cheb ? dinv[i] * rf * inv_th : dinv[i] * rf;
+        if (cheb) dch[i] = zi;
+        zA[i] = zi;
+        c[0] = ri * ri;
+        c[1] = si * (double)zi;
+      }
+      red_put<2>(R, rows, base, c);
+    }
+    double t2[2];
+    if (!red_total<2, L1>(R, rows, g, a.st, t2)) return;
+    rnorm = sqrt(t2[0]);
+    const double res = rnorm / bnrm;
+    if (res <= a.tol) {
+      write_result_m(a, g, total, res, 0);
+      return;
+    }
+    if (total >= a.maxit) {
+      ierr = 1;
+      break;
+    }
+    rzn = t2[1];
+    first = true;  // the recursive residual had drifted: restart from the true one
+  }
+  write_result_m(a, g, total, rnorm / bnrm, ierr);
+}
+
+template <typename V, bool L1, int ELL, bool DYN = false>
 __device__ void pcg_mixed_body(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid& g) {
   if (a.st->abort) return;
   const int n = a.n;
-  const bool contiguous = m.flags != nullptr;
-  if (!fits_group(n, g, contiguous)) {  // unreachable through the launchers: reported as a breakdown
+  if (!fits_group(n, g) || (DYN && !fits_slots(n, g, m.cp_slots))) {
+    // unreachable through the launchers: reported as a breakdown
     write_result_m(a, g, 0, 0.0, 2);
     return;
   }
-  const Rows rows = block_rows(n, g, contiguous);
-  unsigned pass = 0;
-  if (!setup_pass_sync<L1>(a, m.flags, g, rows)) return;
-  const V* __restrict__ dinv = m.dinv;
-  Red R = make_red(m, n);
-  V *rr = m.w32, *zA = m.w32 + n, *p = m.w32 + 2l * n, *q = m.w32 + 3l * n, *d = m.w32 + 4l * n;
-  V *dch = m.w32 + 5l * n, *zB = m.w32 + 6l * n;
+  const Rows rows = block_rows(n, g);
+  Red R = make_red<V, DYN>(m, n);
   const bool cheb = m.cheb_k > 1;
   double bnrm;
   bool diag_bad;
@@ -960,134 +1041,27 @@ __device__ void pcg_mixed_body(const KrylovArgs& a, const MixedArgsT<V>& m, VGri
     write_result_m(a, g, 0, res, 0);
     return;
   }
-  if (m.reliable) {
-    pcg_reliable<V, L1, ELL>(a, m, g, R, rows, bnrm, rnorm, lmax, inv_th, pass);
-    return;
-  }
-  // Restarted refinement. One loop, one call site of the preconditioner: a restart (scaled FP64
-  // residual, after each refinement step) or an inner iteration, then
-  // z = M^-1 rr with its sums, then the decisions.
-  int total = 0, ierr = 0;
-  V* z = zA;
-  bool restart = true, first = true;
-  double rz = 0.0, target = 0.0;
-  V beta = V(0);
-  while (true) {
-    double s2[2] = {0.0, 0.0};  // restart: (rr.z, rr.rr); iteration: (rr.rr, rr.z)
-    if (restart) {
-      const double inv = 1.0 / rnorm;
-      MGPU_TILES(rows, base) {
-        const int i = base + threadIdx.x;
-        double c[2] = {0.0, 0.0};
-        if (i < rows.n) {
-          const V ri = (V)(ldv(&a.r[i]) * inv);
-          rr[i] = ri;
-          d[i] = V(0);
-          if (cheb) {
-            const V di = dinv[i] * ri * inv_th;
-            dch[i] = di;
-            zA[i] = di;
-          } else {
-            const V zi = dinv[i] * ri;
-            zA[i] = zi;
-            c[0] = (double)ri * (double)zi;
-            c[1] = (double)ri * (double)ri;
-          }
-        }
-        if (!cheb) red_put<2>(R, rows, base, c);
-      }
-    } else {
-      // p := z and q := A p on the first inner iteration; afterwards
-      // p := z + beta p and q := A z + beta q in the same pass
-      ++total;
-      pcg_fused_pass<V, L1, ELL>(a, m, R, rows, z, p, q, beta, first);
-      first = false;
-      double pq[1];
-      if (!red_total<1, L1>(R, rows, g, a.st, pq)) return;
-      if (fabs(pq[0]) < DTINY) {
-        ierr = 2;
-        break;
-      }
-      const V af = (V)(rz / pq[0]);
-      MGPU_TILES(rows, base) {
-        const int i = base + threadIdx.x;
-        double c[2] = {0.0, 0.0};
-        if (i < rows.n) {
-          d[i] = vfma(af, p[i], d[i]);
-          const V ri = vfma(-af, q[i], rr[i]);
-          rr[i] = ri;
-          if (cheb) {
-            const V di = dinv[i] * ri * inv_th;
-            dch[i] = di;
-            zA[i] = di;
-          } else {
-            const V zi = dinv[i] * ri;
-            zA[i] = zi;
-            c[0] = (double)ri * (double)ri;
-            c[1] = (double)ri * (double)zi;
-          }
-        }
-        if (!cheb) red_put<2>(R, rows, base, c);
-      }
-    }
-    if (cheb) {
-      if (!vg_sync(g, a.st)) return;
-      double red[2];  // (rr.z, rr.rr)
-      if (!cheb_apply<V, L1, ELL>(a, m, g, R, rows, rr, dch, zA, zB, lmax, z, red, pass)) return;
-      s2[0] = restart ? red[0] : red[1];
-      s2[1] = restart ? red[1] : red[0];
-    } else {
-      z = zA;
-      if (!red_total<2, L1>(R, rows, g, a.st, s2)) return;
-    }
-    if (restart) {
-      rz = s2[0];
-      target = m.tau * m.tau * s2[1];
-      beta = V(0);
-      first = true;
-      restart = false;
-      continue;
-    }
-    if (!(s2[0] <= target || total >= a.maxit)) {
-      if (fabs(rz) < DTINY) {
-        ierr = 2;
-        break;
-      }
-      beta = (V)(s2[1] / rz);
-      rz = s2[1];
-      continue;
-    }
-    // refinement step
-    if (!update_x<V, L1>(a, g, rows, d, rnorm)) return;
-    if (!true_residual<L1>(a, g, R, rows, rnorm)) return;
-    res = rnorm / bnrm;
-    if (res <= a.tol) {
-      write_result_m(a, g, total, res, 0);
-      return;
-    }
-    if (total >= a.maxit) {
-      ierr = 1;
-      break;
-    }
-    restart = true;
-  }
-  write_result_m(a, g, total, res, ierr);
+  if constexpr (sizeof(V) == 4)
+    pcg_hybrid<L1, ELL>(a, m, g, R, rows, bnrm, rnorm, lmax, inv_th);
+  else
+    pcg_reliable<V, L1, ELL>(a, m, g, R, rows, bnrm, rnorm, lmax, inv_th);
 }
 
 // ---------------------------------------------------------------------------
 // BiCGStab (momentum): right Jacobi preconditioning
 // ---------------------------------------------------------------------------
-template <typename V, bool L1, int ELL>
+template <typename V, bool L1, int ELL, bool DYN = false>
 __device__ void bicgstab_mixed_body(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid& g) {
   if (a.st->abort) return;
   const int n = a.n;
-  if (!fits_group(n, g)) {  // unreachable through the launchers: reported as a breakdown
+  if (!fits_group(n, g) || (DYN && !fits_slots(n, g, m.cp_slots))) {
+    // unreachable through the launchers: reported as a breakdown
     write_result_m(a, g, 0, 0.0, 2);
     return;
   }
   const Rows rows = block_rows(n, g);
   const V* __restrict__ dinv = m.dinv;
-  Red R = make_red(m, n);
+  Red R = make_red<V, DYN>(m, n);
   V* W = m.w32;
   V *r = W, *r0 = W + n, *p = W + 2l * n, *v = W + 3l * n, *s = W + 4l * n, *t = W + 5l * n,
         *ph = W + 6l * n, *sh = W + 7l * n, *d = W + 8l * n;
@@ -1239,31 +1213,33 @@ int launch_mixed(const void* fn1, const void* fnN, const KrylovArgs& a, const Mi
   int block = 0;
   int grid = krylov_grid(a.n, block, 0);
   if (grid == 1 && a.n > kBlockMaxRows) grid = 2;
+  // grid kernels: dynamic shared memory for the block's chunk sums (2 sums x
+  // 8 chunks per tile of 256 rows, for the most tiles a block owns)
+  int dyn = 0, cps = 0;
   if (grid > 1) {
     block = 256;
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fnN, block, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fnN, block, (size_t)16 * kBlockMaxChunks);
     if (per < 1) per = 1;
     const long want = ((long)a.n + 2l * block - 1) / (2l * block);
     grid = (int)std::min<long>(std::max<long>(want, 2), (long)sms * per);
+    const long rows_per_block = ((long)a.n + grid - 1) / grid;
+    cps = (int)std::min<long>((rows_per_block + block - 1) / block * (block / 32), kBlockMaxChunks);
+    dyn = 16 * cps;
   }
   if ((long)grid * kBlockMaxRows < a.n) {
     set_error("mixed-precision solve: too many rows per block for the co-resident grid");
     return MGPU_E_ARG;
   }
-  if (m.flags && grid > kMaxPassFlags) {
-    set_error("mixed-precision solve: more blocks than pass counters");
-    return MGPU_E_ARG;
-  }
   KrylovArgs aa = a;
   MixedArgsT<V> mm = m;
+  mm.cp_slots = cps;
   void* args[] = {&aa, &mm};
   cudaError_t e = cudaMemsetAsync(a.bar, 0, sizeof(unsigned long long), s);
-  if (e == cudaSuccess && m.flags) e = cudaMemsetAsync(m.flags, 0, sizeof(unsigned) * (size_t)grid, s);
   if (e != cudaSuccess) return cuda_fail(e, "barrier reset", __FILE__, __LINE__);
-  e = cudaLaunchCooperativeKernel(grid == 1 ? fn1 : fnN, dim3(grid), dim3(block), args, 0, s);
+  e = cudaLaunchCooperativeKernel(grid == 1 ? fn1 : fnN, dim3(grid), dim3(block), args, (size_t)dyn, s);
   if (e != cudaSuccess) return cuda_fail(e, "cooperative launch (mixed)", __FILE__, __LINE__);
   return 0;
 }

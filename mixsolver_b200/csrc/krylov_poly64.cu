@@ -15,13 +15,13 @@ namespace {
 template <bool L1, int ELL>
 __global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : 2) k_pcg_poly64(KrylovArgs a, MixedArgsT<double> m) {
   VGrid g = whole_grid(a.bar, a.partials);
-  pcg_mixed_body<double, L1, ELL>(a, m, g);
+  pcg_mixed_body<double, L1, ELL, !L1>(a, m, g);
 }
 
 template <bool L1, int ELL>
 __global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : 2) k_bicgstab_poly64(KrylovArgs a, MixedArgsT<double> m) {
   VGrid g = whole_grid(a.bar, a.partials);
-  bicgstab_mixed_body<double, L1, ELL>(a, m, g);
+  bicgstab_mixed_body<double, L1, ELL, !L1>(a, m, g);
 }
 
 }  // namespace

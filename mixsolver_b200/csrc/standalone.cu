@@ -10,10 +10,14 @@
 
 #include "assembly.cuh"
 #include "case.cuh"
+#include "device_topo.h"
 #include "mesh_host.h"
 
 namespace mgpu {
 extern unsigned g_spin_limit;  // krylov.cu: the spin_limit tuning key
+extern int g_cheb_degree;      // the cheb_degree and cheb_ratio tuning keys
+extern double g_cheb_ratio;
+extern int g_prefetch_mb;      // l2_prefetch_mb
 }
 
 using namespace mgpu;
@@ -105,6 +109,99 @@ void analyse(int n, const int32_t* row_ptr, const int32_t* col_idx, Pattern& P) 
     P.nup = std::max(P.nup, l + 1);
   }
   bucket(P.nup, P.up_ptr, P.up_rows);
+}
+
+// The pressure solver of the mixed and FP64 polynomial forms on a host CSR
+// system: the case's own kernels (k_pcg_mixed / k_pcg_poly64) with the
+// arguments a case would give them, the ELL copy built on the device.
+template <typename V>
+int poly_solve(int n, const Pattern& P, const double* val, const double* b, double* x, double tol, int maxit,
+                      int cheb_degree, int* it, double* res, int* ierr) {
+  DevBuf B;
+  const int nnz = P.rp[n];
+  int *drp, *dcol, *ddiag, *dferr;
+  double *dval, *db, *dx, *dkw, *dpart, *dred;
+  V *da, *ddinv, *dw;
+  unsigned long long* dbar;
+  DevStatus* dst;
+  MgpuIterRec* drec;
+  TRY(B.up(drp, P.rp.data(), n + 1));
+  TRY(B.up(dcol, P.col.data(), nnz));
+  TRY(B.up(ddiag, P.diag.data(), n));
+  TRY(B.up(dval, val, nnz));
+  TRY(B.up(db, b, n));
+  TRY(B.up(dx, x, n));
+  TRY(B.alloc(dkw, 10 * (size_t)n));
+  TRY(B.alloc(dpart, 4 * 4096));
+  TRY(B.alloc(dred, (size_t)mixed_red_words(n)));
+  TRY(B.alloc(da, nnz));
+  TRY(B.alloc(ddinv, n));
+  TRY(B.alloc(dw, 10 * (size_t)n));
+  TRY(B.alloc(dbar, 1));
+  TRY(B.alloc(dferr, 1));
+  TRY(B.alloc(dst, 1));
+  TRY(B.alloc(drec, 1));
+  int W = 0, *ell = nullptr;
+  long ld = 0;
+  TopoAlloc alloc = [&](int*& q, size_t k) { return B.alloc(q, k); };
+  TRY(device_ell(n, drp, dcol, 8, W, ld, ell, alloc, 0));
+  V* dev = nullptr;
+  double* dev64 = nullptr;  // the mixed form's FP64 conjugate-gradient product
+  if (ell) {
+    TRY(B.alloc(dev, (size_t)W * ld));
+    MGPU_CUDA(cudaMemset(dev, 0, sizeof(V) * (size_t)W * ld));
+    if (sizeof(V) == 4) {
+      TRY(B.alloc(dev64, (size_t)W * ld));
+      MGPU_CUDA(cudaMemset(dev64, 0, sizeof(double) * (size_t)W * ld));
+    }
+  }
+  DevStatus h{};
+  h.nan_key = ~0ull;
+  h.spin_limit = g_spin_limit;
+  MGPU_CUDA(cudaMemcpy(dst, &h, sizeof(h), cudaMemcpyHostToDevice));
+  MGPU_CUDA(cudaMemset(drec, 0, sizeof(MgpuIterRec)));
+  KrylovArgs a{};
+  a.n = n;
+  a.row_ptr = drp;
+  a.col = dcol;
+  a.diag = ddiag;
+  a.aval = dval;
+  a.b = db;
+  a.x = dx;
+  a.r = dkw;
+  a.p = dkw + 2l * n;
+  a.v = dkw + 3l * n;
+  a.s = dkw + 4l * n;
+  a.tol = tol;
+  a.maxit = maxit;
+  a.precond = 1;
+  a.partials = dpart;
+  a.bar = dbar;
+  a.st = dst;
+  a.recs = drec;
+  a.ferr = dferr;
+  const bool mixed = sizeof(V) == 4;
+  const double row_bytes = mixed ? mixed_row_bytes(W) : 16.0 * W + 80.0;
+  const bool big = (double)n * row_bytes > g_prefetch_mb * 1048576.0;
+  MixedArgsT<V> m{da,   ddinv, dw, 1e-4, cheb_degree, g_cheb_ratio, W, ell, dev, dred, (ell && big) ? 1 : 0, 0.0,
+                  (int)ld, 0,  dev64};
+  if constexpr (sizeof(V) == 4)
+    TRY(launch_pcg_mixed(a, m, 0));
+  else
+    TRY(launch_pcg_poly64(a, m, 0));
+  MGPU_CUDA(cudaDeviceSynchronize());
+  MgpuIterRec r{};
+  MGPU_CUDA(cudaMemcpy(&r, drec, sizeof(r), cudaMemcpyDeviceToHost));
+  MGPU_CUDA(cudaMemcpy(&h, dst, sizeof(h), cudaMemcpyDeviceToHost));
+  MGPU_CUDA(cudaMemcpy(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  if (h.timeout) {
+    set_error("a bounded device wait ran out (grid barrier)");
+    return MGPU_E_TIMEOUT;
+  }
+  *it = r.lin_it[0];
+  *res = r.lin_res[0];
+  *ierr = r.lin_ierr[0];
+  return 0;
 }
 
 }  // namespace
@@ -229,6 +326,28 @@ int mgpu_krylov_solve(int n, const int32_t* row_ptr, const int32_t* col_idx, con
   *res = r.lin_res[0];
   *ierr = r.lin_ierr[0];
   return 0;
+}
+
+int mgpu_pcg_poly_solve(int n, const int32_t* row_ptr, const int32_t* col_idx, const double* val, const double* b,
+                        double* x, double tol, int maxit, int precision, int cheb_degree, int* it, double* res,
+                        int* ierr) {
+  if (n <= 0 || !row_ptr || !col_idx || !val || !b || !x || !it || !res || !ierr || maxit < 0 ||
+      (precision != MGPU_PREC_MIXED && precision != MGPU_PREC_FP64_POLY) || n > kMixedMaxRows) {
+    set_error("mgpu_pcg_poly_solve: invalid argument");
+    return MGPU_E_ARG;
+  }
+  Pattern P;
+  analyse(n, row_ptr, col_idx, P);
+  *it = 0;
+  *res = 0.0;
+  *ierr = 0;
+  if (!P.full_diag) {
+    set_error("mgpu_pcg_poly_solve: a row has no diagonal entry");
+    return MGPU_E_ARG;
+  }
+  const int k = cheb_degree > 0 ? cheb_degree : g_cheb_degree;
+  return precision == MGPU_PREC_MIXED ? poly_solve<float>(n, P, val, b, x, tol, maxit, k, it, res, ierr)
+                                      : poly_solve<double>(n, P, val, b, x, tol, maxit, k, it, res, ierr);
 }
 
 int mgpu_csr_matvec(int n, const int32_t* row_ptr, const int32_t* col_idx, const double* val, const double* x,

@@ -328,6 +328,24 @@ def cg_ilu0(row_ptr, col_idx, val, b, x, tol, maxit, norm_mode=0):
     return _krylov(abi.KRY_CG_ILU0, row_ptr, col_idx, val, b, x, tol, maxit, norm_mode)
 
 
+def pcg_poly(row_ptr, col_idx, val, b, x, tol, maxit, precision=abi.PREC_MIXED, cheb_degree=0):
+    """The mixed-precision (or FP64 polynomial) pressure solver on a 1-based
+    CSR system: Chebyshev-Jacobi PCG with reliable updates
+    (mgpu_pcg_poly_solve). Returns (x, it, res, ierr) like cg_ic0."""
+    lib = _lib()
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    ci = np.ascontiguousarray(col_idx, dtype=np.int32)
+    v = np.ascontiguousarray(val, dtype=np.float64)
+    bb = np.ascontiguousarray(b, dtype=np.float64)
+    xx = np.array(x, dtype=np.float64, copy=True)
+    n = len(rp) - 1
+    it, ierr, res = C.c_int(0), C.c_int(0), C.c_double(0.0)
+    abi.check(lib, lib.mgpu_pcg_poly_solve(n, iptr(rp), iptr(ci), dptr(v), dptr(bb), dptr(xx), float(tol), int(maxit),
+                                           int(precision), int(cheb_degree), C.byref(it), C.byref(res),
+                                           C.byref(ierr)), "mgpu_pcg_poly_solve")
+    return xx, it.value, res.value, ierr.value
+
+
 def csr_matvec(row_ptr, col_idx, val, x):
     """csr_matvec (mod_uns_linsolver.f90:40-52)."""
     lib = _lib()

@@ -1108,13 +1108,13 @@ void correct_fields(Case& cs) {
   else
     for (int i = 0; i < m.ncells; ++i) cs.p[i] = cs.p[i] + cs.ctrl.alpha_p * pp[i];
   double rho = cs.ctrl.rho;
-  // the transient drivers assemble with ppe_assembly_mpi at one rank
-  const bool mpi = cs.ts_order > 0;
-  auto dirichlet = [&](int i) { return mpi ? ppe_dirichlet_mpi(cs.bcs, i) : bc_face_p_dirichlet(cs.bcs, i); };
+  // every driver (the transient ones included) corrects the fluxes with the
+  // serial correct_fields and its bc_face_p_dirichlet rule, mod_uns_simple.f90:1703-1724
+  // (mod_uns_simple_mpi.f90:187, 457, 740)
   for (int i = 0; i < m.nfaces; ++i) {
     int c1 = m.c1[i], c0 = m.c0[i];
     if (c1 < 0) {
-      if (cs.bcs.fgrp[i] >= 0 && dirichlet(i)) {
+      if (cs.bcs.fgrp[i] >= 0 && bc_face_p_dirichlet(cs.bcs, i)) {
         double dbf = cs.g.vol[c0] / cs.apc[c0];
         double d[3];
         for (int k = 0; k < 3; ++k) d[k] = cs.g.xf[3 * i + k] - cs.g.xc[3 * c0 + k];

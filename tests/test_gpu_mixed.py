@@ -91,56 +91,6 @@ def test_mixed_piso_meets_gate():
     _check(mesh, ctrl, 5, piso=True, u0=u0)
 
 
-def test_mixed_neighbour_sync_bit_identical():
-    """The optional neighbour sync (tuning key neighbor_sync): a single-system
-    pressure solve runs its Chebyshev passes on contiguous row ranges, each
-    block waiting only for the blocks whose rows it reads. Every sum still runs
-    over fixed row chunks, so the run is bit-identical to the same run with
-    grid barriers (the default)."""
-    mesh, ctrl = cases.channel3d(32, 16, 16, seed=6, outer_max=5, order_fn=S.rcm_order)
-    ctrl.precision = abi.PREC_MIXED
-    ctrl.lin_max = 2000
-    out = []
-    S.set_tuning("single_block_rows", 0)
-    try:
-        for ns in (1, 0):
-            S.set_tuning("neighbor_sync", ns)
-            g = S.UnsCase(mesh, ctrl)
-            ier, log = g.simple_run()
-            assert ier == 0
-            out.append((log, g.fields()))
-    finally:
-        S.set_tuning("neighbor_sync", 0)
-        S.set_tuning("single_block_rows", 32768)
-    for a, b in zip(out[0][0], out[1][0]):
-        assert a["lin_it"] == b["lin_it"] and a["lin_res"] == b["lin_res"]
-    for k in ("u", "p", "flux"):
-        np.testing.assert_array_equal(out[0][1][k], out[1][1][k])
-
-
-def test_restarted_and_reliable_schemes_close():
-    """The pressure PCG's two refinement schemes (restarted inner solves,
-    reliable updates) converge the same systems to the same tolerance."""
-    mesh, ctrl = cases.channel3d(16, 8, 8, seed=4, outer_max=8, order_fn=S.rcm_order)
-    ctrl.precision = abi.PREC_MIXED
-    ctrl.lin_max = 2000
-    ctrl.lin_tol = 1e-11
-    out = []
-    try:
-        for sch in (0, 1):
-            S.set_tuning("mixed_scheme", sch)
-            g = S.UnsCase(mesh, ctrl)
-            ier, log = g.simple_run()
-            assert ier == 0
-            for r in log:
-                assert all(e == 0 for e in r["lin_ierr"][:4]) and all(x <= 1e-11 for x in r["lin_res"][:4])
-            out.append(g.fields())
-    finally:
-        S.set_tuning("mixed_scheme", 1)
-    for k in ("u", "p", "flux"):
-        assert rel(out[0][k], out[1][k]) < 1e-9, k
-
-
 def test_fp64_poly_form_close_to_parity_form():
     """The mixed form's solvers in FP64 throughout (MGPU_PREC_FP64_POLY) against
     the FP64 parity form, both to lin_tol 1e-11: the same fields to 1e-8."""
@@ -159,3 +109,49 @@ def test_fp64_poly_form_close_to_parity_form():
         fields.append(g.fields())
     for k in ("u", "p", "flux"):
         assert rel(fields[1][k], fields[0][k]) < 1e-8, (k, rel(fields[1][k], fields[0][k]))
+
+
+def _ppe(nx, ny, nz):
+    """A pressure-correction system of the jittered channel after 3 oracle
+    SIMPLE iterations (1-based CSR)."""
+    mesh, ctrl = cases.channel3d(nx, ny, nz, seed=2, outer_max=3, order_fn=S.rcm_order)
+    o = O.OracleCase(mesh, ctrl)
+    o.simple_run()
+    con = o.connectivity()
+    aval, rhs, _ = o.stage(5, len(con["col_idx"]))
+    return con["row_ptr"], con["col_idx"], aval, rhs
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_MIXED, abi.PREC_FP64_POLY])
+def test_pcg_poly_solve_on_a_csr_system(prec):
+    """mgpu_pcg_poly_solve: converged on the FP64 residual (checked here with
+    the oracle's csr_matvec), the same answer as cg_ic0 to the tolerance, and
+    the same bits from one block and from a grid of blocks (layout-independent
+    sums)."""
+    rp, ci, aval, rhs = _ppe(24, 12, 12)
+    x0 = np.zeros(len(rp) - 1)
+    tol = 1e-10
+    x1, it1, res1, ierr1 = S.pcg_poly(rp, ci, aval, rhs, x0, tol, 2000, prec)
+    assert ierr1 == 0 and res1 <= tol and it1 > 0
+    true = np.linalg.norm(rhs - O.csr_matvec(rp, ci, aval, x1)) / np.linalg.norm(rhs)
+    assert true <= tol * (1 + 1e-6), true
+    xr, _, _, ierr = S.cg_ic0(rp, ci, aval, rhs, x0, 1e-12, 2000)
+    assert ierr == 0
+    assert rel(x1, xr) < 1e-7, rel(x1, xr)
+    S.set_tuning("single_block_rows", 0)
+    try:
+        x2, it2, res2, ierr2 = S.pcg_poly(rp, ci, aval, rhs, x0, tol, 2000, prec)
+    finally:
+        S.set_tuning("single_block_rows", 32768)
+    assert (it2, ierr2) == (it1, ierr1) and res2 == res1
+    np.testing.assert_array_equal(x2, x1)
+
+
+def test_pcg_poly_solve_jacobi_and_iteration_cap():
+    """Degree 1 is Jacobi PCG; a cap below the need returns ierr 1."""
+    rp, ci, aval, rhs = _ppe(16, 8, 8)
+    x0 = np.zeros(len(rp) - 1)
+    x, it, res, ierr = S.pcg_poly(rp, ci, aval, rhs, x0, 1e-9, 5000, abi.PREC_MIXED, cheb_degree=1)
+    assert ierr == 0 and res <= 1e-9
+    _, it5, res5, ierr5 = S.pcg_poly(rp, ci, aval, rhs, x0, 1e-9, 5, abi.PREC_MIXED)
+    assert ierr5 == 1 and res5 > 1e-9

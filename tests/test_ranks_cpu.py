@@ -67,13 +67,13 @@ def test_hbm_peak_names_its_source(tmp_path, monkeypatch):
 
 def test_krylov_byte_model_matches_the_stated_formulas():
     """The roofline's algorithmic bytes per inner iteration, as stated with the
-    kernels: mixed PCG with a degree-16 Chebyshev-Jacobi polynomial reads
-    128 nnz + 416 N bytes (1302 B per row on the 524,288-cell channel); mixed
-    BiCGStab-Jacobi 16 nnz + 104 N + 8."""
+    kernels: mixed PCG (FP64 conjugate gradients, FP32 degree-16
+    Chebyshev-Jacobi polynomial) reads 132 nnz + 456 N bytes (1370 B per row
+    on the 524,288-cell channel); mixed BiCGStab-Jacobi 16 nnz + 104 N + 8."""
     sys.path.insert(0, ROOT)
     import bench
     N, nnz = 524288, 3629056
     per = lambda m: (bench.krylov_bytes(N, nnz, 10, m, True) - bench.krylov_bytes(N, nnz, 0, m, True)) / 10
-    assert per("pcg") == 128 * nnz + 416 * N
-    assert round(per("pcg") / N) == 1302
+    assert per("pcg") == 132 * nnz + 456 * N
+    assert round(per("pcg") / N) == 1370
     assert per("bicg") == 16 * nnz + 104 * N + 8

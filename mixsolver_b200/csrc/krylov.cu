@@ -52,7 +52,7 @@ int prewarm_streams(int n);  // case.cu
 double g_cheb_ratio = 1000.0; // and the ratio lambda_max / lambda_min of its interval
 int g_rel_delta_pm = 100; // reliable updates: residual replaced after a fall by this many thousandths
 unsigned g_spin_limit = 0; // polls before a bounded barrier wait gives up (0: kSpinLimit, ~2 s)
-int g_mixed_occ = 2;          // single-system mixed solves on a grid: resident blocks per SM (2, 3 or 4)
+int g_mixed_occ = 3;       // mixed and FP64 polynomial kernels: resident blocks per SM (2-4)
 namespace {
 
 __device__ __forceinline__ double ld_relaxed_f64(const double* p) {

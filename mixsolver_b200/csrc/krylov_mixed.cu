@@ -20,13 +20,13 @@ namespace {
 // (tuning key "mixed_blocks_per_sm")
 template <bool L1, int ELL, int OCC = 2>
 __global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : OCC) k_pcg_mixed(KrylovArgs a, MixedArgs m) {
-  VGrid g = whole_grid(a.bar, a.partials);
+  VGrid g = whole_grid(a.bar, a.partials, true);
   pcg_mixed_body<float, L1, ELL, !L1>(a, m, g);
 }
 
 template <bool L1, int ELL, int OCC = 2>
 __global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : OCC) k_bicgstab_mixed(KrylovArgs a, MixedArgs m) {
-  VGrid g = whole_grid(a.bar, a.partials);
+  VGrid g = whole_grid(a.bar, a.partials, true);
   bicgstab_mixed_body<float, L1, ELL, !L1>(a, m, g);
 }
 
@@ -59,7 +59,8 @@ __global__ void __launch_bounds__(256, 2) k_mixed_batch(LanePlan p) {
   __shared__ int s_idx;
   const int li = p.block_lane[blockIdx.x];
   const BatchLane L = p.lanes[li];
-  VGrid g{L.nblocks, (int)blockIdx.x - L.first_block, p.bars + li, p.partials + 8l * L.first_block, 0};
+  VGrid g{L.nblocks, (int)blockIdx.x - L.first_block, p.bars + li, p.partials + 8l * L.first_block, 0,
+          (unsigned long long)L.nblocks};  // lane counters are zeroed before the launch
   if (p.lane_t && g.rank == 0 && threadIdx.x == 0) p.lane_t[2 * li] = globaltimer_ns();
   for (int j = 0;; ++j) {
     __syncthreads();  // every thread is done with the previous system

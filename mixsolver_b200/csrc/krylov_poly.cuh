@@ -35,6 +35,7 @@
 #pragma once
 
 #include <algorithm>
+#include <type_traits>
 
 #include "persist.cuh"
 
@@ -225,6 +226,28 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
+// Runs body(std::integral_constant<int, WC>{}) with WC the ELL width when it
+// is one the passes are compiled for (5: tetrahedra and 2-D quadrilaterals,
+// 7: hexahedra), else WC = 0 (the width read at run time); a compile-time
+// width drops the per-entry width checks from every row of the pass.
+template <int ELL, typename F>
+__device__ __forceinline__ void with_width(int w, F&& body) {
+  if constexpr (ELL == 0) {
+    body(std::integral_constant<int, 0>{});
+  } else {
+    switch (w) {
+      case 5:
+        body(std::integral_constant<int, 5>{});
+        break;
+      case 7:
+        body(std::integral_constant<int, 7>{});
+        break;
+      default:
+        body(std::integral_constant<int, 0>{});
+    }
+  }
+}
+
 // kRows rows per thread in the SpMV passes: every row's loads are issued
 // before any product, so a warp keeps kRows rows of gathers in flight.
 #ifndef MGPU_KROWS
@@ -251,7 +274,7 @@ struct Sp32 {
   const V* __restrict__ a32;
   const V* __restrict__ dinv;
   int pf;  // rows from a tile to the tile whose ELL entries it prefetches into L2 (0: none)
-  long ld; // ELL leading dimension
+  int ld;  // ELL leading dimension (entry t of row i at t * ld + i, below 2^31)
 };
 
 template <typename V>
@@ -260,15 +283,15 @@ __device__ __forceinline__ Sp32<V> sp32_of(const KrylovArgs& a, const MixedArgsT
                  m.pf * kRows * rows.stride, m.ell_ld};
 }
 
-template <typename V, bool L1, int ELL, bool FULL>
+template <typename V, bool L1, int ELL, bool FULL, int WC = 0>
 __device__ __forceinline__ void spmv32_rows(const Sp32<V>& S, const V* x, const int (&i)[kRows],
                                             const bool (&in0)[kRows], V (&y)[kRows]) {
   bool in[kRows];
 #pragma unroll
   for (int r = 0; r < kRows; ++r) in[r] = FULL || in0[r];
   if constexpr (ELL) {
-    constexpr int WMAX = 8;
-    const int W = S.w;
+    constexpr int WMAX = WC ? WC : 8;  // WC: the ELL width known at compile time
+    const int W = WC ? WC : S.w;
     V v[kRows][WMAX], xv[kRows][WMAX];
     int c[kRows][WMAX];
 #pragma unroll
@@ -276,8 +299,8 @@ __device__ __forceinline__ void spmv32_rows(const Sp32<V>& S, const V* x, const 
 #pragma unroll
       for (int t = 0; t < WMAX; ++t)
         if (t < W && in[r]) {
-          c[r][t] = S.ecol[(long)t * S.ld + i[r]];
-          v[r][t] = S.eval[(long)t * S.ld + i[r]];
+          c[r][t] = S.ecol[t * S.ld + i[r]];
+          v[r][t] = S.eval[t * S.ld + i[r]];
         }
     if constexpr (ELL == 2) {
       // the same rows of this block's next tile: DRAM -> L2 while this tile's
@@ -289,8 +312,8 @@ __device__ __forceinline__ void spmv32_rows(const Sp32<V>& S, const V* x, const 
 #pragma unroll
           for (int t = 0; t < WMAX; ++t)
             if (t < W) {
-              prefetch_l2(S.ecol + (long)t * S.ld + j);
-              prefetch_l2(S.eval + (long)t * S.ld + j);
+              prefetch_l2(S.ecol + t * S.ld + j);
+              prefetch_l2(S.eval + t * S.ld + j);
             }
         }
       }
@@ -317,15 +340,15 @@ __device__ __forceinline__ void spmv32_rows(const Sp32<V>& S, const V* x, const 
 // y = A (z + beta pold) with each gathered entry formed as the owner row forms
 // its new search direction (first: y = A z): the product of the new direction
 // computed directly, from vectors no block writes during the pass.
-template <typename V, bool L1, int ELL, bool FULL>
+template <typename V, bool L1, int ELL, bool FULL, int WC = 0>
 __device__ __forceinline__ void spmv32_rows_dir(const Sp32<V>& S, const V* z, const V* pold, V beta, bool first,
                                                 const int (&i)[kRows], const bool (&in0)[kRows], V (&y)[kRows]) {
   bool in[kRows];
 #pragma unroll
   for (int r = 0; r < kRows; ++r) in[r] = FULL || in0[r];
   if constexpr (ELL) {
-    constexpr int WMAX = 8;
-    const int W = S.w;
+    constexpr int WMAX = WC ? WC : 8;  // WC: the ELL width known at compile time
+    const int W = WC ? WC : S.w;
     V v[kRows][WMAX], xv[kRows][WMAX];
     int c[kRows][WMAX];
 #pragma unroll
@@ -333,8 +356,8 @@ __device__ __forceinline__ void spmv32_rows_dir(const Sp32<V>& S, const V* z, co
 #pragma unroll
       for (int t = 0; t < WMAX; ++t)
         if (t < W && in[r]) {
-          c[r][t] = S.ecol[(long)t * S.ld + i[r]];
-          v[r][t] = S.eval[(long)t * S.ld + i[r]];
+          c[r][t] = S.ecol[t * S.ld + i[r]];
+          v[r][t] = S.eval[t * S.ld + i[r]];
         }
     if constexpr (ELL == 2) {
       // the same rows of this block's next tile: DRAM -> L2 while this tile's
@@ -346,8 +369,8 @@ __device__ __forceinline__ void spmv32_rows_dir(const Sp32<V>& S, const V* z, co
 #pragma unroll
           for (int t = 0; t < WMAX; ++t)
             if (t < W) {
-              prefetch_l2(S.ecol + (long)t * S.ld + j);
-              prefetch_l2(S.eval + (long)t * S.ld + j);
+              prefetch_l2(S.ecol + t * S.ld + j);
+              prefetch_l2(S.eval + t * S.ld + j);
             }
         }
       }
@@ -481,7 +504,7 @@ __device__ bool true_residual(const KrylovArgs& a, VGrid& g, Red& R, const Rows&
 
 // x += scale * d, then a barrier (neighbours' x are read next)
 template <typename V, bool L1>
-__device__ bool update_x(const KrylovArgs& a, const VGrid& g, const Rows& rows, const V* d, double scale) {
+__device__ bool update_x(const KrylovArgs& a, VGrid& g, const Rows& rows, const V* d, double scale) {
   for (int i = rows.start + threadIdx.x; i < rows.n; i += rows.stride) a.x[i] = fma(scale, (double)d[i], a.x[i]);
   return vg_sync(g, a.st);
 }
@@ -508,11 +531,13 @@ __device__ __forceinline__ bool cheb_apply(const KrylovArgs& a, const MixedArgsT
     const double rho1 = 1.0 / (2.0 * sg - rho0);
     const V c1 = (V)(rho1 * rho0), c2 = (V)(2.0 * rho1 / de);
     const bool last = (j == m.cheb_k - 1);
+    with_width<ELL>(S.w, [&](auto wc) {
+    constexpr int WC = decltype(wc)::value;
     MGPU_STEPS(rows, base) {
       MGPU_STEP_ROWS(rows, base, ii, in);
       MGPU_SPLIT_FULL(rows, base, FULL, {
         V az[kRows];
-        spmv32_rows<V, L1, ELL, FULL>(S, zc, ii, in, az);
+        spmv32_rows<V, L1, ELL, FULL, WC>(S, zc, ii, in, az);
 _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
           const int i = ii[r];
           double c[2] = {0.0, 0.0};
@@ -531,6 +556,7 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
         }
       })
     }
+    });
     if (last) {
       if (!red_total<2, L1>(R, rows, g, a.st, red)) return false;
     } else if (!vg_sync(g, a.st)) {
@@ -554,11 +580,13 @@ __device__ __forceinline__ void pcg_direct_pass(const KrylovArgs& a, const Mixed
                                                 const Rows& rows, const V* z, const V* pold, V* pnew, V* q, V beta,
                                                 bool first) {
   const Sp32<V> S = sp32_of(a, m, rows);
+  with_width<ELL>(S.w, [&](auto wc) {
+  constexpr int WC = decltype(wc)::value;
   MGPU_STEPS(rows, base) {
     MGPU_STEP_ROWS(rows, base, ii, in);
     MGPU_SPLIT_FULL(rows, base, FULL, {
       V aq[kRows];
-      spmv32_rows_dir<V, L1, ELL, FULL>(S, z, pold, beta, first, ii, in, aq);
+      spmv32_rows_dir<V, L1, ELL, FULL, WC>(S, z, pold, beta, first, ii, in, aq);
 _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
         const int i = ii[r];
         double c[1] = {0.0};
@@ -572,6 +600,7 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
       }
     })
   }
+  });
 }
 
 // v := A ph; r0.v
@@ -579,11 +608,13 @@ template <typename V, bool L1, int ELL>
 __device__ __forceinline__ void bicg_v_pass(const KrylovArgs& a, const MixedArgsT<V>& m, const Red& R, const Rows& rows,
                                             const V* ph, const V* r0, V* v) {
   const Sp32<V> S = sp32_of(a, m, rows);
+  with_width<ELL>(S.w, [&](auto wc) {
+  constexpr int WC = decltype(wc)::value;
   MGPU_STEPS(rows, base) {
     MGPU_STEP_ROWS(rows, base, ii, in);
     MGPU_SPLIT_FULL(rows, base, FULL, {
       V vv[kRows];
-      spmv32_rows<V, L1, ELL, FULL>(S, ph, ii, in, vv);
+      spmv32_rows<V, L1, ELL, FULL, WC>(S, ph, ii, in, vv);
 _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
         const int i = ii[r];
         double c[1] = {0.0};
@@ -595,6 +626,7 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
       }
     })
   }
+  });
 }
 
 // t := A sh; t.t and t.s
@@ -602,11 +634,13 @@ template <typename V, bool L1, int ELL>
 __device__ __forceinline__ void bicg_t_pass(const KrylovArgs& a, const MixedArgsT<V>& m, const Red& R, const Rows& rows,
                                             const V* sh, const V* s, V* t) {
   const Sp32<V> S = sp32_of(a, m, rows);
+  with_width<ELL>(S.w, [&](auto wc) {
+  constexpr int WC = decltype(wc)::value;
   MGPU_STEPS(rows, base) {
     MGPU_STEP_ROWS(rows, base, ii, in);
     MGPU_SPLIT_FULL(rows, base, FULL, {
       V tv[kRows];
-      spmv32_rows<V, L1, ELL, FULL>(S, sh, ii, in, tv);
+      spmv32_rows<V, L1, ELL, FULL, WC>(S, sh, ii, in, tv);
 _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
         const int i = ii[r];
         double c[2] = {0.0, 0.0};
@@ -619,6 +653,7 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
       }
     })
   }
+  });
 }
 
 // ---------------------------------------------------------------------------
@@ -767,7 +802,7 @@ __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid&
 // without an ELL copy), each gathered entry formed as its owner row forms its
 // new direction (first: y = A z): pold FP64, z the FP32 preconditioned
 // residual.
-template <bool L1, int ELL, bool FULL>
+template <bool L1, int ELL, bool FULL, int WC = 0>
 __device__ __forceinline__ void spmv64_rows_dir(const Sp32<float>& S, const double* __restrict__ ev,
                                                 const KrylovArgs& a, const float* z, const double* pold, double beta,
                                                 bool first, const int (&i)[kRows], const bool (&in0)[kRows],
@@ -776,8 +811,8 @@ __device__ __forceinline__ void spmv64_rows_dir(const Sp32<float>& S, const doub
 #pragma unroll
   for (int r = 0; r < kRows; ++r) in[r] = FULL || in0[r];
   if constexpr (ELL) {
-    constexpr int WMAX = 8;
-    const int W = S.w;
+    constexpr int WMAX = WC ? WC : 8;  // WC: the ELL width known at compile time
+    const int W = WC ? WC : S.w;
     double v[kRows][WMAX], xv[kRows][WMAX];
     int c[kRows][WMAX];
 #pragma unroll
@@ -785,8 +820,8 @@ __device__ __forceinline__ void spmv64_rows_dir(const Sp32<float>& S, const doub
 #pragma unroll
       for (int t = 0; t < WMAX; ++t)
         if (t < W && in[r]) {
-          c[r][t] = S.ecol[(long)t * S.ld + i[r]];
-          v[r][t] = ev[(long)t * S.ld + i[r]];
+          c[r][t] = S.ecol[t * S.ld + i[r]];
+          v[r][t] = ev[t * S.ld + i[r]];
         }
     if constexpr (ELL == 2) {
 #pragma unroll
@@ -796,8 +831,8 @@ __device__ __forceinline__ void spmv64_rows_dir(const Sp32<float>& S, const doub
 #pragma unroll
           for (int t = 0; t < WMAX; ++t)
             if (t < W) {
-              prefetch_l2(S.ecol + (long)t * S.ld + j);
-              prefetch_l2(ev + (long)t * S.ld + j);
+              prefetch_l2(S.ecol + t * S.ld + j);
+              prefetch_l2(ev + t * S.ld + j);
             }
         }
       }
@@ -840,11 +875,13 @@ __device__ __forceinline__ void pcg_hybrid_direct_pass(const KrylovArgs& a, cons
                                                        double* pnew, double* q, double beta, bool first) {
   const Sp32<float> S = sp32_of(a, m, rows);
   const double* __restrict__ ev = m.ell64;
+  with_width<ELL>(S.w, [&](auto wc) {
+  constexpr int WC = decltype(wc)::value;
   MGPU_STEPS(rows, base) {
     MGPU_STEP_ROWS(rows, base, ii, in);
     MGPU_SPLIT_FULL(rows, base, FULL, {
       double aq[kRows];
-      spmv64_rows_dir<L1, ELL, FULL>(S, ev, a, z, pold, beta, first, ii, in, aq);
+      spmv64_rows_dir<L1, ELL, FULL, WC>(S, ev, a, z, pold, beta, first, ii, in, aq);
 _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
         const int i = ii[r];
         double c[1] = {0.0};
@@ -858,6 +895,7 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
       }
     })
   }
+  });
 }
 
 // PCG in FP64 (x, the residual, the search direction and q = A p, every sum)

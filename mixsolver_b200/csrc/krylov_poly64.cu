@@ -10,42 +10,54 @@
 #include "krylov_poly.cuh"
 
 namespace mgpu {
+extern int g_mixed_occ;  // krylov.cu: the mixed_blocks_per_sm tuning key
 namespace {
 
-template <bool L1, int ELL>
-__global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : 2) k_pcg_poly64(KrylovArgs a, MixedArgsT<double> m) {
-  VGrid g = whole_grid(a.bar, a.partials);
+// OCC: resident blocks per SM the register budget is sized for (the
+// mixed_blocks_per_sm tuning key, as for the mixed form's kernels)
+template <bool L1, int ELL, int OCC = 2>
+__global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : OCC) k_pcg_poly64(KrylovArgs a, MixedArgsT<double> m) {
+  VGrid g = whole_grid(a.bar, a.partials, true);
   pcg_mixed_body<double, L1, ELL, !L1>(a, m, g);
 }
 
-template <bool L1, int ELL>
-__global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : 2) k_bicgstab_poly64(KrylovArgs a, MixedArgsT<double> m) {
-  VGrid g = whole_grid(a.bar, a.partials);
+template <bool L1, int ELL, int OCC = 2>
+__global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : OCC) k_bicgstab_poly64(KrylovArgs a, MixedArgsT<double> m) {
+  VGrid g = whole_grid(a.bar, a.partials, true);
   bicgstab_mixed_body<double, L1, ELL, !L1>(a, m, g);
 }
+
+// the grid kernel of an ELL mode at the tuned occupancy
+#define MGPU_POLY64_PICK(KNAME)                                                               \
+  const void* pick_##KNAME(int ell) {                                                        \
+    const int occ = g_mixed_occ;                                                             \
+    switch (ell) {                                                                           \
+      case 2:                                                                                \
+        return occ >= 4 ? (const void*)KNAME<false, 2, 4>                                    \
+                        : occ == 3 ? (const void*)KNAME<false, 2, 3> : (const void*)KNAME<false, 2>; \
+      case 1:                                                                                \
+        return occ >= 4 ? (const void*)KNAME<false, 1, 4>                                    \
+                        : occ == 3 ? (const void*)KNAME<false, 1, 3> : (const void*)KNAME<false, 1>; \
+      default:                                                                               \
+        return (const void*)KNAME<false, 0>;                                                 \
+    }                                                                                        \
+  }
+MGPU_POLY64_PICK(k_pcg_poly64)
+MGPU_POLY64_PICK(k_bicgstab_poly64)
+#undef MGPU_POLY64_PICK
 
 }  // namespace
 
 int launch_pcg_poly64(const KrylovArgs& a, const MixedArgsT<double>& m, cudaStream_t s) {
-  switch (ell_mode(m)) {
-    case 2:
-      return launch_mixed((const void*)k_pcg_poly64<true, 1>, (const void*)k_pcg_poly64<false, 2>, a, m, s);
-    case 1:
-      return launch_mixed((const void*)k_pcg_poly64<true, 1>, (const void*)k_pcg_poly64<false, 1>, a, m, s);
-    default:
-      return launch_mixed((const void*)k_pcg_poly64<true, 0>, (const void*)k_pcg_poly64<false, 0>, a, m, s);
-  }
+  const int ell = ell_mode(m);
+  return launch_mixed(ell ? (const void*)k_pcg_poly64<true, 1> : (const void*)k_pcg_poly64<true, 0>,
+                      pick_k_pcg_poly64(ell), a, m, s);
 }
 
 int launch_bicgstab_poly64(const KrylovArgs& a, const MixedArgsT<double>& m, cudaStream_t s) {
-  switch (ell_mode(m)) {
-    case 2:
-      return launch_mixed((const void*)k_bicgstab_poly64<true, 1>, (const void*)k_bicgstab_poly64<false, 2>, a, m, s);
-    case 1:
-      return launch_mixed((const void*)k_bicgstab_poly64<true, 1>, (const void*)k_bicgstab_poly64<false, 1>, a, m, s);
-    default:
-      return launch_mixed((const void*)k_bicgstab_poly64<true, 0>, (const void*)k_bicgstab_poly64<false, 0>, a, m, s);
-  }
+  const int ell = ell_mode(m);
+  return launch_mixed(ell ? (const void*)k_bicgstab_poly64<true, 1> : (const void*)k_bicgstab_poly64<true, 0>,
+                      pick_k_bicgstab_poly64(ell), a, m, s);
 }
 
 }  // namespace mgpu

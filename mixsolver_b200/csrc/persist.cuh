@@ -29,6 +29,11 @@ struct VGrid {
   unsigned long long* bar;  // the group's barrier counter
   double* partials;         // the group's reduction partials (2 halves of 4 * nb)
   int half;                 // half of the partials the next reduction writes
+  // The counter value that opens this block's next barrier, when every
+  // barrier on the counter since it was zeroed went through this object (all
+  // blocks then take the same barriers in the same order); 0 when unknown,
+  // derived from the arrival's returned count instead.
+  unsigned long long next;
   __device__ int gtid() const { return rank * blockDim.x + threadIdx.x; }
   __device__ int gstr() const { return nb * blockDim.x; }
   // Consecutive reductions alternate between the two halves: a block that
@@ -43,8 +48,10 @@ struct VGrid {
   }
 };
 
-__device__ __forceinline__ VGrid whole_grid(unsigned long long* bar, double* partials) {
-  return VGrid{(int)gridDim.x, (int)blockIdx.x, bar, partials, 0};
+// counted: the counter was zeroed for this launch and every barrier of the
+// kernel goes through the returned object (VGrid::next).
+__device__ __forceinline__ VGrid whole_grid(unsigned long long* bar, double* partials, bool counted = false) {
+  return VGrid{(int)gridDim.x, (int)blockIdx.x, bar, partials, 0, counted ? (unsigned long long)gridDim.x : 0ull};
 }
 
 // Bounded barrier of a group over a monotone 64-bit arrival counter (zeroed
@@ -62,7 +69,10 @@ __device__ __forceinline__ VGrid whole_grid(unsigned long long* bar, double* par
 // __syncthreads puts them before the block's later loads. Release and acquire
 // are cumulative in the PTX memory model, so every block's pre-barrier writes
 // are visible to every block after it without a separate fence.
-__device__ bool vg_sync(const VGrid& g, DevStatus* st) {
+// With g.next known the arrival is a reduction whose result nobody waits for
+// (red.release) and the barrier opens at g.next; otherwise the arrival
+// returns the count and the barrier opens at the end of its round.
+__device__ bool vg_sync(VGrid& g, DevStatus* st) {
   __shared__ int s_ok;
   if (g.nb == 1) {
     __syncthreads();
@@ -73,9 +83,15 @@ __device__ bool vg_sync(const VGrid& g, DevStatus* st) {
     int ok = 1;
     unsigned long long* bar = g.bar;
     const unsigned long long nb = g.nb;
-    unsigned long long old;
-    asm volatile("atom.add.release.gpu.global.u64 %0, [%1], 1;" : "=l"(old) : "l"(bar) : "memory");
-    const unsigned long long target = (old / nb + 1ull) * nb;
+    unsigned long long target;
+    if (g.next) {
+      asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(bar) : "memory");
+      target = g.next;
+    } else {
+      unsigned long long old;
+      asm volatile("atom.add.release.gpu.global.u64 %0, [%1], 1;" : "=l"(old) : "l"(bar) : "memory");
+      target = (old / nb + 1ull) * nb;
+    }
     const unsigned limit = (st && st->spin_limit) ? st->spin_limit : kSpinLimit;
     unsigned spins = 0;
     while (ld_acquire_u64(bar) < target) {
@@ -93,12 +109,14 @@ __device__ bool vg_sync(const VGrid& g, DevStatus* st) {
     }
     s_ok = ok;
   }
+  if (g.next) g.next += (unsigned long long)g.nb;
   __syncthreads();
   return s_ok != 0;
 }
 
 __device__ __forceinline__ bool grid_sync(unsigned long long* bar, DevStatus* st) {
-  return vg_sync(VGrid{(int)gridDim.x, (int)blockIdx.x, bar, nullptr, 0}, st);
+  VGrid g{(int)gridDim.x, (int)blockIdx.x, bar, nullptr, 0, 0ull};
+  return vg_sync(g, st);
 }
 
 // Vector loads inside a persistent kernel. A block reads data that other

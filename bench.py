@@ -162,7 +162,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -1095,7 +1095,10 @@ def run_serve(args):
                                "cells log-uniform in [1e4, 2e6] (pool of 13 meshes), Re uniform in [50, 2000]",
                    "budget_gb": args.budget_gb, "active_cells": args.active_cells, "mesh_pool_s": t_pool, "latency_s": {"p50": mx["p50_s"], "p99": mx["p99_s"]},
                    "mixed": mx, "fp64": legs["fp64"],
-                   "note": "the arrival rate exceeds the GPU's service rate: latency grows with the queue"},
+                   "note": (f"arrivals over {args.duration:g} s, the last request answered after {mx['wall_s']:.1f} s: "
+                            + ("the arrival rate exceeds the GPU's service rate, so latency is mostly queueing"
+                               if mx["wall_s"] > 1.5 * args.duration + 30.0 else
+                               "the GPU keeps up with the arrivals, so latency is mostly service time"))},
         "roofline": None,
         "e2e": {"value": mx["throughput_req_s"], "unit": "req/s", "h2d_bytes_per_step": None,
                 "d2h_bytes_per_step": None},

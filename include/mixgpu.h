@@ -65,7 +65,7 @@ extern "C" {
 #define MGPU_PREC_FP64_POLY 2
 
 /* One control "bc" line: mirrors bc_spec_t, mod_uns_control.f90:114-145
- * (thermal plane filters are not part of this path). */
+ * (its thermal plane filters are the MgpuTbcPlane table of MgpuCtrl). */
 typedef struct {
   int32_t zone;
   int32_t btype;
@@ -79,10 +79,26 @@ typedef struct {
   int32_t pad0;
   double lid_coord;
   double lid_vel[3];
-  int32_t ttype; /* thermal type: must be 0 (adiabatic) on this path */
+  int32_t ttype; /* walls and outlets: 0 adiabatic, 1 fixed T (tval), 2 fixed
+                   * heat flux qval into the domain; inlets: T = tval */
   int32_t pad1;
   double tval, qval;
 } MgpuBcSpec;
+
+/* One "tbc_plane" control line (parse_tbc_plane, mod_uns_control.f90:1251-
+ * 1310): on the wall or outlet zone of bc line `bc` (0-based index into
+ * MgpuCtrl.bc), the faces whose centre lies on the plane x[pdir-1] = pcoord
+ * (within 1e-4 of the mesh's largest extent) take ttype / tval / qval instead
+ * of the zone's; the first matching plane of a zone wins (at most 4 a zone). */
+typedef struct {
+  int32_t bc;
+  int32_t pdir; /* 1=x 2=y 3=z */
+  double pcoord;
+  int32_t ttype;
+  int32_t pad0;
+  double tval, qval;
+} MgpuTbcPlane;
+#define MGPU_MAXTBC 32
 
 /* Control scalars: mirrors ctrl_t, mod_uns_control.f90:148-280. */
 typedef struct {
@@ -103,6 +119,18 @@ typedef struct {
   int32_t nbc;
   int32_t n_outer_iter; /* PIMPLE outer iterations per time step (<= 0: 1) */
   MgpuBcSpec bc[MGPU_MAXBC];
+  /* Energy equation (temperature_assembly, mod_uns_simple.f90:1748-2037, the
+   * fluid/LTE branch): energy = 1 solves it after the corrections of every
+   * outer iteration / time step, with the momentum solver, into the solve
+   * slot after the pressure sweeps; 0 skips it (T stays as uploaded, which is
+   * the reference's result while T is uniform and no boundary is thermal). */
+  int32_t energy;
+  int32_t boussinesq; /* 1: -rho*beta*(T - tref)*gravity*V in the momentum rhs */
+  double cp, k_cond, tref, beta;
+  double gravity[3];
+  int32_t ntbc;
+  int32_t pad_e;
+  MgpuTbcPlane tbc[MGPU_MAXTBC];
 } MgpuCtrl;
 
 /* Face-list mesh: mirrors mesh_t/face_t, mod_uns_mesh.f90:17-54. */
@@ -131,7 +159,8 @@ int mgpu_cas_zone_names(const MgpuCasMesh* holder, char* buf, int cap, int* len)
 int mgpu_cas_free(MgpuCasMesh* holder);
 
 /* Per outer iteration (SIMPLE) or time step (PISO) record. Solve slots:
- * 0..2 momentum components, 3.. pressure-correction sweeps. */
+ * 0..2 momentum components, 3.. pressure-correction sweeps, then (energy)
+ * the temperature solve; dT_max = max |T - T before the solve|. */
 #define MGPU_MAXSOLVE 8
 typedef struct {
   int32_t it;
@@ -230,6 +259,15 @@ int mgpu_pcg_poly_solve(int n, const int32_t* row_ptr, const int32_t* col_idx, c
                         const double* b, double* x, double tol, int maxit, int precision, int cheb_degree,
                         int* it, double* res, int* ierr);
 
+/* Temperature fields (fields_t%T, T_old, T_old_old; cell order), for cases
+ * with ctrl.energy: T_old / T_old_old may be NULL (then = T). The download
+ * gives T and its Green-Gauss gradient gt(3,ncells) of the last gradient
+ * pass (either may be NULL). The reference sets the initial T in its driver
+ * (init_T + t_pert sin(pi (x - xmin) / Lx), mod_uns_driver.f90:182-196);
+ * here the host uploads it. */
+int mgpu_temperature_upload(MgpuCase* c, const double* T, const double* T_old, const double* T_old_old);
+int mgpu_temperature_download(MgpuCase* c, double* T, double* gt);
+
 /* y = A x on a host CSR matrix (csr_matvec, mod_uns_linsolver.f90:40-52). */
 int mgpu_csr_matvec(int n, const int32_t* row_ptr, const int32_t* col_idx, const double* val,
                     const double* x, double* y);
@@ -316,7 +354,15 @@ int mgpu_cg_jacobi_noalloc(int n, const int32_t* d_row_ptr, const int32_t* d_col
  * now: creating one later waits for kernels on other streams),
  * "l2_prefetch_mb" (mixed form: a system, or the systems of a batched phase
  * together, streaming more than this many MB per SpMV pass prefetch each
- * tile's successor into L2, default 96). */
+ * tile's successor into L2, default 96), "mixed_blocks_per_sm" (mixed and FP64
+ * polynomial single-system solves: 2-5 resident blocks of 256 threads per SM,
+ * the register budget sized to match, default 5), "batch_blocks_per_sm" (the
+ * same for batched lanes, default 4; set before building a batch),
+ * "spin_limit" (failed polls
+ * after which a grid-barrier wait gives up, 0 = the built-in bound of about
+ * 2 s; for tests of the timeout path), "barrier_poll_ns" (sleep between two
+ * polls of a grid-barrier wait, 0-10000 ns, default 100; 0 polls back to back
+ * and backs off by 64 ns after 256 polls). */
 int mgpu_set_tuning(const char* key, int value);
 
 /* Coupled mode (the coupling driver's hook, mod_mix_driver.f90:1032 calling

@@ -44,6 +44,14 @@ class MgpuBcSpec(C.Structure):
                 ("pad1", C.c_int32), ("tval", C.c_double), ("qval", C.c_double)]
 
 
+MAXTBC = 32
+
+
+class MgpuTbcPlane(C.Structure):
+    _fields_ = [("bc", C.c_int32), ("pdir", C.c_int32), ("pcoord", C.c_double), ("ttype", C.c_int32),
+                ("pad0", C.c_int32), ("tval", C.c_double), ("qval", C.c_double)]
+
+
 class MgpuCtrl(C.Structure):
     _fields_ = [("rho", C.c_double), ("mu", C.c_double), ("alpha_u", C.c_double),
                 ("alpha_p", C.c_double), ("outer_max", C.c_int32), ("lin_max", C.c_int32),
@@ -52,7 +60,10 @@ class MgpuCtrl(C.Structure):
                 ("transient", C.c_int32), ("time_scheme", C.c_int32), ("dt", C.c_double),
                 ("n_time_max", C.c_int32), ("n_correct", C.c_int32), ("body_force", C.c_double * 3),
                 ("inlet_ramp", C.c_int32), ("precision", C.c_int32), ("mixed_tol", C.c_double),
-                ("nbc", C.c_int32), ("n_outer_iter", C.c_int32), ("bc", MgpuBcSpec * MAXBC)]
+                ("nbc", C.c_int32), ("n_outer_iter", C.c_int32), ("bc", MgpuBcSpec * MAXBC),
+                ("energy", C.c_int32), ("boussinesq", C.c_int32), ("cp", C.c_double), ("k_cond", C.c_double),
+                ("tref", C.c_double), ("beta", C.c_double), ("gravity", C.c_double * 3), ("ntbc", C.c_int32),
+                ("pad_e", C.c_int32), ("tbc", MgpuTbcPlane * MAXTBC)]
 
 
 class MgpuMesh(C.Structure):
@@ -99,6 +110,9 @@ class BcSpec:
     uorigin: float = 0.0
     uaxis: int = 2
     lid: Optional[tuple] = None      # (dir, coord, (u, v, w)), the `lid` control line
+    ttype: int = 0                   # thermal type (walls, outlets): 0 adiabatic, 1 fixed T, 2 fixed flux
+    tval: float = 0.0
+    qval: float = 0.0
 
 
 @dataclasses.dataclass
@@ -127,6 +141,16 @@ class Ctrl:
     precision: int = PREC_FP64
     mixed_tol: float = 1.0e-4
     bcs: list = dataclasses.field(default_factory=list)
+    # energy equation (ctrl_t phase-10 fields): solved when energy is set
+    energy: bool = False
+    boussinesq: bool = False
+    cp: float = 1005.0
+    k_cond: float = 0.026
+    tref: float = 0.0
+    beta: float = 0.0
+    gravity: Sequence[float] = (0.0, 0.0, 0.0)
+    # tbc_plane lines: (bc index, dir 1-3, coord, ttype, tval, qval)
+    tbc: list = dataclasses.field(default_factory=list)
 
     def to_c(self) -> MgpuCtrl:
         c = MgpuCtrl()
@@ -153,6 +177,18 @@ class Ctrl:
                 s.has_lid, s.lid_dir, s.lid_coord = 1, int(b.lid[0]), float(b.lid[1])
                 for k in range(3):
                     s.lid_vel[k] = float(b.lid[2][k])
+            s.ttype, s.tval, s.qval = int(b.ttype), float(b.tval), float(b.qval)
+        c.energy = 1 if self.energy else 0
+        c.boussinesq = 1 if self.boussinesq else 0
+        c.cp, c.k_cond, c.tref, c.beta = float(self.cp), float(self.k_cond), float(self.tref), float(self.beta)
+        for k in range(3):
+            c.gravity[k] = float(self.gravity[k])
+        if len(self.tbc) > MAXTBC:
+            raise ValueError("too many tbc_plane lines")
+        c.ntbc = len(self.tbc)
+        for i, (bi, pdir, pc, tt, tv, qv) in enumerate(self.tbc):
+            t = c.tbc[i]
+            t.bc, t.pdir, t.pcoord, t.ttype, t.tval, t.qval = int(bi), int(pdir), float(pc), int(tt), float(tv), float(qv)
         return c
 
 
@@ -213,7 +249,8 @@ EXPORTS = ["mgpu_version", "mgpu_last_error", "mgpu_set_device", "mgpu_case_crea
            "mgpu_batch_step", "mgpu_batch_poll", "mgpu_batch_run", "mgpu_batch_info", "mgpu_batch_plan",
            "mgpu_batch_set_profiling", "mgpu_cas_read", "mgpu_cas_zone_names", "mgpu_cas_free",
            "mgpu_rcm_order_device", "mgpu_mesh_topology", "mgpu_interface_set", "mgpu_interface_mode",
-           "mgpu_interface_extract", "mgpu_pcg_poly_solve"]
+           "mgpu_interface_extract", "mgpu_pcg_poly_solve", "mgpu_temperature_upload",
+           "mgpu_temperature_download"]
 NOALLOC_MAX_ROWS = 131072
 
 _LIB = None
@@ -248,6 +285,8 @@ def load_library(path: str = LIB_PATH):
     lib.mgpu_nan_scan.argtypes = [C.c_void_p, P(C.c_int), P(C.c_int), P(C.c_int), dblp, P(C.c_int)]
     lib.mgpu_krylov_solve.argtypes = [C.c_int, i32p, i32p, dblp, dblp, dblp, C.c_double, C.c_int,
                                       C.c_int, C.c_int, P(C.c_int), dblp, P(C.c_int)]
+    lib.mgpu_temperature_upload.argtypes = [C.c_void_p, dblp, dblp, dblp]
+    lib.mgpu_temperature_download.argtypes = [C.c_void_p, dblp, dblp]
     lib.mgpu_pcg_poly_solve.argtypes = [C.c_int, i32p, i32p, dblp, dblp, dblp, C.c_double, C.c_int,
                                         C.c_int, C.c_int, P(C.c_int), dblp, P(C.c_int)]
     lib.mgpu_csr_matvec.argtypes = [C.c_int, i32p, i32p, dblp, dblp, dblp]

@@ -365,6 +365,8 @@ __device__ __forceinline__ void mom_finish(const DeviceCase& d, const AsmParams&
     rhs = rhs - pf * sfc[f];
   }
   const double vol = d.vol[c];
+  // Boussinesq buoyancy (mod_uns_simple.f90:1229-1240), before the body force
+  if (P.boussinesq) rhs = rhs - P.rho * P.beta * (d.T[c] - P.tref) * P.gravity[comp] * vol;
   if (P.has_body_force) rhs = rhs + P.body_force[comp] * vol;
   const int ts = d.st->ts_order;
   if (ts == 1) {
@@ -393,11 +395,10 @@ __device__ __forceinline__ void b_momentum(const DeviceCase& d, const AsmParams&
   const Ramp rp = ramp_of(d);
   const double* sfc = d.sf + (long)comp * F;
   double* A = d.aval;
-  const int rb = d.row_ptr[c], re = d.row_ptr[c + 1];
-  for (int k = rb; k < re; ++k) A[k] = 0.0;
   double ap = 0.0, rhs = 0.0;
   const int kb = d.cf_ptr[c], ke = d.cf_ptr[c + 1];
-  // interior faces
+  // interior faces; every off-diagonal entry of the row belongs to one of
+  // them (the diagonal is written by mom_finish)
   for (int k = kb; k < ke; ++k) {
     const int f = d.cf[k];
     const int b = d.c1[f];
@@ -407,13 +408,9 @@ __device__ __forceinline__ void b_momentum(const DeviceCase& d, const AsmParams&
     const double Fm = d.flux[f];
     const double D = d.Dm[f];
     const int slot = d.cf_slot[k];
-    if (own) {
-      ap = ap + fmax(Fm, 0.0) + D;
-      A[slot] = A[slot] - (D + fmax(-Fm, 0.0));
-    } else {
-      ap = ap + fmax(-Fm, 0.0) + D;
-      A[slot] = A[slot] - (D + fmax(Fm, 0.0));
-    }
+    const double off = own ? D + fmax(-Fm, 0.0) : D + fmax(Fm, 0.0);
+    ap = own ? ap + fmax(Fm, 0.0) + D : ap + fmax(-Fm, 0.0) + D;
+    A[slot] = (d.cf_first[k] ? 0.0 : A[slot]) - off;
     const double lf = d.lf[f], l1 = 1.0 - lf;
     if (P.conv_blend > 0.0) {
       const int cu = (Fm > 0.0) ? a : b;
@@ -452,10 +449,11 @@ __device__ __forceinline__ void b_mom_interior(const DeviceCase& d, const AsmPar
   if (d.st->abort || c >= d.N) return;
   const int N = d.N, F = d.F;
   double* A = d.aval;
-  const int rb = d.row_ptr[c], re = d.row_ptr[c + 1];
-  for (int k = rb; k < re; ++k) A[k] = 0.0;
   double ap = 0.0, r0 = 0.0, r1 = 0.0, r2 = 0.0;
   const int kb = d.cf_ptr[c], ke = d.cf_ptr[c + 1];
+  // every off-diagonal entry of the row belongs to an interior face: written
+  // at its first face, added to at a later one (0 - x is the reference's sum
+  // from its zeroed row); the diagonal is written by mom_finish
   for (int k = kb; k < ke; ++k) {
     const int f = d.cf[k];
     const int b = d.c1[f];
@@ -465,13 +463,9 @@ __device__ __forceinline__ void b_mom_interior(const DeviceCase& d, const AsmPar
     const double Fm = d.flux[f];
     const double D = d.Dm[f];
     const int slot = d.cf_slot[k];
-    if (own) {
-      ap = ap + fmax(Fm, 0.0) + D;
-      A[slot] = A[slot] - (D + fmax(-Fm, 0.0));
-    } else {
-      ap = ap + fmax(-Fm, 0.0) + D;
-      A[slot] = A[slot] - (D + fmax(Fm, 0.0));
-    }
+    const double off = own ? D + fmax(-Fm, 0.0) : D + fmax(Fm, 0.0);
+    ap = own ? ap + fmax(Fm, 0.0) + D : ap + fmax(-Fm, 0.0) + D;
+    A[slot] = (d.cf_first[k] ? 0.0 : A[slot]) - off;
     const double lf = d.lf[f], l1 = 1.0 - lf;
     if (P.nonorth_corr > 0.0) {
       const double t0 = d.tv[f], t1 = d.tv[F + f], t2 = d.tv[2 * F + f], mn = d.mnc[f];
@@ -595,7 +589,10 @@ __device__ __forceinline__ void b_ppe(const DeviceCase& d, const AsmParams& P, c
   if (d.st->abort || c >= d.N) return;
   double* A = d.pval;
   const int rb = d.row_ptr[c], re = d.row_ptr[c + 1], dg = d.diag[c];
-  for (int k = rb; k < re; ++k) A[k] = 0.0;
+  // the diagonal sums in a register in the reference's face order; each
+  // off-diagonal entry is written at its first face (0 - af: the reference's
+  // zeroed row) and added to at a later one
+  double adg = 0.0;
   double rhs = 0.0;
   for (int k = d.cf_ptr[c]; k < d.cf_ptr[c + 1]; ++k) {
     const int f = d.cf[k];
@@ -609,7 +606,7 @@ __device__ __forceinline__ void b_ppe(const DeviceCase& d, const AsmParams& P, c
       if (gi >= 0 && p_dirichlet(d.groups[gi].btype, d.iface_pdir)) {
         const double dbf = d.vol[c] / d.apc[c];
         const double af = P.rho * dbf * d.area[f] / d.dn[f];
-        if (p_dirichlet(d.groups[gi].btype, d.iface_pdir, d.st->ts_order > 0)) A[dg] = A[dg] + af;
+        if (p_dirichlet(d.groups[gi].btype, d.iface_pdir, d.st->ts_order > 0)) adg = adg + af;
         d.af[f] = af;
       }
       rhs = rhs - d.flux[f];
@@ -618,9 +615,9 @@ __device__ __forceinline__ void b_ppe(const DeviceCase& d, const AsmParams& P, c
     const double lf = d.lf[f];
     const double dbf = lf * d.vol[a] / d.apc[a] + (1.0 - lf) * d.vol[b] / d.apc[b];
     const double af = P.rho * dbf * d.area[f] / d.dn[f];
-    A[dg] = A[dg] + af;
+    adg = adg + af;
     const int slot = d.cf_slot[k];
-    A[slot] = A[slot] - af;
+    A[slot] = (d.cf_first[k] ? 0.0 : A[slot]) - af;
     if (a == c) {
       rhs = rhs - d.flux[f];
       d.af[f] = af;
@@ -628,6 +625,7 @@ __device__ __forceinline__ void b_ppe(const DeviceCase& d, const AsmParams& P, c
       rhs = rhs + d.flux[f];
     }
   }
+  A[dg] = adg;
   // the pin of cell 1 when no face is pressure-Dirichlet (serial rule for
   // SIMPLE, the one-rank mpi rule for the transient drivers)
   if (!(P.has_pdir || (d.iface_pdir && d.n_iface > 0 && d.st->ts_order == 0))) {
@@ -704,10 +702,11 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) 
 }
 
 // Diagnostics of one outer iteration / step: max|imbalance|, max|du|,
-// max|u| (transient), first non-finite value (min over cell*4+field).
+// max|u| (transient), max|T - T before its solve| (energy), first non-finite
+// value (min over cell*5+field, fields u, v, w, p, T).
 __device__ __forceinline__ void b_diag(const DeviceCase& d, int transient, const int c) {
   if (d.st->abort) return;
-  double im = 0.0, du = 0.0, um = 0.0;
+  double im = 0.0, du = 0.0, um = 0.0, dT = 0.0;
   unsigned long long key = ~0ull;
   if (c < d.N) {
     const int N = d.N;
@@ -717,22 +716,25 @@ __device__ __forceinline__ void b_diag(const DeviceCase& d, int transient, const
     }
     im = fabs(im);
     const double* ref = transient ? d.u_old : d.uo;
-    const double v[4] = {d.u[c], d.u[N + c], d.u[2 * N + c], d.p[c]};
+    const double v[5] = {d.u[c], d.u[N + c], d.u[2 * N + c], d.p[c], d.T[c]};
 #pragma unroll
     for (int q = 0; q < 3; ++q) du = fmax(du, fabs(v[q] - ref[(long)q * N + c]));
     if (transient) um = norm3(v[0], v[1], v[2]);
+    if (d.energy) dT = fabs(v[4] - d.Tprev[c]);
 #pragma unroll
-    for (int q = 3; q >= 0; --q)
-      if (!isfinite(v[q])) key = (unsigned long long)c * 4ull + (unsigned long long)q;
+    for (int q = 4; q >= 0; --q)
+      if (!isfinite(v[q])) key = (unsigned long long)c * 5ull + (unsigned long long)q;
     if (isnan(im)) im = 0.0;  // a non-finite field is reported by the scan
     if (isnan(du)) du = 0.0;
     if (isnan(um)) um = 0.0;
+    if (isnan(dT)) dT = 0.0;
   }
   // warp-level max (exact, order-independent) before the atomics
   for (int o = 16; o > 0; o >>= 1) {
     im = fmax(im, __shfl_xor_sync(0xffffffffu, im, o));
     du = fmax(du, __shfl_xor_sync(0xffffffffu, du, o));
     um = fmax(um, __shfl_xor_sync(0xffffffffu, um, o));
+    dT = fmax(dT, __shfl_xor_sync(0xffffffffu, dT, o));
     unsigned long long ko = __shfl_xor_sync(0xffffffffu, key, o);
     key = ko < key ? ko : key;
   }
@@ -740,6 +742,7 @@ __device__ __forceinline__ void b_diag(const DeviceCase& d, int transient, const
     atomic_max_pos(&d.st->imbal_bits, im);
     atomic_max_pos(&d.st->du_bits, du);
     if (transient) atomic_max_pos(&d.st->umax_bits, um);
+    if (d.energy) atomic_max_pos(&d.st->dT_bits, dT);
     if (key != ~0ull) atomicMin(&d.st->nan_key, key);
   }
 }
@@ -754,8 +757,8 @@ __device__ void b_diag_finalize(const DeviceCase& d, const AsmParams& P, int tra
   MgpuIterRec* rec = d.recs + st->cur_it;
   if (st->nan_key != ~0ull) {
     const unsigned long long k = st->nan_key;
-    const int cell = (int)(k >> 2), q = (int)(k & 3ull);
-    const double v = q < 3 ? d.u[(long)q * d.N + cell] : d.p[cell];
+    const int cell = (int)(k / 5ull), q = (int)(k % 5ull);
+    const double v = q < 3 ? d.u[(long)q * d.N + cell] : q == 3 ? d.p[cell] : d.T[cell];
     st->nan_field = q + 1;
     st->nan_cell = cell + 1;
     st->nan_val = v;
@@ -778,7 +781,8 @@ __device__ void b_diag_finalize(const DeviceCase& d, const AsmParams& P, int tra
   rec->itl_max = itl_max;
   rec->ressum = ressum;
   rec->imbal = imbal;
-  rec->dT_max = 0.0;
+  const double dTm = d.energy ? __longlong_as_double((long long)st->dT_bits) : 0.0;
+  rec->dT_max = dTm;
   if (transient) {
     st->t_now = st->t_now + P.dt;
     du = du / P.dt;
@@ -788,9 +792,9 @@ __device__ void b_diag_finalize(const DeviceCase& d, const AsmParams& P, int tra
     rec->t_now = st->t_now;
   }
   rec->du_max = du;
-  st->imbal_bits = st->du_bits = st->umax_bits = 0ull;
+  st->imbal_bits = st->du_bits = st->umax_bits = st->dT_bits = 0ull;
   st->cur_it = st->cur_it + 1;
-  if (!transient && imbal < P.outer_tol && du < P.outer_tol && 0.0 < P.outer_tol) {
+  if (!transient && imbal < P.outer_tol && du < P.outer_tol && dTm < P.outer_tol) {
     st->converged = 1;
     st->abort = 1;
   }
@@ -826,6 +830,10 @@ __device__ __forceinline__ void b_begin_iter(const DeviceCase& d, int transient,
       d.uo[i] = d.u[i];
     }
   }
+  if (transient && d.energy && i < d.N) {
+    d.T_old_old[i] = d.T_old[i];
+    d.T_old[i] = d.T[i];
+  }
   if (i == 0) {
     MgpuIterRec* rec = d.recs + d.st->cur_it;
     rec->nsolve = 0;
@@ -840,6 +848,175 @@ __device__ __forceinline__ void b_begin_iter(const DeviceCase& d, int transient,
 }
 __global__ void k_begin_iter(DeviceCase d, int transient, int time_scheme, int inlet_ramp) {
   b_begin_iter(d, transient, time_scheme, inlet_ramp, blockIdx.x * (long)blockDim.x + threadIdx.x);
+}
+
+// ---------------- energy equation ------------------------------------------
+
+// The temperature gradient gt (compute_gradients, mod_uns_fields.f90:219-237):
+// Green-Gauss over the face values (interior: linear interpolation; boundary:
+// bc_face_T's face temperature) in the cell's face order, as k_gradients.
+__device__ __forceinline__ void b_tgrad(const DeviceCase& d, const int c) {
+  if (d.st->abort || c >= d.N) return;
+  const int N = d.N, F = d.F;
+  double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+  for (int k = d.cf_ptr[c]; k < d.cf_ptr[c + 1]; ++k) {
+    const int f = d.cf[k];
+    const int a = d.c0[f], b = d.c1[f];
+    double phi;
+    if (b >= 0) {
+      const double lf = d.lf[f];
+      phi = lf * d.T[a] + (1.0 - lf) * d.T[b];
+    } else {
+      double qf;
+      bool neu;
+      bc_face_T(d.groups[d.fgrp[f]], d.xf[f], d.xf[F + f], d.xf[2 * F + f], d.T[a], phi, qf, neu);
+    }
+    const double s0 = d.sf[f], s1 = d.sf[F + f], s2 = d.sf[2 * F + f];
+    if (a == c) {
+      g0 = g0 + phi * s0;
+      g1 = g1 + phi * s1;
+      g2 = g2 + phi * s2;
+    } else {
+      g0 = g0 - phi * s0;
+      g1 = g1 - phi * s1;
+      g2 = g2 - phi * s2;
+    }
+  }
+  const double v = d.vol[c];
+  d.gt[c] = g0 / v;
+  d.gt[N + c] = g1 / v;
+  d.gt[2 * N + c] = g2 / v;
+}
+__global__ void __launch_bounds__(256) k_tgrad(DeviceCase d) { b_tgrad(d, blockIdx.x * blockDim.x + threadIdx.x); }
+
+// temperature_limiter, mod_uns_simple.f90:2302-2361: Barth-Jespersen psi_T
+// from the neighbour and boundary-face temperatures (min / max are exact in
+// any order)
+__device__ __forceinline__ void b_tlimiter(const DeviceCase& d, const int c) {
+  if (d.st->abort || c >= d.N) return;
+  const int N = d.N, F = d.F;
+  const double tc = d.T[c];
+  double pmin = tc, pmax = tc;
+  for (int k = d.cf_ptr[c]; k < d.cf_ptr[c + 1]; ++k) {
+    const int f = d.cf[k];
+    const int a = d.c0[f], b = d.c1[f];
+    double v;
+    if (b >= 0) {
+      v = d.T[a == c ? b : a];
+    } else {
+      double qf;
+      bool neu;
+      bc_face_T(d.groups[d.fgrp[f]], d.xf[f], d.xf[F + f], d.xf[2 * F + f], tc, v, qf, neu);
+    }
+    pmin = fmin(pmin, v);
+    pmax = fmax(pmax, v);
+  }
+  const double g0 = d.gt[c], g1 = d.gt[N + c], g2 = d.gt[2 * N + c];
+  const double x0 = d.xc[c], x1 = d.xc[N + c], x2 = d.xc[2 * N + c];
+  double psi = 1.0;
+  for (int k = d.cf_ptr[c]; k < d.cf_ptr[c + 1]; ++k) {
+    const int f = d.cf[k];
+    const double fr = tc + dot3(g0, g1, g2, d.xf[f] - x0, d.xf[F + f] - x1, d.xf[2 * F + f] - x2);
+    const double df = fr - tc;
+    if (df > 0.0)
+      psi = fmin(psi, (pmax - tc) / df);
+    else if (df < 0.0)
+      psi = fmin(psi, (pmin - tc) / df);
+  }
+  d.psiT[c] = fmax(0.0, fmin(1.0, psi));
+}
+__global__ void __launch_bounds__(256) k_tlimiter(DeviceCase d) { b_tlimiter(d, blockIdx.x * blockDim.x + threadIdx.x); }
+
+// temperature_assembly, mod_uns_simple.f90:1748-2037, the clear-fluid
+// branch (porosity 1, no porous or solid zones, LTE): k_eff = 1 k + (1 - 1) 0
+// and the dispersion terms add 0, formed with the reference's expressions.
+// Row c of A (the momentum matrix's storage), rhs(c) and ap(c) (unrelaxed):
+// the interior faces in the cell's face order, then its boundary faces, the
+// time term and the relaxation, each in the reference's order of sums. The
+// interior geometry reuses the face constants (dn, sf.d, and sf - d
+// area^2/sf.d, the non-orthogonal vector) that equal the reference's
+// per-face expressions.
+__device__ __forceinline__ void b_temperature(const DeviceCase& d, const AsmParams& P, const int c) {
+  if (d.st->abort || c >= d.N) return;
+  const int N = d.N, F = d.F;
+  double* A = d.aval;
+  const double k_eff = 1.0 * P.k_cond + (1.0 - 1.0) * 0.0;
+  double ap = 0.0, rhs = 0.0;
+  const int kb = d.cf_ptr[c], ke = d.cf_ptr[c + 1];
+  for (int k = kb; k < ke; ++k) {
+    const int f = d.cf[k];
+    const int b = d.c1[f];
+    if (b < 0) continue;
+    const int a = d.c0[f];
+    const bool own = (a == c);
+    const double FT = P.cp * d.flux[f];
+    const double lf = d.lf[f];
+    double kf = lf * k_eff + (1.0 - lf) * k_eff;
+    kf = kf + (lf * 0.0 + (1.0 - lf) * 0.0);
+    const double area = d.area[f];
+    const double DT = P.nonorth_corr > 0.0 ? kf * (area * area) / d.dsf[f] : kf * area / d.dn[f];
+    const double off = own ? DT + fmax(-FT, 0.0) : DT + fmax(FT, 0.0);
+    ap = own ? ap + fmax(FT, 0.0) + DT : ap + fmax(-FT, 0.0) + DT;
+    const int slot = d.cf_slot[k];
+    A[slot] = (d.cf_first[k] ? 0.0 : A[slot]) - off;
+    if (P.conv_blend > 0.0) {
+      const int cu = (FT > 0.0) ? a : b;
+      const double dc = P.conv_blend * FT *
+                        (d.psiT[cu] * dot3(d.gt[cu], d.gt[N + cu], d.gt[2 * N + cu], d.xf[f] - d.xc[cu],
+                                           d.xf[F + f] - d.xc[N + cu], d.xf[2 * F + f] - d.xc[2 * N + cu]));
+      rhs = own ? rhs - dc : rhs + dc;
+    }
+    if (P.nonorth_corr > 0.0) {
+      const double l1 = 1.0 - lf;
+      const double gf0 = lf * d.gt[a] + l1 * d.gt[b];
+      const double gf1 = lf * d.gt[N + a] + l1 * d.gt[N + b];
+      const double gf2 = lf * d.gt[2 * N + a] + l1 * d.gt[2 * N + b];
+      const double noc = P.nonorth_corr * kf * dot3(gf0, gf1, gf2, d.tv[f], d.tv[F + f], d.tv[2 * F + f]);
+      rhs = own ? rhs + noc : rhs - noc;
+    }
+  }
+  const double tc = d.T[c];
+  for (int k = kb; k < ke; ++k) {
+    const int f = d.cf[k];
+    if (d.c1[f] >= 0) continue;
+    const DevGroup& g = d.groups[d.fgrp[f]];
+    double T_face, q_face;
+    bool neu;
+    bc_face_T(g, d.xf[f], d.xf[F + f], d.xf[2 * F + f], tc, T_face, q_face, neu);
+    double kf = 1.0 * P.k_cond + (1.0 - 1.0) * 0.0;
+    kf = kf + 0.0;
+    const double DT = kf * d.area[f] / d.dn[f];
+    const double FT = P.cp * d.flux[f];
+    if (!neu) {
+      ap = ap + DT + fmax(FT, 0.0);
+      rhs = rhs + DT * T_face - fmin(FT, 0.0) * T_face;
+    } else {
+      if (fabs(q_face) > 0.0) rhs = rhs + q_face * d.area[f];
+      if (g.btype == MGPU_BC_POUTLET || g.btype == MGPU_BC_OUTFLOW) ap = ap + fmax(FT, 0.0);
+    }
+  }
+  const double vol = d.vol[c];
+  const int ts = d.st->ts_order;
+  if (ts == 1) {
+    const double at = (1.0 * P.rho * P.cp + (1.0 - 1.0) * 0.0 * 0.0) * vol / P.dt;
+    ap = ap + at;
+    rhs = rhs + at * d.T_old[c];
+  } else if (ts == 2) {
+    const double at = (1.0 * P.rho * P.cp + (1.0 - 1.0) * 0.0 * 0.0) * vol / (2.0 * P.dt);
+    ap = ap + 3.0 * at;
+    rhs = rhs + at * (4.0 * d.T_old[c] - d.T_old_old[c]);
+  }
+  if (ts > 0 && !P.pimple) {
+    A[d.diag[c]] = ap;
+  } else {
+    A[d.diag[c]] = ap / P.alpha_u;
+    rhs = rhs + (1.0 - P.alpha_u) / P.alpha_u * ap * tc;
+  }
+  d.rhs[c] = rhs;
+  d.ap[c] = ap;
+}
+__global__ void __launch_bounds__(256) k_temperature(DeviceCase d, AsmParams P) {
+  b_temperature(d, P, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------- batched launches -----------------------------------------
@@ -914,6 +1091,20 @@ int geometry_setup(DeviceCase& d, const double* x, const int* fptr, const int* f
 int launch_gradients(const DeviceCase& d, const AsmParams& P, cudaStream_t s) {
   k_gradients<<<GRID(d.N)>>>(d, P);
   MGPU_LAUNCH_CHECK("k_gradients");
+  if (d.energy) {
+    k_tgrad<<<GRID(d.N)>>>(d);
+    MGPU_LAUNCH_CHECK("k_tgrad");
+  }
+  return 0;
+}
+
+int launch_temperature(const DeviceCase& d, const AsmParams& P, cudaStream_t s) {
+  if (P.conv_blend > 0.0) {
+    k_tlimiter<<<GRID(d.N)>>>(d);
+    MGPU_LAUNCH_CHECK("k_tlimiter");
+  }
+  k_temperature<<<GRID(d.N)>>>(d, P);
+  MGPU_LAUNCH_CHECK("k_temperature");
   return 0;
 }
 int launch_limiter(const DeviceCase& d, const AsmParams& P, int comp, cudaStream_t s) {

@@ -16,6 +16,9 @@ struct AsmParams {
   int has_outflow;  // any outflow zone: global outflow rescale
   int inlet_ramp;
   int pimple;       // transient momentum keeps the alpha_u relaxation (ctrl%pimple)
+  // energy equation (ctrl_t phase-10 fields)
+  int boussinesq;
+  double cp, k_cond, tref, beta, gravity[3];
 };
 
 // One case of a batched assembly launch: its arrays, its parameters, the
@@ -65,6 +68,8 @@ int launch_batch_asm(int op, int arg, const AsmBatch& b, cudaStream_t s);
 int geometry_setup(DeviceCase& d, const double* x, const int* fptr, const int* fnodes, double* pcen,
                    const AsmParams& P, cudaStream_t s);
 int launch_gradients(const DeviceCase& d, const AsmParams& P, cudaStream_t s);
+// energy: psi_T (conv_blend > 0), then the row of the temperature equation per cell
+int launch_temperature(const DeviceCase& d, const AsmParams& P, cudaStream_t s);
 int launch_limiter(const DeviceCase& d, const AsmParams& P, int comp, cudaStream_t s);
 int launch_momentum(const DeviceCase& d, const AsmParams& P, int comp, cudaStream_t s);
 // conv_blend = 0: launch_mom_interior once per outer iteration, then before

@@ -764,6 +764,11 @@ int mgpu_batch_create(MgpuCase* const* cases, int ncases, MgpuBatch** out) {
         set_error("mgpu_batch_create: null or repeated case");
         return MGPU_E_ARG;
       }
+  for (int k = 0; k < ncases; ++k)
+    if (cases[k]->d.energy) {
+      set_error("mgpu_batch_create: cases with the energy equation are stepped one by one (mgpu_simple_run ...)");
+      return MGPU_E_ARG;
+    }
   MgpuBatch* b = new MgpuBatch();
   b->cases.assign(cases, cases + ncases);
   b->gen.assign(ncases, -1);

@@ -97,6 +97,21 @@ __global__ void k_cells_to_planes(const double* __restrict__ src, long n, int pl
 }
 
 // iface_vel(:, f) / iface_p(f) of the listed faces (0-based), u AoS (3, n)
+// cf_first: 1 for a cell-face entry whose CSR slot no earlier entry of the
+// same cell has (boundary faces, which have no slot: 0)
+__global__ void k_slot_first(int N, const int* __restrict__ cf_ptr, const int* __restrict__ cf_slot,
+                             unsigned char* __restrict__ first) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  const int kb = cf_ptr[c], ke = cf_ptr[c + 1];
+  for (int k = kb; k < ke; ++k) {
+    const int s = cf_slot[k];
+    bool f = s >= 0;
+    for (int j = kb; j < k && f; ++j) f = cf_slot[j] != s;
+    first[k] = f ? 1 : 0;
+  }
+}
+
 __global__ void k_iface_scatter(int n, const int* __restrict__ faces, const double* __restrict__ u,
                                 const double* __restrict__ p, long F, double* ivel, double* ip) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -214,7 +229,7 @@ MixedArgs mixed_args(const MgpuCase* c, bool bicg) {
   const bool big = (double)c->d.N * mixed_row_bytes(c->d.ell_w) > g_prefetch_mb * 1048576.0;
   return MixedArgs{c->d.a32,   c->d.dinv32, c->d.w32,  c->ctrl.mixed_tol > 0.0 ? c->ctrl.mixed_tol : 1e-4,
                    bicg ? 1 : g_cheb_degree, g_cheb_ratio, c->d.ell_w, c->d.ell_col, c->d.ell_val,
-                   c->d.red32, (c->d.ell_col && big) ? 1 : 0, g_rel_delta_pm * 1e-3, c->d.ell_ld, 0,
+                   c->d.red32, (c->d.ell_col && big) ? 1 : 0, 0.0, c->d.ell_ld, 0,
                    c->d.ell_val64};
 }
 
@@ -296,7 +311,33 @@ KrylovArgs ppe_args(MgpuCase* c, int slot, bool transient) {
   return a;
 }
 
+KrylovArgs temperature_args(MgpuCase* c, int slot, bool transient) {
+  KrylovArgs a = base_args(c);
+  a.aval = c->d.aval;
+  a.b = c->d.rhs;
+  a.x = c->d.T;
+  a.precond = c->ctrl.mom_solver == MGPU_MOM_JACOBI ? 1 : 0;
+  a.zero_x = 0;
+  a.mpi_mode = transient ? 1 : 0;
+  a.slot = slot;
+  a.ier_breakdown = c->P.pimple ? 55 : (transient ? 35 : 22);
+  return a;
+}
+
 namespace {
+
+// The temperature equation of a driver step (mod_uns_simple.f90:200-210,
+// mod_uns_simple_mpi.f90:467-479 / 750-760): T before the solve kept for
+// dT_max, the assembly (limiter first with conv_blend), the solve from the
+// current T with the momentum solver into record slot `slot`.
+int temperature_step(MgpuCase* c, int slot, bool transient) {
+  DeviceCase& d = c->d;
+  cudaStream_t s = c->stream;
+  MGPU_CUDA(cudaMemcpyAsync(d.Tprev, d.T, sizeof(double) * d.N, cudaMemcpyDeviceToDevice, s));
+  TRY(launch_temperature(d, c->P, s));
+  c->launches += c->P.conv_blend > 0.0 ? 2 : 1;
+  return krylov(c, temperature_args(c, slot, transient), true, s);  // slots past the record: not logged
+}
 
 int momentum_solve(MgpuCase* c, int comp, bool transient) {
   return krylov(c, mom_args(c, comp, transient), true, c->stream);
@@ -341,6 +382,7 @@ int reset_status(MgpuCase* c, int ts_order, int nrec) {
   h.nan_key = ~0ull;
   h.it_limit = nrec > 1 ? nrec - 1 : 0;
   h.spin_limit = g_spin_limit;
+  h.poll_ns = g_poll_ns;
   MGPU_CUDA(cudaMemcpyAsync(c->d.st, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
   MGPU_CUDA(cudaMemsetAsync(c->d.bar, 0, sizeof(unsigned long long), c->stream));
   MGPU_CUDA(cudaMemsetAsync(c->d.recs, 0, sizeof(MgpuIterRec) * (size_t)nrec, c->stream));
@@ -427,6 +469,7 @@ int outer_iteration(MgpuCase* c, bool transient) {
     TRY(launch_correct(d, P, s));
     c->launches += 2;
   }
+  if (d.energy) TRY(temperature_step(c, 3 + ncorr, transient));
   TRY(launch_diag(d, P, transient ? 1 : 0, s));
   c->launches += 2;
   return 0;
@@ -467,6 +510,8 @@ int pimple_step(MgpuCase* c) {
       c->launches++;
     }
   }
+  // the temperature once per step, with the final corrected velocity
+  if (d.energy) TRY(temperature_step(c, 3 + ncorr, true));
   TRY(launch_diag(d, P, 1, s));
   c->launches += 2;
   return 0;
@@ -563,6 +608,9 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
     d.nlev_lo = t.nlev_lo;
     d.nlev_up = t.nlev_up;
     d.nnz = t.nnz;
+    if ((e = c->alloc(d.cf_first, (size_t)t.ncf))) return fail(e);
+    k_slot_first<<<ceil_div(N, 256), 256, 0, c->stream>>>(d.N, d.cf_ptr, d.cf_slot, d.cf_first);
+    MGPU_CUDA(cudaGetLastError());
   }
   d.ngroups = (int)groups.size();
   if ((e = c->alloc(d.xf, 3 * F)) || (e = c->alloc(d.sf, 3 * F)) || (e = c->alloc(d.area, F)) ||
@@ -627,6 +675,29 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
   P.inlet_ramp = ctrl->inlet_ramp;
   for (int k = 0; k < 3; ++k) P.body_force[k] = ctrl->body_force[k];
   P.has_body_force = (ctrl->body_force[0] != 0.0 || ctrl->body_force[1] != 0.0 || ctrl->body_force[2] != 0.0);
+  P.boussinesq = ctrl->boussinesq ? 1 : 0;
+  P.cp = ctrl->cp;
+  P.k_cond = ctrl->k_cond;
+  P.tref = ctrl->tref;
+  P.beta = ctrl->beta;
+  for (int k = 0; k < 3; ++k) P.gravity[k] = ctrl->gravity[k];
+  d.energy = ctrl->energy ? 1 : 0;
+  // T for every case (the NaN scan reads it; zero without the energy
+  // equation), its history, gradient and solve scratch when it is solved
+  if ((e = c->alloc(d.T, N))) return fail(e);
+  MGPU_CUDA(cudaMemsetAsync(d.T, 0, sizeof(double) * N, c->stream));
+  if (d.energy) {
+    if ((e = c->alloc(d.T_old, N)) || (e = c->alloc(d.T_old_old, N)) || (e = c->alloc(d.gt, 3 * N)) ||
+        (e = c->alloc(d.Tprev, N)) || (ctrl->conv_blend > 0.0 && (e = c->alloc(d.psiT, N))))
+      return fail(e);
+    MGPU_CUDA(cudaMemsetAsync(d.T_old, 0, sizeof(double) * N, c->stream));
+    MGPU_CUDA(cudaMemsetAsync(d.T_old_old, 0, sizeof(double) * N, c->stream));
+    MGPU_CUDA(cudaMemsetAsync(d.gt, 0, sizeof(double) * 3 * N, c->stream));
+  }
+  if (P.boussinesq && !d.energy) {
+    set_error("mgpu_case_create: boussinesq needs the energy equation (ctrl.energy)");
+    return fail(MGPU_E_ARG);
+  }
   P.has_pdir = 0;
   for (int k = 0; k < hm.F; ++k)
     if (hm.c1[k] < 0 && (groups[fgrp[k]].btype == MGPU_BC_POUTLET || groups[fgrp[k]].btype == MGPU_BC_FARFIELD))
@@ -885,7 +956,7 @@ int mgpu_nan_scan(MgpuCase* c, int* ifin, int* field, int* cell, double* val, in
 
 int mgpu_case_stage(MgpuCase* c, int what, int ts_order, const double* apc, double* aval, double* rhs, double* ap,
                     const double* pp) {
-  if (!c || what < 0 || what > 6) return MGPU_E_ARG;
+  if (!c || what < 0 || what > 7 || (what == 7 && !c->d.energy)) return MGPU_E_ARG;
   DeviceCase& d = c->d;
   cudaStream_t s = c->stream;
   const long N = d.N;
@@ -905,6 +976,8 @@ int mgpu_case_stage(MgpuCase* c, int what, int ts_order, const double* apc, doub
     TRY(launch_rhiechow(d, c->P, s));
   } else if (what == 5) {
     TRY(launch_ppe(d, c->P, s));
+  } else if (what == 7) {
+    TRY(launch_temperature(d, c->P, s));
   } else {
     if (!pp) return MGPU_E_ARG;
     MGPU_CUDA(cudaMemcpyAsync(d.pp, pp, sizeof(double) * N, cudaMemcpyHostToDevice, s));
@@ -913,9 +986,48 @@ int mgpu_case_stage(MgpuCase* c, int what, int ts_order, const double* apc, doub
   }
   MGPU_CUDA(cudaStreamSynchronize(s));
   const double* A = (what == 5) ? d.pval : d.aval;
-  if (aval && (what >= 1 && what <= 5)) TRY(copy_sync(aval, A, sizeof(double) * d.nnz, cudaMemcpyDeviceToHost, c->stream));
-  if (rhs && (what >= 1 && what <= 5)) TRY(copy_sync(rhs, d.rhs, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
-  if (ap && (what >= 1 && what <= 3)) TRY(copy_sync(ap, d.ap, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
+  const bool rows = (what >= 1 && what <= 5) || what == 7;
+  if (aval && rows) TRY(copy_sync(aval, A, sizeof(double) * d.nnz, cudaMemcpyDeviceToHost, c->stream));
+  if (rhs && rows) TRY(copy_sync(rhs, d.rhs, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
+  if (ap && ((what >= 1 && what <= 3) || what == 7))
+    TRY(copy_sync(ap, d.ap, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
+  return 0;
+}
+
+int mgpu_temperature_upload(MgpuCase* c, const double* T, const double* T_old, const double* T_old_old) {
+  if (!c || !T) return MGPU_E_ARG;
+  DeviceCase& d = c->d;
+  const size_t bytes = sizeof(double) * (size_t)d.N;
+  MGPU_CUDA(cudaMemcpyAsync(d.T, T, bytes, cudaMemcpyHostToDevice, c->stream));
+  if (d.energy) {
+    if (T_old)
+      MGPU_CUDA(cudaMemcpyAsync(d.T_old, T_old, bytes, cudaMemcpyHostToDevice, c->stream));
+    else
+      MGPU_CUDA(cudaMemcpyAsync(d.T_old, d.T, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    if (T_old_old)
+      MGPU_CUDA(cudaMemcpyAsync(d.T_old_old, T_old_old, bytes, cudaMemcpyHostToDevice, c->stream));
+    else
+      MGPU_CUDA(cudaMemcpyAsync(d.T_old_old, d.T, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  MGPU_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int mgpu_temperature_download(MgpuCase* c, double* T, double* gt) {
+  if (!c) return MGPU_E_ARG;
+  DeviceCase& d = c->d;
+  const long N = d.N;
+  if (T) TRY(copy_sync(T, d.T, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
+  if (gt) {
+    if (!d.energy) {
+      std::memset(gt, 0, sizeof(double) * 3 * N);
+    } else {
+      std::vector<double> planes(3 * N);
+      TRY(copy_sync(planes.data(), d.gt, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, c->stream));
+      for (long i = 0; i < N; ++i)
+        for (int k = 0; k < 3; ++k) gt[3 * i + k] = planes[k * N + i];
+    }
+  }
   return 0;
 }
 

@@ -23,12 +23,14 @@ struct DevStatus {
   double nan_val;
   double t_now;
   unsigned long long imbal_bits, du_bits, umax_bits;  // max-reductions (bit patterns of x >= 0)
-  unsigned long long nan_key;                          // min (cell*4+field)
+  unsigned long long dT_bits;                          // max |T - T before its solve|
+  unsigned long long nan_key;                          // min (cell*5+field), fields u, v, w, p, T
   // solves of the earlier outer iterations of a PIMPLE step: largest
   // iteration count, sum of the momentum residuals (in solve order)
   int acc_itl;
   double acc_res;
   unsigned spin_limit;  // polls before a bounded barrier wait gives up (0: the default, ~2 s)
+  unsigned poll_ns;     // sleep between a barrier wait's polls (0: poll back to back)
 };
 
 // Krylov solve arguments (matrix, preconditioner data, work, result slot).
@@ -83,7 +85,7 @@ struct MixedArgsT {
   V* ell_val;          // values in the same layout (padding: 0)
   double* red;         // chunk reduction partials: mixed_red_words(N) doubles
   int pf;              // 1: each SpMV tile prefetches the next tile's ELL entries into L2
-  double rel_delta;    // PCG reliable updates: replace the recursive residual once its norm fell by this factor
+  double rel_delta;    // FP64 polynomial PCG: replace the recursive residual once its norm fell by this factor (0: only to confirm convergence)
   int ell_ld;    // leading dimension of the ELL arrays: N rounded up to a multiple of 4
   // single-system grid launches: chunk-sum slots per sum a block keeps in its
   // dynamic shared memory (set at launch; 0 elsewhere)
@@ -150,6 +152,15 @@ struct DeviceCase {
   // cells
   double *vol = nullptr, *xc = nullptr;  // xc: 3 SoA planes
   int *cf_ptr = nullptr, *cf = nullptr, *cf_slot = nullptr;
+  // per cell-face entry: 1 when no earlier entry of the cell has the same CSR
+  // slot (two faces between the same two cells share one), so the assembly
+  // writes the slot instead of adding to it
+  unsigned char* cf_first = nullptr;
+  // energy equation: T (N), its history, gradient (3 planes of N), T before
+  // the solve, limiter (conv_blend > 0); energy: the equation is solved
+  double *T = nullptr, *T_old = nullptr, *T_old_old = nullptr, *gt = nullptr, *Tprev = nullptr,
+         *psiT = nullptr;
+  int energy = 0;
   // per-face constants (bit-identical to recomputing them in the face loops)
   double *dn = nullptr;   // interior |xc1-xc0|, boundary |xf-xc0|
   double *dsf = nullptr;  // interior (xc1-xc0).sf

@@ -86,8 +86,8 @@ extern int g_cheb_degree;
 extern double g_cheb_ratio;
 extern int g_batch_reserve;
 extern int g_prefetch_mb;
-extern int g_rel_delta_pm;
 extern unsigned g_spin_limit;
+extern unsigned g_poll_ns;
 
 KrylovArgs base_args(MgpuCase* c);
 MixedArgs mixed_args(const MgpuCase* c, bool bicg);

@@ -77,6 +77,11 @@ struct DevGroup {
   double prfl_mean, prfl_span, prfl_origin;
   double lid_coord, lid_tol;
   double lid_vel[3];
+  // thermal data (walls, outlets, inlets): zone type/values, plane filters
+  int ttype, ntbc;
+  double tval, qval, tbc_tol;
+  int tbc_pdir[4], tbc_ttype[4];  // pdir 0-based
+  double tbc_pcoord[4], tbc_tval[4], tbc_qval[4];
 };
 
 // Boundary state in effect besides the groups: the cold-start ramp factors and
@@ -186,6 +191,41 @@ __device__ inline double bc_face_p(const DevGroup& g, const Ramp& rp, double pP,
   if (g.btype == MGPU_BC_POUTLET || g.btype == MGPU_BC_FARFIELD) return g.pval * rp.pval;
   if (g.btype == MGPU_BC_INTERFACE && rp.ipdir) return rp.ip[face];
   return pP;
+}
+
+// bc_face_T, mod_uns_bc.f90:560-703 (the clear-fluid branch): the face
+// temperature and heat flux of a boundary face and whether it is Neumann.
+// Interface faces take the peer's temperature, 0 on this path.
+__device__ inline void bc_face_T(const DevGroup& g, double xf0, double xf1, double xf2, double T_cell,
+                                 double& T_face, double& q_face, bool& neumann) {
+  T_face = T_cell;
+  q_face = 0.0;
+  neumann = true;
+  const int bt = g.btype;
+  if (bt == MGPU_BC_WALL || bt == MGPU_BC_POUTLET || bt == MGPU_BC_OUTFLOW) {
+    int tt = g.ttype;
+    double tv = g.tval, qv = g.qval;
+    const double xf[3] = {xf0, xf1, xf2};
+    for (int ipl = 0; ipl < g.ntbc; ++ipl)
+      if (fabs(xf[g.tbc_pdir[ipl]] - g.tbc_pcoord[ipl]) <= g.tbc_tol) {
+        tt = g.tbc_ttype[ipl];
+        tv = g.tbc_tval[ipl];
+        qv = g.tbc_qval[ipl];
+        break;
+      }
+    if (tt == 1) {
+      neumann = false;
+      T_face = tv;
+    } else if (tt == 2) {
+      q_face = qv;
+    }
+  } else if (bt == MGPU_BC_VINLET || bt == MGPU_BC_VINLET_PARAB || bt == MGPU_BC_MASSINLET) {
+    neumann = false;
+    T_face = g.tval;
+  } else if (bt == MGPU_BC_INTERFACE) {
+    neumann = false;
+    T_face = 0.0;
+  }
 }
 
 // bc_face_p_dirichlet, mod_uns_bc.f90:879-893 (ipdir: g_iface_p_dir); the

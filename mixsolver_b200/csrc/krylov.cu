@@ -50,9 +50,10 @@ int g_batch_reserve = 0;  // block slots batched launches leave to other streams
 int g_prefetch_mb = 96;   // mixed systems whose streamed bytes exceed this prefetch into L2
 int prewarm_streams(int n);  // case.cu
 double g_cheb_ratio = 1000.0; // and the ratio lambda_max / lambda_min of its interval
-int g_rel_delta_pm = 100; // reliable updates: residual replaced after a fall by this many thousandths
 unsigned g_spin_limit = 0; // polls before a bounded barrier wait gives up (0: kSpinLimit, ~2 s)
-int g_mixed_occ = 3;       // mixed and FP64 polynomial kernels: resident blocks per SM (2-4)
+unsigned g_poll_ns = 100;  // sleep between the polls of a barrier wait (ns)
+int g_mixed_occ = 5;       // mixed and FP64 polynomial kernels: resident blocks per SM (2-5)
+int g_batch_occ = 4;       // batched lane kernel: resident blocks per SM (2-5)
 namespace {
 
 __device__ __forceinline__ double ld_relaxed_f64(const double* p) {
@@ -753,12 +754,14 @@ int set_tuning(const char* key, int value) {
     g_batch_reserve = value;
   } else if (k == "l2_prefetch_mb" && value >= 0) {
     g_prefetch_mb = value;
-  } else if (k == "reliable_delta_permille" && value >= 1 && value <= 900) {
-    g_rel_delta_pm = value;
-  } else if (k == "mixed_blocks_per_sm" && value >= 2 && value <= 4) {
+  } else if (k == "mixed_blocks_per_sm" && value >= 2 && value <= 5) {
     g_mixed_occ = value;
+  } else if (k == "batch_blocks_per_sm" && value >= 2 && value <= 5) {
+    g_batch_occ = value;
   } else if (k == "spin_limit" && value >= 0) {
     g_spin_limit = (unsigned)value;
+  } else if (k == "barrier_poll_ns" && value >= 0 && value <= 10000) {
+    g_poll_ns = (unsigned)value;
   } else if (k == "stream_pool" && value >= 0 && value <= 1024) {
     if (int e = prewarm_streams(value)) return e;
   } else {

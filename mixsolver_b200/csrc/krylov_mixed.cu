@@ -4,11 +4,13 @@
 // and the batched lane kernel that runs many systems in one launch.
 
 #include <algorithm>
+#include <type_traits>
 
 #include "krylov_poly.cuh"
 
 namespace mgpu {
 extern int g_mixed_occ;  // krylov.cu: the mixed_blocks_per_sm tuning key
+extern int g_batch_occ;  // krylov.cu: the batch_blocks_per_sm tuning key
 namespace {
 
 // ---------------------------------------------------------------------------
@@ -16,7 +18,7 @@ namespace {
 // ---------------------------------------------------------------------------
 
 // OCC: resident blocks per SM the register budget is sized for (2: 128
-// registers a thread; 3: 80; 4: 64), chosen at launch for both solvers
+// registers a thread; 3: 80; 4: 64; 5: 48), chosen at launch for both solvers
 // (tuning key "mixed_blocks_per_sm")
 template <bool L1, int ELL, int OCC = 2>
 __global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : OCC) k_pcg_mixed(KrylovArgs a, MixedArgs m) {
@@ -54,8 +56,8 @@ __device__ __forceinline__ int lane_fetch(const LanePlan& p, int cls) {
 // synchronises with __syncthreads): one body per kernel, inlined, with
 // the system's descriptor read through a read-only pointer, keeps the
 // descriptor fields out of the register budget.
-template <bool PCG, int ELL>
-__global__ void __launch_bounds__(256, 2) k_mixed_batch(LanePlan p) {
+template <bool PCG, int ELL, int OCC = 2>
+__global__ void __launch_bounds__(256, OCC) k_mixed_batch(LanePlan p) {
   __shared__ int s_idx;
   const int li = p.block_lane[blockIdx.x];
   const BatchLane L = p.lanes[li];
@@ -89,69 +91,73 @@ __global__ void __launch_bounds__(256, 2) k_mixed_batch(LanePlan p) {
   if (p.lane_t && g.rank == 0 && threadIdx.x == 0) p.lane_t[2 * li + 1] = globaltimer_ns();
 }
 
+// f(std::integral_constant<int, OCC>{}) for the compiled occupancy nearest
+// below occ (2 to 5 blocks per SM)
+template <typename F>
+const void* by_occ(int occ, F&& f) {
+  switch (occ >= 5 ? 5 : occ) {
+    case 5:
+      return f(std::integral_constant<int, 5>{});
+    case 4:
+      return f(std::integral_constant<int, 4>{});
+    case 3:
+      return f(std::integral_constant<int, 3>{});
+    default:
+      return f(std::integral_constant<int, 2>{});
+  }
+}
+
 // ell: 0 CSR, 1 ELL, 2 ELL with the L2 prefetch of the next tile
-const void* batch_kernel(bool pcg, int ell) {
-  if (pcg)
-    return ell == 2 ? (const void*)k_mixed_batch<true, 2>
-                    : ell == 1 ? (const void*)k_mixed_batch<true, 1> : (const void*)k_mixed_batch<true, 0>;
-  return ell == 2 ? (const void*)k_mixed_batch<false, 2>
-                  : ell == 1 ? (const void*)k_mixed_batch<false, 1> : (const void*)k_mixed_batch<false, 0>;
+const void* batch_kernel(bool pcg, int ell, int occ) {
+  return by_occ(occ, [&](auto o) {
+    constexpr int O = decltype(o)::value;
+    if (pcg)
+      return ell == 2 ? (const void*)k_mixed_batch<true, 2, O>
+                      : ell == 1 ? (const void*)k_mixed_batch<true, 1, O> : (const void*)k_mixed_batch<true, 0, O>;
+    return ell == 2 ? (const void*)k_mixed_batch<false, 2, O>
+                    : ell == 1 ? (const void*)k_mixed_batch<false, 1, O> : (const void*)k_mixed_batch<false, 0, O>;
+  });
 }
 
 }  // namespace
 
 int launch_pcg_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s) {
-  const void* one = ell_mode(m) == 0 ? (const void*)k_pcg_mixed<true, 0> : (const void*)k_pcg_mixed<true, 1>;
-  const void* grid = nullptr;
-  switch (ell_mode(m)) {
-    case 2:
-      grid = g_mixed_occ >= 4 ? (const void*)k_pcg_mixed<false, 2, 4>
-                            : g_mixed_occ == 3 ? (const void*)k_pcg_mixed<false, 2, 3> : (const void*)k_pcg_mixed<false, 2>;
-      break;
-    case 1:
-      grid = g_mixed_occ >= 4 ? (const void*)k_pcg_mixed<false, 1, 4>
-                            : g_mixed_occ == 3 ? (const void*)k_pcg_mixed<false, 1, 3> : (const void*)k_pcg_mixed<false, 1>;
-      break;
-    default:
-      grid = (const void*)k_pcg_mixed<false, 0>;
-  }
+  const int ell = ell_mode(m);
+  const void* one = ell == 0 ? (const void*)k_pcg_mixed<true, 0> : (const void*)k_pcg_mixed<true, 1>;
+  const void* grid = by_occ(g_mixed_occ, [&](auto o) {
+    constexpr int O = decltype(o)::value;
+    return ell == 2 ? (const void*)k_pcg_mixed<false, 2, O>
+                    : ell == 1 ? (const void*)k_pcg_mixed<false, 1, O> : (const void*)k_pcg_mixed<false, 0, O>;
+  });
   return launch_mixed(one, grid, a, m, s);
 }
 
 int launch_bicgstab_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s) {
-  const void* one = ell_mode(m) == 0 ? (const void*)k_bicgstab_mixed<true, 0> : (const void*)k_bicgstab_mixed<true, 1>;
-  const void* grid = nullptr;
-  switch (ell_mode(m)) {
-    case 2:
-      grid = g_mixed_occ >= 4 ? (const void*)k_bicgstab_mixed<false, 2, 4>
-                            : g_mixed_occ == 3 ? (const void*)k_bicgstab_mixed<false, 2, 3>
-                                             : (const void*)k_bicgstab_mixed<false, 2>;
-      break;
-    case 1:
-      grid = g_mixed_occ >= 4 ? (const void*)k_bicgstab_mixed<false, 1, 4>
-                            : g_mixed_occ == 3 ? (const void*)k_bicgstab_mixed<false, 1, 3>
-                                             : (const void*)k_bicgstab_mixed<false, 1>;
-      break;
-    default:
-      grid = (const void*)k_bicgstab_mixed<false, 0>;
-  }
+  const int ell = ell_mode(m);
+  const void* one = ell == 0 ? (const void*)k_bicgstab_mixed<true, 0> : (const void*)k_bicgstab_mixed<true, 1>;
+  const void* grid = by_occ(g_mixed_occ, [&](auto o) {
+    constexpr int O = decltype(o)::value;
+    return ell == 2 ? (const void*)k_bicgstab_mixed<false, 2, O>
+                    : ell == 1 ? (const void*)k_bicgstab_mixed<false, 1, O> : (const void*)k_bicgstab_mixed<false, 0, O>;
+  });
   return launch_mixed(one, grid, a, m, s);
 }
 
 int batch_capacity(bool pcg, int ell) {
   constexpr int kDevs = 64;  // per device: the GPUs of a node may differ
-  static int cap[kDevs][6] = {};
+  static int cap[kDevs][6][6] = {};
   const int idx = (pcg ? 3 : 0) + ell;
+  const int occ = std::min(std::max(g_batch_occ, 2), 5);
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= kDevs) dev = 0;
-  if (cap[dev][idx] == 0) {
+  if (cap[dev][idx][occ] == 0) {
     int sms = 0, per = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel(pcg, ell), 256, 0);
-    cap[dev][idx] = sms * (per < 1 ? 1 : per);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch_kernel(pcg, ell, occ), 256, 0);
+    cap[dev][idx][occ] = sms * (per < 1 ? 1 : per);
   }
-  return cap[dev][idx];
+  return cap[dev][idx][occ];
 }
 
 int launch_mixed_batch(const LanePlan& p, bool pcg, int ell, cudaStream_t s) {
@@ -165,7 +171,7 @@ int launch_mixed_batch(const LanePlan& p, bool pcg, int ell, cudaStream_t s) {
   if (e != cudaSuccess) return cuda_fail(e, "lane barrier reset", __FILE__, __LINE__);
   LanePlan pp = p;
   void* args[] = {(void*)&pp};
-  e = cudaLaunchCooperativeKernel(batch_kernel(pcg, ell), dim3(p.nblocks), dim3(256), args, 0, s);
+  e = cudaLaunchCooperativeKernel(batch_kernel(pcg, ell, g_batch_occ), dim3(p.nblocks), dim3(256), args, 0, s);
   if (e != cudaSuccess) return cuda_fail(e, "cooperative launch (batched)", __FILE__, __LINE__);
   return 0;
 }

@@ -660,18 +660,18 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
 // PCG (pressure correction): Jacobi or Chebyshev-Jacobi preconditioned
 // ---------------------------------------------------------------------------
 
-// Reliable updates. One FP32 CG stream runs on the residual scaled by the
-// fixed factor sc = 1 / |b - A x0|; every iteration adds its step to the FP64
-// solution (x += alpha |r0| p); whenever the FP32 residual's norm has fallen
-// by rel_delta since the last replacement, or says the solve has converged,
-// an FP64 pass forms r = b - A x and puts sc r in its place. The search
-// direction p, its product q and r.z are kept across a replacement, so the
-// Krylov space is not thrown away as in a restarted refinement; the true
-// residual decides convergence. q = A p is formed directly every iteration
-// (pcg_direct_pass), not recurred: in FP32 the recurrence drifts from A p and
-// costs iterations. On entry a.r holds b - A x0 and rnorm0 its
-// norm. Barriers: every pass that writes x, rr or z ends in a reduction
-// (one grid barrier), which is also the barrier before the next SpMV pass.
+// PCG in working precision V on the residual scaled by the fixed factor
+// sc = 1 / |b - A x0|, with reliable updates: every iteration adds its step to
+// the FP64 solution (x += alpha |r0| p); whenever the recursive residual's norm
+// has fallen by rel_delta since the last replacement (rel_delta 0: never), or
+// says the solve has converged, an FP64 pass forms r = b - A x and puts sc r
+// in its place, keeping p, q and r.z, so the Krylov space survives; the true
+// residual decides convergence. The FP64 polynomial form runs it with
+// V = double and rel_delta 0 (plain FP64 PCG, b - A x only to confirm). q = A
+// p is formed directly every iteration (pcg_direct_pass), not recurred. On
+// entry a.r holds b - A x0 and rnorm0 its norm. Barriers: every pass that
+// writes x, rr or z ends in a reduction (one grid barrier), which is also the
+// barrier before the next SpMV pass.
 template <typename V, bool L1, int ELL>
 __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid& g, Red& R, const Rows& rows,
                              double bnrm, double rnorm0, double lmax, V inv_th) {

@@ -7,6 +7,8 @@
 // stream with x in FP64 and replaces the recursive residual by b - A x only to
 // confirm convergence (reliable updates with no intermediate replacement).
 
+#include <algorithm>
+
 #include "krylov_poly.cuh"
 
 namespace mgpu {
@@ -27,20 +29,20 @@ __global__ void __launch_bounds__(L1 ? 512 : 256, L1 ? 1 : OCC) k_bicgstab_poly6
   bicgstab_mixed_body<double, L1, ELL, !L1>(a, m, g);
 }
 
-// the grid kernel of an ELL mode at the tuned occupancy
-#define MGPU_POLY64_PICK(KNAME)                                                               \
-  const void* pick_##KNAME(int ell) {                                                        \
-    const int occ = g_mixed_occ;                                                             \
-    switch (ell) {                                                                           \
-      case 2:                                                                                \
-        return occ >= 4 ? (const void*)KNAME<false, 2, 4>                                    \
-                        : occ == 3 ? (const void*)KNAME<false, 2, 3> : (const void*)KNAME<false, 2>; \
-      case 1:                                                                                \
-        return occ >= 4 ? (const void*)KNAME<false, 1, 4>                                    \
-                        : occ == 3 ? (const void*)KNAME<false, 1, 3> : (const void*)KNAME<false, 1>; \
-      default:                                                                               \
-        return (const void*)KNAME<false, 0>;                                                 \
-    }                                                                                        \
+// the grid kernel of an ELL mode at the tuned occupancy (2 to 5 blocks per SM)
+#define MGPU_POLY64_PICK(KNAME)                                                   \
+  const void* pick_##KNAME(int ell) {                                            \
+    switch (std::min(std::max(g_mixed_occ, 2), 5) * 3 + ell) {                   \
+      case 5 * 3 + 2: return (const void*)KNAME<false, 2, 5>;                    \
+      case 5 * 3 + 1: return (const void*)KNAME<false, 1, 5>;                    \
+      case 4 * 3 + 2: return (const void*)KNAME<false, 2, 4>;                    \
+      case 4 * 3 + 1: return (const void*)KNAME<false, 1, 4>;                    \
+      case 3 * 3 + 2: return (const void*)KNAME<false, 2, 3>;                    \
+      case 3 * 3 + 1: return (const void*)KNAME<false, 1, 3>;                    \
+      case 2 * 3 + 2: return (const void*)KNAME<false, 2, 2>;                    \
+      case 2 * 3 + 1: return (const void*)KNAME<false, 1, 2>;                    \
+      default: return (const void*)KNAME<false, 0, 2>;                           \
+    }                                                                            \
   }
 MGPU_POLY64_PICK(k_pcg_poly64)
 MGPU_POLY64_PICK(k_bicgstab_poly64)

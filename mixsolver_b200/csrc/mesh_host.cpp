@@ -204,10 +204,30 @@ int build_groups(const HostMesh& m, const MgpuCtrl& ctrl, std::vector<DevGroup>&
       }
       g.uspeed = sp.mdot / ctrl.rho;
     }
-    if (sp.ttype != 0 || sp.tval != 0.0 || sp.qval != 0.0) {
-      why = "thermal boundary values: the energy equation is not part of this path";
+    if (!ctrl.energy && (sp.ttype != 0 || sp.tval != 0.0 || sp.qval != 0.0)) {
+      why = "thermal boundary values need ctrl.energy (the temperature equation)";
       return MGPU_E_ARG;
     }
+    g.ttype = sp.ttype;
+    g.tval = sp.tval;
+    g.qval = sp.qval;
+    g.ntbc = 0;
+    for (int t = 0; t < ctrl.ntbc && t < MGPU_MAXTBC; ++t) {
+      const MgpuTbcPlane& pl = ctrl.tbc[t];
+      if (pl.bc != i) continue;
+      if (g.ntbc >= 4 || pl.pdir < 1 || pl.pdir > 3) {
+        ier = 15;
+        why = "tbc_plane: at most 4 planes a zone, direction 1|2|3";
+        return MGPU_E_BC;
+      }
+      g.tbc_pdir[g.ntbc] = pl.pdir - 1;
+      g.tbc_pcoord[g.ntbc] = pl.pcoord;
+      g.tbc_ttype[g.ntbc] = pl.ttype;
+      g.tbc_tval[g.ntbc] = pl.tval;
+      g.tbc_qval[g.ntbc] = pl.qval;
+      ++g.ntbc;
+    }
+    g.tbc_tol = g.ntbc > 0 ? 1.0e-4 * crange : 0.0;
     g.has_lid = sp.has_lid ? 1 : 0;
     g.lid_dir = sp.lid_dir - 1;
     if (g.has_lid && (sp.lid_dir < 1 || sp.lid_dir > 3)) {

@@ -92,11 +92,18 @@ __device__ bool vg_sync(VGrid& g, DevStatus* st) {
       asm volatile("atom.add.release.gpu.global.u64 %0, [%1], 1;" : "=l"(old) : "l"(bar) : "memory");
       target = (old / nb + 1ull) * nb;
     }
-    const unsigned limit = (st && st->spin_limit) ? st->spin_limit : kSpinLimit;
+    const unsigned pns = st ? st->poll_ns : 0u;
+    // the built-in bound counts polls of ~60 ns; a back-off stretches each
+    const unsigned limit = (st && st->spin_limit)
+                               ? st->spin_limit
+                               : (unsigned)((unsigned long long)kSpinLimit * 64ull / (64ull + pns));
     unsigned spins = 0;
     while (ld_acquire_u64(bar) < target) {
       ++spins;
-      if (spins > 256u) __nanosleep(64);
+      if (pns)
+        __nanosleep(pns);
+      else if (spins > 256u)
+        __nanosleep(64);
       if ((spins & 4095u) == 0 && st && ld_acquire_i32(&st->timeout) != 0) {
         ok = 0;
         break;

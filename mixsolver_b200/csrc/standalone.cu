@@ -15,6 +15,7 @@
 
 namespace mgpu {
 extern unsigned g_spin_limit;  // krylov.cu: the spin_limit tuning key
+extern unsigned g_poll_ns;     // krylov.cu: the barrier_poll_ns tuning key
 extern int g_cheb_degree;      // the cheb_degree and cheb_ratio tuning keys
 extern double g_cheb_ratio;
 extern int g_prefetch_mb;      // l2_prefetch_mb
@@ -158,6 +159,7 @@ int poly_solve(int n, const Pattern& P, const double* val, const double* b, doub
   DevStatus h{};
   h.nan_key = ~0ull;
   h.spin_limit = g_spin_limit;
+  h.poll_ns = g_poll_ns;
   MGPU_CUDA(cudaMemcpy(dst, &h, sizeof(h), cudaMemcpyHostToDevice));
   MGPU_CUDA(cudaMemset(drec, 0, sizeof(MgpuIterRec)));
   KrylovArgs a{};
@@ -266,6 +268,7 @@ int mgpu_krylov_solve(int n, const int32_t* row_ptr, const int32_t* col_idx, con
   DevStatus h{};
   h.nan_key = ~0ull;
   h.spin_limit = g_spin_limit;
+  h.poll_ns = g_poll_ns;
   MGPU_CUDA(cudaMemcpy(dst, &h, sizeof(h), cudaMemcpyHostToDevice));
   MGPU_CUDA(cudaMemset(dbar, 0, sizeof(unsigned long long)));
   MGPU_CUDA(cudaMemset(drec, 0, sizeof(MgpuIterRec)));

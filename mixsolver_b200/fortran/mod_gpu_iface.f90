@@ -34,6 +34,14 @@ module mod_gpu_iface
       real(c_double)     :: tval = 0.0_c_double, qval = 0.0_c_double
    end type mgpu_bc_spec
 
+   ! MgpuTbcPlane: one tbc_plane line (bc: 0-based index of its bc line)
+   type, bind(C), public :: mgpu_tbc_plane
+      integer(c_int32_t) :: bc = 0, pdir = 0
+      real(c_double)     :: pcoord = 0.0_c_double
+      integer(c_int32_t) :: ttype = 0, pad0 = 0
+      real(c_double)     :: tval = 0.0_c_double, qval = 0.0_c_double
+   end type mgpu_tbc_plane
+
    ! MgpuCtrl: the ctrl_t scalars of this path plus the library's options
    type, bind(C), public :: mgpu_ctrl
       real(c_double)     :: rho, mu, alpha_u, alpha_p
@@ -47,6 +55,11 @@ module mod_gpu_iface
       real(c_double)     :: mixed_tol
       integer(c_int32_t) :: nbc, n_outer_iter
       type(mgpu_bc_spec) :: bc(32)
+      integer(c_int32_t) :: energy, boussinesq
+      real(c_double)     :: cp, k_cond, tref, beta
+      real(c_double)     :: gravity(3)
+      integer(c_int32_t) :: ntbc, pad_e
+      type(mgpu_tbc_plane) :: tbc(32)
    end type mgpu_ctrl
 
    ! MgpuMesh: the face list of mesh_t, flattened
@@ -64,7 +77,8 @@ module mod_gpu_iface
    end type mgpu_iter_rec
 
    public :: mgpu_set_device, mgpu_last_error, mgpu_case_create, mgpu_case_destroy, &
-             mgpu_fields_upload, mgpu_fields_download, mgpu_simple_run, mgpu_piso_run, &
+             mgpu_fields_upload, mgpu_fields_download, mgpu_temperature_upload, &
+             mgpu_temperature_download, mgpu_simple_run, mgpu_piso_run, &
              mgpu_pimple_run, mgpu_nan_scan, mgpu_krylov_solve, mgpu_csr_matvec, mgpu_set_tuning, &
              mgpu_error_message
 
@@ -102,6 +116,18 @@ module mod_gpu_iface
          import :: c_int, c_ptr
          type(c_ptr), value :: case_h, u, p, flux, gp, gu, apc
       end function mgpu_fields_download
+
+      integer(c_int) function mgpu_temperature_upload(case_h, T, T_old, T_old_old) &
+            bind(C, name='mgpu_temperature_upload')
+         import :: c_int, c_ptr
+         type(c_ptr), value :: case_h, T, T_old, T_old_old
+      end function mgpu_temperature_upload
+
+      integer(c_int) function mgpu_temperature_download(case_h, T, gt) &
+            bind(C, name='mgpu_temperature_download')
+         import :: c_int, c_ptr
+         type(c_ptr), value :: case_h, T, gt
+      end function mgpu_temperature_download
 
       integer(c_int) function mgpu_simple_run(case_h, nsteps, log, logcap, nrec, ier) &
             bind(C, name='mgpu_simple_run')

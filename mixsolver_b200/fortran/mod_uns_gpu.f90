@@ -87,7 +87,7 @@ contains
    subroutine pack_ctrl(ctrl, cc)
       type(ctrl_t),    intent(in)  :: ctrl
       type(mgpu_ctrl), intent(out) :: cc
-      integer :: i
+      integer :: i, k
       character(len=32) :: form
       cc%rho = ctrl%rho
       cc%mu = ctrl%mu
@@ -134,6 +134,27 @@ contains
          cc%bc(i)%tval = ctrl%bc(i)%tval
          cc%bc(i)%qval = ctrl%bc(i)%qval
       end do
+      ! the energy equation, which the reference's drivers always solve
+      cc%energy = 1
+      cc%boussinesq = merge(1, 0, ctrl%boussinesq)
+      cc%cp = ctrl%cp
+      cc%k_cond = ctrl%k_cond
+      cc%tref = ctrl%tref
+      cc%beta = ctrl%beta
+      cc%gravity = ctrl%gravity
+      cc%ntbc = 0
+      do i = 1, cc%nbc
+         do k = 1, ctrl%bc(i)%ntbc_plane
+            if (cc%ntbc >= 32) exit
+            cc%ntbc = cc%ntbc + 1
+            cc%tbc(cc%ntbc)%bc = i - 1
+            cc%tbc(cc%ntbc)%pdir = ctrl%bc(i)%tbc_pdir(k)
+            cc%tbc(cc%ntbc)%pcoord = ctrl%bc(i)%tbc_pcoord(k)
+            cc%tbc(cc%ntbc)%ttype = ctrl%bc(i)%tbc_pttype(k)
+            cc%tbc(cc%ntbc)%tval = ctrl%bc(i)%tbc_ptval(k)
+            cc%tbc(cc%ntbc)%qval = ctrl%bc(i)%tbc_pqval(k)
+         end do
+      end do
    end subroutine pack_ctrl
 
    ! The resident case of this mesh (made on first use or after the mesh changed).
@@ -167,13 +188,18 @@ contains
       type(fields_t), target, intent(inout) :: fld
       integer,                intent(out)   :: ier
       integer(c_int) :: rc, nrec, cier
-      type(c_ptr) :: uo, uoo
+      type(c_ptr) :: uo, uoo, to, too
       ier = 0
       uo = c_null_ptr
       uoo = c_null_ptr
+      to = c_null_ptr
+      too = c_null_ptr
       if (kind /= 1 .and. allocated(fld%u_old)) uo = c_loc(fld%u_old)
       if (kind /= 1 .and. allocated(fld%u_old_old)) uoo = c_loc(fld%u_old_old)
+      if (kind /= 1 .and. allocated(fld%T_old)) to = c_loc(fld%T_old)
+      if (kind /= 1 .and. allocated(fld%T_old_old)) too = c_loc(fld%T_old_old)
       rc = mgpu_fields_upload(g_case, c_loc(fld%u), c_loc(fld%p), c_loc(fld%flux), uo, uoo)
+      if (rc == MGPU_OK) rc = mgpu_temperature_upload(g_case, c_loc(fld%T), to, too)
       if (rc == MGPU_OK) then
          select case (kind)
          case (1)
@@ -186,6 +212,7 @@ contains
       end if
       if (rc == MGPU_OK) rc = mgpu_fields_download(g_case, c_loc(fld%u), c_loc(fld%p), c_loc(fld%flux), &
                                                    c_loc(fld%gp), c_loc(fld%gu), c_loc(fld%apc))
+      if (rc == MGPU_OK) rc = mgpu_temperature_download(g_case, c_loc(fld%T), c_loc(fld%gt))
       if (rc /= MGPU_OK) then
          write(*,'(a,i0,2a)') '[uns-gpu] run failed, status ', rc, ': ', trim(mgpu_error_message())
          ier = GPU_IER

@@ -70,6 +70,21 @@ class UnsCase:
         abi.check(lib, lib.mgpu_fields_upload(self.h, dptr(u), dptr(p), dptr(flux), dptr(u_old), dptr(u_old_old)),
                   "mgpu_fields_upload")
 
+    def upload_T(self, T, T_old=None, T_old_old=None):
+        """fields_t%T (and its history; None: = T) for a case with ctrl.energy
+        (mgpu_temperature_upload)."""
+        conv = lambda a: None if a is None else np.ascontiguousarray(a, np.float64)
+        lib = _lib()
+        abi.check(lib, lib.mgpu_temperature_upload(self.h, dptr(conv(T)), dptr(conv(T_old)), dptr(conv(T_old_old))),
+                  "mgpu_temperature_upload")
+
+    def temperature(self):
+        """(T (N), gt (N, 3)): the temperature and its last Green-Gauss gradient."""
+        T, gt = np.zeros(self.N), np.zeros((self.N, 3))
+        lib = _lib()
+        abi.check(lib, lib.mgpu_temperature_download(self.h, dptr(T), dptr(gt)), "mgpu_temperature_download")
+        return T, gt
+
     FIELD_SHAPES = {"u": ("N", 3), "p": ("N",), "flux": ("F",), "gp": ("N", 3), "gu": ("N", 3, 3), "apc": ("N",)}
 
     def fields(self, out=None):

@@ -232,6 +232,13 @@ struct Group {
   int lid_dir = 0;
   double lid_coord = 0, lid_tol = 0, lid_vel[3] = {0, 0, 0};
   vector<int> faces;
+  // thermal data (bc_group_t, mod_uns_bc.f90:95-105): zone-level type and
+  // values, plane filters and their match tolerance
+  int ttype = 0;
+  double tval = 0, qval = 0;
+  int ntbc = 0, tbc_pdir[4] = {0, 0, 0, 0}, tbc_ttype[4] = {0, 0, 0, 0};
+  double tbc_pcoord[4] = {0, 0, 0, 0}, tbc_tval[4] = {0, 0, 0, 0}, tbc_qval[4] = {0, 0, 0, 0};
+  double tbc_tol = 0;
 };
 struct BC {
   vector<Group> gb;
@@ -280,6 +287,22 @@ int build_bc(const Mesh& m, const MgpuCtrl& ctrl, BC& bcs) {
     gb.lid_coord = sp.lid_coord;
     for (int k = 0; k < 3; ++k) gb.lid_vel[k] = sp.lid_vel[k];
     if (gb.has_lid) gb.lid_tol = 1.0e-4 * crange;
+    gb.ttype = sp.ttype;
+    gb.tval = sp.tval;
+    gb.qval = sp.qval;
+    // tbc_plane lines of this zone (parse_tbc_plane keeps at most 4, in order)
+    for (int t = 0; t < ctrl.ntbc && t < MGPU_MAXTBC; ++t) {
+      const MgpuTbcPlane& pl = ctrl.tbc[t];
+      if (pl.bc != i) continue;
+      if (gb.ntbc >= 4) return 15;
+      gb.tbc_pdir[gb.ntbc] = pl.pdir;
+      gb.tbc_pcoord[gb.ntbc] = pl.pcoord;
+      gb.tbc_ttype[gb.ntbc] = pl.ttype;
+      gb.tbc_tval[gb.ntbc] = pl.tval;
+      gb.tbc_qval[gb.ntbc] = pl.qval;
+      ++gb.ntbc;
+    }
+    if (gb.ntbc > 0) gb.tbc_tol = 1.0e-4 * crange;
     int nb = 0;
     bool zone_known = false;
     for (int k = 0; k < m.nfaces; ++k) {
@@ -383,6 +406,67 @@ inline bool ppe_dirichlet_mpi(const BC& bcs, int i) {
   if (g < 0) return false;
   int bt = bcs.gb[g].btype;
   return bt == MGPU_BC_POUTLET || bt == MGPU_BC_FARFIELD;
+}
+
+// bc_face_T, mod_uns_bc.f90:560-703 (without the porous/solid phase split):
+// T_face, q_face and whether the face is Neumann. Interface faces take the
+// peer's temperature, which this path holds at 0 (bcs%iface_T as allocated).
+void bc_face_T(const BC& bcs, int i, const double* xf, double T_cell, double& T_face, double& q_face,
+               bool& is_neumann) {
+  const Group& gb = bcs.gb[bcs.fgrp[i]];
+  T_face = T_cell;
+  q_face = 0.0;
+  is_neumann = true;
+  auto typed = [&](bool wall) {
+    int tt = gb.ttype;
+    double tv = gb.tval, qv = gb.qval;
+    for (int ipl = 0; ipl < gb.ntbc; ++ipl)
+      if (std::fabs(xf[gb.tbc_pdir[ipl] - 1] - gb.tbc_pcoord[ipl]) <= gb.tbc_tol) {
+        tt = gb.tbc_ttype[ipl];
+        tv = gb.tbc_tval[ipl];
+        qv = gb.tbc_qval[ipl];
+        break;
+      }
+    if (tt == 1) {
+      is_neumann = false;
+      T_face = tv;
+      q_face = 0.0;
+    } else if (tt == 2) {
+      is_neumann = true;
+      q_face = qv;
+      T_face = T_cell;
+    } else if (wall || tt == 0) {
+      is_neumann = true;
+      q_face = 0.0;
+      T_face = T_cell;
+    }
+  };
+  switch (gb.btype) {
+    case MGPU_BC_WALL:
+      typed(true);
+      break;
+    case MGPU_BC_SYMMETRY:
+    case MGPU_BC_FARFIELD:
+      break;
+    case MGPU_BC_VINLET:
+    case MGPU_BC_VINLET_PARAB:
+    case MGPU_BC_MASSINLET:
+      is_neumann = false;
+      T_face = gb.tval;
+      q_face = 0.0;
+      break;
+    case MGPU_BC_POUTLET:
+    case MGPU_BC_OUTFLOW:
+      typed(false);
+      break;
+    case MGPU_BC_INTERFACE:
+      is_neumann = false;
+      q_face = 0.0;
+      T_face = 0.0;
+      break;
+    default:
+      break;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -688,6 +772,7 @@ struct Case {
   CSR amat, pmat;
   // fields_t (mod_uns_fields.f90:29-79); u, gu cell-major like the Fortran arrays
   vector<double> u, p, gp, gu, flux, lf, apc, u_old, u_old_old;
+  vector<double> T, T_old, T_old_old, gt;  // fields_t%T, T_old, T_old_old, gt (3 per cell)
   int ts_order = 0;
   bool pimple = false;  // ctrl%pimple: pimple_run sets it for its run
   vector<double> rhs, ap, pp, phif, dpp, psi;
@@ -760,8 +845,8 @@ void grad_scalar(const Case& cs, const double* phif, double* grad, int gstride, 
 }
 
 // compute_gradients, mod_uns_fields.f90:164-258. gu is stored gu(comp,dir,cell)
-// like the Fortran array. The temperature gradients are identically zero on
-// this path (T == 0, adiabatic boundaries) and are not formed.
+// like the Fortran array. The temperature gradient gt (:219-237) is formed when
+// the energy equation is solved (otherwise T is uniform and unused).
 void compute_gradients(Case& cs) {
   const Mesh& m = cs.m;
   vector<double>& phif = cs.phif;
@@ -789,6 +874,20 @@ void compute_gradients(Case& cs) {
     grad_scalar(cs, phif.data(), tmp.data(), 3, 0);
     for (int c = 0; c < m.ncells; ++c)
       for (int d = 0; d < 3; ++d) cs.gu[9 * c + comp + 3 * d] = tmp[3 * c + d];
+  }
+  if (cs.ctrl.energy) {
+    for (int i = 0; i < m.nfaces; ++i) {
+      int c0 = m.c0[i], c1 = m.c1[i];
+      if (c1 >= 0) {
+        phif[i] = cs.lf[i] * cs.T[c0] + (1.0 - cs.lf[i]) * cs.T[c1];
+      } else {
+        double tf, qf;
+        bool neum;
+        bc_face_T(cs.bcs, i, &cs.g.xf[3 * i], cs.T[c0], tf, qf, neum);
+        phif[i] = tf;
+      }
+    }
+    grad_scalar(cs, phif.data(), cs.gt.data(), 3, 0);
   }
 }
 
@@ -948,6 +1047,10 @@ void momentum_assembly(Case& cs, int comp) {
     }
     rhs[c0] = rhs[c0] - pf * cs.g.sf[3 * i + comp];
   }
+  // Boussinesq buoyancy, mod_uns_simple.f90:1229-1240
+  if (ctrl.boussinesq)
+    for (int kk = 0; kk < N; ++kk)
+      rhs[kk] = rhs[kk] - ctrl.rho * ctrl.beta * (cs.T[kk] - ctrl.tref) * ctrl.gravity[comp] * cs.g.vol[kk];
   if (ctrl.body_force[0] != 0.0 || ctrl.body_force[1] != 0.0 || ctrl.body_force[2] != 0.0)
     for (int kk = 0; kk < N; ++kk) rhs[kk] = rhs[kk] + ctrl.body_force[comp] * cs.g.vol[kk];
   if (cs.ts_order == 1) {
@@ -969,6 +1072,160 @@ void momentum_assembly(Case& cs, int comp) {
     for (int kk = 0; kk < N; ++kk) {
       A.val[pos_of(A, kk, kk)] = ap[kk] / ctrl.alpha_u;
       rhs[kk] = rhs[kk] + (1.0 - ctrl.alpha_u) / ctrl.alpha_u * ap[kk] * cs.u[3 * kk + comp];
+    }
+  }
+}
+
+// temperature_limiter, mod_uns_simple.f90:2302-2361 (Barth-Jespersen psi_T)
+void temperature_limiter(const Case& cs, vector<double>& psi) {
+  const Mesh& m = cs.m;
+  const int N = m.ncells;
+  vector<double> pmin(cs.T.begin(), cs.T.end()), pmax(cs.T.begin(), cs.T.end());
+  for (int i = 0; i < m.nfaces; ++i) {
+    int c0 = m.c0[i], c1 = m.c1[i];
+    if (c1 >= 0) {
+      pmin[c0] = std::min(pmin[c0], cs.T[c1]);
+      pmax[c0] = std::max(pmax[c0], cs.T[c1]);
+      pmin[c1] = std::min(pmin[c1], cs.T[c0]);
+      pmax[c1] = std::max(pmax[c1], cs.T[c0]);
+    } else if (cs.bcs.fgrp[i] >= 0) {
+      double tf, qf;
+      bool neum;
+      bc_face_T(cs.bcs, i, &cs.g.xf[3 * i], cs.T[c0], tf, qf, neum);
+      pmin[c0] = std::min(pmin[c0], tf);
+      pmax[c0] = std::max(pmax[c0], tf);
+    }
+  }
+  psi.assign(N, 1.0);
+  auto side = [&](int c, int i) {
+    double d[3];
+    for (int k = 0; k < 3; ++k) d[k] = cs.g.xf[3 * i + k] - cs.g.xc[3 * c + k];
+    const double tc = cs.T[c];
+    const double fr = tc + dot3(&cs.gt[3 * c], d);
+    const double df = fr - tc;
+    if (df > 0.0)
+      psi[c] = std::min(psi[c], (pmax[c] - tc) / df);
+    else if (df < 0.0)
+      psi[c] = std::min(psi[c], (pmin[c] - tc) / df);
+  };
+  for (int i = 0; i < m.nfaces; ++i) {
+    side(m.c0[i], i);
+    if (m.c1[i] >= 0) side(m.c1[i], i);
+  }
+  for (int i = 0; i < N; ++i) psi[i] = std::max(0.0, std::min(1.0, psi[i]));
+}
+
+// temperature_assembly, mod_uns_simple.f90:1748-2037, the branch this path
+// takes: a clear fluid (porosity 1, no solid or porous zones, LTE, no
+// dispersion), so k_eff = 1 k + 0 k_s and the dispersion terms add 0. Writes
+// the CSR values into amat, rhs and ap (the unrelaxed ap_T).
+void temperature_assembly(Case& cs) {
+  const Mesh& m = cs.m;
+  const MgpuCtrl& ctrl = cs.ctrl;
+  const int N = m.ncells;
+  CSR& A = cs.amat;
+  std::fill(A.val.begin(), A.val.end(), 0.0);
+  cs.rhs.assign(N, 0.0);
+  cs.ap.assign(N, 0.0);
+  vector<double>& rhs = cs.rhs;
+  vector<double>& ap = cs.ap;
+  vector<double> psiT;
+  if (ctrl.conv_blend > 0.0) temperature_limiter(cs, psiT);
+  // porosity = 1, k_s = 0: k_eff = 1 * k + (1 - 1) * 0
+  const double k_eff = 1.0 * ctrl.k_cond + (1.0 - 1.0) * 0.0;
+  double sd = 0.0;
+  for (int i = 0; i < m.nfaces; ++i) {
+    int c1 = m.c1[i], c0 = m.c0[i];
+    if (c1 < 0) continue;
+    const double FT = ctrl.cp * cs.flux[i];
+    double dvec[3];
+    for (int k = 0; k < 3; ++k) dvec[k] = cs.g.xc[3 * c1 + k] - cs.g.xc[3 * c0 + k];
+    const double dn = norm2_scaled(dvec, 3);
+    double kf = cs.lf[i] * k_eff + (1.0 - cs.lf[i]) * k_eff;
+    kf = kf + (cs.lf[i] * 0.0 + (1.0 - cs.lf[i]) * 0.0);  // dispersion of a clear fluid
+    const double area = cs.g.area[i];
+    double DT;
+    if (ctrl.nonorth_corr > 0.0) {
+      sd = dot3(&cs.g.sf[3 * i], dvec);
+      DT = kf * (area * area) / sd;
+    } else {
+      DT = kf * area / dn;
+    }
+    ap[c0] = ap[c0] + std::max(FT, 0.0) + DT;
+    ap[c1] = ap[c1] + std::max(-FT, 0.0) + DT;
+    int kd = pos_of(A, c0, c1);
+    A.val[kd] = A.val[kd] - (DT + std::max(-FT, 0.0));
+    kd = pos_of(A, c1, c0);
+    A.val[kd] = A.val[kd] - (DT + std::max(FT, 0.0));
+    if (ctrl.conv_blend > 0.0) {
+      double dc;
+      if (FT > 0.0) {
+        double d[3];
+        for (int k = 0; k < 3; ++k) d[k] = cs.g.xf[3 * i + k] - cs.g.xc[3 * c0 + k];
+        dc = psiT[c0] * dot3(&cs.gt[3 * c0], d);
+      } else {
+        double d[3];
+        for (int k = 0; k < 3; ++k) d[k] = cs.g.xf[3 * i + k] - cs.g.xc[3 * c1 + k];
+        dc = psiT[c1] * dot3(&cs.gt[3 * c1], d);
+      }
+      dc = ctrl.conv_blend * FT * dc;
+      rhs[c0] = rhs[c0] - dc;
+      rhs[c1] = rhs[c1] + dc;
+    }
+    if (ctrl.nonorth_corr > 0.0) {
+      double gf[3], w[3];
+      const double a2 = area * area / sd;
+      for (int k = 0; k < 3; ++k) {
+        gf[k] = cs.lf[i] * cs.gt[3 * c0 + k] + (1.0 - cs.lf[i]) * cs.gt[3 * c1 + k];
+        w[k] = cs.g.sf[3 * i + k] - dvec[k] * a2;
+      }
+      const double noc = ctrl.nonorth_corr * kf * dot3(gf, w);
+      rhs[c0] = rhs[c0] + noc;
+      rhs[c1] = rhs[c1] - noc;
+    }
+  }
+  for (int i = 0; i < m.nfaces; ++i) {
+    if (cs.bcs.fgrp[i] < 0) continue;
+    const int c0 = m.c0[i];
+    double T_face, q_face;
+    bool is_neumann;
+    bc_face_T(cs.bcs, i, &cs.g.xf[3 * i], cs.T[c0], T_face, q_face, is_neumann);
+    double d[3];
+    for (int k = 0; k < 3; ++k) d[k] = cs.g.xf[3 * i + k] - cs.g.xc[3 * c0 + k];
+    const double dw = norm2_scaled(d, 3);
+    double kf = 1.0 * ctrl.k_cond + (1.0 - 1.0) * 0.0;
+    kf = kf + 0.0;  // dispersion of a clear fluid
+    const double DT = kf * cs.g.area[i] / dw;
+    const double FT = ctrl.cp * cs.flux[i];
+    if (!is_neumann) {
+      ap[c0] = ap[c0] + DT + std::max(FT, 0.0);
+      rhs[c0] = rhs[c0] + DT * T_face - std::min(FT, 0.0) * T_face;
+    } else {
+      if (std::fabs(q_face) > 0.0) rhs[c0] = rhs[c0] + q_face * cs.g.area[i];
+      const int bt = cs.bcs.gb[cs.bcs.fgrp[i]].btype;
+      if (bt == MGPU_BC_POUTLET || bt == MGPU_BC_OUTFLOW) ap[c0] = ap[c0] + std::max(FT, 0.0);
+    }
+  }
+  // time term: (rho cp)_eff = 1 rho cp + (1 - 1) rho_s cp_s
+  if (cs.ts_order == 1) {
+    for (int kk = 0; kk < N; ++kk) {
+      const double at = (1.0 * ctrl.rho * ctrl.cp + (1.0 - 1.0) * 0.0 * 0.0) * cs.g.vol[kk] / ctrl.dt;
+      ap[kk] = ap[kk] + at;
+      rhs[kk] = rhs[kk] + at * cs.T_old[kk];
+    }
+  } else if (cs.ts_order == 2) {
+    for (int kk = 0; kk < N; ++kk) {
+      const double at = (1.0 * ctrl.rho * ctrl.cp + (1.0 - 1.0) * 0.0 * 0.0) * cs.g.vol[kk] / (2.0 * ctrl.dt);
+      ap[kk] = ap[kk] + 3.0 * at;
+      rhs[kk] = rhs[kk] + at * (4.0 * cs.T_old[kk] - cs.T_old_old[kk]);
+    }
+  }
+  if (cs.ts_order > 0 && !cs.pimple) {
+    for (int kk = 0; kk < N; ++kk) A.val[pos_of(A, kk, kk)] = ap[kk];
+  } else {
+    for (int kk = 0; kk < N; ++kk) {
+      A.val[pos_of(A, kk, kk)] = ap[kk] / ctrl.alpha_u;
+      rhs[kk] = rhs[kk] + (1.0 - ctrl.alpha_u) / ctrl.alpha_u * ap[kk] * cs.T[kk];
     }
   }
 }
@@ -1142,13 +1399,13 @@ int nan_scan(const Case& cs, int& field, int& cell, double& val, int& kind) {
   val = 0.0;
   kind = 0;
   for (int ic = 0; ic < cs.m.ncells; ++ic) {
-    double v4[4] = {cs.u[3 * ic], cs.u[3 * ic + 1], cs.u[3 * ic + 2], cs.p[ic]};
-    for (int f = 0; f < 4; ++f)
-      if (!std::isfinite(v4[f])) {
+    double v5[5] = {cs.u[3 * ic], cs.u[3 * ic + 1], cs.u[3 * ic + 2], cs.p[ic], cs.T[ic]};
+    for (int f = 0; f < 5; ++f)
+      if (!std::isfinite(v5[f])) {
         field = f + 1;
         cell = ic + 1;
-        val = v4[f];
-        kind = std::isnan(v4[f]) ? 1 : 2;
+        val = v5[f];
+        kind = std::isnan(v5[f]) ? 1 : 2;
         return 1;
       }
   }
@@ -1192,6 +1449,36 @@ void solve_ppe(Case& cs, int norm_mode, int& itl, double& resl, int& ierr) {
   cs.pp.assign(N, 0.0);
   int pk = cs.ctrl.ppe_precond == MGPU_PPE_IC0 ? 2 : (cs.ctrl.ppe_precond == MGPU_PPE_ILU0 ? 0 : 1);
   pcg(cs.pmat, cs.rhs.data(), cs.pp.data(), cs.ctrl.lin_tol, cs.ctrl.lin_max, itl, resl, ierr, pk, Norm{norm_mode});
+}
+
+// The temperature solve: bicgstab_ilu0 on amat from the current T (the
+// reference's, mod_uns_simple.f90:205 / mod_uns_simple_mpi.f90:469, 752); the
+// preconditioner follows the momentum solver like the momentum solves.
+void solve_temperature(Case& cs, int norm_mode, int& itl, double& resl, int& ierr) {
+  int pk = cs.ctrl.mom_solver == MGPU_MOM_JACOBI ? 1 : 0;
+  bicgstab(cs.amat, cs.rhs.data(), cs.T.data(), cs.ctrl.lin_tol, cs.ctrl.lin_max, itl, resl, ierr, pk, Norm{norm_mode});
+}
+
+// Energy step of the drivers: Tprev, assembly, solve into record slot ns;
+// dT_max = max |T - Tprev|. Returns false on a breakdown.
+bool energy_step(Case& cs, int norm_mode, MgpuIterRec& rec, int& ns, int& itl_max, double& dT_max) {
+  const int N = cs.m.ncells;
+  vector<double> Tprev = cs.T;
+  temperature_assembly(cs);
+  int itl, ierr;
+  double resl;
+  solve_temperature(cs, norm_mode, itl, resl, ierr);
+  if (ns < MGPU_MAXSOLVE) {
+    rec.lin_it[ns] = itl;
+    rec.lin_res[ns] = resl;
+    rec.lin_ierr[ns] = ierr;
+    ++ns;
+  }
+  if (ierr == 2) return false;
+  itl_max = std::max(itl_max, itl);
+  dT_max = 0.0;
+  for (int i = 0; i < N; ++i) dT_max = std::max(dT_max, std::fabs(cs.T[i] - Tprev[i]));
+  return true;
 }
 
 // simple_run, mod_uns_simple.f90:88-288
@@ -1240,14 +1527,20 @@ int simple_run(Case& cs, int nsteps, MgpuIterRec* log, int logcap, int* nrec) {
     if (ierr == 2) return 21;
     itl_max = std::max(itl_max, itl);
     correct_fields(cs);
-    // temperature: rhs == 0 on this path -> bicgstab_ilu0 returns x=0, it=0
+    // 5b. temperature equation (without ctrl.energy T is uniform with no
+    // thermal boundary: the reference's solve then returns at once)
+    double dT_max = 0.0;
+    if (ctrl.energy) {
+      int ns = 4;
+      if (!energy_step(cs, 0, rec, ns, itl_max, dT_max)) return 22;
+      rec.nsolve = ns;
+    }
     int fld, cell, kind;
     double val;
     if (nan_scan(cs, fld, cell, val, kind)) return 60;
     double imbal = max_imbalance(cs) / flux_ref;
     double du_max = 0.0;
     for (int i = 0; i < 3 * N; ++i) du_max = std::max(du_max, std::fabs(cs.u[i] - uo[i]));
-    double dT_max = 0.0;
     rec.itl_max = itl_max;
     rec.imbal = imbal;
     rec.du_max = du_max;
@@ -1277,6 +1570,8 @@ int piso_run(Case& cs, int nsteps, MgpuIterRec* log, int logcap, int* nrec) {
   for (int it = 1; it <= n_steps; ++it) {
     cs.u_old_old = cs.u_old;
     cs.u_old = cs.u;
+    cs.T_old_old = cs.T_old;
+    cs.T_old = cs.T;
     cs.ts_order = (it == 1 || ctrl.time_scheme == 1) ? 1 : 2;
     MgpuIterRec rec;
     std::memset(&rec, 0, sizeof(rec));
@@ -1311,6 +1606,8 @@ int piso_run(Case& cs, int nsteps, MgpuIterRec* log, int logcap, int* nrec) {
       itl_max = std::max(itl_max, itl);
       correct_fields(cs);
     }
+    // 4b. temperature equation (mod_uns_simple_mpi.f90:467-479)
+    if (ctrl.energy && !energy_step(cs, 1, rec, ns, itl_max, rec.dT_max)) return 35;
     rec.nsolve = ns;
     t_now = t_now + ctrl.dt;
     double imbal = max_imbalance(cs) / flux_ref;
@@ -1362,6 +1659,8 @@ int pimple_run_body(Case& cs, int nsteps, MgpuIterRec* log, int logcap, int* nre
   for (int it = 1; it <= n_steps; ++it) {
     cs.u_old_old = cs.u_old;
     cs.u_old = cs.u;
+    cs.T_old_old = cs.T_old;
+    cs.T_old = cs.T;
     cs.ts_order = (it == 1 || ctrl.time_scheme == 1) ? 1 : 2;
     MgpuIterRec rec;
     std::memset(&rec, 0, sizeof(rec));
@@ -1399,6 +1698,8 @@ int pimple_run_body(Case& cs, int nsteps, MgpuIterRec* log, int logcap, int* nre
         correct_fields(cs);
       }
     }
+    // temperature once per step, after the outer iterations (mod_uns_simple_mpi.f90:750-759)
+    if (ctrl.energy && !energy_step(cs, 1, rec, ns, itl_max, rec.dT_max)) return 55;
     rec.nsolve = ns;
     t_now = t_now + ctrl.dt;
     double imbal = max_imbalance(cs) / flux_ref;
@@ -1505,6 +1806,10 @@ int orc_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, OrcCase** out, i
   cs.apc.assign(N, 1.0);
   cs.u_old.assign(3 * N, 0.0);
   cs.u_old_old.assign(3 * N, 0.0);
+  cs.T.assign(N, 0.0);
+  cs.T_old.assign(N, 0.0);
+  cs.T_old_old.assign(N, 0.0);
+  cs.gt.assign(3 * N, 0.0);
   init_lf(cs);
   build_cell_csr(cs.m, cs.conn, cs.amat);
   cs.pmat = cs.amat;
@@ -1537,6 +1842,22 @@ int orc_fields_download(OrcCase* c, double* u, double* p, double* flux, double* 
   if (gp) std::copy(cs.gp.begin(), cs.gp.end(), gp);
   if (gu) std::copy(cs.gu.begin(), cs.gu.end(), gu);
   if (apc) std::copy(cs.apc.begin(), cs.apc.end(), apc);
+  return 0;
+}
+
+int orc_temperature_upload(OrcCase* c, const double* T, const double* T_old, const double* T_old_old) {
+  Case& cs = c->cs;
+  const int N = cs.m.ncells;
+  if (T) cs.T.assign(T, T + N);
+  cs.T_old = T_old ? vector<double>(T_old, T_old + N) : cs.T;
+  cs.T_old_old = T_old_old ? vector<double>(T_old_old, T_old_old + N) : cs.T;
+  return 0;
+}
+
+int orc_temperature_download(OrcCase* c, double* T, double* gt) {
+  const Case& cs = c->cs;
+  if (T) std::copy(cs.T.begin(), cs.T.end(), T);
+  if (gt) std::copy(cs.gt.begin(), cs.gt.end(), gt);
   return 0;
 }
 
@@ -1604,6 +1925,11 @@ int orc_stage(OrcCase* c, int what, double* aval, double* rhs, double* ap, const
   } else if (what == 6) {
     cs.pp.assign(pp_in, pp_in + cs.m.ncells);
     correct_fields(cs);
+  } else if (what == 7) {
+    temperature_assembly(cs);
+    if (aval) std::copy(cs.amat.val.begin(), cs.amat.val.end(), aval);
+    if (rhs) std::copy(cs.rhs.begin(), cs.rhs.end(), rhs);
+    if (ap) std::copy(cs.ap.begin(), cs.ap.end(), ap);
   } else {
     return MGPU_E_ARG;
   }

@@ -37,6 +37,8 @@ def lib():
         L.orc_case_destroy.argtypes = [C.c_void_p]
         L.orc_fields_upload.argtypes = [C.c_void_p, dp, dp, dp, dp, dp]
         L.orc_fields_download.argtypes = [C.c_void_p, dp, dp, dp, dp, dp, dp]
+        L.orc_temperature_upload.argtypes = [C.c_void_p, dp, dp, dp]
+        L.orc_temperature_download.argtypes = [C.c_void_p, dp, dp]
         L.orc_simple_run.argtypes = [C.c_void_p, C.c_int, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int)]
         L.orc_piso_run.argtypes = [C.c_void_p, C.c_int, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int)]
         L.orc_pimple_run.argtypes = [C.c_void_p, C.c_int, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int)]
@@ -94,6 +96,15 @@ class OracleCase:
         lib().orc_fields_download(self.h, dptr(u), dptr(p), dptr(flux), dptr(gp), dptr(gu), dptr(apc))
         # gu(comp,dir,cell) column-major == [cell][dir][comp] row-major
         return dict(u=u, p=p, flux=flux, gp=gp, gu=gu.transpose(0, 2, 1).copy(), apc=apc)
+
+    def upload_T(self, T, T_old=None, T_old_old=None):
+        conv = lambda a: None if a is None else np.ascontiguousarray(a, np.float64)
+        lib().orc_temperature_upload(self.h, dptr(conv(T)), dptr(conv(T_old)), dptr(conv(T_old_old)))
+
+    def temperature(self):
+        T, gt = np.zeros(self.N), np.zeros((self.N, 3))
+        lib().orc_temperature_download(self.h, dptr(T), dptr(gt))
+        return T, gt
 
     def _run(self, fn, nsteps, logcap):
         recs = (MgpuIterRec * max(logcap, 1))()

@@ -21,6 +21,11 @@ Produces
     outflow, walls, symmetry) as a compact mesh fixture, and the oracle's run
     to convergence on it beside the iteration line and convergence count its
     README records for the reference binary.
+  * natconv_cavity_mesh.npz, natconv_ra1e4_pin.json -- the reference's
+    Rayleigh-Benard case at Ra = 1e4 (cases/natconv, 40 x 40 cavity with the
+    energy equation and Boussinesq buoyancy) as a compact mesh fixture, and
+    the oracle's run to convergence beside the iteration count and Nusselt
+    number its README records.
   * oracle_cases.npz -- oracle histories and final fields on small synthetic
     workloads (the same generators the CUDA tests use), used by the CPU suite
     to detect any change in the oracle's results.
@@ -41,10 +46,12 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 from casread import read_cas  # noqa: E402
-from fixtures import LOWSPEED_MESH, LOWSPEED_PIN, decode_mesh, encode_mesh, lowspeed_control  # noqa: E402
+from fixtures import (LOWSPEED_MESH, LOWSPEED_PIN, NATCONV_MESH, NATCONV_PIN, decode_mesh,  # noqa: E402
+                      encode_mesh, lowspeed_control, mirror_asymmetry, natconv_control, natconv_initial_T,
+                      nusselt)
 from mixsolver_b200 import cases  # noqa: E402
-from mixsolver_b200.abi import (BC_SYMMETRY, BC_WALL, MOM_ILU0, PPE_IC0, BcSpec,  # noqa: E402
-                                Ctrl)
+from mixsolver_b200.abi import (BC_SYMMETRY, BC_WALL, MOM_ILU0, MOM_JACOBI, PPE_IC0, PPE_JACOBI,  # noqa: E402
+                                BcSpec, Ctrl)
 from oracle import oracle as O  # noqa: E402
 
 REF = os.environ.get("MIXSOLVER_REF", "")
@@ -160,6 +167,48 @@ def make_lowspeed():
     print("lowspeed: converged after", len(log), "du_max", last["du_max"])
 
 
+def make_natconv():
+    """The reference's Rayleigh-Benard case at Ra = 1e4 (cases/natconv:
+    cavity.cas, fluid/rb_Ra1e4.control; README.md section 3 records 2245
+    iterations and Nu = 2.1601 on this 40 x 40 mesh): its mesh as a compact
+    fixture, plus the oracle's run to convergence on it (the driver's initial
+    temperature, thermal_wall_report's Nusselt number)."""
+    mesh = read_cas(os.path.join(REF, "cases/natconv/cavity.cas"))
+    np.savez_compressed(NATCONV_MESH, **encode_mesh(mesh))
+    assert np.array_equal(decode_mesh(NATCONV_MESH).x, mesh.x)
+    ctrl = natconv_control()
+    oc = O.OracleCase(mesh, ctrl)
+    geo = oc.geometry()
+    oc.upload_T(natconv_initial_T(mesh, geo["xc"]))
+    ier, log = oc.simple_run(logcap=20000)
+    T, _ = oc.temperature()
+    nu = nusselt(mesh, geo, T, ctrl)
+    # The initial temperature is symmetric about the mid-plane x = L/2; the
+    # reference's single roll grows from the asymmetric errors of its
+    # direction-dependent ILU(0) momentum and temperature solves. With Jacobi
+    # (mirror-invariant) solves the same case settles on the symmetric
+    # two-roll branch instead.
+    jc = natconv_control()
+    jc.mom_solver, jc.ppe_precond = MOM_JACOBI, PPE_JACOBI
+    oj = O.OracleCase(mesh, jc)
+    oj.upload_T(natconv_initial_T(mesh, geo["xc"]))
+    ier_j, log_j = oj.simple_run(logcap=20000)
+    Tj, _ = oj.temperature()
+    out = dict(oracle_sha=oracle_hash(), mesh="cases/natconv/cavity.cas", ier=ier, converged_after=len(log),
+               nusselt=nu, T_min=float(T.min()), T_max=float(T.max()),
+               asymmetry=mirror_asymmetry(mesh, geo["xc"], T),
+               head=[dict(it=r["it"], lin_it=list(r["lin_it"][:5]), dT_max=r["dT_max"], du_max=r["du_max"])
+                     for r in log[:5]],
+               published=dict(converged_after=2245, nusselt="2.1601"),
+               jacobi_branch=dict(solvers="BiCGStab+Jacobi momentum and temperature, PCG+Jacobi pressure",
+                                  ier=ier_j, converged_after=len(log_j), nusselt=nusselt(mesh, geo, Tj, jc),
+                                  asymmetry=mirror_asymmetry(mesh, geo["xc"], Tj)))
+    with open(NATCONV_PIN, "w") as f:
+        json.dump(out, f, indent=1)
+    print("natconv: converged after", len(log), "Nu", nu, "; Jacobi solves:", len(log_j), "Nu",
+          out["jacobi_branch"]["nusselt"])
+
+
 def hist_arrays(log):
     return dict(lin_it=np.array([r["lin_it"] for r in log], np.int32),
                 lin_res=np.array([r["lin_res"] for r in log]),
@@ -190,12 +239,15 @@ def make_cases():
 
 
 if __name__ == "__main__":
-    if "--lowspeed-only" not in sys.argv:
+    only = "--lowspeed-only" in sys.argv or "--natconv-only" in sys.argv
+    if not only:
         make_cases()
     if os.path.isdir(REF):
-        if "--lowspeed-only" not in sys.argv:
+        if not only:
             make_ghia()
-        make_lowspeed()
+        if "--natconv-only" not in sys.argv:
+            make_lowspeed()
+        make_natconv()
     else:
-        print("MIXSOLVER_REF not set to a reference checkout; ghia_pin.json and the channel_lowspeed "
-              "fixtures left unchanged")
+        print("MIXSOLVER_REF not set to a reference checkout; ghia_pin.json, the channel_lowspeed and the "
+              "natconv fixtures left unchanged")

@@ -41,14 +41,17 @@ def test_struct_layouts():
     assert C.sizeof(abi.MgpuBcSpec) == 4 * 2 + 8 * 3 + 8 * 5 + 4 * 4 + 8 * 4 + 4 * 2 + 8 * 2
     assert C.sizeof(abi.MgpuMesh) == 16 + 6 * 8
     assert C.sizeof(abi.MgpuIterRec) == 16 + 4 * 8 * 2 + 8 * 8 + 7 * 8
+    assert C.sizeof(abi.MgpuTbcPlane) == 4 * 2 + 8 + 4 * 2 + 8 * 2
     assert C.sizeof(abi.MgpuCtrl) == (4 * 8 + 2 * 4 + 4 * 8 + 4 * 4 + 8 + 2 * 4 + 3 * 8 + 2 * 4 + 8 + 2 * 4
-                                      + 32 * C.sizeof(abi.MgpuBcSpec))
+                                      + 32 * C.sizeof(abi.MgpuBcSpec)
+                                      + 2 * 4 + 4 * 8 + 3 * 8 + 2 * 4 + 32 * C.sizeof(abi.MgpuTbcPlane))
 
 
 def test_struct_offsets_match_compiled_header(tmp_path):
     """Every field offset and struct size of the ctypes mirrors equals what a C
     compiler makes of include/mixgpu.h."""
-    structs = [abi.MgpuBcSpec, abi.MgpuCtrl, abi.MgpuMesh, abi.MgpuIterRec, abi.MgpuTiming, abi.MgpuBatchInfo]
+    structs = [abi.MgpuBcSpec, abi.MgpuTbcPlane, abi.MgpuCtrl, abi.MgpuMesh, abi.MgpuIterRec, abi.MgpuTiming,
+               abi.MgpuBatchInfo]
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for st in structs:
         lines.append(f'  printf("{st.__name__} size %zu\\n", sizeof({st.__name__}));')

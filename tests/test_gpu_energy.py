@@ -1,0 +1,286 @@
+"""The energy equation (temperature_assembly, mod_uns_simple.f90:1748-2037,
+clear-fluid branch) with Boussinesq buoyancy, thermal boundary conditions
+(bc_face_T, mod_uns_bc.f90:560-703) and the temperature's place in the
+SIMPLE / PISO / PIMPLE drivers, on the GPU against the oracle."""
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from mixsolver_b200 import abi, cases, meshgen
+from mixsolver_b200 import solver as S
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+sys.path.insert(0, GOLD)
+from fixtures import (NATCONV_MESH, NATCONV_PIN, decode_mesh, mirror_asymmetry, natconv_control,  # noqa: E402
+                      natconv_initial_T, nusselt)
+
+FIELD_TOL = 1e-9
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib(gpu_lib):
+    return gpu_lib
+
+
+def rel_l2(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def thermal_box(nonorth=1.0, conv_blend=0.0, transient=False):
+    """A 10 x 5 x 5 jittered box (RCM order) with the thermal boundary kinds
+    besides the plane filters (which the natconv case exercises): velocity
+    inlet at T = 1.5 (x = 0), pressure outlet with a heat flux of -0.1 (x = 2),
+    a wall at T = 0.5 (y = 0), a heated wall (flux 0.3, y = 1), symmetry (z);
+    Boussinesq buoyancy along -y."""
+    zones = (4, 5, 6, 7, 8, 8)
+    mesh = meshgen.box_hex(10, 5, 5, lx=2.0, jitter=0.1, seed=31, zones=zones)
+    mesh = cases.rcm_renumber(meshgen.shuffle_cells(mesh, 32), S.rcm_order)
+    _, ctrl = cases.channel3d(4, 2, 2, outer_max=10)
+    ctrl.mu = 2e-2
+    ctrl.mom_solver = abi.MOM_ILU0
+    ctrl.ppe_precond = abi.PPE_IC0
+    ctrl.lin_max = 300
+    ctrl.nonorth_corr = nonorth
+    ctrl.conv_blend = conv_blend
+    B = abi.BcSpec
+    ctrl.bcs = [B(zone=4, btype=abi.BC_VINLET, uvel=(0.5, 0.0, 0.0), tval=1.5),
+                B(zone=5, btype=abi.BC_POUTLET, pval=0.0, ttype=2, qval=-0.1),
+                B(zone=6, btype=abi.BC_WALL, ttype=1, tval=0.5),
+                B(zone=7, btype=abi.BC_WALL, ttype=2, qval=0.3),
+                B(zone=8, btype=abi.BC_SYMMETRY)]
+    ctrl.energy, ctrl.boussinesq = True, True
+    ctrl.cp, ctrl.k_cond, ctrl.beta, ctrl.tref, ctrl.gravity = 2.0, 0.05, 0.2, 1.0, (0.0, -1.0, 0.0)
+    if transient:
+        ctrl.transient, ctrl.dt, ctrl.n_time_max, ctrl.n_correct = True, 2e-2, 5, 2
+    return mesh, ctrl
+
+
+def natconv(outer_max=10000, precision=abi.PREC_FP64):
+    mesh = decode_mesh(NATCONV_MESH)
+    ctrl = natconv_control(outer_max)
+    ctrl.precision = precision
+    return mesh, ctrl
+
+
+def _pair(mesh, ctrl, T0, u=None, p=None, flux=None):
+    g, o = S.UnsCase(mesh, ctrl), O.OracleCase(mesh, ctrl)
+    for c in (g, o):
+        if u is not None:
+            c.upload(u=u, p=p, flux=flux)
+        c.upload_T(T0)
+    return g, o
+
+
+@pytest.mark.parametrize("name", ["box", "box_blend", "natconv"])
+def test_temperature_stages_bit_exact(name):
+    """gt (gradient stage), the Boussinesq momentum rows and the temperature
+    row, rhs and ap (stage 7), steady and transient, bit for bit."""
+    if name == "natconv":
+        mesh, ctrl = natconv(20)
+    else:
+        mesh, ctrl = thermal_box(nonorth=1.0 if name == "box" else 0.0, conv_blend=0.0 if name == "box" else 1.0)
+    rng = np.random.default_rng(7)
+    u = rng.standard_normal((mesh.ncells, 3)) * 0.1
+    p = rng.standard_normal(mesh.ncells) * 0.01
+    flux = rng.standard_normal(mesh.nfaces) * 1e-3
+    T0 = 1.0 + 0.3 * rng.standard_normal(mesh.ncells)
+    g, o = _pair(mesh, ctrl, T0, u, p, flux)
+    nnz = len(S.build_connectivity(mesh)["col_idx"])
+    apc = 1.0 + rng.random(mesh.ncells)
+    for ts in (0, 1):
+        o.set_apc(apc, ts)
+        g.stage(0, ts, apc)
+        o.stage(0)
+        np.testing.assert_array_equal(g.temperature()[1], o.temperature()[1])
+        for what in (1, 2, 3, 7):
+            ag, rg, pg = g.stage(what, ts, apc, nnz)
+            ao, ro, po = o.stage(what, nnz)
+            np.testing.assert_array_equal(ag, ao, err_msg=f"A stage {what} ts {ts}")
+            np.testing.assert_array_equal(rg, ro, err_msg=f"rhs stage {what} ts {ts}")
+            np.testing.assert_array_equal(pg, po, err_msg=f"ap stage {what} ts {ts}")
+
+
+def _compare(log_g, log_o, fg, fo, Tg, To):
+    assert len(log_g) == len(log_o)
+    for a, b in zip(log_g, log_o):
+        assert a["lin_it"] == b["lin_it"], (a["it"], a["lin_it"], b["lin_it"])
+        assert a["lin_ierr"] == b["lin_ierr"]
+        assert a["nsolve"] == b["nsolve"]
+        if b["dT_max"] > 0:
+            assert abs(a["dT_max"] - b["dT_max"]) <= 1e-6 * b["dT_max"] + 1e-15
+    for k in ("u", "p", "flux"):
+        assert rel_l2(fg[k], fo[k]) < FIELD_TOL, (k, rel_l2(fg[k], fo[k]))
+    assert rel_l2(Tg, To) < FIELD_TOL
+
+
+def test_simple_energy_box_matches_oracle():
+    mesh, ctrl = thermal_box()
+    T0 = np.full(mesh.ncells, 1.0)
+    g, o = _pair(mesh, ctrl, T0)
+    ier_g, log_g = g.simple_run()
+    ier_o, log_o = o.simple_run()
+    assert ier_g == ier_o == 0
+    assert log_g[0]["nsolve"] == 5 and log_g[0]["lin_it"][4] > 0
+    _compare(log_g, log_o, g.fields(), o.fields(), g.temperature()[0], o.temperature()[0])
+
+
+def _ensemble(mesh, ctrl, u0, T0, run):
+    """Oracle runs from u0 scaled by (1 + e), e in {0, +-3e-16, +-1e-15}.
+
+    From the second corrector on, a pressure solve starts from the imbalance
+    the previous one left, so its iteration count follows round-off: on the
+    transient thermal box the oracle's own count for step 3's second corrector
+    is 14, 18 or 19 across these starts. The GPU is held to their spread."""
+    runs = []
+    for e in (0.0, 3e-16, -3e-16, 1e-15, -1e-15):
+        o = O.OracleCase(mesh, ctrl)
+        o.upload(u=u0 * (1.0 + e))
+        o.upload_T(T0)
+        ier, log = getattr(o, run)()
+        assert ier == 0
+        runs.append((log, o.fields(), o.temperature()[0]))
+    return runs
+
+
+def _compare_ensemble(log_g, fg, Tg, runs):
+    log_o, fo, To = runs[0]
+    assert len(log_g) == len(log_o)
+    for k, a in enumerate(log_g):
+        ens = np.array([r[0][k]["lin_it"] for r in runs])
+        lo, hi = ens.min(0), ens.max(0)
+        got = np.array(a["lin_it"])
+        assert np.all((got >= lo) & (got <= hi)), (k + 1, got, lo, hi)
+        same = lo == hi
+        assert np.all(got[same] == lo[same])
+        assert a["lin_ierr"] == log_o[k]["lin_ierr"]
+        assert a["nsolve"] == log_o[k]["nsolve"]
+        assert abs(a["dT_max"] - log_o[k]["dT_max"]) <= 1e-6 * log_o[k]["dT_max"] + 1e-15
+    for k in ("u", "p", "flux"):
+        assert rel_l2(fg[k], fo[k]) < FIELD_TOL, (k, rel_l2(fg[k], fo[k]))
+    assert rel_l2(Tg, To) < FIELD_TOL
+
+
+def test_piso_energy_box_matches_oracle():
+    """Transient: T_old history, the BDF/Euler time term of the energy
+    equation, the temperature solve after the correctors (slot 3 + n_correct),
+    the distributed solvers' norm rule."""
+    mesh, ctrl = thermal_box(transient=True)
+    T0 = 1.0 + 0.1 * np.random.default_rng(3).standard_normal(mesh.ncells)
+    u0 = 0.05 * np.random.default_rng(4).standard_normal((mesh.ncells, 3))
+    g = S.UnsCase(mesh, ctrl)
+    g.upload(u=u0)
+    g.upload_T(T0)
+    ier_g, log_g = g.piso_run()
+    assert ier_g == 0
+    assert log_g[0]["nsolve"] == 6
+    _compare_ensemble(log_g, g.fields(), g.temperature()[0], _ensemble(mesh, ctrl, u0, T0, "piso_run"))
+
+
+def test_pimple_energy_box_matches_oracle():
+    mesh, ctrl = thermal_box(transient=True)
+    ctrl.n_outer_iter = 2
+    T0 = 1.0 + 0.1 * np.random.default_rng(5).standard_normal(mesh.ncells)
+    u0 = np.zeros((mesh.ncells, 3))
+    g = S.UnsCase(mesh, ctrl)
+    g.upload_T(T0)
+    ier_g, log_g = g.pimple_run()
+    assert ier_g == 0
+    # a zero start scales to itself: perturb the ensemble through T instead
+    runs = []
+    for e in (0.0, 3e-16, -3e-16, 1e-15, -1e-15):
+        o = O.OracleCase(mesh, ctrl)
+        o.upload_T(T0 * (1.0 + e))
+        ier, log = o.pimple_run()
+        assert ier == 0
+        runs.append((log, o.fields(), o.temperature()[0]))
+    _compare_ensemble(log_g, g.fields(), g.temperature()[0], runs)
+
+
+@pytest.fixture(scope="module")
+def natconv_fp64():
+    """The reference's Rayleigh-Benard case at Ra = 1e4 run to convergence by
+    the FP64 form on the GPU."""
+    mesh, ctrl = natconv()
+    geo = O.OracleCase(mesh, ctrl).geometry()
+    g = S.UnsCase(mesh, ctrl)
+    g.upload_T(natconv_initial_T(mesh, geo["xc"]))
+    ier, log = g.simple_run(logcap=20000)
+    return dict(mesh=mesh, geo=geo, ctrl=ctrl, ier=ier, log=log, fields=g.fields(), T=g.temperature()[0])
+
+
+def test_natconv_ra1e4_on_gpu_is_the_reference_result(natconv_fp64):
+    """cases/natconv, README.md section 3: 2245 iterations, Nu = 2.1601. The
+    same iteration count and Nusselt number as the reference and the oracle,
+    the first iterations' solves equal."""
+    r = natconv_fp64
+    nu = nusselt(r["mesh"], r["geo"], r["T"], r["ctrl"])
+    pin = json.load(open(NATCONV_PIN))
+    print("natconv GPU:", len(r["log"]), "iterations, Nu", nu, "oracle", pin["nusselt"])
+    assert r["ier"] == 0
+    assert len(r["log"]) == pin["converged_after"] == 2245
+    assert f"{nu:.4f}" == "2.1601"
+    assert abs(nu - pin["nusselt"]) < 1e-9
+    for a, b in zip(r["log"][:5], pin["head"]):
+        assert list(a["lin_it"][:5]) == b["lin_it"], (a["it"], a["lin_it"], b["lin_it"])
+
+
+def test_natconv_mixed_form_keeps_the_reference_state(natconv_fp64):
+    """The reference's converged single roll is a fixed point of the mixed
+    form: started from the FP64 form's final u, p, flux and T, the mixed form
+    converges again within a few iterations, every solve on the FP64 residual,
+    with the same Nusselt number."""
+    r = natconv_fp64
+    mesh, ctrl = natconv(outer_max=200, precision=abi.PREC_MIXED)
+    g = S.UnsCase(mesh, ctrl)
+    g.upload(u=r["fields"]["u"], p=r["fields"]["p"], flux=r["fields"]["flux"])
+    g.upload_T(r["T"])
+    ier, log = g.simple_run(logcap=400)
+    nu = nusselt(mesh, r["geo"], g.temperature()[0], ctrl)
+    print("natconv mixed from the FP64 state:", len(log), "iterations, Nu", nu)
+    assert ier == 0 and len(log) < 200
+    assert all(e == 0 for rec in log for e in rec["lin_ierr"][:5])
+    assert abs(nu - 2.16013) < 1e-4
+    assert rel_l2(g.temperature()[0] - 300.5, r["T"] - 300.5) < 1e-4
+
+
+def test_natconv_mixed_form_symmetric_branch(natconv_fp64):
+    """From the driver's initial temperature (symmetric about x = L/2) the
+    mixed form's Jacobi and Chebyshev-Jacobi solves, which commute with the
+    mirror, keep the symmetric two-roll state, as the oracle does with Jacobi
+    solves (Nu 1.5154 after 1582 iterations); the reference's single roll
+    grows out of its ILU(0) solves' direction-dependent errors."""
+    mesh, ctrl = natconv(precision=abi.PREC_MIXED)
+    geo = natconv_fp64["geo"]
+    g = S.UnsCase(mesh, ctrl)
+    g.upload_T(natconv_initial_T(mesh, geo["xc"]))
+    ier, log = g.simple_run(logcap=20000)
+    T = g.temperature()[0]
+    nu = nusselt(mesh, geo, T, ctrl)
+    jb = json.load(open(NATCONV_PIN))["jacobi_branch"]
+    asym = mirror_asymmetry(mesh, geo["xc"], T)
+    print("natconv mixed:", len(log), "iterations, Nu", nu, "asymmetry", asym, "; oracle (Jacobi):",
+          jb["converged_after"], jb["nusselt"])
+    assert ier == 0
+    assert all(e == 0 for rec in log for e in rec["lin_ierr"][:5])
+    assert abs(len(log) - jb["converged_after"]) <= 0.1 * jb["converged_after"]
+    assert abs(nu - jb["nusselt"]) < 2e-3
+    assert asym < 1e-2
+
+
+def test_energy_requires_its_flag():
+    """Thermal boundary values or Boussinesq without ctrl.energy are refused at
+    case creation; batches take no energy cases."""
+    mesh, ctrl = thermal_box()
+    ctrl.energy = False
+    with pytest.raises(RuntimeError):
+        S.UnsCase(mesh, ctrl)
+    mesh, ctrl = thermal_box()
+    g = S.UnsCase(mesh, ctrl)
+    with pytest.raises(RuntimeError):
+        S.CaseBatch([g])

@@ -202,3 +202,31 @@ def test_channel_lowspeed_full_run_reproduces_pin():
     pin = json.load(open(LOWSPEED_PIN))
     assert ier == 0 and len(log) == pin["converged_after"] == 773
     assert log[-1]["du_max"] == pin["final_du_max"]
+
+
+from fixtures import (NATCONV_MESH, NATCONV_PIN, natconv_control, natconv_initial_T,  # noqa: E402
+                      nusselt)
+
+
+def test_natconv_ra1e4_is_the_reference_result():
+    """The energy equation with Boussinesq buoyancy: the oracle on the
+    reference's own Rayleigh-Benard case (cases/natconv/cavity.cas with
+    fluid/rb_Ra1e4.control: 40 x 40 cavity, hot bottom / cold top through
+    tbc_plane lines, conv_blend 1, the driver's perturbed initial T) converges
+    after 2245 outer iterations with Nu = 2.1601, as cases/natconv/README.md
+    section 3 records for the reference binary (run here in full, about 16 s)."""
+    mesh = decode_mesh(NATCONV_MESH)
+    assert mesh.ncells == 1600
+    ctrl = natconv_control()
+    oc = O.OracleCase(mesh, ctrl)
+    geo = oc.geometry()
+    oc.upload_T(natconv_initial_T(mesh, geo["xc"]))
+    ier, log = oc.simple_run(logcap=20000)
+    T, _ = oc.temperature()
+    nu = nusselt(mesh, geo, T, ctrl)
+    pin = json.load(open(NATCONV_PIN))
+    assert pin["oracle_sha"] == oracle_sha(), "oracle changed: rerun tests/golden/make_golden.py"
+    assert ier == 0 and len(log) == pin["converged_after"] == pin["published"]["converged_after"] == 2245
+    assert f"{nu:.4f}" == pin["published"]["nusselt"] == "2.1601"
+    assert nu == pin["nusselt"]
+    assert log[-1]["dT_max"] < ctrl.outer_tol and log[-1]["du_max"] < ctrl.outer_tol

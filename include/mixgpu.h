@@ -247,11 +247,12 @@ int mgpu_krylov_solve(int n, const int32_t* row_ptr, const int32_t* col_idx, con
  * host CSR system (arrays 1-based as in mgpu_krylov_solve; no reference
  * counterpart: it stands in for cg_ic0, mod_uns_linsolver.f90:405-461, with
  * the same contract): PCG with a Chebyshev-Jacobi polynomial of degree
- * cheb_degree (<= 0: the cheb_degree tuning key; 1: Jacobi) and reliable
- * updates.
- *   precision: MGPU_PREC_MIXED (FP32 matrix copy, vectors and polynomial;
- *              x, every dot product and the residual replacements in FP64) or
- *              MGPU_PREC_FP64_POLY (the same in FP64).
+ * cheb_degree (<= 0: the cheb_degree tuning key; 1: Jacobi).
+ *   precision: MGPU_PREC_MIXED (the conjugate-gradient recurrence in FP64:
+ *              x, r, p, A p and every dot product; the polynomial applied in
+ *              FP32 to an FP32 copy of r with an FP32 copy of A; a true
+ *              residual b - A x checked when r converges) or
+ *              MGPU_PREC_FP64_POLY (the polynomial in FP64 too).
  *   x: initial guess in, solution out. Converged when |b - A x| / |b| <= tol on
  *   the FP64 residual (ierr 0), else ierr 1 after maxit iterations, 2 on a
  *   breakdown. At most 2^23 rows; every row needs its diagonal entry. */
@@ -355,8 +356,9 @@ int mgpu_cg_jacobi_noalloc(int n, const int32_t* d_row_ptr, const int32_t* d_col
  * "l2_prefetch_mb" (mixed form: a system, or the systems of a batched phase
  * together, streaming more than this many MB per SpMV pass prefetch each
  * tile's successor into L2, default 96), "mixed_blocks_per_sm" (mixed and FP64
- * polynomial single-system solves: 2-5 resident blocks of 256 threads per SM,
- * the register budget sized to match, default 5), "batch_blocks_per_sm" (the
+ * polynomial single-system solves: 2-8 resident blocks of 256 threads per SM
+ * (the FP64 polynomial form 2-5), the register budget sized to match,
+ * default 5), "batch_blocks_per_sm" (the
  * same for batched lanes, default 4; set before building a batch),
  * "spin_limit" (failed polls
  * after which a grid-barrier wait gives up, 0 = the built-in bound of about
@@ -377,14 +379,22 @@ int mgpu_set_tuning(const char* key, int value);
  * face pressure (velocity extrapolated; pressure-Dirichlet in the SIMPLE
  * pressure correction; the transient drivers' ppe_assembly_mpi keeps only
  * pressure outlets and far fields Dirichlet, as in the reference).
+ * mgpu_interface_set_T: set_interface_T / set_interface_q /
+ * set_interface_T_mode (mod_uns_bc.f90:750-793) for a case with the energy
+ * equation: per listed face (1-based) the peer's temperature, its heat flux
+ * into the domain and the mode (0: Dirichlet T_face = T, 1: Neumann with that
+ * flux; bc_face_T, mod_uns_bc.f90:671-696); T, q and mode each may be NULL;
+ * zero at creation (Dirichlet at 0, as bcs%iface_T is allocated).
  * mgpu_interface_extract: uns_solver_extract_iface (mod_uns_driver.f90:274-
  * 330) for fluid owner cells: every interface face (bc order, then face
- * order), 1-based, with its owner cell's u(3) and p; *n = their number (at
- * most cap written). Density (ctrl.rho) and temperature (none on this path)
- * are the caller's. The slip and zhang interface variants are not provided. */
+ * order), 1-based, with its owner cell's u(3), p and T; *n = their number (at
+ * most cap written); u, p and T each may be NULL. Density (ctrl.rho) is the
+ * caller's. The slip, zhang and LTNE interface variants are not provided. */
 int mgpu_interface_set(MgpuCase* c, int n, const int32_t* faces, const double* u, const double* p);
+int mgpu_interface_set_T(MgpuCase* c, int n, const int32_t* faces, const double* T, const double* q,
+                         const int32_t* mode);
 int mgpu_interface_mode(MgpuCase* c, int p_dirichlet);
-int mgpu_interface_extract(MgpuCase* c, int cap, int32_t* faces, double* u, double* p, int* n);
+int mgpu_interface_extract(MgpuCase* c, int cap, int32_t* faces, double* u, double* p, double* T, int* n);
 
 /* Timing of the last run on the case's stream (CUDA events): total device ms
  * and, for the dominant kernel family, launches and summed device ms. */

@@ -248,7 +248,7 @@ EXPORTS = ["mgpu_version", "mgpu_last_error", "mgpu_set_device", "mgpu_case_crea
            "mgpu_case_finish", "mgpu_batch_create", "mgpu_batch_destroy", "mgpu_batch_set_policy",
            "mgpu_batch_step", "mgpu_batch_poll", "mgpu_batch_run", "mgpu_batch_info", "mgpu_batch_plan",
            "mgpu_batch_set_profiling", "mgpu_cas_read", "mgpu_cas_zone_names", "mgpu_cas_free",
-           "mgpu_rcm_order_device", "mgpu_mesh_topology", "mgpu_interface_set", "mgpu_interface_mode",
+           "mgpu_rcm_order_device", "mgpu_mesh_topology", "mgpu_interface_set", "mgpu_interface_set_T", "mgpu_interface_mode",
            "mgpu_interface_extract", "mgpu_pcg_poly_solve", "mgpu_temperature_upload",
            "mgpu_temperature_download"]
 NOALLOC_MAX_ROWS = 131072
@@ -296,7 +296,8 @@ def load_library(path: str = LIB_PATH):
     lib.mgpu_rcm_order_device.argtypes = [P(MgpuMesh), i32p]
     lib.mgpu_interface_set.argtypes = [C.c_void_p, C.c_int, i32p, dblp, dblp]
     lib.mgpu_interface_mode.argtypes = [C.c_void_p, C.c_int]
-    lib.mgpu_interface_extract.argtypes = [C.c_void_p, C.c_int, i32p, dblp, dblp, P(C.c_int)]
+    lib.mgpu_interface_set_T.argtypes = [C.c_void_p, C.c_int, i32p, dblp, dblp, i32p]
+    lib.mgpu_interface_extract.argtypes = [C.c_void_p, C.c_int, i32p, dblp, dblp, dblp, P(C.c_int)]
     lib.mgpu_mesh_topology.argtypes = [P(MgpuMesh), C.c_int] + [i32p] * 12
     lib.mgpu_case_stage.argtypes = [C.c_void_p, C.c_int, C.c_int, dblp, dblp, dblp, dblp, dblp]
     lib.mgpu_cg_jacobi_noalloc.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

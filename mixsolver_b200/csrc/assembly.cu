@@ -27,7 +27,17 @@ namespace {
 // value afterwards, as the reference's module variables are -- so the
 // gradients a run computes before its first iteration see the previous value.
 __device__ __forceinline__ Ramp ramp_of(const DeviceCase& d) {
-  return Ramp{d.ramp[0], d.ramp[1], d.iface_vel, d.iface_p, (long)d.F, d.iface_pdir};
+  return Ramp{d.ramp[0],     d.ramp[1],    d.iface_vel, d.iface_p,       (long)d.F,
+              d.iface_pdir, d.iface_T,    d.iface_q,   d.iface_tmode};
+}
+// the interface temperature data alone (bc_face_T reads no ramp factor)
+__device__ __forceinline__ Ramp thermal_iface(const DeviceCase& d) {
+  Ramp r{1.0, 1.0};
+  r.F = d.F;
+  r.iT = d.iface_T;
+  r.iq = d.iface_q;
+  r.itm = d.iface_tmode;
+  return r;
 }
 
 // ---------------- geometry (setup) ----------------------------------------
@@ -869,7 +879,8 @@ __device__ __forceinline__ void b_tgrad(const DeviceCase& d, const int c) {
     } else {
       double qf;
       bool neu;
-      bc_face_T(d.groups[d.fgrp[f]], d.xf[f], d.xf[F + f], d.xf[2 * F + f], d.T[a], phi, qf, neu);
+      bc_face_T(d.groups[d.fgrp[f]], thermal_iface(d), f, d.xf[f], d.xf[F + f], d.xf[2 * F + f], d.T[a], phi, qf,
+                neu);
     }
     const double s0 = d.sf[f], s1 = d.sf[F + f], s2 = d.sf[2 * F + f];
     if (a == c) {
@@ -906,7 +917,7 @@ __device__ __forceinline__ void b_tlimiter(const DeviceCase& d, const int c) {
     } else {
       double qf;
       bool neu;
-      bc_face_T(d.groups[d.fgrp[f]], d.xf[f], d.xf[F + f], d.xf[2 * F + f], tc, v, qf, neu);
+      bc_face_T(d.groups[d.fgrp[f]], thermal_iface(d), f, d.xf[f], d.xf[F + f], d.xf[2 * F + f], tc, v, qf, neu);
     }
     pmin = fmin(pmin, v);
     pmax = fmax(pmax, v);
@@ -982,7 +993,7 @@ __device__ __forceinline__ void b_temperature(const DeviceCase& d, const AsmPara
     const DevGroup& g = d.groups[d.fgrp[f]];
     double T_face, q_face;
     bool neu;
-    bc_face_T(g, d.xf[f], d.xf[F + f], d.xf[2 * F + f], tc, T_face, q_face, neu);
+    bc_face_T(g, thermal_iface(d), f, d.xf[f], d.xf[F + f], d.xf[2 * F + f], tc, T_face, q_face, neu);
     double kf = 1.0 * P.k_cond + (1.0 - 1.0) * 0.0;
     kf = kf + 0.0;
     const double DT = kf * d.area[f] / d.dn[f];

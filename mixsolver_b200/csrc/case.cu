@@ -125,16 +125,30 @@ __global__ void k_iface_scatter(int n, const int* __restrict__ faces, const doub
   if (p) ip[f] = p[k];
 }
 
-// the owner cell's u (AoS) and p of every interface face
+// iface_T(f) / iface_q(f) / iface_T_mode(f) of the listed faces (0-based)
+__global__ void k_iface_scatter_T(int n, const int* __restrict__ faces, const double* __restrict__ T,
+                                  const double* __restrict__ q, const int* __restrict__ mode, double* iT, double* iq,
+                                  int* itm) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int f = faces[k];
+  if (T) iT[f] = T[k];
+  if (q) iq[f] = q[k];
+  if (mode) itm[f] = mode[k];
+}
+
+// the owner cell's u (AoS), p and T of every interface face
 __global__ void k_iface_gather(int n, const int* __restrict__ faces, const int* __restrict__ c0,
-                               const double* __restrict__ u, const double* __restrict__ p, long N, double* out) {
+                               const double* __restrict__ u, const double* __restrict__ p,
+                               const double* __restrict__ T, long N, double* out) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const int c = c0[faces[k]];
-  out[4l * k] = u[c];
-  out[4l * k + 1] = u[N + c];
-  out[4l * k + 2] = u[2 * N + c];
-  out[4l * k + 3] = p[c];
+  out[5l * k] = u[c];
+  out[5l * k + 1] = u[N + c];
+  out[5l * k + 2] = u[2 * N + c];
+  out[5l * k + 3] = p[c];
+  out[5l * k + 4] = T[c];
 }
 
 int launch_planes_to_cells(const double* src, long n, int planes, bool grad, double* dst, cudaStream_t s) {
@@ -711,9 +725,14 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
         for (int k = 0; k < hm.F; ++k)
           if (hm.c1[k] < 0 && fgrp[k] == gi) c->iface_faces.push_back(k);
     if ((e = c->upload(c->d_iface_faces, c->iface_faces))) return fail(e);
-    if ((e = c->alloc(d.iface_vel, 3 * F)) || (e = c->alloc(d.iface_p, F))) return fail(e);
+    if ((e = c->alloc(d.iface_vel, 3 * F)) || (e = c->alloc(d.iface_p, F)) || (e = c->alloc(d.iface_T, F)) ||
+        (e = c->alloc(d.iface_q, F)) || (e = c->alloc(d.iface_tmode, F)))
+      return fail(e);
     MGPU_CUDA(cudaMemsetAsync(d.iface_vel, 0, sizeof(double) * 3 * F, c->stream));
     MGPU_CUDA(cudaMemsetAsync(d.iface_p, 0, sizeof(double) * F, c->stream));
+    MGPU_CUDA(cudaMemsetAsync(d.iface_T, 0, sizeof(double) * F, c->stream));
+    MGPU_CUDA(cudaMemsetAsync(d.iface_q, 0, sizeof(double) * F, c->stream));
+    MGPU_CUDA(cudaMemsetAsync(d.iface_tmode, 0, sizeof(int) * F, c->stream));
   }
   for (auto& g : groups)
     if (g.btype == MGPU_BC_OUTFLOW) c->has_outflow = 1;
@@ -1064,13 +1083,51 @@ int mgpu_interface_set(MgpuCase* c, int n, const int32_t* faces, const double* u
   return 0;
 }
 
+int mgpu_interface_set_T(MgpuCase* c, int n, const int32_t* faces, const double* T, const double* q,
+                         const int32_t* mode) {
+  if (!c || n < 0 || (n > 0 && !faces)) return MGPU_E_ARG;
+  if (c->d.n_iface == 0 || !c->d.energy) {
+    set_error("mgpu_interface_set_T: the case has no interface zone or no energy equation");
+    return MGPU_E_ARG;
+  }
+  if (n == 0 || (!T && !q && !mode)) return 0;
+  std::vector<int> f0(n);
+  for (int k = 0; k < n; ++k) {
+    if (faces[k] < 1 || faces[k] > c->d.F || (mode && mode[k] != 0 && mode[k] != 1)) {
+      set_error("mgpu_interface_set_T: face index or mode out of range");
+      return MGPU_E_ARG;
+    }
+    f0[k] = faces[k] - 1;
+  }
+  cudaStream_t s = c->stream;
+  int *df = nullptr, *dm = nullptr;
+  double *dT = nullptr, *dq = nullptr;
+  MGPU_CUDA(cudaMallocAsync((void**)&df, sizeof(int) * n, s));
+  if (T) MGPU_CUDA(cudaMallocAsync((void**)&dT, sizeof(double) * n, s));
+  if (q) MGPU_CUDA(cudaMallocAsync((void**)&dq, sizeof(double) * n, s));
+  if (mode) MGPU_CUDA(cudaMallocAsync((void**)&dm, sizeof(int) * n, s));
+  MGPU_CUDA(cudaMemcpyAsync(df, f0.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+  if (T) MGPU_CUDA(cudaMemcpyAsync(dT, T, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  if (q) MGPU_CUDA(cudaMemcpyAsync(dq, q, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  if (mode) MGPU_CUDA(cudaMemcpyAsync(dm, mode, sizeof(int) * n, cudaMemcpyHostToDevice, s));
+  k_iface_scatter_T<<<ceil_div(n, 256), 256, 0, s>>>(n, df, dT, dq, dm, c->d.iface_T, c->d.iface_q,
+                                                     c->d.iface_tmode);
+  MGPU_LAUNCH_CHECK("k_iface_scatter_T");
+  cudaFreeAsync(df, s);
+  if (dT) cudaFreeAsync(dT, s);
+  if (dq) cudaFreeAsync(dq, s);
+  if (dm) cudaFreeAsync(dm, s);
+  MGPU_CUDA(cudaStreamSynchronize(s));
+  return 0;
+}
+
 int mgpu_interface_mode(MgpuCase* c, int p_dirichlet) {
   if (!c) return MGPU_E_ARG;
   c->d.iface_pdir = p_dirichlet ? 1 : 0;
   return 0;
 }
 
-int mgpu_interface_extract(MgpuCase* c, int cap, int32_t* faces, double* u, double* p, int* n) {
+int mgpu_interface_extract(MgpuCase* c, int cap, int32_t* faces, double* u, double* p, double* T, int* n) {
   if (!c || !n) return MGPU_E_ARG;
   const int m = (int)c->iface_faces.size();
   *n = m;
@@ -1078,18 +1135,20 @@ int mgpu_interface_extract(MgpuCase* c, int cap, int32_t* faces, double* u, doub
   const int k = std::min(m, cap);
   cudaStream_t s = c->stream;
   double* out = nullptr;
-  MGPU_CUDA(cudaMallocAsync((void**)&out, sizeof(double) * 4 * k, s));
-  k_iface_gather<<<ceil_div(k, 256), 256, 0, s>>>(k, c->d_iface_faces, c->d.c0, c->d.u, c->d.p, c->d.N, out);
+  MGPU_CUDA(cudaMallocAsync((void**)&out, sizeof(double) * 5 * k, s));
+  k_iface_gather<<<ceil_div(k, 256), 256, 0, s>>>(k, c->d_iface_faces, c->d.c0, c->d.u, c->d.p, c->d.T, c->d.N,
+                                                  out);
   MGPU_LAUNCH_CHECK("k_iface_gather");
-  std::vector<double> h(4 * (size_t)k);
-  MGPU_CUDA(cudaMemcpyAsync(h.data(), out, sizeof(double) * 4 * k, cudaMemcpyDeviceToHost, s));
+  std::vector<double> h(5 * (size_t)k);
+  MGPU_CUDA(cudaMemcpyAsync(h.data(), out, sizeof(double) * 5 * k, cudaMemcpyDeviceToHost, s));
   cudaFreeAsync(out, s);
   MGPU_CUDA(cudaStreamSynchronize(s));
   for (int j = 0; j < k; ++j) {
     if (faces) faces[j] = c->iface_faces[j] + 1;
     if (u)
-      for (int q = 0; q < 3; ++q) u[3 * j + q] = h[4 * j + q];
-    if (p) p[j] = h[4 * j + 3];
+      for (int q = 0; q < 3; ++q) u[3 * j + q] = h[5 * j + q];
+    if (p) p[j] = h[5 * j + 3];
+    if (T) T[j] = h[5 * j + 4];
   }
   return 0;
 }

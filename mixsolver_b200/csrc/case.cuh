@@ -208,6 +208,10 @@ struct DeviceCase {
   double *iface_vel = nullptr, *iface_p = nullptr;
   int n_iface = 0;     // interface faces
   int iface_pdir = 0;  // 1: pressure is the interface constraint (g_iface_p_dir)
+  // the peer's face temperature and heat flux (F each) and the per-face mode
+  // (0 Dirichlet, 1 Neumann), interface cases only
+  double *iface_T = nullptr, *iface_q = nullptr;
+  int* iface_tmode = nullptr;
 };
 
 // Launch helpers implemented in the .cu files.

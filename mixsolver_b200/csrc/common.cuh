@@ -93,6 +93,9 @@ struct Ramp {
   const double* ip = nullptr;    // iface_p
   long F = 0;
   int ipdir = 0;                 // g_iface_p_dir
+  const double* iT = nullptr;    // iface_T (energy cases)
+  const double* iq = nullptr;    // iface_q
+  const int* itm = nullptr;      // iface_T_mode: 0 Dirichlet, 1 Neumann
 };
 
 #ifdef __CUDACC__
@@ -196,8 +199,8 @@ __device__ inline double bc_face_p(const DevGroup& g, const Ramp& rp, double pP,
 // bc_face_T, mod_uns_bc.f90:560-703 (the clear-fluid branch): the face
 // temperature and heat flux of a boundary face and whether it is Neumann.
 // Interface faces take the peer's temperature, 0 on this path.
-__device__ inline void bc_face_T(const DevGroup& g, double xf0, double xf1, double xf2, double T_cell,
-                                 double& T_face, double& q_face, bool& neumann) {
+__device__ inline void bc_face_T(const DevGroup& g, const Ramp& rp, long face, double xf0, double xf1, double xf2,
+                                 double T_cell, double& T_face, double& q_face, bool& neumann) {
   T_face = T_cell;
   q_face = 0.0;
   neumann = true;
@@ -222,9 +225,13 @@ __device__ inline void bc_face_T(const DevGroup& g, double xf0, double xf1, doub
   } else if (bt == MGPU_BC_VINLET || bt == MGPU_BC_VINLET_PARAB || bt == MGPU_BC_MASSINLET) {
     neumann = false;
     T_face = g.tval;
-  } else if (bt == MGPU_BC_INTERFACE) {
-    neumann = false;
-    T_face = 0.0;
+  } else if (bt == MGPU_BC_INTERFACE) {  // the peer's temperature, or its heat flux (CHT mode)
+    if (rp.itm[face] == 1) {
+      q_face = rp.iq[face];
+    } else {
+      neumann = false;
+      T_face = rp.iT[face];
+    }
   }
 }
 

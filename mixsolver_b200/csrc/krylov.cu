@@ -754,7 +754,7 @@ int set_tuning(const char* key, int value) {
     g_batch_reserve = value;
   } else if (k == "l2_prefetch_mb" && value >= 0) {
     g_prefetch_mb = value;
-  } else if (k == "mixed_blocks_per_sm" && value >= 2 && value <= 5) {
+  } else if (k == "mixed_blocks_per_sm" && value >= 2 && value <= 8) {
     g_mixed_occ = value;
   } else if (k == "batch_blocks_per_sm" && value >= 2 && value <= 5) {
     g_batch_occ = value;

@@ -107,6 +107,27 @@ const void* by_occ(int occ, F&& f) {
   }
 }
 
+// single-system solves also come in 6-8 blocks per SM (40 and 32 registers)
+template <typename F>
+const void* by_occ8(int occ, F&& f) {
+  switch (occ >= 8 ? 8 : occ) {
+    case 8:
+      return f(std::integral_constant<int, 8>{});
+    case 7:
+      return f(std::integral_constant<int, 7>{});
+    case 6:
+      return f(std::integral_constant<int, 6>{});
+    case 5:
+      return f(std::integral_constant<int, 5>{});
+    case 4:
+      return f(std::integral_constant<int, 4>{});
+    case 3:
+      return f(std::integral_constant<int, 3>{});
+    default:
+      return f(std::integral_constant<int, 2>{});
+  }
+}
+
 // ell: 0 CSR, 1 ELL, 2 ELL with the L2 prefetch of the next tile
 const void* batch_kernel(bool pcg, int ell, int occ) {
   return by_occ(occ, [&](auto o) {
@@ -124,7 +145,7 @@ const void* batch_kernel(bool pcg, int ell, int occ) {
 int launch_pcg_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s) {
   const int ell = ell_mode(m);
   const void* one = ell == 0 ? (const void*)k_pcg_mixed<true, 0> : (const void*)k_pcg_mixed<true, 1>;
-  const void* grid = by_occ(g_mixed_occ, [&](auto o) {
+  const void* grid = by_occ8(g_mixed_occ, [&](auto o) {
     constexpr int O = decltype(o)::value;
     return ell == 2 ? (const void*)k_pcg_mixed<false, 2, O>
                     : ell == 1 ? (const void*)k_pcg_mixed<false, 1, O> : (const void*)k_pcg_mixed<false, 0, O>;
@@ -135,7 +156,7 @@ int launch_pcg_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s) {
 int launch_bicgstab_mixed(const KrylovArgs& a, const MixedArgs& m, cudaStream_t s) {
   const int ell = ell_mode(m);
   const void* one = ell == 0 ? (const void*)k_bicgstab_mixed<true, 0> : (const void*)k_bicgstab_mixed<true, 1>;
-  const void* grid = by_occ(g_mixed_occ, [&](auto o) {
+  const void* grid = by_occ8(g_mixed_occ, [&](auto o) {
     constexpr int O = decltype(o)::value;
     return ell == 2 ? (const void*)k_bicgstab_mixed<false, 2, O>
                     : ell == 1 ? (const void*)k_bicgstab_mixed<false, 1, O> : (const void*)k_bicgstab_mixed<false, 0, O>;

@@ -173,6 +173,47 @@ module mod_gpu_iface
          real(c_double),     intent(out)   :: res
       end function mgpu_krylov_solve
 
+      integer(c_int) function mgpu_pcg_poly_solve(n, row_ptr, col_idx, val, b, x, tol, maxit, precision, &
+                                                  cheb_degree, it, res, ierr) bind(C, name='mgpu_pcg_poly_solve')
+         import :: c_int, c_int32_t, c_double
+         integer(c_int),     value         :: n, maxit, precision, cheb_degree
+         integer(c_int32_t), intent(in)    :: row_ptr(*), col_idx(*)
+         real(c_double),     intent(in)    :: val(*), b(*)
+         real(c_double),     intent(inout) :: x(*)
+         real(c_double),     value         :: tol
+         integer(c_int),     intent(out)   :: it, ierr
+         real(c_double),     intent(out)   :: res
+      end function mgpu_pcg_poly_solve
+
+      ! coupled mode (mod_mix_driver.f90 calling uns_solver_step with the
+      ! peer's interface data, and uns_solver_extract_iface)
+      integer(c_int) function mgpu_interface_set(case_h, n, faces, u, p) bind(C, name='mgpu_interface_set')
+         import :: c_int, c_ptr
+         type(c_ptr),    value :: case_h, faces, u, p
+         integer(c_int), value :: n
+      end function mgpu_interface_set
+
+      integer(c_int) function mgpu_interface_set_T(case_h, n, faces, T, q, mode) &
+            bind(C, name='mgpu_interface_set_T')
+         import :: c_int, c_ptr
+         type(c_ptr),    value :: case_h, faces, T, q, mode
+         integer(c_int), value :: n
+      end function mgpu_interface_set_T
+
+      integer(c_int) function mgpu_interface_mode(case_h, p_dirichlet) bind(C, name='mgpu_interface_mode')
+         import :: c_int, c_ptr
+         type(c_ptr),    value :: case_h
+         integer(c_int), value :: p_dirichlet
+      end function mgpu_interface_mode
+
+      integer(c_int) function mgpu_interface_extract(case_h, cap, faces, u, p, T, n) &
+            bind(C, name='mgpu_interface_extract')
+         import :: c_int, c_ptr
+         type(c_ptr),    value       :: case_h, faces, u, p, T
+         integer(c_int), value       :: cap
+         integer(c_int), intent(out) :: n
+      end function mgpu_interface_extract
+
       integer(c_int) function mgpu_csr_matvec(n, row_ptr, col_idx, val, x, y) bind(C, name='mgpu_csr_matvec')
          import :: c_int, c_int32_t, c_double
          integer(c_int),     value       :: n

@@ -151,17 +151,32 @@ class UnsCase:
         lib = _lib()
         abi.check(lib, lib.mgpu_interface_mode(self.h, 1 if p_dirichlet else 0), "mgpu_interface_mode")
 
-    def interface_extract(self):
-        """uns_solver_extract_iface for fluid owner cells: (faces 1-based, u (n, 3), p (n))."""
+    def interface_set_T(self, faces, T=None, q=None, mode=None):
+        """set_interface_T / set_interface_q / set_interface_T_mode (energy
+        cases): faces 1-based; the peer's face temperature, heat flux into the
+        domain and per-face mode (0 Dirichlet, 1 Neumann)."""
+        faces = np.ascontiguousarray(faces, np.int32)
+        T = None if T is None else np.ascontiguousarray(T, np.float64)
+        q = None if q is None else np.ascontiguousarray(q, np.float64)
+        mode = None if mode is None else np.ascontiguousarray(mode, np.int32)
+        lib = _lib()
+        abi.check(lib, lib.mgpu_interface_set_T(self.h, len(faces), iptr(faces), dptr(T), dptr(q), iptr(mode)),
+                  "mgpu_interface_set_T")
+
+    def interface_extract(self, with_T=False):
+        """uns_solver_extract_iface for fluid owner cells: (faces 1-based, u (n, 3), p (n)),
+        and T (n) with ``with_T``."""
         lib = _lib()
         n = C.c_int(0)
-        abi.check(lib, lib.mgpu_interface_extract(self.h, 0, None, None, None, C.byref(n)), "mgpu_interface_extract")
+        abi.check(lib, lib.mgpu_interface_extract(self.h, 0, None, None, None, None, C.byref(n)),
+                  "mgpu_interface_extract")
         faces = np.zeros(n.value, np.int32)
         u = np.zeros((n.value, 3))
         p = np.zeros(n.value)
-        abi.check(lib, lib.mgpu_interface_extract(self.h, n.value, iptr(faces), dptr(u), dptr(p), C.byref(n)),
-                  "mgpu_interface_extract")
-        return faces, u, p
+        T = np.zeros(n.value)
+        abi.check(lib, lib.mgpu_interface_extract(self.h, n.value, iptr(faces), dptr(u), dptr(p), dptr(T),
+                                                  C.byref(n)), "mgpu_interface_extract")
+        return (faces, u, p, T) if with_T else (faces, u, p)
 
     def nan_scan(self):
         """(ifin, field, cell, value, kind) of the first non-finite value."""

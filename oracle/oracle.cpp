@@ -248,6 +248,10 @@ struct BC {
   // iface_p(nfaces), g_iface_p_dir
   vector<double> iface_vel, iface_p;
   bool iface_p_dir = false;
+  // iface_T, iface_q, iface_T_mode (mod_uns_bc.f90:125-144): the peer's face
+  // temperature, its heat flux into the domain, 0 Dirichlet / 1 Neumann
+  vector<double> iface_T, iface_q;
+  vector<int> iface_T_mode;
 };
 
 // build_bc, mod_uns_bc.f90:155-393 (interface zones are not part of this path)
@@ -410,7 +414,7 @@ inline bool ppe_dirichlet_mpi(const BC& bcs, int i) {
 
 // bc_face_T, mod_uns_bc.f90:560-703 (without the porous/solid phase split):
 // T_face, q_face and whether the face is Neumann. Interface faces take the
-// peer's temperature, which this path holds at 0 (bcs%iface_T as allocated).
+// peer's temperature (iface_T), or its heat flux in the CHT mode (:687-691).
 void bc_face_T(const BC& bcs, int i, const double* xf, double T_cell, double& T_face, double& q_face,
                bool& is_neumann) {
   const Group& gb = bcs.gb[bcs.fgrp[i]];
@@ -460,9 +464,15 @@ void bc_face_T(const BC& bcs, int i, const double* xf, double T_cell, double& T_
       typed(false);
       break;
     case MGPU_BC_INTERFACE:
+      if (bcs.iface_T_mode[i] == 1) {
+        is_neumann = true;
+        q_face = bcs.iface_q[i];
+        T_face = T_cell;
+        break;
+      }
       is_neumann = false;
       q_face = 0.0;
-      T_face = 0.0;
+      T_face = bcs.iface_T[i];
       break;
     default:
       break;
@@ -1798,6 +1808,9 @@ int orc_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, OrcCase** out, i
   int N = cs.m.ncells, F = cs.m.nfaces;
   cs.bcs.iface_vel.assign(3 * (size_t)F, 0.0);  // build_bc's zero-initialised interface data
   cs.bcs.iface_p.assign(F, 0.0);
+  cs.bcs.iface_T.assign(F, 0.0);
+  cs.bcs.iface_q.assign(F, 0.0);
+  cs.bcs.iface_T_mode.assign(F, 0);
   cs.u.assign(3 * N, 0.0);
   cs.p.assign(N, 0.0);
   cs.gp.assign(3 * N, 0.0);
@@ -1956,6 +1969,21 @@ int orc_interface_set(OrcCase* c, int n, const int32_t* faces, const double* u, 
   return 0;
 }
 
+// set_interface_T / set_interface_q / set_interface_T_mode
+// (mod_uns_bc.f90:750-793): faces 1-based
+int orc_interface_set_T(OrcCase* c, int n, const int32_t* faces, const double* T, const double* q,
+                        const int32_t* mode) {
+  BC& b = c->cs.bcs;
+  for (int k = 0; k < n; ++k) {
+    const int i = faces[k] - 1;
+    if (i < 0 || i >= c->cs.m.nfaces) return MGPU_E_ARG;
+    if (T) b.iface_T[i] = T[k];
+    if (q) b.iface_q[i] = q[k];
+    if (mode) b.iface_T_mode[i] = mode[k];
+  }
+  return 0;
+}
+
 // set_iface_p_dirichlet (mod_uns_bc.f90:810-813)
 int orc_interface_mode(OrcCase* c, int flag) {
   c->cs.bcs.iface_p_dir = flag != 0;
@@ -1964,7 +1992,7 @@ int orc_interface_mode(OrcCase* c, int flag) {
 
 // uns_solver_extract_iface (mod_uns_driver.f90:274-330), fluid owner cells:
 // interface groups in order, their faces in face order
-int orc_interface_extract(OrcCase* c, int cap, int32_t* faces, double* u, double* p, int* n) {
+int orc_interface_extract(OrcCase* c, int cap, int32_t* faces, double* u, double* p, double* T, int* n) {
   const Case& cs = c->cs;
   int k = 0;
   for (const Group& g : cs.bcs.gb) {
@@ -1976,6 +2004,7 @@ int orc_interface_extract(OrcCase* c, int cap, int32_t* faces, double* u, double
         if (u)
           for (int q = 0; q < 3; ++q) u[3 * k + q] = cs.u[3 * c0 + q];
         if (p) p[k] = cs.p[c0];
+        if (T) T[k] = cs.T[c0];
       }
       ++k;
     }

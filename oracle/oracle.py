@@ -49,7 +49,8 @@ def lib():
         L.orc_nan_scan.argtypes = [C.c_void_p, P(C.c_int), P(C.c_int), P(C.c_int), dp, P(C.c_int)]
         L.orc_interface_set.argtypes = [C.c_void_p, C.c_int, ip, dp, dp]
         L.orc_interface_mode.argtypes = [C.c_void_p, C.c_int]
-        L.orc_interface_extract.argtypes = [C.c_void_p, C.c_int, ip, dp, dp, P(C.c_int)]
+        L.orc_interface_set_T.argtypes = [C.c_void_p, C.c_int, ip, dp, dp, ip]
+        L.orc_interface_extract.argtypes = [C.c_void_p, C.c_int, ip, dp, dp, dp, P(C.c_int)]
         L.orc_krylov_solve.argtypes = [C.c_int, ip, ip, dp, dp, dp, C.c_double, C.c_int, C.c_int,
                                        C.c_int, P(C.c_int), dp, P(C.c_int)]
         L.orc_csr_matvec.argtypes = [C.c_int, ip, ip, dp, dp, dp]
@@ -157,15 +158,22 @@ class OracleCase:
         p = None if p is None else np.ascontiguousarray(p, np.float64)
         assert lib().orc_interface_set(self.h, len(faces), iptr(faces), dptr(u), dptr(p)) == 0
 
+    def interface_set_T(self, faces, T=None, q=None, mode=None):
+        faces = np.ascontiguousarray(faces, np.int32)
+        T = None if T is None else np.ascontiguousarray(T, np.float64)
+        q = None if q is None else np.ascontiguousarray(q, np.float64)
+        mode = None if mode is None else np.ascontiguousarray(mode, np.int32)
+        assert lib().orc_interface_set_T(self.h, len(faces), iptr(faces), dptr(T), dptr(q), iptr(mode)) == 0
+
     def interface_mode(self, p_dirichlet):
         lib().orc_interface_mode(self.h, 1 if p_dirichlet else 0)
 
-    def interface_extract(self):
+    def interface_extract(self, with_T=False):
         n = C.c_int(0)
-        lib().orc_interface_extract(self.h, 0, None, None, None, C.byref(n))
-        faces, u, p = np.zeros(n.value, np.int32), np.zeros((n.value, 3)), np.zeros(n.value)
-        lib().orc_interface_extract(self.h, n.value, iptr(faces), dptr(u), dptr(p), C.byref(n))
-        return faces, u, p
+        lib().orc_interface_extract(self.h, 0, None, None, None, None, C.byref(n))
+        faces, u, p, T = np.zeros(n.value, np.int32), np.zeros((n.value, 3)), np.zeros(n.value), np.zeros(n.value)
+        lib().orc_interface_extract(self.h, n.value, iptr(faces), dptr(u), dptr(p), dptr(T), C.byref(n))
+        return (faces, u, p, T) if with_T else (faces, u, p)
 
     def nan_scan(self):
         ifin, field, cell, kind = C.c_int(), C.c_int(), C.c_int(), C.c_int()

@@ -273,6 +273,75 @@ def test_natconv_mixed_form_symmetric_branch(natconv_fp64):
     assert asym < 1e-2
 
 
+def thermal_iface_box():
+    """The thermal box with its x = 2 end a coupling interface (zone 5): the
+    peer's face velocity (outflow) and, per face, its temperature (Dirichlet)
+    or its heat flux (the CHT mode) on alternate faces."""
+    mesh, ctrl = thermal_box()
+    ctrl.bcs[1] = abi.BcSpec(zone=5, btype=abi.BC_INTERFACE)
+    faces = np.nonzero((mesh.zone == 5) & (mesh.c1 == 0))[0] + 1
+    xf = S.compute_geometry(mesh)["xf"][faces - 1]
+    u = np.stack([0.5 * np.ones(len(faces)), 0.02 * np.sin(3.0 * xf[:, 1]), np.zeros(len(faces))], 1)
+    T = 1.2 + 0.1 * xf[:, 1]
+    q = -0.05 + 0.02 * xf[:, 2]
+    mode = (np.arange(len(faces)) % 2).astype(np.int32)
+    return mesh, ctrl, faces, u, T, q, mode
+
+
+def test_interface_temperature_parity_and_extract():
+    """bc_face_T's interface branch (mod_uns_bc.f90:671-696): the peer's
+    temperature, or its heat flux where iface_T_mode = 1, in the gradient and
+    temperature stages (bit for bit) and through a SIMPLE run; then
+    uns_solver_extract_iface's T (the owner cells' temperature)."""
+    mesh, ctrl, faces, u, T, q, mode = thermal_iface_box()
+    rng = np.random.default_rng(41)
+    T0 = 1.0 + 0.2 * rng.standard_normal(mesh.ncells)
+    g, o = _pair(mesh, ctrl, T0)
+    for c in (g, o):
+        c.interface_set(faces, u=u)
+        c.interface_set_T(faces, T=T, q=q, mode=mode)
+    nnz = len(S.build_connectivity(mesh)["col_idx"])
+    apc = 1.0 + rng.random(mesh.ncells)
+    o.set_apc(apc, 0)
+    g.stage(0, 0, apc)
+    o.stage(0)
+    np.testing.assert_array_equal(g.temperature()[1], o.temperature()[1])
+    for a, b in zip(g.stage(7, 0, apc, nnz), o.stage(7, nnz)):
+        np.testing.assert_array_equal(a, b)
+    g, o = _pair(mesh, ctrl, T0)
+    for c in (g, o):
+        c.interface_set(faces, u=u)
+        c.interface_set_T(faces, T=T, q=q, mode=mode)
+    ier_g, log_g = g.simple_run()
+    ier_o, log_o = o.simple_run()
+    assert ier_g == ier_o == 0
+    Tg, To = g.temperature()[0], o.temperature()[0]
+    _compare(log_g, log_o, g.fields(), o.fields(), Tg, To)
+    fa, _, pa, ta = g.interface_extract(with_T=True)
+    fb, _, _, tb = o.interface_extract(with_T=True)
+    np.testing.assert_array_equal(fa, faces)
+    np.testing.assert_array_equal(fa, fb)
+    owner = mesh.c0[faces - 1] - 1
+    np.testing.assert_array_equal(ta, Tg[owner])
+    np.testing.assert_array_equal(pa, g.fields()["p"][owner])
+    assert rel_l2(ta, tb) < FIELD_TOL
+
+
+def test_interface_temperature_refusals():
+    """set_interface_T needs an interface zone and the energy equation; modes
+    are 0 or 1."""
+    mesh, ctrl, faces, u, T, q, mode = thermal_iface_box()
+    g = S.UnsCase(mesh, ctrl)
+    with pytest.raises(RuntimeError):
+        g.interface_set_T(faces, mode=np.full(len(faces), 2, np.int32))
+    with pytest.raises(RuntimeError):
+        g.interface_set_T([mesh.nfaces + 1], T=[1.0])
+    mesh, ctrl = thermal_box()
+    g = S.UnsCase(mesh, ctrl)
+    with pytest.raises(RuntimeError):
+        g.interface_set_T(faces, T=T)
+
+
 def test_energy_requires_its_flag():
     """Thermal boundary values or Boussinesq without ctrl.energy are refused at
     case creation; batches take no energy cases."""

@@ -952,7 +952,7 @@ def run_batch(args):
                      "peak_source": peak_source},
         "e2e": {"value": world * args.cases * e2e_steps / e2e_t, "unit": "case_iters/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "gpu_launches": i1["launches_per_iter"] * args.steps,
+        "gpu_launches": i1["gpu_launches"] - i0["gpu_launches"],
         "clocks": clk.summary(), "wall_s": wall, "active_after": active,
     }
     close_ranks(world)

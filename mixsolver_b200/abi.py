@@ -94,7 +94,8 @@ class MgpuBatchInfo(C.Structure):
                 ("autotuned", C.c_int32), ("graph", C.c_int32), ("lanes", C.c_int32), ("blocks", C.c_int32),
                 ("launches_per_iter", C.c_int32), ("tune_ms", C.c_double), ("step_ms", C.c_double),
                 ("iters", C.c_int64), ("phase_ms", C.c_double * 8), ("asm_ms", C.c_double),
-                ("lane_max_ms", C.c_double), ("lane_mean_ms", C.c_double), ("profiled_iters", C.c_int64)]
+                ("lane_max_ms", C.c_double), ("lane_mean_ms", C.c_double), ("profiled_iters", C.c_int64),
+                ("gpu_launches", C.c_int64)]
 
 
 @dataclasses.dataclass

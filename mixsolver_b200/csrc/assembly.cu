@@ -19,6 +19,8 @@
 
 namespace mgpu {
 
+extern int g_gather_faces;  // krylov.cu: the gather_faces tuning key
+
 namespace {
 
 // The ramp factors in effect (g_inlet_ramp_factor, g_pval_ramp_factor of
@@ -213,6 +215,13 @@ __global__ void k_face_consts(DeviceCase d, AsmParams P) {
 // ---------------- per-iteration kernels ------------------------------------
 
 // compute_gradients: Green-Gauss gp and gu (gu plane = comp*3 + dir)
+// Green-Gauss gradients of p and u (compute_gradients / grad_scalar,
+// mod_uns_fields.f90:164-374): one thread per cell, its faces in the cell's
+// order. K faces at a time go through three load phases (face indices; face
+// data and the other cell; the other cell's values) before any sum, so a
+// thread waits about three memory latencies per K faces instead of three per
+// face; the sums keep the face order and association (bit-exact for every K).
+template <int K = 1>
 __device__ __forceinline__ void b_gradients(const DeviceCase& d, const AsmParams& P, const int c) {
   if (d.st->abort || c >= d.N) return;
   const int N = d.N, F = d.F;
@@ -221,37 +230,74 @@ __device__ __forceinline__ void b_gradients(const DeviceCase& d, const AsmParams
   double g[12];
 #pragma unroll
   for (int k = 0; k < 12; ++k) g[k] = 0.0;
-  for (int k = d.cf_ptr[c]; k < d.cf_ptr[c + 1]; ++k) {
-    const int f = d.cf[k];
-    const int a = d.c0[f], b = d.c1[f];
-    double pf, w0, w1, w2;
-    if (b >= 0) {
-      const double lf = d.lf[f], l1 = 1.0 - lf;
-      pf = lf * d.p[a] + l1 * d.p[b];
-      w0 = lf * u0[a] + l1 * u0[b];
-      w1 = lf * u1[a] + l1 * u1[b];
-      w2 = lf * u2[a] + l1 * u2[b];
-    } else {
-      const DevGroup& gr = d.groups[d.fgrp[f]];
-      pf = bc_face_p(gr, rp, d.p[a], f);
-      bc_face_vel(gr, rp, d.xf[f], d.xf[F + f], d.xf[2 * F + f], d.sf[f], d.sf[F + f], d.sf[2 * F + f], u0[a],
-                  u1[a], u2[a], w0, w1, w2, f);
-    }
-    const double s0 = d.sf[f], s1 = d.sf[F + f], s2 = d.sf[2 * F + f];
-    const double phi[4] = {pf, w0, w1, w2};
-    if (a == c) {
+  const int kb = d.cf_ptr[c], ke = d.cf_ptr[c + 1];
+  const double pc = d.p[c], uc0 = u0[c], uc1 = u1[c], uc2 = u2[c];
+  for (int k0 = kb; k0 < ke; k0 += K) {
+    int fk[K], ok[K];
+    bool own[K];
+    double lf[K], S0[K], S1[K], S2[K], po[K], w0o[K], w1o[K], w2o[K];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        g[3 * q + 0] = g[3 * q + 0] + phi[q] * s0;
-        g[3 * q + 1] = g[3 * q + 1] + phi[q] * s1;
-        g[3 * q + 2] = g[3 * q + 2] + phi[q] * s2;
+    for (int j = 0; j < K; ++j) fk[j] = k0 + j < ke ? d.cf[k0 + j] : -1;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      ok[j] = -1;
+      own[j] = true;
+      lf[j] = S0[j] = S1[j] = S2[j] = 0.0;
+      if (fk[j] >= 0) {
+        const int f = fk[j];
+        const int a = d.c0[f], b = d.c1[f];
+        own[j] = a == c;
+        ok[j] = b < 0 ? -1 : (own[j] ? b : a);
+        lf[j] = d.lf[f];
+        S0[j] = d.sf[f];
+        S1[j] = d.sf[F + f];
+        S2[j] = d.sf[2 * F + f];
       }
-    } else {
+    }
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        g[3 * q + 0] = g[3 * q + 0] - phi[q] * s0;
-        g[3 * q + 1] = g[3 * q + 1] - phi[q] * s1;
-        g[3 * q + 2] = g[3 * q + 2] - phi[q] * s2;
+    for (int j = 0; j < K; ++j) {
+      po[j] = w0o[j] = w1o[j] = w2o[j] = 0.0;
+      if (ok[j] >= 0) {
+        po[j] = d.p[ok[j]];
+        w0o[j] = u0[ok[j]];
+        w1o[j] = u1[ok[j]];
+        w2o[j] = u2[ok[j]];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      if (fk[j] < 0) break;
+      const int f = fk[j];
+      double pf, w0, w1, w2;
+      if (ok[j] >= 0) {
+        // the face's owner (a) and neighbour (b) values, as oriented
+        const double l = lf[j], l1 = 1.0 - l;
+        const bool o = own[j];
+        pf = l * (o ? pc : po[j]) + l1 * (o ? po[j] : pc);
+        w0 = l * (o ? uc0 : w0o[j]) + l1 * (o ? w0o[j] : uc0);
+        w1 = l * (o ? uc1 : w1o[j]) + l1 * (o ? w1o[j] : uc1);
+        w2 = l * (o ? uc2 : w2o[j]) + l1 * (o ? w2o[j] : uc2);
+      } else {  // a boundary face: its owner is this cell
+        const DevGroup& gr = d.groups[d.fgrp[f]];
+        pf = bc_face_p(gr, rp, pc, f);
+        bc_face_vel(gr, rp, d.xf[f], d.xf[F + f], d.xf[2 * F + f], S0[j], S1[j], S2[j], uc0, uc1, uc2, w0, w1, w2,
+                    f);
+      }
+      const double phi[4] = {pf, w0, w1, w2};
+      if (own[j]) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          g[3 * q + 0] = g[3 * q + 0] + phi[q] * S0[j];
+          g[3 * q + 1] = g[3 * q + 1] + phi[q] * S1[j];
+          g[3 * q + 2] = g[3 * q + 2] + phi[q] * S2[j];
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          g[3 * q + 0] = g[3 * q + 0] - phi[q] * S0[j];
+          g[3 * q + 1] = g[3 * q + 1] - phi[q] * S1[j];
+          g[3 * q + 2] = g[3 * q + 2] - phi[q] * S2[j];
+        }
       }
     }
   }
@@ -261,8 +307,9 @@ __device__ __forceinline__ void b_gradients(const DeviceCase& d, const AsmParams
 #pragma unroll
   for (int k = 0; k < 9; ++k) d.gu[k * N + c] = g[3 + k] / v;
 }
+template <int K>
 __global__ void __launch_bounds__(256) k_gradients(DeviceCase d, AsmParams P) {
-  b_gradients(d, P, blockIdx.x * blockDim.x + threadIdx.x);
+  b_gradients<K>(d, P, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // velocity_limiter for one component (Barth-Jespersen psi)
@@ -454,56 +501,112 @@ __global__ void __launch_bounds__(256) k_momentum(DeviceCase d, AsmParams P, int
 // ap are the same for every component; the three rhs sums are kept apart, each
 // receiving its component's terms in the reference's order. Out: the row of A,
 // mom_ap(c), mom_rhs(comp, c); mom_finish<true> completes each component after
-// the previous component's solve.
+// the previous component's solve. K faces' loads at a time (as b_gradients);
+// NO: the non-orthogonal correction is on.
+template <int K = 1, bool NO = true>
 __device__ __forceinline__ void b_mom_interior(const DeviceCase& d, const AsmParams& P, const int c) {
   if (d.st->abort || c >= d.N) return;
   const int N = d.N, F = d.F;
   double* A = d.aval;
   double ap = 0.0, r0 = 0.0, r1 = 0.0, r2 = 0.0;
   const int kb = d.cf_ptr[c], ke = d.cf_ptr[c + 1];
+  const bool nonorth = NO && P.nonorth_corr > 0.0;
+  const double pc = d.p[c];
+  // the cell's own gradient, read once (K = 1: at each face, as the loads
+  // then overlap nothing anyway)
+  double guc[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) guc[q] = (nonorth && K > 1) ? d.gu[q * N + c] : 0.0;
   // every off-diagonal entry of the row belongs to an interior face: written
   // at its first face, added to at a later one (0 - x is the reference's sum
   // from its zeroed row); the diagonal is written by mom_finish
-  for (int k = kb; k < ke; ++k) {
-    const int f = d.cf[k];
-    const int b = d.c1[f];
-    if (b < 0) continue;
-    const int a = d.c0[f];
-    const bool own = (a == c);
-    const double Fm = d.flux[f];
-    const double D = d.Dm[f];
-    const int slot = d.cf_slot[k];
-    const double off = own ? D + fmax(-Fm, 0.0) : D + fmax(Fm, 0.0);
-    ap = own ? ap + fmax(Fm, 0.0) + D : ap + fmax(-Fm, 0.0) + D;
-    A[slot] = (d.cf_first[k] ? 0.0 : A[slot]) - off;
-    const double lf = d.lf[f], l1 = 1.0 - lf;
-    if (P.nonorth_corr > 0.0) {
-      const double t0 = d.tv[f], t1 = d.tv[F + f], t2 = d.tv[2 * F + f], mn = d.mnc[f];
-      double nc[3];
+  for (int k0 = kb; k0 < ke; k0 += K) {
+    int fk[K], ok[K], slot[K];
+    bool own[K], first[K];
+    double Fm[K], Dm[K], lf[K], S0[K], S1[K], S2[K], po[K];
+    double tv0[K], tv1[K], tv2[K], mn[K], guo[K][9];
 #pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const double gf0 = lf * d.gu[(q * 3 + 0) * N + a] + l1 * d.gu[(q * 3 + 0) * N + b];
-        const double gf1 = lf * d.gu[(q * 3 + 1) * N + a] + l1 * d.gu[(q * 3 + 1) * N + b];
-        const double gf2 = lf * d.gu[(q * 3 + 2) * N + a] + l1 * d.gu[(q * 3 + 2) * N + b];
-        nc[q] = mn * dot3(gf0, gf1, gf2, t0, t1, t2);
-      }
-      r0 = own ? r0 + nc[0] : r0 - nc[0];
-      r1 = own ? r1 + nc[1] : r1 - nc[1];
-      r2 = own ? r2 + nc[2] : r2 - nc[2];
+    for (int j = 0; j < K; ++j) {
+      fk[j] = k0 + j < ke ? d.cf[k0 + j] : -1;
+      slot[j] = k0 + j < ke ? d.cf_slot[k0 + j] : -1;
+      first[j] = k0 + j < ke ? d.cf_first[k0 + j] != 0 : false;
     }
-    const double pf = lf * d.p[a] + l1 * d.p[b];
-    const double S0 = d.sf[f], S1 = d.sf[F + f], S2 = d.sf[2 * F + f];
-    r0 = own ? r0 - pf * S0 : r0 + pf * S0;
-    r1 = own ? r1 - pf * S1 : r1 + pf * S1;
-    r2 = own ? r2 - pf * S2 : r2 + pf * S2;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      ok[j] = -1;
+      own[j] = true;
+      Fm[j] = Dm[j] = lf[j] = S0[j] = S1[j] = S2[j] = 0.0;
+      tv0[j] = tv1[j] = tv2[j] = mn[j] = 0.0;
+      if (fk[j] >= 0) {
+        const int f = fk[j];
+        const int a = d.c0[f], b = d.c1[f];
+        own[j] = a == c;
+        ok[j] = b < 0 ? -1 : (own[j] ? b : a);
+        if (b >= 0) {
+          Fm[j] = d.flux[f];
+          Dm[j] = d.Dm[f];
+          lf[j] = d.lf[f];
+          S0[j] = d.sf[f];
+          S1[j] = d.sf[F + f];
+          S2[j] = d.sf[2 * F + f];
+          if (nonorth) {
+            tv0[j] = d.tv[f];
+            tv1[j] = d.tv[F + f];
+            tv2[j] = d.tv[2 * F + f];
+            mn[j] = d.mnc[f];
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      po[j] = ok[j] >= 0 ? d.p[ok[j]] : 0.0;
+#pragma unroll
+      for (int q = 0; q < 9; ++q) guo[j][q] = (nonorth && ok[j] >= 0) ? d.gu[q * N + ok[j]] : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      if (fk[j] < 0) break;
+      if (ok[j] < 0) continue;
+      const bool own_ = own[j];
+      const double off = own_ ? Dm[j] + fmax(-Fm[j], 0.0) : Dm[j] + fmax(Fm[j], 0.0);
+      ap = own_ ? ap + fmax(Fm[j], 0.0) + Dm[j] : ap + fmax(-Fm[j], 0.0) + Dm[j];
+      A[slot[j]] = (first[j] ? 0.0 : A[slot[j]]) - off;
+      const double l = lf[j], l1 = 1.0 - l;
+      if (nonorth) {
+        double nc[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          // gradient components at the owner (a) and neighbour (b), as oriented
+          double gc[3];
+#pragma unroll
+          for (int r = 0; r < 3; ++r) gc[r] = K > 1 ? guc[q * 3 + r] : d.gu[(q * 3 + r) * N + c];
+          const double a0 = own_ ? gc[0] : guo[j][q * 3 + 0], b0 = own_ ? guo[j][q * 3 + 0] : gc[0];
+          const double a1 = own_ ? gc[1] : guo[j][q * 3 + 1], b1 = own_ ? guo[j][q * 3 + 1] : gc[1];
+          const double a2 = own_ ? gc[2] : guo[j][q * 3 + 2], b2 = own_ ? guo[j][q * 3 + 2] : gc[2];
+          const double gf0 = l * a0 + l1 * b0;
+          const double gf1 = l * a1 + l1 * b1;
+          const double gf2 = l * a2 + l1 * b2;
+          nc[q] = mn[j] * dot3(gf0, gf1, gf2, tv0[j], tv1[j], tv2[j]);
+        }
+        r0 = own_ ? r0 + nc[0] : r0 - nc[0];
+        r1 = own_ ? r1 + nc[1] : r1 - nc[1];
+        r2 = own_ ? r2 + nc[2] : r2 - nc[2];
+      }
+      const double pf = l * (own_ ? pc : po[j]) + l1 * (own_ ? po[j] : pc);
+      r0 = own_ ? r0 - pf * S0[j] : r0 + pf * S0[j];
+      r1 = own_ ? r1 - pf * S1[j] : r1 + pf * S1[j];
+      r2 = own_ ? r2 - pf * S2[j] : r2 + pf * S2[j];
+    }
   }
   d.mom_ap[c] = ap;
   d.mom_rhs[c] = r0;
   d.mom_rhs[N + c] = r1;
   d.mom_rhs[2 * N + c] = r2;
 }
+template <int K, bool NO>
 __global__ void __launch_bounds__(256) k_mom_interior(DeviceCase d, AsmParams P) {
-  b_mom_interior(d, P, blockIdx.x * blockDim.x + threadIdx.x);
+  b_mom_interior<K, NO>(d, P, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 __device__ __forceinline__ void b_mom_finish(const DeviceCase& d, const AsmParams& P, int comp, const int c) {
@@ -595,6 +698,9 @@ __device__ void b_outflow(const DeviceCase& d) {
 __global__ void k_outflow(DeviceCase d) { b_outflow(d); }
 
 // ppe_assembly: row c of the pressure-correction matrix, rhs(c), pin, pp := 0
+// The pressure-correction row of a cell (ppe_assembly, mod_uns_simple.f90:
+// 1552-1644), its faces in order, K faces' loads at a time (as b_gradients).
+template <int K = 1>
 __device__ __forceinline__ void b_ppe(const DeviceCase& d, const AsmParams& P, const int c) {
   if (d.st->abort || c >= d.N) return;
   double* A = d.pval;
@@ -604,35 +710,72 @@ __device__ __forceinline__ void b_ppe(const DeviceCase& d, const AsmParams& P, c
   // zeroed row) and added to at a later one
   double adg = 0.0;
   double rhs = 0.0;
-  for (int k = d.cf_ptr[c]; k < d.cf_ptr[c + 1]; ++k) {
-    const int f = d.cf[k];
-    const int a = d.c0[f], b = d.c1[f];
-    if (b < 0) {
-      const int gi = d.fgrp[f];
-      // af of a pressure-Dirichlet face (the serial rule, which the flux
-      // correction uses in every driver); it enters the matrix under the
-      // driver's own rule (the transient drivers' ppe_assembly_mpi leaves
-      // interface faces out)
-      if (gi >= 0 && p_dirichlet(d.groups[gi].btype, d.iface_pdir)) {
-        const double dbf = d.vol[c] / d.apc[c];
-        const double af = P.rho * dbf * d.area[f] / d.dn[f];
-        if (p_dirichlet(d.groups[gi].btype, d.iface_pdir, d.st->ts_order > 0)) adg = adg + af;
-        d.af[f] = af;
-      }
-      rhs = rhs - d.flux[f];
-      continue;
+  const int kb = d.cf_ptr[c], ke = d.cf_ptr[c + 1];
+  const double volc = d.vol[c], apcc = d.apc[c];
+  for (int k0 = kb; k0 < ke; k0 += K) {
+    int fk[K], ok[K], slot[K];
+    bool own[K], first[K];
+    double lf[K], ar[K], dn[K], fl[K], volo[K], apco[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      fk[j] = k0 + j < ke ? d.cf[k0 + j] : -1;
+      slot[j] = k0 + j < ke ? d.cf_slot[k0 + j] : -1;
+      first[j] = k0 + j < ke ? d.cf_first[k0 + j] != 0 : false;
     }
-    const double lf = d.lf[f];
-    const double dbf = lf * d.vol[a] / d.apc[a] + (1.0 - lf) * d.vol[b] / d.apc[b];
-    const double af = P.rho * dbf * d.area[f] / d.dn[f];
-    adg = adg + af;
-    const int slot = d.cf_slot[k];
-    A[slot] = (d.cf_first[k] ? 0.0 : A[slot]) - af;
-    if (a == c) {
-      rhs = rhs - d.flux[f];
-      d.af[f] = af;
-    } else {
-      rhs = rhs + d.flux[f];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      ok[j] = -1;
+      own[j] = true;
+      lf[j] = ar[j] = dn[j] = fl[j] = 0.0;
+      if (fk[j] >= 0) {
+        const int f = fk[j];
+        const int a = d.c0[f], b = d.c1[f];
+        own[j] = a == c;
+        ok[j] = b < 0 ? -1 : (own[j] ? b : a);
+        lf[j] = d.lf[f];
+        ar[j] = d.area[f];
+        dn[j] = d.dn[f];
+        fl[j] = d.flux[f];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      volo[j] = ok[j] >= 0 ? d.vol[ok[j]] : 0.0;
+      apco[j] = ok[j] >= 0 ? d.apc[ok[j]] : 1.0;
+    }
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      if (fk[j] < 0) break;
+      const int f = fk[j];
+      if (ok[j] < 0) {
+        const int gi = d.fgrp[f];
+        // af of a pressure-Dirichlet face (the serial rule, which the flux
+        // correction uses in every driver); it enters the matrix under the
+        // driver's own rule (the transient drivers' ppe_assembly_mpi leaves
+        // interface faces out)
+        if (gi >= 0 && p_dirichlet(d.groups[gi].btype, d.iface_pdir)) {
+          const double dbf = volc / apcc;
+          const double af = P.rho * dbf * ar[j] / dn[j];
+          if (p_dirichlet(d.groups[gi].btype, d.iface_pdir, d.st->ts_order > 0)) adg = adg + af;
+          d.af[f] = af;
+        }
+        rhs = rhs - fl[j];
+        continue;
+      }
+      const bool o = own[j];
+      // the owner (a) and neighbour (b) terms, as the face orients them
+      const double va = o ? volc : volo[j], pa = o ? apcc : apco[j];
+      const double vb = o ? volo[j] : volc, pb = o ? apco[j] : apcc;
+      const double dbf = lf[j] * va / pa + (1.0 - lf[j]) * vb / pb;
+      const double af = P.rho * dbf * ar[j] / dn[j];
+      adg = adg + af;
+      A[slot[j]] = (first[j] ? 0.0 : A[slot[j]]) - af;
+      if (o) {
+        rhs = rhs - fl[j];
+        d.af[f] = af;
+      } else {
+        rhs = rhs + fl[j];
+      }
     }
   }
   A[dg] = adg;
@@ -649,35 +792,66 @@ __device__ __forceinline__ void b_ppe(const DeviceCase& d, const AsmParams& P, c
   d.rhs[c] = rhs;
   d.pp[c] = 0.0;
 }
+template <int K>
 __global__ void __launch_bounds__(256) k_ppe(DeviceCase d, AsmParams P) {
-  b_ppe(d, P, blockIdx.x * blockDim.x + threadIdx.x);
+  b_ppe<K>(d, P, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // correct_fields, cell part: Green-Gauss grad(p') and the u, p updates
+// The velocity and pressure correction of a cell (correct_fields,
+// mod_uns_simple.f90:1649-1739): the Green-Gauss gradient of p' over its faces
+// in order, K faces' loads at a time (as b_gradients).
+template <int K = 1>
 __device__ __forceinline__ void b_correct_cells(const DeviceCase& d, const AsmParams& P, const int c) {
   if (d.st->abort || c >= d.N) return;
   const int N = d.N, F = d.F;
   double g0 = 0.0, g1 = 0.0, g2 = 0.0;
-  for (int k = d.cf_ptr[c]; k < d.cf_ptr[c + 1]; ++k) {
-    const int f = d.cf[k];
-    const int a = d.c0[f], b = d.c1[f];
-    double phif;
-    if (b >= 0) {
-      const double lf = d.lf[f];
-      phif = lf * d.pp[a] + (1.0 - lf) * d.pp[b];
-    } else {
-      const int gi = d.fgrp[f];
-      phif = (gi >= 0 && p_dirichlet(d.groups[gi].btype, d.iface_pdir)) ? 0.0 : d.pp[a];
+  const int kb = d.cf_ptr[c], ke = d.cf_ptr[c + 1];
+  const double ppc = d.pp[c];
+  for (int k0 = kb; k0 < ke; k0 += K) {
+    int fk[K], ok[K];
+    bool own[K];
+    double lf[K], S0[K], S1[K], S2[K], ppo[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) fk[j] = k0 + j < ke ? d.cf[k0 + j] : -1;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      ok[j] = -1;
+      own[j] = true;
+      lf[j] = S0[j] = S1[j] = S2[j] = 0.0;
+      if (fk[j] >= 0) {
+        const int f = fk[j];
+        const int a = d.c0[f], b = d.c1[f];
+        own[j] = a == c;
+        ok[j] = b < 0 ? -1 : (own[j] ? b : a);
+        lf[j] = d.lf[f];
+        S0[j] = d.sf[f];
+        S1[j] = d.sf[F + f];
+        S2[j] = d.sf[2 * F + f];
+      }
     }
-    const double s0 = d.sf[f], s1 = d.sf[F + f], s2 = d.sf[2 * F + f];
-    if (a == c) {
-      g0 = g0 + phif * s0;
-      g1 = g1 + phif * s1;
-      g2 = g2 + phif * s2;
-    } else {
-      g0 = g0 - phif * s0;
-      g1 = g1 - phif * s1;
-      g2 = g2 - phif * s2;
+#pragma unroll
+    for (int j = 0; j < K; ++j) ppo[j] = ok[j] >= 0 ? d.pp[ok[j]] : 0.0;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      if (fk[j] < 0) break;
+      double phif;
+      if (ok[j] >= 0) {
+        const bool o = own[j];
+        phif = lf[j] * (o ? ppc : ppo[j]) + (1.0 - lf[j]) * (o ? ppo[j] : ppc);
+      } else {
+        const int gi = d.fgrp[fk[j]];
+        phif = (gi >= 0 && p_dirichlet(d.groups[gi].btype, d.iface_pdir)) ? 0.0 : ppc;
+      }
+      if (own[j]) {
+        g0 = g0 + phif * S0[j];
+        g1 = g1 + phif * S1[j];
+        g2 = g2 + phif * S2[j];
+      } else {
+        g0 = g0 - phif * S0[j];
+        g1 = g1 - phif * S1[j];
+        g2 = g2 - phif * S2[j];
+      }
     }
   }
   const double vol = d.vol[c];
@@ -688,10 +862,11 @@ __device__ __forceinline__ void b_correct_cells(const DeviceCase& d, const AsmPa
   d.u[c] = d.u[c] - va * g0;
   d.u[N + c] = d.u[N + c] - va * g1;
   d.u[2 * N + c] = d.u[2 * N + c] - va * g2;
-  d.p[c] = (d.st->ts_order > 0) ? d.p[c] + d.pp[c] : d.p[c] + P.alpha_p * d.pp[c];
+  d.p[c] = (d.st->ts_order > 0) ? d.p[c] + ppc : d.p[c] + P.alpha_p * ppc;
 }
+template <int K>
 __global__ void __launch_bounds__(256) k_correct_cells(DeviceCase d, AsmParams P) {
-  b_correct_cells(d, P, blockIdx.x * blockDim.x + threadIdx.x);
+  b_correct_cells<K>(d, P, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // correct_fields, flux part
@@ -1060,18 +1235,18 @@ __device__ __forceinline__ const BatchCase& stage_case(unsigned char* raw, const
   }
 
 MGPU_BATCHED(fill_apc, RANGE_N, if (i < d.N) d.apc[i] = 1.0)
-MGPU_BATCHED(gradients, RANGE_N, b_gradients(d, P, (int)i))
+MGPU_BATCHED(gradients, RANGE_N, b_gradients<3>(d, P, (int)i))
 MGPU_BATCHED(rhiechow_piso, RANGE_F, if (sc.transient) b_rhiechow(d, P, (int)i))
 MGPU_BATCHED(begin_iter, RANGE_3N, b_begin_iter(d, sc.transient, sc.time_scheme, P.inlet_ramp, i))
 MGPU_BATCHED(limiter, RANGE_N, if (P.conv_blend > 0.0) b_limiter(d, P, arg, (int)i))
 MGPU_BATCHED(momentum, RANGE_N, b_momentum(d, P, arg, (int)i))
-MGPU_BATCHED(mom_interior, RANGE_N, b_mom_interior(d, P, (int)i))
+MGPU_BATCHED(mom_interior, RANGE_N, b_mom_interior<3>(d, P, (int)i))
 MGPU_BATCHED(mom_finish, RANGE_N, b_mom_finish(d, P, arg, (int)i))
 MGPU_BATCHED(apc, RANGE_N, b_apc(d, sc.transient ? 1.0 : P.alpha_u, (int)i))
 MGPU_BATCHED(rhiechow, RANGE_F, b_rhiechow(d, P, (int)i))
 MGPU_BATCHED(outflow, RANGE_ONE, if (sc.has_outflow) b_outflow(d))
-MGPU_BATCHED(ppe, RANGE_N, if (arg < sc.ncorr) b_ppe(d, P, (int)i))
-MGPU_BATCHED(correct_cells, RANGE_N, if (arg < sc.ncorr) b_correct_cells(d, P, (int)i))
+MGPU_BATCHED(ppe, RANGE_N, if (arg < sc.ncorr) b_ppe<3>(d, P, (int)i))
+MGPU_BATCHED(correct_cells, RANGE_N, if (arg < sc.ncorr) b_correct_cells<3>(d, P, (int)i))
 MGPU_BATCHED(correct_flux, RANGE_F, if (arg < sc.ncorr) b_correct_flux(d, (int)i))
 MGPU_BATCHED(diag, RANGE_N, b_diag(d, sc.transient, (int)i))
 MGPU_BATCHED(diag_finalize, RANGE_ONE, if (threadIdx.x == 0) b_diag_finalize(d, P, sc.transient))
@@ -1083,6 +1258,18 @@ MGPU_BATCHED(diag_finalize, RANGE_ONE, if (threadIdx.x == 0) b_diag_finalize(d, 
 // ---------------- launchers -------------------------------------------------
 
 #define GRID(n) ceil_div((n), 256), 256, 0, s
+// a cell-gather kernel K<k> for the chunk size the gather_faces key selects
+#define MGPU_GATHER_LAUNCH(KERNEL, ...)             \
+  do {                                              \
+    if (g_gather_faces >= 6)                        \
+      KERNEL<6 __VA_ARGS__><<<GRID(d.N)>>>(d, P);   \
+    else if (g_gather_faces >= 3)                   \
+      KERNEL<3 __VA_ARGS__><<<GRID(d.N)>>>(d, P);   \
+    else if (g_gather_faces == 2)                   \
+      KERNEL<2 __VA_ARGS__><<<GRID(d.N)>>>(d, P);   \
+    else                                            \
+      KERNEL<1 __VA_ARGS__><<<GRID(d.N)>>>(d, P);   \
+  } while (0)
 
 int geometry_setup(DeviceCase& d, const double* x, const int* fptr, const int* fnodes, double* pcen,
                    const AsmParams& P, cudaStream_t s) {
@@ -1100,7 +1287,7 @@ int geometry_setup(DeviceCase& d, const double* x, const int* fptr, const int* f
 }
 
 int launch_gradients(const DeviceCase& d, const AsmParams& P, cudaStream_t s) {
-  k_gradients<<<GRID(d.N)>>>(d, P);
+  MGPU_GATHER_LAUNCH(k_gradients);
   MGPU_LAUNCH_CHECK("k_gradients");
   if (d.energy) {
     k_tgrad<<<GRID(d.N)>>>(d);
@@ -1129,7 +1316,10 @@ int launch_momentum(const DeviceCase& d, const AsmParams& P, int comp, cudaStrea
   return 0;
 }
 int launch_mom_interior(const DeviceCase& d, const AsmParams& P, cudaStream_t s) {
-  k_mom_interior<<<GRID(d.N)>>>(d, P);
+  if (P.nonorth_corr > 0.0)
+    MGPU_GATHER_LAUNCH(k_mom_interior, , true);
+  else
+    MGPU_GATHER_LAUNCH(k_mom_interior, , false);
   MGPU_LAUNCH_CHECK("k_mom_interior");
   return 0;
 }
@@ -1159,12 +1349,12 @@ int launch_outflow(const DeviceCase& d, cudaStream_t s) {
   return 0;
 }
 int launch_ppe(const DeviceCase& d, const AsmParams& P, cudaStream_t s) {
-  k_ppe<<<GRID(d.N)>>>(d, P);
+  MGPU_GATHER_LAUNCH(k_ppe);
   MGPU_LAUNCH_CHECK("k_ppe");
   return 0;
 }
 int launch_correct(const DeviceCase& d, const AsmParams& P, cudaStream_t s) {
-  k_correct_cells<<<GRID(d.N)>>>(d, P);
+  MGPU_GATHER_LAUNCH(k_correct_cells);
   MGPU_LAUNCH_CHECK("k_correct_cells");
   k_correct_flux<<<GRID(d.F)>>>(d);
   MGPU_LAUNCH_CHECK("k_correct_flux");

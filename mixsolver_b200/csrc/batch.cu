@@ -225,6 +225,11 @@ struct MgpuBatch {
   cudaGraphExec_t exec = nullptr;
   bool use_graph = true;
   int launches_per_iter = 0;
+  // kernels this batch has run: counted at every launch site; a graph's
+  // kernels once per replay (graph_kernels: counted while capturing, when
+  // nothing runs)
+  int64_t launched = 0;
+  int64_t graph_kernels = 0;
   double tune_ms = 0.0, step_ms = 0.0;
   int64_t iters = 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -340,13 +345,24 @@ int build_launches(MgpuBatch* b, BatchPhase& ph, const Policy& P) {
   return 0;
 }
 
+// one batched assembly kernel over every member, counted
+int batch_op(MgpuBatch* b, int op, int arg) {
+  b->launched++;
+  return launch_batch_asm(op, arg, b->asmb, b->stream);
+}
+
 int run_phase(MgpuBatch* b, const BatchPhase& ph) {
-  for (const auto& L : ph.launches) TRY(launch_mixed_batch(L.plan, L.pcg, L.ell, b->stream));
+  for (const auto& L : ph.launches) {
+    TRY(launch_mixed_batch(L.plan, L.pcg, L.ell, b->stream));
+    b->launched++;
+  }
   for (int m : ph.fp64) {
     MgpuCase* c = b->cases[m];
     const bool tr = c->run_mode == 1;
     const KrylovArgs a = ph.pcg ? ppe_args(c, std::min(3 + ph.icorr, MGPU_MAXSOLVE - 1), tr) : mom_args(c, ph.comp, tr);
+    const int64_t before = c->launches;
     TRY(krylov(c, a, !ph.pcg, b->stream));
+    b->launched += c->launches - before;
   }
   return 0;
 }
@@ -477,6 +493,7 @@ int measure_passes(MgpuBatch* b) {
   int* d_its = nullptr;
   TRY(dev_alloc(d_its, (size_t)K * MGPU_MAXSOLVE, b->stream));
   k_gather_its<<<(K + 127) / 128, 128, 0, b->stream>>>(b->d_cases, K, d_its);
+  b->launched++;
   std::vector<int> its((size_t)K * MGPU_MAXSOLVE);
   cudaError_t e = cudaMemcpyAsync(its.data(), d_its, sizeof(int) * its.size(), cudaMemcpyDeviceToHost, b->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
@@ -501,18 +518,15 @@ int measure_passes(MgpuBatch* b) {
 // component's solve); else the boundary faces, sources and relaxation after
 // the one interior pass (BOP_MOM_INTERIOR) of the iteration.
 int momentum_assembly(MgpuBatch* b, int comp) {
-  const AsmBatch& A = b->asmb;
-  cudaStream_t s = b->stream;
   if (b->any_blend) {
-    TRY(launch_batch_asm(BOP_LIMITER, comp, A, s));
-    return launch_batch_asm(BOP_MOMENTUM, comp, A, s);
+    TRY(batch_op(b, BOP_LIMITER, comp));
+    return batch_op(b, BOP_MOMENTUM, comp);
   }
-  return launch_batch_asm(BOP_MOM_FINISH, comp, A, s);
+  return batch_op(b, BOP_MOM_FINISH, comp);
 }
 
 // profile.
 int profiled_iteration(MgpuBatch* b) {
-  const AsmBatch& A = b->asmb;
   cudaStream_t s = b->stream;
   if (!b->d_lane_t) TRY(dev_alloc(b->d_lane_t, 2 * (size_t)b->cap, b->stream));
   while (b->pev.size() < 32) {
@@ -524,8 +538,8 @@ int profiled_iteration(MgpuBatch* b) {
   auto mark = [&]() { cudaEventRecord(b->pev[ne++], s); };
   std::vector<int> kind;  // per interval: -1 assembly, else the phase index
   mark();
-  TRY(launch_batch_asm(BOP_BEGIN_ITER, 0, A, s));
-  if (!b->any_blend) TRY(launch_batch_asm(BOP_MOM_INTERIOR, 0, A, s));
+  TRY(batch_op(b, BOP_BEGIN_ITER, 0));
+  if (!b->any_blend) TRY(batch_op(b, BOP_MOM_INTERIOR, 0));
   for (int comp = 0; comp < 3; ++comp) {
     TRY(momentum_assembly(b, comp));
     mark();
@@ -534,13 +548,13 @@ int profiled_iteration(MgpuBatch* b) {
     mark();
     kind.push_back(comp);
   }
-  TRY(launch_batch_asm(BOP_APC, 0, A, s));
-  TRY(launch_batch_asm(BOP_GRADIENTS, 0, A, s));
-  TRY(launch_batch_asm(BOP_RHIECHOW, 0, A, s));
-  if (b->any_outflow) TRY(launch_batch_asm(BOP_OUTFLOW, 0, A, s));
+  TRY(batch_op(b, BOP_APC, 0));
+  TRY(batch_op(b, BOP_GRADIENTS, 0));
+  TRY(batch_op(b, BOP_RHIECHOW, 0));
+  if (b->any_outflow) TRY(batch_op(b, BOP_OUTFLOW, 0));
   std::vector<LanePlan> saved;
   for (int ic = 0; ic < b->maxcorr; ++ic) {
-    TRY(launch_batch_asm(BOP_PPE, ic, A, s));
+    TRY(batch_op(b, BOP_PPE, ic));
     mark();
     kind.push_back(-1);
     BatchPhase& ph = b->phases[3 + ic];
@@ -550,11 +564,11 @@ int profiled_iteration(MgpuBatch* b) {
     TRY(rc);
     mark();
     kind.push_back(3 + ic);
-    TRY(launch_batch_asm(BOP_CORRECT_CELLS, ic, A, s));
-    TRY(launch_batch_asm(BOP_CORRECT_FLUX, ic, A, s));
+    TRY(batch_op(b, BOP_CORRECT_CELLS, ic));
+    TRY(batch_op(b, BOP_CORRECT_FLUX, ic));
   }
-  TRY(launch_batch_asm(BOP_DIAG, 0, A, s));
-  TRY(launch_batch_asm(BOP_DIAG_FINALIZE, 0, A, s));
+  TRY(batch_op(b, BOP_DIAG, 0));
+  TRY(batch_op(b, BOP_DIAG_FINALIZE, 0));
   mark();
   kind.push_back(-1);
   MGPU_CUDA(cudaStreamSynchronize(s));
@@ -585,20 +599,19 @@ int profiled_iteration(MgpuBatch* b) {
 
 // One outer iteration / time step of every member.
 int enqueue_iteration(MgpuBatch* b, bool tune) {
-  const AsmBatch& A = b->asmb;
   cudaStream_t s = b->stream;
-  TRY(launch_batch_asm(BOP_BEGIN_ITER, 0, A, s));
-  if (!b->any_blend) TRY(launch_batch_asm(BOP_MOM_INTERIOR, 0, A, s));
+  TRY(batch_op(b, BOP_BEGIN_ITER, 0));
+  if (!b->any_blend) TRY(batch_op(b, BOP_MOM_INTERIOR, 0));
   for (int comp = 0; comp < 3; ++comp) {
     TRY(momentum_assembly(b, comp));
     TRY(run_phase(b, b->phases[comp]));
   }
-  TRY(launch_batch_asm(BOP_APC, 0, A, s));
-  TRY(launch_batch_asm(BOP_GRADIENTS, 0, A, s));
-  TRY(launch_batch_asm(BOP_RHIECHOW, 0, A, s));
-  if (b->any_outflow) TRY(launch_batch_asm(BOP_OUTFLOW, 0, A, s));
+  TRY(batch_op(b, BOP_APC, 0));
+  TRY(batch_op(b, BOP_GRADIENTS, 0));
+  TRY(batch_op(b, BOP_RHIECHOW, 0));
+  if (b->any_outflow) TRY(batch_op(b, BOP_OUTFLOW, 0));
   for (int ic = 0; ic < b->maxcorr; ++ic) {
-    TRY(launch_batch_asm(BOP_PPE, ic, A, s));
+    TRY(batch_op(b, BOP_PPE, ic));
     BatchPhase& ph = b->phases[3 + ic];
     if (tune && ic == 0) {
       // Run the first pressure solve on the modelled plan, then re-plan every
@@ -645,16 +658,16 @@ int enqueue_iteration(MgpuBatch* b, bool tune) {
       b->tuned = true;
       for (auto& p : b->phases) TRY(build_launches(b, p, b->policy));
       b->launches_per_iter = count_launches(b);
-      TRY(launch_batch_asm(BOP_CORRECT_CELLS, ic, A, s));
-      TRY(launch_batch_asm(BOP_CORRECT_FLUX, ic, A, s));
+      TRY(batch_op(b, BOP_CORRECT_CELLS, ic));
+      TRY(batch_op(b, BOP_CORRECT_FLUX, ic));
       continue;
     }
     TRY(run_phase(b, ph));
-    TRY(launch_batch_asm(BOP_CORRECT_CELLS, ic, A, s));
-    TRY(launch_batch_asm(BOP_CORRECT_FLUX, ic, A, s));
+    TRY(batch_op(b, BOP_CORRECT_CELLS, ic));
+    TRY(batch_op(b, BOP_CORRECT_FLUX, ic));
   }
-  TRY(launch_batch_asm(BOP_DIAG, 0, A, s));
-  TRY(launch_batch_asm(BOP_DIAG_FINALIZE, 0, A, s));
+  TRY(batch_op(b, BOP_DIAG, 0));
+  TRY(batch_op(b, BOP_DIAG_FINALIZE, 0));
   return 0;
 }
 
@@ -666,7 +679,10 @@ int capture(MgpuBatch* b) {
     b->use_graph = false;
     return 0;
   }
+  const int64_t before = b->launched;
   const int rc = enqueue_iteration(b, false);
+  b->graph_kernels = b->launched - before;  // recorded, not run
+  b->launched = before;
   cudaGraph_t g = nullptr;
   const cudaError_t e = cudaStreamEndCapture(s, &g);
   if (rc != 0 || e != cudaSuccess || !g) {
@@ -833,10 +849,12 @@ int mgpu_batch_step(MgpuBatch* b, int iters, int* active) {
       TRY(profiled_iteration(b));
     } else if (b->use_graph) {
       if (!b->exec) TRY(capture(b));
-      if (b->exec)
+      if (b->exec) {
         MGPU_CUDA(cudaGraphLaunch(b->exec, b->stream));
-      else
+        b->launched += b->graph_kernels;
+      } else {
         TRY(enqueue_iteration(b, false));
+      }
     } else {
       TRY(enqueue_iteration(b, false));
     }
@@ -845,6 +863,7 @@ int mgpu_batch_step(MgpuBatch* b, int iters, int* active) {
   MGPU_CUDA(cudaMemsetAsync(b->d_flags + K, 0, 2 * sizeof(int), b->stream));
   k_batch_flags<<<(K + 127) / 128, 128, 0, b->stream>>>(b->d_cases, K, b->d_flags);
   MGPU_LAUNCH_CHECK("k_batch_flags");
+  b->launched++;
   int cnt[2] = {0, 0};
   MGPU_CUDA(cudaMemcpyAsync(cnt, b->d_flags + K, sizeof(cnt), cudaMemcpyDeviceToHost, b->stream));
   MGPU_CUDA(cudaEventRecord(b->e1, b->stream));
@@ -870,6 +889,7 @@ int mgpu_batch_poll(MgpuBatch* b, int* done) {
   MGPU_CUDA(cudaMemsetAsync(b->d_flags + K, 0, 2 * sizeof(int), b->stream));
   k_batch_flags<<<(K + 127) / 128, 128, 0, b->stream>>>(b->d_cases, K, b->d_flags);
   MGPU_LAUNCH_CHECK("k_batch_flags");
+  b->launched++;
   MGPU_CUDA(cudaMemcpyAsync(h.data(), b->d_flags, sizeof(int) * K, cudaMemcpyDeviceToHost, b->stream));
   MGPU_CUDA(cudaStreamSynchronize(b->stream));
   for (int j = 0; j < K; ++j) done[b->live[j]] = h[j];
@@ -942,6 +962,7 @@ int mgpu_batch_info(const MgpuBatch* b, MgpuBatchInfo* info) {
   r.autotuned = b->policy_tuned ? 1 : 0;
   r.graph = b->exec ? 1 : 0;
   r.launches_per_iter = b->launches_per_iter;
+  r.gpu_launches = b->launched;
   if (b->phases.size() > 3)
     for (const auto& L : b->phases[3].launches) {
       r.lanes += L.plan.nlanes;

@@ -52,7 +52,8 @@ int prewarm_streams(int n);  // case.cu
 double g_cheb_ratio = 1000.0; // and the ratio lambda_max / lambda_min of its interval
 unsigned g_spin_limit = 0; // polls before a bounded barrier wait gives up (0: kSpinLimit, ~2 s)
 unsigned g_poll_ns = 100;  // sleep between the polls of a barrier wait (ns)
-int g_mixed_occ = 5;       // mixed and FP64 polynomial kernels: resident blocks per SM (2-5)
+int g_mixed_occ = 5;       // mixed kernels: resident blocks per SM (2-8; FP64 polynomial 2-5)
+int g_gather_faces = 3;    // assembly gathers: faces whose loads a thread issues together (1, 2, 3, 6)
 int g_batch_occ = 4;       // batched lane kernel: resident blocks per SM (2-5)
 namespace {
 
@@ -760,6 +761,8 @@ int set_tuning(const char* key, int value) {
     g_batch_occ = value;
   } else if (k == "spin_limit" && value >= 0) {
     g_spin_limit = (unsigned)value;
+  } else if (k == "gather_faces" && value >= 1 && value <= 6) {
+    g_gather_faces = value;
   } else if (k == "barrier_poll_ns" && value >= 0 && value <= 10000) {
     g_poll_ns = (unsigned)value;
   } else if (k == "stream_pool" && value >= 0 && value <= 1024) {

@@ -7,7 +7,9 @@
   python -m mixsolver_b200.prof_cases asm      # FP64 form of the channel, 2 outer iterations
                                                # (assembly kernels)
 
-Each prints its solve counts and the run's device time."""
+Each prints its solve counts and the run's device time. Library tuning keys
+(mgpu_set_tuning) may follow as KEY=VALUE arguments, e.g.
+  python -m mixsolver_b200.prof_cases asm gather_faces=1"""
 from __future__ import annotations
 
 import sys
@@ -17,7 +19,12 @@ from . import solver as S
 
 
 def main(argv=None) -> int:
-    what = (argv or sys.argv[1:] or ["channel"])[0]
+    argv = list(argv if argv is not None else sys.argv[1:])
+    for kv in [a for a in argv if "=" in a]:
+        k, v = kv.split("=", 1)
+        S.set_tuning(k, int(v))
+        argv.remove(kv)
+    what = (argv or ["channel"])[0]
     if what in ("channel", "asm"):
         mesh, ctrl = cases.channel3d(128, 64, 64, seed=0, outer_max=10**6, order_fn=S.rcm_order,
                                      mom=abi.MOM_JACOBI, ppe=abi.PPE_ILU0)

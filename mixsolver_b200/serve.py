@@ -94,8 +94,8 @@ class GpuBackend:
         batch.step(iters)
 
     def launches(self, batch) -> int:
-        """Kernel launches of one batched iteration (a host-side count)."""
-        return int(batch.info()["launches_per_iter"])
+        """Kernels the batch has run so far (the library's own count)."""
+        return int(batch.info()["gpu_launches"])
 
     def poll(self, batch) -> np.ndarray:
         return batch.poll()
@@ -228,11 +228,12 @@ class Server:
                     batch = self.be.batch(members)
                     self.batches_built += 1
                 ts = self.clock()
+                count = getattr(self.be, "launches", None)
+                n0 = int(count(batch)) if count is not None else 0
                 self.be.step(batch, self.tick_iters)
                 self.ticks += 1
-                count = getattr(self.be, "launches", None)
                 if count is not None:
-                    self.gpu_launches += int(count(batch)) * self.tick_iters
+                    self.gpu_launches += int(count(batch)) - n0
                 flags = self.be.poll(batch)
                 now = self.clock() - t0
                 self.t_build += ts - tb

@@ -201,6 +201,26 @@ def test_step_and_poll_interface():
     B.close()
 
 
+def test_launch_count_is_measured():
+    """mgpu_batch_info's gpu_launches counts the kernels a batch runs: a CUDA
+    graph replay adds the kernels it recorded, which equal the launches of one
+    iteration launch by launch; each step adds its flag kernel."""
+    specs = _cavities(abi.PREC_MIXED, sizes=(5, 7), iters=30)
+    objs = [S.UnsCase(m, c) for m, c in specs]
+    for g in objs:
+        assert g.begin(0) == 0
+    B = S.CaseBatch(objs, policy=(16384, 8))
+    B.step(2)
+    i0 = B.info()
+    B.step(3)
+    i1 = B.info()
+    assert i1["graph"] == 1
+    assert i1["gpu_launches"] - i0["gpu_launches"] == 3 * i1["launches_per_iter"] + 1
+    B.close()
+    for g in objs:
+        g.finish()
+
+
 def test_sized_lanes_keep_their_own_system():
     """Few big systems each get a lane sized by their work; with the capacity
     shrunk (block slots reserved) the narrow lanes are too small for the

@@ -509,6 +509,50 @@ def test_bc_stage_kernels_bit_exact(name):
         np.testing.assert_array_equal(fg[k], fo[k], err_msg=k)
 
 
+@pytest.mark.parametrize("gather", [1, 6])
+@pytest.mark.parametrize("name", ["mass_outflow", "vinlet_farfield", "tet"])
+def test_gather_chunks_bit_exact(name, gather):
+    """The assembly gathers load a cell's faces in chunks (gather_faces, 3
+    by default and in every other test); every chunk size gives the oracle's
+    bits, on hexes (6 faces: whole and split chunks) and tets (4 faces: a
+    partly filled chunk), with every boundary kind's branch."""
+    if name == "tet":
+        mesh, ctrl = cases.tet_box(3, dt=1e-3, steps=2)
+    else:
+        mesh, ctrl = bc_case(name)
+    nnz = len(S.build_connectivity(mesh)["col_idx"])
+    S.set_tuning("gather_faces", gather)
+    try:
+        g = S.UnsCase(mesh, ctrl)
+        o = O.OracleCase(mesh, ctrl)
+        u, p, flux = _seed_fields(mesh, seed=17)
+        apc = 1.0 + np.random.default_rng(18).random(mesh.ncells)
+        for c in (g, o):
+            c.upload(u=u, p=p, flux=flux)
+        o.set_apc(apc, 0)
+        g.stage(0, 0, apc)
+        o.stage(0)
+        fg, fo = g.fields(), o.fields()
+        np.testing.assert_array_equal(fg["gp"], fo["gp"])
+        np.testing.assert_array_equal(fg["gu"], fo["gu"])
+        for comp in (1, 2, 3):
+            for a, b in zip(g.stage(comp, 0, apc, nnz), o.stage(comp, nnz)):
+                np.testing.assert_array_equal(a, b)
+        g.stage(4, 0, apc)
+        o.stage(4)
+        np.testing.assert_array_equal(g.fields()["flux"], o.fields()["flux"])
+        for a, b in zip(g.stage(5, 0, apc, nnz)[:2], o.stage(5, nnz)[:2]):
+            np.testing.assert_array_equal(a, b)
+        pp = np.random.default_rng(19).standard_normal(mesh.ncells) * 1e-3
+        g.stage(6, 0, apc, pp=pp)
+        o.stage(6, pp=pp)
+        fg, fo = g.fields(), o.fields()
+        for k in ("u", "p", "flux"):
+            np.testing.assert_array_equal(fg[k], fo[k], err_msg=k)
+    finally:
+        S.set_tuning("gather_faces", 3)
+
+
 @pytest.mark.parametrize("name", BC_CASES)
 def test_bc_simple_parity(name):
     """Whole SIMPLE runs on each boundary mix (outflow rescale and inlet ramp

@@ -119,9 +119,17 @@ def test_rejected_case_is_answered_with_its_error():
 
 
 def test_launch_count_follows_the_ticks():
+    """The server adds what the backend's own counter grew by over each tick
+    (the library counts the kernels a batch runs, graph replays included)."""
     class Counting(FakeBackend):
+        n = 0
+
+        def step(self, batch, iters):
+            super().step(batch, iters)
+            self.n += 7 * iters
+
         def launches(self, batch):
-            return 7
+            return self.n
 
     be = Counting()
     srv = serve.Server(be, budget_bytes=60_000_000, active_cells=30000, tick_iters=5, bytes_per_cell=1000)

@@ -607,7 +607,9 @@ int mgpu_case_create(const MgpuMesh* mesh, const MgpuCtrl* ctrl, MgpuCase** out,
   const TopoAlloc keep = [c](int*& p, size_t n) { return c->alloc(p, n); };
   {
     DeviceTopo t;
-    if ((e = device_topology(d.N, d.F, d.c0, d.c1, t, keep, c->stream))) return fail(e);
+    // the mixed and FP64 polynomial forms run no triangular sweeps
+    const bool levels = ctrl->precision == MGPU_PREC_FP64;
+    if ((e = device_topology(d.N, d.F, d.c0, d.c1, t, keep, c->stream, levels))) return fail(e);
     d.cf_ptr = t.cf_ptr;
     d.cf = t.cf;
     d.cf_slot = t.cf_slot;

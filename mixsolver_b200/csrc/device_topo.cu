@@ -409,7 +409,7 @@ __global__ void k_bface_fill(int N, const int* __restrict__ cf_ptr, const int* _
 }  // namespace
 
 int device_topology(int N, int F, const int* c0, const int* c1, DeviceTopo& t, const TopoAlloc& alloc,
-                    cudaStream_t s) {
+                    cudaStream_t s, bool levels) {
   Tmp T(s);
   t.N = N;
   t.F = F;
@@ -483,8 +483,10 @@ int device_topology(int N, int F, const int* c0, const int* c1, DeviceTopo& t, c
   k_mirror<<<gN, 256, 0, s>>>(N, t.row_ptr, t.col, t.mirror);
   MGPU_LAUNCH_CHECK("k_mirror");
   // level sets of the triangular sweeps
-  DT_TRY(level_sets(T, N, t.row_ptr, t.col, t.diag, true, t, alloc));
-  DT_TRY(level_sets(T, N, t.row_ptr, t.col, t.diag, false, t, alloc));
+  if (levels) {
+    DT_TRY(level_sets(T, N, t.row_ptr, t.col, t.diag, true, t, alloc));
+    DT_TRY(level_sets(T, N, t.row_ptr, t.col, t.diag, false, t, alloc));
+  }
   MGPU_CUDA(cudaStreamSynchronize(s));
   return 0;
 }

@@ -23,9 +23,11 @@ struct DeviceTopo {
 using TopoAlloc = std::function<int(int*&, size_t)>;
 
 // From the device face arrays c0, c1 (0-based, c1 = -1 on the boundary).
-// Waits for stream s before returning.
+// levels: build the triangular level sets too (only the FP64 form's ILU(0) /
+// IC(0) sweeps read them; without them lo_ptr, up_ptr, ... stay null and
+// nlev_lo = nlev_up = 0). Waits for stream s before returning.
 int device_topology(int N, int F, const int* c0, const int* c1, DeviceTopo& t, const TopoAlloc& alloc,
-                    cudaStream_t s);
+                    cudaStream_t s, bool levels = true);
 // Widest row W of the pattern and, when W <= max_width, its column-major ELL
 // copy: entry t of row i at t * ld + i with ld = N rounded up to a multiple of
 // 4 (every column starts 16-byte aligned), padding the row itself.

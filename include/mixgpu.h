@@ -364,8 +364,8 @@ int mgpu_cg_jacobi_noalloc(int n, const int32_t* d_row_ptr, const int32_t* d_col
  * after which a grid-barrier wait gives up, 0 = the built-in bound of about
  * 2 s; for tests of the timeout path), "gather_faces" (assembly kernels: the
  * faces of a cell whose loads a thread issues before summing, 1, 2, 3 or 6
- * (4 and 5 take 3), default 3; results are the same
- * bits for every value), "barrier_poll_ns" (sleep between two
+ * (4 and 5 take 3); 0, the default, gives each kernel its measured best;
+ * results are the same bits for every value), "barrier_poll_ns" (sleep between two
  * polls of a grid-barrier wait, 0-10000 ns, default 100; 0 polls back to back
  * and backs off by 64 ns after 256 polls). */
 int mgpu_set_tuning(const char* key, int value);

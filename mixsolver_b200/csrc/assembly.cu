@@ -1235,18 +1235,18 @@ __device__ __forceinline__ const BatchCase& stage_case(unsigned char* raw, const
   }
 
 MGPU_BATCHED(fill_apc, RANGE_N, if (i < d.N) d.apc[i] = 1.0)
-MGPU_BATCHED(gradients, RANGE_N, b_gradients<3>(d, P, (int)i))
+MGPU_BATCHED(gradients, RANGE_N, b_gradients<1>(d, P, (int)i))
 MGPU_BATCHED(rhiechow_piso, RANGE_F, if (sc.transient) b_rhiechow(d, P, (int)i))
 MGPU_BATCHED(begin_iter, RANGE_3N, b_begin_iter(d, sc.transient, sc.time_scheme, P.inlet_ramp, i))
 MGPU_BATCHED(limiter, RANGE_N, if (P.conv_blend > 0.0) b_limiter(d, P, arg, (int)i))
 MGPU_BATCHED(momentum, RANGE_N, b_momentum(d, P, arg, (int)i))
-MGPU_BATCHED(mom_interior, RANGE_N, b_mom_interior<3>(d, P, (int)i))
+MGPU_BATCHED(mom_interior, RANGE_N, b_mom_interior<2>(d, P, (int)i))
 MGPU_BATCHED(mom_finish, RANGE_N, b_mom_finish(d, P, arg, (int)i))
 MGPU_BATCHED(apc, RANGE_N, b_apc(d, sc.transient ? 1.0 : P.alpha_u, (int)i))
 MGPU_BATCHED(rhiechow, RANGE_F, b_rhiechow(d, P, (int)i))
 MGPU_BATCHED(outflow, RANGE_ONE, if (sc.has_outflow) b_outflow(d))
-MGPU_BATCHED(ppe, RANGE_N, if (arg < sc.ncorr) b_ppe<3>(d, P, (int)i))
-MGPU_BATCHED(correct_cells, RANGE_N, if (arg < sc.ncorr) b_correct_cells<3>(d, P, (int)i))
+MGPU_BATCHED(ppe, RANGE_N, if (arg < sc.ncorr) b_ppe<2>(d, P, (int)i))
+MGPU_BATCHED(correct_cells, RANGE_N, if (arg < sc.ncorr) b_correct_cells<2>(d, P, (int)i))
 MGPU_BATCHED(correct_flux, RANGE_F, if (arg < sc.ncorr) b_correct_flux(d, (int)i))
 MGPU_BATCHED(diag, RANGE_N, b_diag(d, sc.transient, (int)i))
 MGPU_BATCHED(diag_finalize, RANGE_ONE, if (threadIdx.x == 0) b_diag_finalize(d, P, sc.transient))
@@ -1258,17 +1258,20 @@ MGPU_BATCHED(diag_finalize, RANGE_ONE, if (threadIdx.x == 0) b_diag_finalize(d, 
 // ---------------- launchers -------------------------------------------------
 
 #define GRID(n) ceil_div((n), 256), 256, 0, s
-// a cell-gather kernel K<k> for the chunk size the gather_faces key selects
-#define MGPU_GATHER_LAUNCH(KERNEL, ...)             \
-  do {                                              \
-    if (g_gather_faces >= 6)                        \
-      KERNEL<6 __VA_ARGS__><<<GRID(d.N)>>>(d, P);   \
-    else if (g_gather_faces >= 3)                   \
-      KERNEL<3 __VA_ARGS__><<<GRID(d.N)>>>(d, P);   \
-    else if (g_gather_faces == 2)                   \
-      KERNEL<2 __VA_ARGS__><<<GRID(d.N)>>>(d, P);   \
-    else                                            \
-      KERNEL<1 __VA_ARGS__><<<GRID(d.N)>>>(d, P);   \
+// a cell-gather kernel KERNEL<k> for chunk size k: the gather_faces key if
+// set, else the kernel's own measured best DEF (B200, 524k channel: 1 for the
+// gradients, 2 for the momentum interior, PPE and cell correction)
+#define MGPU_GATHER_LAUNCH(KERNEL, DEF, ...)                    \
+  do {                                                          \
+    const int k_ = g_gather_faces > 0 ? g_gather_faces : (DEF); \
+    if (k_ >= 6)                                                \
+      KERNEL<6 __VA_ARGS__><<<GRID(d.N)>>>(d, P);               \
+    else if (k_ >= 3)                                           \
+      KERNEL<3 __VA_ARGS__><<<GRID(d.N)>>>(d, P);               \
+    else if (k_ == 2)                                           \
+      KERNEL<2 __VA_ARGS__><<<GRID(d.N)>>>(d, P);               \
+    else                                                        \
+      KERNEL<1 __VA_ARGS__><<<GRID(d.N)>>>(d, P);               \
   } while (0)
 
 int geometry_setup(DeviceCase& d, const double* x, const int* fptr, const int* fnodes, double* pcen,
@@ -1287,7 +1290,7 @@ int geometry_setup(DeviceCase& d, const double* x, const int* fptr, const int* f
 }
 
 int launch_gradients(const DeviceCase& d, const AsmParams& P, cudaStream_t s) {
-  MGPU_GATHER_LAUNCH(k_gradients);
+  MGPU_GATHER_LAUNCH(k_gradients, 1);
   MGPU_LAUNCH_CHECK("k_gradients");
   if (d.energy) {
     k_tgrad<<<GRID(d.N)>>>(d);
@@ -1317,9 +1320,9 @@ int launch_momentum(const DeviceCase& d, const AsmParams& P, int comp, cudaStrea
 }
 int launch_mom_interior(const DeviceCase& d, const AsmParams& P, cudaStream_t s) {
   if (P.nonorth_corr > 0.0)
-    MGPU_GATHER_LAUNCH(k_mom_interior, , true);
+    MGPU_GATHER_LAUNCH(k_mom_interior, 2, , true);
   else
-    MGPU_GATHER_LAUNCH(k_mom_interior, , false);
+    MGPU_GATHER_LAUNCH(k_mom_interior, 2, , false);
   MGPU_LAUNCH_CHECK("k_mom_interior");
   return 0;
 }
@@ -1349,12 +1352,12 @@ int launch_outflow(const DeviceCase& d, cudaStream_t s) {
   return 0;
 }
 int launch_ppe(const DeviceCase& d, const AsmParams& P, cudaStream_t s) {
-  MGPU_GATHER_LAUNCH(k_ppe);
+  MGPU_GATHER_LAUNCH(k_ppe, 2);
   MGPU_LAUNCH_CHECK("k_ppe");
   return 0;
 }
 int launch_correct(const DeviceCase& d, const AsmParams& P, cudaStream_t s) {
-  MGPU_GATHER_LAUNCH(k_correct_cells);
+  MGPU_GATHER_LAUNCH(k_correct_cells, 2);
   MGPU_LAUNCH_CHECK("k_correct_cells");
   k_correct_flux<<<GRID(d.F)>>>(d);
   MGPU_LAUNCH_CHECK("k_correct_flux");

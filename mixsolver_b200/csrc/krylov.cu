@@ -53,7 +53,7 @@ double g_cheb_ratio = 1000.0; // and the ratio lambda_max / lambda_min of its in
 unsigned g_spin_limit = 0; // polls before a bounded barrier wait gives up (0: kSpinLimit, ~2 s)
 unsigned g_poll_ns = 100;  // sleep between the polls of a barrier wait (ns)
 int g_mixed_occ = 5;       // mixed kernels: resident blocks per SM (2-8; FP64 polynomial 2-5)
-int g_gather_faces = 3;    // assembly gathers: faces whose loads a thread issues together (1, 2, 3, 6)
+int g_gather_faces = 0;    // assembly gathers: faces whose loads a thread issues together (0: per kernel)
 int g_batch_occ = 4;       // batched lane kernel: resident blocks per SM (2-5)
 namespace {
 
@@ -761,7 +761,7 @@ int set_tuning(const char* key, int value) {
     g_batch_occ = value;
   } else if (k == "spin_limit" && value >= 0) {
     g_spin_limit = (unsigned)value;
-  } else if (k == "gather_faces" && value >= 1 && value <= 6) {
+  } else if (k == "gather_faces" && value >= 0 && value <= 6) {
     g_gather_faces = value;
   } else if (k == "barrier_poll_ns" && value >= 0 && value <= 10000) {
     g_poll_ns = (unsigned)value;

@@ -509,11 +509,11 @@ def test_bc_stage_kernels_bit_exact(name):
         np.testing.assert_array_equal(fg[k], fo[k], err_msg=k)
 
 
-@pytest.mark.parametrize("gather", [1, 6])
+@pytest.mark.parametrize("gather", [1, 3, 6])
 @pytest.mark.parametrize("name", ["mass_outflow", "vinlet_farfield", "tet"])
 def test_gather_chunks_bit_exact(name, gather):
-    """The assembly gathers load a cell's faces in chunks (gather_faces, 3
-    by default and in every other test); every chunk size gives the oracle's
+    """The assembly gathers load a cell's faces in chunks (gather_faces; by
+    default each kernel's own size, 1 or 2, in every other test); every chunk size gives the oracle's
     bits, on hexes (6 faces: whole and split chunks) and tets (4 faces: a
     partly filled chunk), with every boundary kind's branch."""
     if name == "tet":
@@ -550,7 +550,7 @@ def test_gather_chunks_bit_exact(name, gather):
         for k in ("u", "p", "flux"):
             np.testing.assert_array_equal(fg[k], fo[k], err_msg=k)
     finally:
-        S.set_tuning("gather_faces", 3)
+        S.set_tuning("gather_faces", 0)
 
 
 @pytest.mark.parametrize("name", BC_CASES)

@@ -214,7 +214,7 @@ def hbm_peak():
         return 6650.0, "6.65 TB/s earlier measurement on this pool (of fallback)"
 
 
-def krylov_bytes(n, nnz, its, method, mixed=False, tol=1e-8, tau=1e-4, cheb_k=16):
+def krylov_bytes(n, nnz, its, method, mixed=False, tol=1e-8, tau=1e-4, cheb_k=None):
     """Algorithmic bytes of one Krylov solve: the unique footprint of every
     pass over the system (matrix entries once, each vector read or written
     once per pass), in the solver's own arithmetic types.
@@ -238,6 +238,9 @@ def krylov_bytes(n, nnz, its, method, mixed=False, tol=1e-8, tau=1e-4, cheb_k=16
       12 nnz) and, per refinement step, one FP64 true residual and the x
       update."""
     import math
+    if cheb_k is None:  # the degree the library runs with (the cheb_degree tuning key)
+        from mixsolver_b200 import solver as S
+        cheb_k = S.get_tuning("cheb_degree")
     if mixed:
         true_res = 12 * nnz + 4 * (n + 1) + 28 * n
         if method == "pcg":

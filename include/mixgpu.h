@@ -369,6 +369,9 @@ int mgpu_cg_jacobi_noalloc(int n, const int32_t* d_row_ptr, const int32_t* d_col
  * polls of a grid-barrier wait, 0-10000 ns, default 100; 0 polls back to back
  * and backs off by 64 ns after 256 polls). */
 int mgpu_set_tuning(const char* key, int value);
+/* The value in effect of a mgpu_set_tuning key (every key but stream_pool),
+ * e.g. the Chebyshev degree a byte model of the mixed pressure solve needs. */
+int mgpu_get_tuning(const char* key, int* value);
 
 /* Coupled mode (the coupling driver's hook, mod_mix_driver.f90:1032 calling
  * uns_solver_step with interface data). A zone given a bc line of type

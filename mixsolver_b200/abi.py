@@ -244,7 +244,7 @@ EXPORTS = ["mgpu_version", "mgpu_last_error", "mgpu_set_device", "mgpu_case_crea
            "mgpu_case_destroy", "mgpu_case_device_bytes", "mgpu_fields_upload",
            "mgpu_fields_download", "mgpu_simple_run", "mgpu_piso_run", "mgpu_pimple_run", "mgpu_nan_scan",
            "mgpu_krylov_solve", "mgpu_csr_matvec", "mgpu_build_connectivity", "mgpu_geometry",
-           "mgpu_rcm_order", "mgpu_case_stage", "mgpu_cg_jacobi_noalloc", "mgpu_set_tuning",
+           "mgpu_rcm_order", "mgpu_case_stage", "mgpu_cg_jacobi_noalloc", "mgpu_set_tuning", "mgpu_get_tuning",
            "mgpu_case_solve_times", "mgpu_case_timing", "mgpu_case_set_profiling", "mgpu_case_begin",
            "mgpu_case_finish", "mgpu_batch_create", "mgpu_batch_destroy", "mgpu_batch_set_policy",
            "mgpu_batch_step", "mgpu_batch_poll", "mgpu_batch_run", "mgpu_batch_info", "mgpu_batch_plan",
@@ -305,6 +305,7 @@ def load_library(path: str = LIB_PATH):
                                            C.c_double, C.c_int, C.c_int, C.c_void_p, P(C.c_int), dblp,
                                            P(C.c_int)]
     lib.mgpu_set_tuning.argtypes = [C.c_char_p, C.c_int]
+    lib.mgpu_get_tuning.argtypes = [C.c_char_p, P(C.c_int)]
     lib.mgpu_case_solve_times.argtypes = [C.c_void_p, dblp, C.c_int, P(C.c_int)]
     lib.mgpu_case_timing.argtypes = [C.c_void_p, P(MgpuTiming)]
     lib.mgpu_case_set_profiling.argtypes = [C.c_void_p, C.c_int]

@@ -774,6 +774,43 @@ int set_tuning(const char* key, int value) {
   return 0;
 }
 
+int get_tuning(const char* key, int* value) {
+  const std::string k(key ? key : "");
+  if (!value) return MGPU_E_ARG;
+  if (k == "single_block_rows") {
+    *value = g_single_block_rows;
+  } else if (k == "sweep_threads") {
+    *value = g_sweep_threads;
+  } else if (k == "cheb_degree") {
+    *value = g_cheb_degree;
+  } else if (k == "cheb_ratio") {
+    *value = (int)g_cheb_ratio;
+  } else if (k == "min_blocks") {
+    *value = g_min_blocks;
+  } else if (k == "sweep_sleep_ns") {
+    *value = g_sweep_sleep;
+  } else if (k == "batch_reserve_blocks") {
+    *value = g_batch_reserve;
+  } else if (k == "l2_prefetch_mb") {
+    *value = g_prefetch_mb;
+  } else if (k == "mixed_blocks_per_sm") {
+    *value = g_mixed_occ;
+  } else if (k == "batch_blocks_per_sm") {
+    *value = g_batch_occ;
+  } else if (k == "spin_limit") {
+    *value = (int)g_spin_limit;
+  } else if (k == "gather_faces") {
+    *value = g_gather_faces;
+  } else if (k == "barrier_poll_ns") {
+    *value = (int)g_poll_ns;
+  } else {
+    set_error("mgpu_get_tuning: unknown key: " + k);
+    return MGPU_E_ARG;
+  }
+  return 0;
+}
+
 }  // namespace mgpu
 
 extern "C" int mgpu_set_tuning(const char* key, int value) { return mgpu::set_tuning(key, value); }
+extern "C" int mgpu_get_tuning(const char* key, int* value) { return mgpu::get_tuning(key, value); }

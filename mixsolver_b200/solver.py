@@ -320,6 +320,14 @@ def set_tuning(key: str, value: int) -> None:
     abi.check(lib, lib.mgpu_set_tuning(key.encode(), int(value)), "mgpu_set_tuning")
 
 
+def get_tuning(key: str) -> int:
+    """The value in effect of a tuning key (mgpu_get_tuning)."""
+    lib = _lib()
+    v = C.c_int(0)
+    abi.check(lib, lib.mgpu_get_tuning(key.encode(), C.byref(v)), "mgpu_get_tuning")
+    return int(v.value)
+
+
 def _krylov(method, row_ptr, col_idx, val, b, x, tol, maxit, norm_mode=0):
     lib = _lib()
     n = len(row_ptr) - 1

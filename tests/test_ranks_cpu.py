@@ -73,7 +73,10 @@ def test_krylov_byte_model_matches_the_stated_formulas():
     sys.path.insert(0, ROOT)
     import bench
     N, nnz = 524288, 3629056
-    per = lambda m: (bench.krylov_bytes(N, nnz, 10, m, True) - bench.krylov_bytes(N, nnz, 0, m, True)) / 10
+    def per(m, k=16):
+        return (bench.krylov_bytes(N, nnz, 10, m, True, cheb_k=k) - bench.krylov_bytes(N, nnz, 0, m, True, cheb_k=k)) / 10
     assert per("pcg") == 132 * nnz + 456 * N
     assert round(per("pcg") / N) == 1370
+    # degree k: one FP64 pass and k - 1 FP32 passes
+    assert per("pcg", 24) == (12 + 8 * 23) * nnz + (96 + 24 * 23) * N
     assert per("bicg") == 16 * nnz + 104 * N + 8

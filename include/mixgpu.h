@@ -347,7 +347,7 @@ int mgpu_cg_jacobi_noalloc(int n, const int32_t* d_row_ptr, const int32_t* d_col
  * "sweep_sleep_ns" (back-off of a long wait in that sweep, default 0),
  * "min_blocks" (least number of blocks of a multi-block solve, default 1),
  * "cheb_degree" (mixed form: degree of the Chebyshev-Jacobi pressure
- * preconditioner, 1 = plain Jacobi, default 16), "cheb_ratio" (lambda_max over
+ * preconditioner, 1 = plain Jacobi, default 24), "cheb_ratio" (lambda_max over
  * lambda_min of its interval, default 1000), "batch_reserve_blocks" (block
  * slots a batched launch leaves free for other streams, so a case being set
  * up while a batch steps is not held up behind its persistent kernels,

@@ -45,7 +45,7 @@ int g_sweep_threads = 65536;
 int g_sweep_sleep = 0;
 int g_min_blocks = 1;
 }  // namespace
-int g_cheb_degree = 16;      // mixed form: Chebyshev-Jacobi degree of the pressure preconditioner
+int g_cheb_degree = 24;      // mixed form: Chebyshev-Jacobi degree of the pressure preconditioner
 int g_batch_reserve = 0;  // block slots batched launches leave to other streams
 int g_prefetch_mb = 96;   // mixed systems whose streamed bytes exceed this prefetch into L2
 int prewarm_streams(int n);  // case.cu

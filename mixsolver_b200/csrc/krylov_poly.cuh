@@ -672,6 +672,13 @@ _Pragma("unroll") for (int r = 0; r < kRows; ++r) {
 // entry a.r holds b - A x0 and rnorm0 its norm. Barriers: every pass that
 // writes x, rr or z ends in a reduction (one grid barrier), which is also the
 // barrier before the next SpMV pass.
+// After a residual replacement in pcg_reliable: start a new direction when
+// the replacement came from convergence of the recursive residual (its check
+// failed), or when the recursive residual had drifted by more than 2x.
+__device__ __forceinline__ bool rel_delta_restart(double rr_true2, double rr_rec2, bool converged) {
+  return converged || rr_true2 > 4.0 * rr_rec2;
+}
+
 template <typename V, bool L1, int ELL>
 __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid& g, Red& R, const Rows& rows,
                              double bnrm, double rnorm0, double lmax, V inv_th) {
@@ -786,10 +793,14 @@ __device__ void pcg_reliable(const KrylovArgs& a, const MixedArgsT<V>& m, VGrid&
     }
     rr_ref = (rnorm * sc) * (rnorm * sc);
     rzn = t2[1];
-    // the recursive residual had drifted from the true one by more than a
-    // factor 2: the kept direction no longer suits the replaced residual, so
-    // the next iteration starts a new direction (beta = 0)
-    if (rr_ref > 4.0 * rec2) first = true;
+    // the recursive residual reached the tolerance (or, with rel_delta > 0,
+    // fell by delta) while the true one did not: the kept direction belongs to
+    // the drifted residual. A restart from the true residual (beta = 0) keeps
+    // a solve at its attainable accuracy stagnating instead of diverging; the
+    // FP64 polynomial form at lin_tol 1e-12 and degree 24 diverged on the
+    // channel's second pressure system when the direction was kept up to a
+    // drift of 2x.
+    if (rel_delta_restart(rr_ref, rec2, s2[0] <= stop2)) first = true;
   }
   write_result_m(a, g, total, rnorm / bnrm, ierr);
 }

@@ -457,12 +457,13 @@ def run_ours(args):
         "accuracy": accuracy,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
-                     # DRAM bytes of one pressure-solve launch from an ncu capture of this
-                     # workload (profiles/k_pcg_mixed_channel524k.md)
-                     "traffic": 283.4e6 if mixed else None,
-                     "resident": "L2: the FP32 system (~44 MB) stays in the 126 MB L2 across the solve's passes, "
-                                 "DRAM carries 0.5 % of the algorithmic bytes (ncu); frac is an HBM-equivalent "
-                                 "rate, see l2 for the fraction of the L2 roofline",
+                     # DRAM bytes of one pressure-solve launch (36 iterations at the default
+                     # degree 24) from an ncu capture of this workload
+                     # (profiles/k_pcg_mixed_channel524k.md)
+                     "traffic": 1.914e9 if mixed and S.get_tuning("cheb_degree") == 24 else None,
+                     "resident": "L2: the system (~94 MB with its FP64 copy) stays in the 126 MB L2 across the "
+                                 "solve's passes, DRAM carries 5 % of the algorithmic bytes (ncu); frac is an "
+                                 "HBM-equivalent rate, see l2 for the fraction of the L2 roofline",
                      "l2": {"achieved": achieved, "peak": l2peak, "unit": "GB/s",
                             "frac": (achieved / l2peak) if achieved else None,
                             "peak_source": "L2-resident c = a + b over 3 x 16 MiB buffers, graph-replayed, "
@@ -653,7 +654,11 @@ def run_piso(args):
                    "speedup_vs_fp64": value / (world * args.fp64_steps / (t64 / 1e3)),
                    "rel_l2_vs_fp64": rel, "rel_l2_after_steps": args.fp64_steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "frac": (achieved / peak) if achieved else None,
+                     # DRAM bytes of one pressure-solve launch (the first corrector, 105
+                     # iterations at the default degree 24) from an ncu capture of this
+                     # workload (profiles/k_pcg_mixed_piso3M.md)
+                     "traffic": 539.5e9 if S.get_tuning("cheb_degree") == 24 else None,
                      "kernel": "k_pcg_mixed (pressure solves)",
                      "algorithmic_bytes_per_launch": float(np.mean(ppe_bytes)), "avg_launch_ms": ppe_launch_ms,
                      "launches": len(ppe_ms), "all_krylov_solves_gbs": family,

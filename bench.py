@@ -412,7 +412,8 @@ def run_ours(args):
         # the run's end state for the e2e leg below is the timed state's successor
         f = f_a
     # end to end through the public API: host fields in (page-locked), one outer
-    # iteration, fields out into page-locked arrays
+    # iteration and the fields out into page-locked arrays in one call
+    # (mgpu_simple_run_fields: gp, gu and apc copied while the pressure solve runs)
     h2d = (3 * N + N + F) * 8
     d2h = (3 * N + N + F + 3 * N + 9 * N + N) * 8
     hbuf = pinned_fields(case)
@@ -423,8 +424,7 @@ def run_ours(args):
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         case.upload(u=hbuf["u"], p=hbuf["p"], flux=hbuf["flux"])
-        ier, _ = case.simple_run(1, logcap=1)
-        case.fields(out=hbuf)
+        ier, _, _ = case.simple_run_fields(1, out=hbuf, logcap=1)
     e2e_t = max_over_ranks(time.perf_counter() - t0, world)
     e2e = {"value": world * e2e_steps / e2e_t, "unit": UNIT, "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h}

@@ -209,6 +209,18 @@ int mgpu_fields_download(MgpuCase* c, double* u, double* p, double* flux, double
  * on convergence. log: optional, capacity logcap records; *nrec = records
  * written. *ier: 0, 20 momentum breakdown, 21 PPE breakdown, 60 non-finite. */
 int mgpu_simple_run(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nrec, int* ier);
+/* mgpu_simple_run followed by mgpu_fields_download, for callers that copy the
+ * fields back after every call (simple_run_gpu, the coupling loop): the same
+ * results, with the copies of gp, gu and apc overlapping the last
+ * iteration's pressure solve. Those three are final once that iteration's
+ * gradients are formed, and go to the host on a second stream when their
+ * arrays are page-locked (pageable arrays, or a run that stops before its
+ * last iteration, copy everything at the end). Any output may be NULL. The
+ * first call on a case creates that stream and a device buffer of 12 doubles
+ * per cell. No reference counterpart: simple_run leaves its fields in
+ * memory the host already owns. */
+int mgpu_simple_run_fields(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nrec, int* ier,
+                           double* u, double* p, double* flux, double* gp, double* gu, double* apc);
 
 /* Transient PISO: piso_run_mpi at one rank (mod_uns_simple_mpi.f90:298-571).
  * *ier: 0, 30 transient=false, 31 dt<=0, 33 momentum breakdown, 34 PPE

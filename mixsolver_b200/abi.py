@@ -242,7 +242,7 @@ def records_to_list(recs, n: int) -> list:
 # Every symbol include/mixgpu.h declares (checked by the CPU test suite).
 EXPORTS = ["mgpu_version", "mgpu_last_error", "mgpu_set_device", "mgpu_case_create",
            "mgpu_case_destroy", "mgpu_case_device_bytes", "mgpu_fields_upload",
-           "mgpu_fields_download", "mgpu_simple_run", "mgpu_piso_run", "mgpu_pimple_run", "mgpu_nan_scan",
+           "mgpu_fields_download", "mgpu_simple_run_fields", "mgpu_simple_run", "mgpu_piso_run", "mgpu_pimple_run", "mgpu_nan_scan",
            "mgpu_krylov_solve", "mgpu_csr_matvec", "mgpu_build_connectivity", "mgpu_geometry",
            "mgpu_rcm_order", "mgpu_case_stage", "mgpu_cg_jacobi_noalloc", "mgpu_set_tuning", "mgpu_get_tuning",
            "mgpu_case_solve_times", "mgpu_case_timing", "mgpu_case_set_profiling", "mgpu_case_begin",
@@ -278,6 +278,8 @@ def load_library(path: str = LIB_PATH):
     lib.mgpu_fields_upload.argtypes = [C.c_void_p, dblp, dblp, dblp, dblp, dblp]
     lib.mgpu_fields_download.argtypes = [C.c_void_p, dblp, dblp, dblp, dblp, dblp, dblp]
     lib.mgpu_simple_run.argtypes = [C.c_void_p, C.c_int, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int)]
+    lib.mgpu_simple_run_fields.argtypes = [C.c_void_p, C.c_int, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int),
+                                           dblp, dblp, dblp, dblp, dblp, dblp]
     lib.mgpu_piso_run.argtypes = [C.c_void_p, C.c_int, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int)]
     lib.mgpu_pimple_run.argtypes = [C.c_void_p, C.c_int, P(MgpuIterRec), C.c_int, P(C.c_int), P(C.c_int)]
     lib.mgpu_cas_read.argtypes = [C.c_char_p, P(MgpuMesh), P(C.c_void_p), P(C.c_int)]

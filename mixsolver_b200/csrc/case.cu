@@ -460,6 +460,29 @@ int end_run(MgpuCase* c, int nsteps_done, MgpuIterRec* log, int logcap, int* nre
   return 0;
 }
 
+// The armed last iteration of mgpu_simple_run_fields: gp and gu transposed to
+// cell-major order into stage2 on the case's stream, then gp, gu and apc
+// copied to the caller's page-locked arrays on copy_stream, which runs beside
+// the rest of the iteration (nothing later in the run writes these fields).
+int enqueue_early_copy(MgpuCase* c) {
+  const long N = c->d.N;
+  cudaStream_t s = c->stream;
+  MgpuCase::EarlyCopy& e = c->early;
+  if (e.gp) TRY(launch_planes_to_cells(c->d.gp, N, 3, false, c->stage2, s));
+  if (e.gu) TRY(launch_planes_to_cells(c->d.gu, N, 9, true, c->stage2 + 3 * N, s));
+  c->launches += (e.gp ? 1 : 0) + (e.gu ? 1 : 0);
+  MGPU_CUDA(cudaEventRecord(c->ev_early, s));
+  MGPU_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev_early, 0));
+  cudaStream_t cs = c->copy_stream;
+  if (e.gp) MGPU_CUDA(cudaMemcpyAsync(e.gp, c->stage2, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, cs));
+  if (e.gu) MGPU_CUDA(cudaMemcpyAsync(e.gu, c->stage2 + 3 * N, sizeof(double) * 9 * N, cudaMemcpyDeviceToHost, cs));
+  if (e.apc) MGPU_CUDA(cudaMemcpyAsync(e.apc, c->d.apc, sizeof(double) * N, cudaMemcpyDeviceToHost, cs));
+  MGPU_CUDA(cudaEventRecord(c->ev_copied, cs));
+  e.armed = false;
+  e.done = true;
+  return 0;
+}
+
 int outer_iteration(MgpuCase* c, bool transient) {
   DeviceCase& d = c->d;
   const AsmParams& P = c->P;
@@ -469,6 +492,7 @@ int outer_iteration(MgpuCase* c, bool transient) {
   TRY(assemble_and_solve_momentum(c, transient));
   TRY(launch_apc(d, transient ? 1.0 : P.alpha_u, s));
   TRY(launch_gradients(d, P, s));
+  if (c->early.armed) TRY(enqueue_early_copy(c));
   TRY(launch_rhiechow(d, P, s));
   c->launches += 3;
   if (c->has_outflow) {
@@ -861,8 +885,20 @@ int mgpu_fields_download(MgpuCase* c, double* u, double* p, double* flux, double
   return 0;
 }
 
+static int simple_run_armed(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nrec, int* ier);
+
 int mgpu_simple_run(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nrec, int* ier) {
   if (!c || !ier) return MGPU_E_ARG;
+  c->early = MgpuCase::EarlyCopy{};
+  return simple_run_armed(c, nsteps, log, logcap, nrec, ier);
+}
+
+// mgpu_simple_run's body; the early copies of c->early (if any are set) are
+// armed for the run's last iteration
+static int simple_run_armed(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nrec, int* ier) {
+  if (!c || !ier) return MGPU_E_ARG;
+  c->early.armed = false;
+  c->early.done = false;
   *ier = 0;
   if (nrec) *nrec = 0;
   int it_max = c->ctrl.outer_max;
@@ -875,6 +911,7 @@ int mgpu_simple_run(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* 
   TRY(launch_gradients(c->d, c->P, c->stream));
   c->launches += 2;
   for (int it = 0; it < it_max; ++it) {
+    c->early.armed = c->early.gp || c->early.gu || c->early.apc ? it + 1 == it_max : false;
     TRY(outer_iteration(c, false));
     if ((it + 1) % 64 == 0 && it + 1 < it_max) {
       // stop enqueuing once a run has aborted (convergence, breakdown, NaN)
@@ -885,6 +922,54 @@ int mgpu_simple_run(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* 
     }
   }
   return end_run(c, it_max, log, logcap, nrec, ier);
+}
+
+namespace {
+bool page_locked(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+}  // namespace
+
+int mgpu_simple_run_fields(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nrec, int* ier, double* u,
+                           double* p, double* flux, double* gp, double* gu, double* apc) {
+  if (!c || !ier) return MGPU_E_ARG;
+  const bool early = (gp || gu || apc) && (!gp || page_locked(gp)) && (!gu || page_locked(gu)) &&
+                     (!apc || page_locked(apc));
+  if (early) {
+    if (!c->copy_stream) {
+      MGPU_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+      MGPU_CUDA(cudaEventCreateWithFlags(&c->ev_early, cudaEventDisableTiming));
+      MGPU_CUDA(cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming));
+    }
+    const size_t need = 12 * (size_t)c->d.N;
+    if (c->stage2_n < need) {
+      if (c->stage2) MGPU_CUDA(cudaFreeAsync(c->stage2, c->stream));
+      void* q = nullptr;
+      MGPU_CUDA(cudaMallocAsync(&q, sizeof(double) * need, c->stream));
+      c->stage2 = (double*)q;
+      c->stage2_n = need;
+    }
+  }
+  // mgpu_simple_run with the early copies armed for its last iteration
+  c->early = MgpuCase::EarlyCopy{};
+  if (early) {
+    c->early.gp = gp;
+    c->early.gu = gu;
+    c->early.apc = apc;
+  }
+  const int rc = simple_run_armed(c, nsteps, log, logcap, nrec, ier);
+  const bool done = c->early.done;
+  c->early = MgpuCase::EarlyCopy{};
+  if (done) MGPU_CUDA(cudaEventSynchronize(c->ev_copied));
+  if (rc != 0) return rc;
+  // the rest (all of it when the run stopped before its last iteration or the
+  // arrays are pageable), as mgpu_fields_download
+  return mgpu_fields_download(c, u, p, flux, done ? nullptr : gp, done ? nullptr : gu, done ? nullptr : apc);
 }
 
 int mgpu_piso_run(MgpuCase* c, int nsteps, MgpuIterRec* log, int logcap, int* nrec, int* ier) {

@@ -49,6 +49,17 @@ struct MgpuCase {
   int run_gen = 0;    // counts mgpu_case_begin calls
   double* stage = nullptr;  // device staging of cell-major field copies (grown on demand)
   size_t stage_n = 0;
+  // mgpu_simple_run_fields: the last iteration's gp, gu and apc, final once
+  // its gradients are formed, go to page-locked host arrays on copy_stream
+  // while the iteration's pressure solve runs (gp and gu through stage2)
+  struct EarlyCopy {
+    double *gp = nullptr, *gu = nullptr, *apc = nullptr;
+    bool armed = false, done = false;
+  } early;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_early = nullptr, ev_copied = nullptr;
+  double* stage2 = nullptr;
+  size_t stage2_n = 0;
   std::vector<int> iface_faces;     // interface faces (0-based), bc order then face order
   int* d_iface_faces = nullptr;     // the same on the device
 
@@ -74,8 +85,13 @@ struct MgpuCase {
     for (auto e : ev_pool) cudaEventDestroy(e);
     if (ev_run0) cudaEventDestroy(ev_run0);
     if (ev_run1) cudaEventDestroy(ev_run1);
+    if (ev_copied) cudaEventSynchronize(ev_copied);
+    if (ev_early) cudaEventDestroy(ev_early);
+    if (ev_copied) cudaEventDestroy(ev_copied);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     for (void* p : allocs) cudaFreeAsync(p, stream);
     if (stage) cudaFreeAsync(stage, stream);
+    if (stage2) cudaFreeAsync(stage2, stream);
     if (stream) mgpu::release_stream(stream);
   }
 };

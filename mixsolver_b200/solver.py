@@ -87,6 +87,37 @@ class UnsCase:
 
     FIELD_SHAPES = {"u": ("N", 3), "p": ("N",), "flux": ("F",), "gp": ("N", 3), "gu": ("N", 3, 3), "apc": ("N",)}
 
+    def _field_arrays(self, out):
+        N, F = self.N, self.F
+        dims = {"N": N, "F": F}
+        if out is None:
+            return {k: np.empty(tuple(dims.get(d, d) for d in shp)) for k, shp in self.FIELD_SHAPES.items()}
+        arrs = {}
+        for k, a in out.items():
+            want = tuple(dims.get(d, d) for d in self.FIELD_SHAPES[k])
+            if a.dtype != np.float64 or a.shape != want or not a.flags.c_contiguous:
+                raise ValueError(f"fields(out): {k} must be C-contiguous float64 of shape {want}")
+            arrs[k] = a
+        return arrs
+
+    def simple_run_fields(self, nsteps: int = 0, out=None, logcap: int = 4096):
+        """simple_run then fields(out) in one call (mgpu_simple_run_fields): the
+        same results, the gp, gu and apc copies overlapping the last
+        iteration's pressure solve when their arrays are page-locked. Returns
+        (ier, records, fields) with fields as fields() returns them."""
+        arrs = self._field_arrays(out)
+        g = lambda k: dptr(arrs[k]) if k in arrs else None
+        recs = (MgpuIterRec * max(logcap, 1))()
+        nrec, ier = C.c_int(0), C.c_int(0)
+        lib = _lib()
+        abi.check(lib, lib.mgpu_simple_run_fields(self.h, int(nsteps), recs, int(logcap), C.byref(nrec),
+                                                  C.byref(ier), g("u"), g("p"), g("flux"), g("gp"), g("gu"),
+                                                  g("apc")), "mgpu_simple_run_fields")
+        res = dict(arrs)
+        if "gu" in res:
+            res["gu"] = res["gu"].transpose(0, 2, 1)
+        return ier.value, records_to_list(recs, min(nrec.value, logcap)), res
+
     def fields(self, out=None):
         """Host copies of u (N,3), p (N), flux (F), gp (N,3), gu (N,3,3) indexed
         [cell, component, direction] and apc (N).
@@ -96,17 +127,7 @@ class UnsCase:
         fields are read back. Its "gu" array receives the C-ABI's layout
         gu(component, direction, cell), i.e. [cell, direction, component]; the
         returned "gu" is its transposed view."""
-        N, F = self.N, self.F
-        dims = {"N": N, "F": F}
-        if out is None:
-            arrs = {k: np.empty(tuple(dims.get(d, d) for d in shp)) for k, shp in self.FIELD_SHAPES.items()}
-        else:
-            arrs = {}
-            for k, a in out.items():
-                want = tuple(dims.get(d, d) for d in self.FIELD_SHAPES[k])
-                if a.dtype != np.float64 or a.shape != want or not a.flags.c_contiguous:
-                    raise ValueError(f"fields(out): {k} must be C-contiguous float64 of shape {want}")
-                arrs[k] = a
+        arrs = self._field_arrays(out)
         g = lambda k: dptr(arrs[k]) if k in arrs else None
         lib = _lib()
         abi.check(lib, lib.mgpu_fields_download(self.h, g("u"), g("p"), g("flux"), g("gp"), g("gu"), g("apc")),

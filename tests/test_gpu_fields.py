@@ -56,3 +56,49 @@ def test_fields_out_matches_fields():
     with pytest.raises(ValueError):
         c.fields(out={"u": np.zeros((c.N, 2))})
     c.close()
+
+
+def _pinned(ref):
+    import torch
+    return {k: torch.empty(v.shape, dtype=torch.float64, pin_memory=True).numpy() for k, v in ref.items()}
+
+
+@pytest.mark.parametrize("what", ["pinned", "pageable", "converges_early", "stops_at_check"])
+def test_simple_run_fields_matches_run_then_download(what):
+    """mgpu_simple_run_fields gives what mgpu_simple_run followed by
+    mgpu_fields_download gives, bit for bit: with page-locked arrays (gp, gu
+    and apc copied during the last iteration), pageable ones (all copied at
+    the end), a run that converges before its last iteration (that iteration
+    then changes nothing) and one that stops at the abort check after 64
+    iterations, before its last one (everything copied at the end)."""
+    mesh, ctrl = cases.cavity3d(12, outer_max=200)
+    nsteps = 6
+    if what == "converges_early":
+        ctrl.outer_tol = 5e-2
+        nsteps = 12
+    elif what == "stops_at_check":
+        ctrl.outer_tol = 5e-2
+        nsteps = 100
+    a, b = S.UnsCase(mesh, ctrl), S.UnsCase(mesh, ctrl)
+    ier_a, log_a = a.simple_run(nsteps)
+    ref = a.fields()
+    out = _pinned(ref) if what != "pageable" else {k: np.empty(v.shape) for k, v in ref.items()}
+    for k in out:
+        out[k][...] = np.nan
+    ier_b, log_b, got = b.simple_run_fields(nsteps, out=out)
+    assert ier_a == ier_b == 0
+    assert len(log_a) == len(log_b)
+    if what in ("converges_early", "stops_at_check"):
+        assert len(log_b) < nsteps
+    for ra, rb in zip(log_a, log_b):
+        assert ra["lin_it"] == rb["lin_it"] and ra["du_max"] == rb["du_max"]
+    for k in ref:
+        np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+    # a second call on the same case (the copy stream and buffer reused)
+    ier_a, _ = a.simple_run(2)
+    ref2 = a.fields()
+    ier_b, _, got2 = b.simple_run_fields(2, out=out)
+    for k in ref2:
+        np.testing.assert_array_equal(got2[k], ref2[k], err_msg=k)
+    a.close()
+    b.close()

@@ -137,6 +137,15 @@ module mod_gpu_iface
          integer(c_int), intent(out) :: nrec, ier
       end function mgpu_simple_run
 
+      integer(c_int) function mgpu_simple_run_fields(case_h, nsteps, log, logcap, nrec, ier, &
+                                                     u, p, flux, gp, gu, apc) &
+            bind(C, name='mgpu_simple_run_fields')
+         import :: c_int, c_ptr
+         type(c_ptr),    value       :: case_h, log, u, p, flux, gp, gu, apc
+         integer(c_int), value       :: nsteps, logcap
+         integer(c_int), intent(out) :: nrec, ier
+      end function mgpu_simple_run_fields
+
       integer(c_int) function mgpu_piso_run(case_h, nsteps, log, logcap, nrec, ier) &
             bind(C, name='mgpu_piso_run')
          import :: c_int, c_ptr
@@ -227,6 +236,12 @@ module mod_gpu_iface
          character(kind=c_char), intent(in) :: key(*)
          integer(c_int), value              :: value
       end function mgpu_set_tuning
+
+      integer(c_int) function mgpu_get_tuning(key, value) bind(C, name='mgpu_get_tuning')
+         import :: c_int, c_char
+         character(kind=c_char), intent(in) :: key(*)
+         integer(c_int), intent(out)        :: value
+      end function mgpu_get_tuning
    end interface
 
 contains

@@ -203,15 +203,19 @@ contains
       if (rc == MGPU_OK) then
          select case (kind)
          case (1)
-            rc = mgpu_simple_run(g_case, int(nsteps, c_int), c_null_ptr, 0_c_int, nrec, cier)
+            ! run and download in one call: gp, gu and apc are copied during the
+            ! last iteration's pressure solve when their arrays are page-locked
+            rc = mgpu_simple_run_fields(g_case, int(nsteps, c_int), c_null_ptr, 0_c_int, nrec, cier, &
+                                        c_loc(fld%u), c_loc(fld%p), c_loc(fld%flux), c_loc(fld%gp), &
+                                        c_loc(fld%gu), c_loc(fld%apc))
          case (2)
             rc = mgpu_piso_run(g_case, int(nsteps, c_int), c_null_ptr, 0_c_int, nrec, cier)
          case default
             rc = mgpu_pimple_run(g_case, int(nsteps, c_int), c_null_ptr, 0_c_int, nrec, cier)
          end select
       end if
-      if (rc == MGPU_OK) rc = mgpu_fields_download(g_case, c_loc(fld%u), c_loc(fld%p), c_loc(fld%flux), &
-                                                   c_loc(fld%gp), c_loc(fld%gu), c_loc(fld%apc))
+      if (rc == MGPU_OK .and. kind /= 1) rc = mgpu_fields_download(g_case, c_loc(fld%u), c_loc(fld%p), &
+                                                   c_loc(fld%flux), c_loc(fld%gp), c_loc(fld%gu), c_loc(fld%apc))
       if (rc == MGPU_OK) rc = mgpu_temperature_download(g_case, c_loc(fld%T), c_loc(fld%gt))
       if (rc /= MGPU_OK) then
          write(*,'(a,i0,2a)') '[uns-gpu] run failed, status ', rc, ': ', trim(mgpu_error_message())

@@ -238,9 +238,10 @@ def krylov_bytes(n, nnz, its, method, mixed=False, tol=1e-8, tau=1e-4, cheb_k=No
       12 nnz) and, per refinement step, one FP64 true residual and the x
       update."""
     import math
-    if cheb_k is None:  # the degree the library runs with (the cheb_degree tuning key)
+    if cheb_k is None:  # the degree the library runs with for n rows (the cheb_* tuning keys)
         from mixsolver_b200 import solver as S
-        cheb_k = S.get_tuning("cheb_degree")
+        big = S.get_tuning("cheb_large_rows")
+        cheb_k = S.get_tuning("cheb_degree_large" if 0 < big <= n else "cheb_degree")
     if mixed:
         true_res = 12 * nnz + 4 * (n + 1) + 28 * n
         if method == "pcg":
@@ -538,6 +539,9 @@ def run_reference(args):
 
 
 PISO_METRIC = "PISO time steps/s, mixed vs FP64 GPU, rel L2 of u, p vs FP64"
+# DRAM bytes of the first corrector's pressure solve on the 3.07 M-tet box, by
+# Chebyshev degree, from ncu captures (profiles/k_pcg_mixed_piso3M.md)
+PISO_TRAFFIC = {24: 539.5e9}
 
 
 def run_piso(args):
@@ -655,10 +659,12 @@ def run_piso(args):
                    "rel_l2_vs_fp64": rel, "rel_l2_after_steps": args.fp64_steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
-                     # DRAM bytes of one pressure-solve launch (the first corrector, 105
-                     # iterations at the default degree 24) from an ncu capture of this
-                     # workload (profiles/k_pcg_mixed_piso3M.md)
-                     "traffic": 539.5e9 if S.get_tuning("cheb_degree") == 24 else None,
+                     # DRAM bytes of one pressure-solve launch (the first corrector) from
+                     # an ncu capture of this workload at the degree in effect
+                     # (profiles/k_pcg_mixed_piso3M.md)
+                     "traffic": PISO_TRAFFIC.get(S.get_tuning("cheb_degree_large")
+                                                 if 0 < S.get_tuning("cheb_large_rows") <= N
+                                                 else S.get_tuning("cheb_degree")),
                      "kernel": "k_pcg_mixed (pressure solves)",
                      "algorithmic_bytes_per_launch": float(np.mean(ppe_bytes)), "avg_launch_ms": ppe_launch_ms,
                      "launches": len(ppe_ms), "all_krylov_solves_gbs": family,

@@ -259,7 +259,8 @@ int mgpu_krylov_solve(int n, const int32_t* row_ptr, const int32_t* col_idx, con
  * host CSR system (arrays 1-based as in mgpu_krylov_solve; no reference
  * counterpart: it stands in for cg_ic0, mod_uns_linsolver.f90:405-461, with
  * the same contract): PCG with a Chebyshev-Jacobi polynomial of degree
- * cheb_degree (<= 0: the cheb_degree tuning key; 1: Jacobi).
+ * cheb_degree (<= 0: the tuning keys, as for a case's pressure solve of n
+ * rows; 1: Jacobi).
  *   precision: MGPU_PREC_MIXED (the conjugate-gradient recurrence in FP64:
  *              x, r, p, A p and every dot product; the polynomial applied in
  *              FP32 to an FP32 copy of r with an FP32 copy of A; a true
@@ -360,7 +361,10 @@ int mgpu_cg_jacobi_noalloc(int n, const int32_t* d_row_ptr, const int32_t* d_col
  * "min_blocks" (least number of blocks of a multi-block solve, default 1),
  * "cheb_degree" (mixed form: degree of the Chebyshev-Jacobi pressure
  * preconditioner, 1 = plain Jacobi, default 24), "cheb_ratio" (lambda_max over
- * lambda_min of its interval, default 1000), "batch_reserve_blocks" (block
+ * lambda_min of its interval, default 1000), "cheb_large_rows",
+ * "cheb_degree_large", "cheb_ratio_large" (pressure systems of at least that
+ * many rows take that degree and ratio instead; defaults 1048576, 48, 10000;
+ * 0 rows: never), "batch_reserve_blocks" (block
  * slots a batched launch leaves free for other streams, so a case being set
  * up while a batch steps is not held up behind its persistent kernels,
  * default 0), "stream_pool" (create this many streams for cases and batches

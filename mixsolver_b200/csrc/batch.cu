@@ -65,6 +65,14 @@ int least_width(long n) {
 // Estimated passes of a solve when no iteration count is known yet: PCG with
 // a degree-k polynomial preconditioner needs ~n^(1/3) iterations on these
 // 3-D pressure systems, k + 1 passes each; BiCGStab about 6 iterations of 4.
+// the Chebyshev degree a pressure solve of n rows runs with
+int cheb_degree_of(long n) {
+  int k = 1;
+  double r = 0.0;
+  cheb_params(n, k, r);
+  return k;
+}
+
 double model_passes(long n, bool pcg, int cheb_k) {
   return pcg ? std::max(5.0, std::cbrt((double)n)) * (std::max(cheb_k, 1) + 1) : 24.0;
 }
@@ -298,7 +306,7 @@ int build_launches(MgpuBatch* b, BatchPhase& ph, const Policy& P) {
         n.push_back(c->d.N);
         passes.push_back(k < (int)ph.passes.size() && ph.passes[k] > 0
                              ? ph.passes[k]
-                             : model_passes(c->d.N, ph.pcg, ph.pcg ? g_cheb_degree : 1));
+                             : model_passes(c->d.N, ph.pcg, ph.pcg ? cheb_degree_of(c->d.N) : 1));
       }
     }
     if (items.empty()) continue;
@@ -503,10 +511,12 @@ int measure_passes(MgpuBatch* b) {
   for (int j = 0; j < K; ++j) live_of[b->live[j]] = j;
   for (auto& ph : b->phases) {
     const int slot = ph.pcg ? std::min(3 + ph.icorr, MGPU_MAXSOLVE - 1) : ph.comp;
-    const double per = ph.pcg ? (double)(std::max(g_cheb_degree, 1) + 1) : 4.0;
     ph.passes.assign(ph.mixed.size(), 0.0);
-    for (size_t k = 0; k < ph.mixed.size(); ++k)
+    for (size_t k = 0; k < ph.mixed.size(); ++k) {
+      const long n = b->cases[ph.mixed[k]]->d.N;
+      const double per = ph.pcg ? (double)(std::max(cheb_degree_of(n), 1) + 1) : 4.0;
       ph.passes[k] = 3.0 + per * std::max(0, its[(size_t)live_of[ph.mixed[k]] * MGPU_MAXSOLVE + slot]);
+    }
   }
   return 0;
 }
@@ -936,7 +946,7 @@ int mgpu_batch_plan(int nsys, const int* rows, const double* passes, int split_r
   }
   const std::vector<int> n(rows, rows + nsys);
   std::vector<double> ps(nsys);
-  for (int i = 0; i < nsys; ++i) ps[i] = passes ? passes[i] : model_passes(n[i], true, g_cheb_degree);
+  for (int i = 0; i < nsys; ++i) ps[i] = passes ? passes[i] : model_passes(n[i], true, cheb_degree_of(n[i]));
   const LaneSet L = plan_lanes(n, ps, Policy{split_rows, wide_lanes}, capacity);
   for (size_t c = 0; c < L.queue.size(); ++c)
     for (int i : L.queue[c])

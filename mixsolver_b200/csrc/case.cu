@@ -241,18 +241,25 @@ MixedArgs mixed_args(const MgpuCase* c, bool bicg) {
   // a system larger than the L2 share given by l2_prefetch_mb streams from
   // DRAM: its SpMV tiles prefetch the next tile's ELL entries
   const bool big = (double)c->d.N * mixed_row_bytes(c->d.ell_w) > g_prefetch_mb * 1048576.0;
+  int k = 1;
+  double ratio = g_cheb_ratio;
+  if (!bicg) cheb_params(c->d.N, k, ratio);
   return MixedArgs{c->d.a32,   c->d.dinv32, c->d.w32,  c->ctrl.mixed_tol > 0.0 ? c->ctrl.mixed_tol : 1e-4,
-                   bicg ? 1 : g_cheb_degree, g_cheb_ratio, c->d.ell_w, c->d.ell_col, c->d.ell_val,
+                   k,          ratio,       c->d.ell_w, c->d.ell_col, c->d.ell_val,
                    c->d.red32, (c->d.ell_col && big) ? 1 : 0, 0.0, c->d.ell_ld, 0,
                    c->d.ell_val64};
 }
 
 // The same solves in FP64 throughout (MGPU_PREC_FP64_POLY): PCG keeps one
-// Krylov stream and checks b - A x only at its end (no intermediate
-// replacement); BiCGStab solves to the tolerance in one pass.
+// Krylov stream and checks b - A x when the recursive residual converges
+// (restarting from it when the check fails); BiCGStab solves to the tolerance
+// in one pass.
 MixedArgsT<double> poly64_args(const MgpuCase* c, bool bicg) {
   const bool big = (double)c->d.N * (16.0 * c->d.ell_w + 8.0 * 10) > g_prefetch_mb * 1048576.0;
-  return MixedArgsT<double>{c->d.a64, c->d.dinv64, c->d.w64, 0.0, bicg ? 1 : g_cheb_degree, g_cheb_ratio,
+  int k = 1;
+  double ratio = g_cheb_ratio;
+  if (!bicg) cheb_params(c->d.N, k, ratio);
+  return MixedArgsT<double>{c->d.a64, c->d.dinv64, c->d.w64, 0.0, k, ratio,
                             c->d.ell_w, c->d.ell_col, c->d.ell_val64, c->d.red32,
                             (c->d.ell_col && big) ? 1 : 0, 0.0, c->d.ell_ld};
 }

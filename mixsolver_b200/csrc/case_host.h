@@ -100,6 +100,9 @@ namespace mgpu {
 
 extern int g_cheb_degree;
 extern double g_cheb_ratio;
+// the Chebyshev degree and interval ratio of a pressure solve of n rows
+// (the cheb_* tuning keys; large systems take the large pair)
+void cheb_params(long n, int& k, double& ratio);
 extern int g_batch_reserve;
 extern int g_prefetch_mb;
 extern unsigned g_spin_limit;

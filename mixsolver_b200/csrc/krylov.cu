@@ -50,6 +50,18 @@ int g_batch_reserve = 0;  // block slots batched launches leave to other streams
 int g_prefetch_mb = 96;   // mixed systems whose streamed bytes exceed this prefetch into L2
 int prewarm_streams(int n);  // case.cu
 double g_cheb_ratio = 1000.0; // and the ratio lambda_max / lambda_min of its interval
+// systems of at least g_cheb_large_rows rows (0: none) take the large pair: their
+// smallest eigenvalues sit lower, and a wider interval with a higher degree
+// pays (3.07 M-tet PISO: 4.50 -> 4.81 steps/s; a 524k channel loses 1-2 %)
+int g_cheb_large_rows = 1 << 20;
+int g_cheb_degree_large = 48;
+double g_cheb_ratio_large = 10000.0;
+// the Chebyshev degree and interval ratio of a pressure solve of n rows
+void cheb_params(long n, int& k, double& ratio) {
+  const bool large = g_cheb_large_rows > 0 && n >= g_cheb_large_rows;
+  k = large ? g_cheb_degree_large : g_cheb_degree;
+  ratio = large ? g_cheb_ratio_large : g_cheb_ratio;
+}
 unsigned g_spin_limit = 0; // polls before a bounded barrier wait gives up (0: kSpinLimit, ~2 s)
 unsigned g_poll_ns = 100;  // sleep between the polls of a barrier wait (ns)
 int g_mixed_occ = 5;       // mixed kernels: resident blocks per SM (2-8; FP64 polynomial 2-5)
@@ -747,6 +759,12 @@ int set_tuning(const char* key, int value) {
     g_cheb_degree = value;
   } else if (k == "cheb_ratio" && value >= 2) {
     g_cheb_ratio = value;
+  } else if (k == "cheb_large_rows" && value >= 0) {
+    g_cheb_large_rows = value;
+  } else if (k == "cheb_degree_large" && value >= 1 && value <= 64) {
+    g_cheb_degree_large = value;
+  } else if (k == "cheb_ratio_large" && value >= 2) {
+    g_cheb_ratio_large = value;
   } else if (k == "min_blocks" && value >= 1) {
     g_min_blocks = value;
   } else if (k == "sweep_sleep_ns" && value >= 0 && value <= 100000) {
@@ -785,6 +803,12 @@ int get_tuning(const char* key, int* value) {
     *value = g_cheb_degree;
   } else if (k == "cheb_ratio") {
     *value = (int)g_cheb_ratio;
+  } else if (k == "cheb_large_rows") {
+    *value = g_cheb_large_rows;
+  } else if (k == "cheb_degree_large") {
+    *value = g_cheb_degree_large;
+  } else if (k == "cheb_ratio_large") {
+    *value = (int)g_cheb_ratio_large;
   } else if (k == "min_blocks") {
     *value = g_min_blocks;
   } else if (k == "sweep_sleep_ns") {

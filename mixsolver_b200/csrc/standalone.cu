@@ -18,6 +18,7 @@ extern unsigned g_spin_limit;  // krylov.cu: the spin_limit tuning key
 extern unsigned g_poll_ns;     // krylov.cu: the barrier_poll_ns tuning key
 extern int g_cheb_degree;      // the cheb_degree and cheb_ratio tuning keys
 extern double g_cheb_ratio;
+void cheb_params(long n, int& k, double& ratio);  // krylov.cu
 extern int g_prefetch_mb;      // l2_prefetch_mb
 }
 
@@ -117,7 +118,7 @@ void analyse(int n, const int32_t* row_ptr, const int32_t* col_idx, Pattern& P) 
 // arguments a case would give them, the ELL copy built on the device.
 template <typename V>
 int poly_solve(int n, const Pattern& P, const double* val, const double* b, double* x, double tol, int maxit,
-                      int cheb_degree, int* it, double* res, int* ierr) {
+                      int cheb_degree, double cheb_ratio, int* it, double* res, int* ierr) {
   DevBuf B;
   const int nnz = P.rp[n];
   int *drp, *dcol, *ddiag, *dferr;
@@ -185,7 +186,7 @@ int poly_solve(int n, const Pattern& P, const double* val, const double* b, doub
   const bool mixed = sizeof(V) == 4;
   const double row_bytes = mixed ? mixed_row_bytes(W) : 16.0 * W + 80.0;
   const bool big = (double)n * row_bytes > g_prefetch_mb * 1048576.0;
-  MixedArgsT<V> m{da,   ddinv, dw, 1e-4, cheb_degree, g_cheb_ratio, W, ell, dev, dred, (ell && big) ? 1 : 0, 0.0,
+  MixedArgsT<V> m{da,   ddinv, dw, 1e-4, cheb_degree, cheb_ratio, W, ell, dev, dred, (ell && big) ? 1 : 0, 0.0,
                   (int)ld, 0,  dev64};
   if constexpr (sizeof(V) == 4)
     TRY(launch_pcg_mixed(a, m, 0));
@@ -348,9 +349,11 @@ int mgpu_pcg_poly_solve(int n, const int32_t* row_ptr, const int32_t* col_idx, c
     set_error("mgpu_pcg_poly_solve: a row has no diagonal entry");
     return MGPU_E_ARG;
   }
-  const int k = cheb_degree > 0 ? cheb_degree : g_cheb_degree;
-  return precision == MGPU_PREC_MIXED ? poly_solve<float>(n, P, val, b, x, tol, maxit, k, it, res, ierr)
-                                      : poly_solve<double>(n, P, val, b, x, tol, maxit, k, it, res, ierr);
+  int k = cheb_degree;
+  double ratio = g_cheb_ratio;
+  if (k <= 0) cheb_params(n, k, ratio);  // the tuning keys, as a case's pressure solve of n rows
+  return precision == MGPU_PREC_MIXED ? poly_solve<float>(n, P, val, b, x, tol, maxit, k, ratio, it, res, ierr)
+                                      : poly_solve<double>(n, P, val, b, x, tol, maxit, k, ratio, it, res, ierr);
 }
 
 int mgpu_csr_matvec(int n, const int32_t* row_ptr, const int32_t* col_idx, const double* val, const double* x,

@@ -541,7 +541,7 @@ def run_reference(args):
 PISO_METRIC = "PISO time steps/s, mixed vs FP64 GPU, rel L2 of u, p vs FP64"
 # DRAM bytes of the first corrector's pressure solve on the 3.07 M-tet box, by
 # Chebyshev degree, from ncu captures (profiles/k_pcg_mixed_piso3M.md)
-PISO_TRAFFIC = {24: 539.5e9}
+PISO_TRAFFIC = {24: 539.5e9, 48: 527.1e9}
 
 
 def run_piso(args):

@@ -166,6 +166,11 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi takes a moment to start: wait (at most 2 s) for its first
+            # row, so a short timed region still gets samples
+            t0 = time.perf_counter()
+            while not self.rows and time.perf_counter() - t0 < 2.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
